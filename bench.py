@@ -1,0 +1,344 @@
+"""Element-cycle benchmark: element-updates/s of the split-FP32 path vs plain FP64.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload shell_plate|hex_block|mixed_mesh|batched_parts]
+
+One step = one complete run of the workload (all its cycles) from the uploaded
+initial state; the state is reset between steps outside the timed region and
+L2 is flushed (a 256 MB write) before every timed step.  Under torchrun each
+rank runs its own replica of the workload (independent decks: weak scaling,
+no data-path collective); timing is the max over ranks of device time.
+Prints one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: (deck factory, cycles, description)
+    "shell_plate": ("c2_shell_plate", 2000,
+                    "200x200 BT shells, 5 IP, LAW2 Johnson-Cook Al, 2 MPa pressure, 2000 cycles"),
+    "hex_block": ("c1_hex_block", 1000, "10x10x40 hexas, LAW1 steel, -10 m/s, clamped base, 1000 cycles"),
+    "mixed_mesh": ("c4_mixed_mesh", 5000,
+                   "100x100x200 LAW2 steel hexas + 80,000-shell skin, -20 m/s, 5000 cycles"),
+    "batched_parts": ("c3_batched_parts", 500, "64 uneven hex/shell parts, own dt each, 500 cycles"),
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="shell_plate", choices=sorted(WORKLOADS))
+    ap.add_argument("--cycles", type=int, default=0, help="override cycles per step")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def make_deck(name):
+    from openradioss_b200 import decks
+    fn = getattr(decks, WORKLOADS[name][0])
+    return fn()
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """Samples nvidia-smi SM clocks and throttle reasons during the timed region."""
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[0]))
+                mx = float(r[1])
+                for k, n in enumerate(names):
+                    if r[4 + k].lower().startswith("active"):
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                pass
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def cpu_baseline(deck, cycles, budget_s, fast=True):
+    """Times the CPU oracle (C++ restatement of the reference path, OpenMP on
+    all host threads) on a bounded sample of the workload's cycles."""
+    from oracle.oracle import Oracle
+    from openradioss_b200 import abi, decks
+    nthreads = os.cpu_count() or 1
+    nel = decks.num_elements(deck)
+    o = Oracle(deck, precision=abi.OR_PREC_FP64, nthreads=nthreads, fast=fast)
+    t0 = time.perf_counter()
+    o.step(2)
+    t1 = (time.perf_counter() - t0) / 2
+    n = int(max(3, min(cycles, budget_s / max(t1, 1e-9))))
+    t0 = time.perf_counter()
+    o.step(n)
+    dt = time.perf_counter() - t0
+    return {"value": nel * n / dt, "unit": "element-updates/s", "cores": nthreads, "kind": "port",
+            "sample": f"first {n + 2} of {cycles} cycles of the same deck (2 untimed), FP64, "
+                      f"C++ restatement of the reference CPU path, OpenMP {nthreads} threads"}
+
+
+def reference_arm(args, rank, world):
+    deck = make_deck(args.workload)
+    from openradioss_b200 import decks
+    from oracle.oracle import Oracle
+    from openradioss_b200 import abi
+    cycles = args.cycles or WORKLOADS[args.workload][1]
+    if rank != 0:
+        return
+    nthreads = os.cpu_count() or 1
+    nel = decks.num_elements(deck)
+    o = Oracle(deck, precision=abi.OR_PREC_FP64, nthreads=nthreads, fast=True)
+    t0 = time.perf_counter()
+    o.step(1)
+    t1 = time.perf_counter() - t0
+    per_step = int(max(2, min(cycles, (150.0 / max(1, args.steps + args.warmup)) / max(t1, 1e-9))))
+    for _ in range(args.warmup):
+        o.step(per_step)
+    ts = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        o.step(per_step)
+        ts.append(time.perf_counter() - t0)
+    tot = sum(ts)
+    value = nel * per_step * args.steps / tot
+    sample = (f"{per_step} cycles per step of the {args.workload} deck (of {cycles}), FP64, "
+              f"C++ restatement of the reference CPU path, OpenMP {nthreads} threads")
+    line = {"metric": "element-updates/s", "value": value, "unit": "element-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": args.workload, "description": WORKLOADS[args.workload][2],
+                       "elements": nel, "cycles_per_step": per_step},
+            "cpu_baseline": {"value": value, "unit": "element-updates/s", "cores": nthreads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "element-updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        return reference_arm(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    from openradioss_b200 import abi, build, decks, roofline
+    from openradioss_b200.ecycle import ECycle
+    build.build()
+    deck = make_deck(args.workload)
+    cycles = args.cycles or WORKLOADS[args.workload][1]
+    nel = decks.num_elements(deck)
+    nnod = decks.num_nodes(deck)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def timed_runs(h, nsteps, nwarm):
+        s = torch.cuda.ExternalStream(h.stream())
+        ms, launches = [], 0
+        for k in range(nwarm + nsteps):
+            h.reset()
+            flush.fill_(float(k))
+            torch.cuda.synchronize()
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            h.step(cycles)
+            e1.record(s)
+            torch.cuda.synchronize()
+            if k >= nwarm:
+                ms.append(e0.elapsed_time(e1))
+                launches += h.launch_count()
+        return ms, launches
+
+    # ---- split form (the headline) ----
+    hs = ECycle(deck, precision=abi.OR_PREC_SPLIT, device=local, graph=1)
+    timed_runs(hs, 0, 1)                      # graph capture + first-touch outside timing
+    sampler = ClockSampler(local)
+    sampler.start()
+    ms_split, launches = timed_runs(hs, args.steps, args.warmup)
+    clocks = sampler.stop()
+    t_split = sum(ms_split) / len(ms_split)
+    d_split = hs.get_nodes()["d"]
+
+    # ---- plain FP64 form ----
+    hd = ECycle(deck, precision=abi.OR_PREC_FP64, device=local, graph=1)
+    timed_runs(hd, 0, 1)
+    nfp = max(2, args.steps // 2)
+    ms_fp64, _ = timed_runs(hd, nfp, 1)
+    t_fp64 = sum(ms_fp64) / len(ms_fp64)
+    d_fp64 = hd.get_nodes()["d"]
+    split_err = float(np.abs(d_split - d_fp64).max() / max(np.abs(d_fp64).max(), 1e-300))
+    del hd
+
+    # max over ranks of the mean step time
+    tt = torch.tensor([t_split, t_fp64], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    t_split, t_fp64 = float(tt[0]), float(tt[1])
+    value = world * nel * cycles / (t_split * 1e-3)
+    value_fp64 = world * nel * cycles / (t_fp64 * 1e-3)
+
+    # ---- per-kernel device times (eager launches with CUDA events on the handle's stream) ----
+    hp = ECycle(deck, precision=abi.OR_PREC_SPLIT, device=local, graph=0)
+    kcyc = min(cycles, 200)
+    hp.step(kcyc)
+    hp.reset()
+    hp.step(kcyc)
+    ph = hp.phase_times()
+    del hp
+    s = 4
+    eb_hex = sum(g["ixs"].shape[0] * roofline.hex_bytes(s, g["mat"]["law"]) for p in deck["parts"] for g in p["hex"])
+    eb_shell = sum(g["ixc"].shape[0] * roofline.shell_bytes(s, g["prop"]["npt"]) for p in deck["parts"] for g in p["shell"])
+    eb, nb, _ = roofline.deck_bytes(deck, s)
+    peak, peak_src = roofline.measured_peak()
+    kern = {"hex": (ph["hex"] / kcyc, eb_hex), "shell": (ph["shell"] / kcyc, eb_shell), "node": (ph["node"] / kcyc, nb)}
+    dom = max(kern, key=lambda k: kern[k][0])
+    dom_ms, dom_bytes = kern[dom]
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get(args.workload, {}).get(f"{dom}_split")
+        except (OSError, ValueError):
+            traffic = None
+    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9 if dom_ms > 0 else 0.0
+    cyc_bytes = eb + nb
+    cyc_achieved = cyc_bytes * cycles / (t_split * 1e-3) / 1e9
+
+    # ---- end to end through the C-ABI with host buffers ----
+    n0 = deck["parts"]
+    host = []
+    for p in n0:
+        n = p["x"].shape[0]
+        host.append({k: torch.from_numpy(np.ascontiguousarray(a, np.float64)).pin_memory().numpy()
+                     for k, a in (("x", p["x"]), ("d", np.zeros((n, 3))), ("v", p["v"]), ("vr", p["vr"]))})
+    h2d = sum(sum(a.nbytes for a in hb.values()) for hb in host)
+    d2h = h2d
+    import ctypes as C
+    e2e_t = []
+    for k in range(args.warmup + max(2, args.steps // 2)):
+        hs.reset()
+        flush.fill_(float(k))
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        for pi, hb in enumerate(host):
+            hs._call("set_nodes", pi, *(hb[q].ctypes.data_as(C.POINTER(C.c_double)) for q in ("x", "d", "v", "vr")))
+        hs.step(cycles)
+        for pi, hb in enumerate(host):
+            hs._call("get_nodes", pi, *(hb[q].ctypes.data_as(C.POINTER(C.c_double)) for q in ("x", "d", "v", "vr")))
+        t1 = time.perf_counter()
+        if k >= args.warmup:
+            e2e_t.append(t1 - t0)
+    te = torch.tensor([sum(e2e_t) / len(e2e_t)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * nel * cycles / float(te[0])
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(deck, cycles, args.cpu_seconds)
+
+    if rank == 0:
+        line = {
+            "metric": "element-updates/s", "value": value, "unit": "element-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_split, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic (seeded numpy decks with the workload's shapes)",
+            "config": {"workload": args.workload, "description": WORKLOADS[args.workload][2],
+                       "elements_per_gpu": nel, "nodes_per_gpu": nnod, "cycles_per_step": cycles,
+                       "precision": "split: FP32 element/material math, FP64 X/D/volumes/energies",
+                       "l2": "256 MB buffer written before every timed step",
+                       "cuda_graph_cycles": 32, "tile_hex": 256, "tile_shell": 256},
+            "fp64": {"value": value_fp64, "ms_per_step": t_fp64, "dtype": "f64"},
+            "split_over_fp64": value / value_fp64,
+            "split_rel_disp_error_vs_fp64": split_err,
+            "roofline": {"bound": "hbm", "kernel": f"{dom}_patch_kernel" if dom != "node" else "node_kernel",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "algorithmic_bytes_per_launch": dom_bytes,
+                         "avg_launch_ms": dom_ms, "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)"},
+            "cycle_roofline": {"algorithmic_bytes_per_cycle": cyc_bytes,
+                               "bytes_per_element_update": cyc_bytes / nel,
+                               "achieved": cyc_achieved, "frac": cyc_achieved / peak,
+                               "kernel_ms_per_cycle": {k: v[0] for k, v in kern.items()}},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "element-updates/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "clocks": clocks,
+            "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+    del hs
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,216 @@
+/*
+ * or_ecycle.h -- C-ABI of the B200 explicit element cycle.
+ *
+ * One handle replaces, for the element groups handed to it, the in-scope body
+ * of one OpenRadioss RESOL cycle:
+ *
+ *   FORINTC / FORINT          engine/source/engine/resol.F:4012, :4096
+ *     (CFORC3 BT shells  engine/source/elements/shell/coque/cforc3.F:82,
+ *      SFORC3 1-pt hexas engine/source/elements/solid/solide/sforc3.F:125)
+ *   ASSPAR4 skyline sum       engine/source/assembly/asspar4.F:160-175
+ *   element dt min            engine/source/engine/resol.F:5853-5858, :6080, :6226
+ *   ACCELE                    engine/source/assembly/accele.F:63-123
+ *   BCS10 / BCS1V             engine/source/constraints/general/bcs/bcs10.F:30
+ *   VELOCITY                  engine/source/assembly/velocity.F:56-84
+ *   DEPLA                     engine/source/assembly/displacement.F:69-110
+ *
+ * The calling convention follows the reference's own C-ABI precedent
+ * (engine/source/coupling/coupling_c_interface.h: opaque handle, int status,
+ * create / configure / advance / destroy) so that the Fortran engine binds it
+ * with ISO_C_BINDING exactly like coupling_adapter.F90:50-150.
+ *
+ * Conventions
+ *  - Every function returns 0 on success and a positive OR_E_* code on error;
+ *    or_ecycle_last_error() returns the message.  The library never exits.
+ *  - Arrays are plain host pointers in the reference's Fortran layouts:
+ *      X, D, V, VR     3 x numnod, node-major   (X(3,NUMNOD))
+ *      IXS             11 x nel, 1-based node numbers in rows 2..9 (NIXS=11)
+ *      IXC             7 x nel,  1-based node numbers in rows 2..5 (NIXC=7)
+ *      SIG (solid)     nel x 6, component-major  SIG(I+NEL*(J-1))
+ *      SIG (shell IP)  npt x 5 x nel:  [ip][component][element]
+ *  - The library copies inputs to device memory on the add/set calls and owns
+ *    the device mirrors; the caller keeps ownership of its host arrays.
+ *  - A handle holds one or more independent "parts"; each part has its own
+ *    nodes, element groups and time step (one part = one reference domain).
+ *  - The handle is not thread-safe; call it from one host thread.
+ */
+#ifndef OR_ECYCLE_H
+#define OR_ECYCLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define OR_OK               0
+#define OR_E_ARG            1   /* bad argument (null pointer, size, index)      */
+#define OR_E_CUDA           2   /* CUDA runtime error                            */
+#define OR_E_STATE          3   /* call out of order (e.g. step before finalize) */
+#define OR_E_NEGVOL         4   /* zero/negative volume (SCHKJABT3, MSGID 166)    */
+#define OR_E_DTMIN          5   /* element time step <= DTMIN (MQVISCB/CDT3)     */
+#define OR_E_NAN            6   /* NaN/Inf in nodal acceleration                 */
+#define OR_E_TIMEOUT        7   /* bounded host wait expired                     */
+#define OR_E_UNSUPPORTED    8   /* option outside the implemented path           */
+#define OR_E_NOMEM          9   /* device allocation failed                      */
+
+/* precision forms */
+#define OR_PREC_FP64        0   /* plain FP64 everywhere ("-prec=dp")                    */
+#define OR_PREC_SPLIT       1   /* FP32 element/material math, FP64 X, D, volumes, energies */
+
+/* material laws */
+#define OR_LAW_ELASTIC      1   /* /MAT/ELAST        (m1law.F, sigeps01c.F)           */
+#define OR_LAW_JOHNSON_COOK 2   /* /MAT/PLAS_JOHNS   (m2law.F, sigeps02c.F, m2cplr.F) */
+
+typedef struct or_ecycle or_ecycle;
+
+typedef struct {
+  int    precision;     /* OR_PREC_FP64 or OR_PREC_SPLIT                             */
+  int    device;        /* CUDA device ordinal                                       */
+  double dtfac_solid;   /* DTFAC1(1), default 0.9 (lectur.F:405-425)                 */
+  double dtfac_shell;   /* DTFAC1(3), default 0.9                                    */
+  double dtmin_solid;   /* DTMIN1(1); element dt <= this is OR_E_DTMIN               */
+  double dtmin_shell;   /* DTMIN1(3)                                                 */
+  double dtmx;          /* DTMX, default 1e20 (freform.F:584)                        */
+  double dt_growth;     /* growth cap factor of resol.F:6080; the reference
+                           multiplies by the REAL literal 1.1, i.e. (double)1.1f     */
+  int    graph;         /* 1: replay step() through a captured CUDA graph            */
+  int    block_hex;     /* threads per block, hex kernel   (0 = autotuned)           */
+  int    block_shell;   /* threads per block, shell kernel (0 = autotuned)           */
+  int    block_node;    /* threads per block, nodal kernel (0 = autotuned)           */
+} or_ecycle_config;
+
+/* PM(.,MAT) entries used on the path (hm_read_mat02_jc.F90, m1law.F, m2law.F) */
+typedef struct {
+  int    law;           /* OR_LAW_*                                     */
+  double rho0;          /* PM(1)                                        */
+  double young;         /* PM(20)                                       */
+  double nu;            /* PM(21)                                       */
+  double shear;         /* PM(22)  G                                    */
+  double bulk;          /* PM(32)  C1 / BULK                            */
+  double a11;           /* PM(24)  E/(1-nu^2)                           */
+  double a12;           /* PM(25)  nu*A11                               */
+  double ssp_shell;     /* PM(27)  sqrt(E/rho)                          */
+  double jc_a;          /* uparam(1) CA  (LAW2)                         */
+  double jc_b;          /* uparam(2) CB                                 */
+  double jc_n;          /* uparam(3) CN                                 */
+  double epsmax;        /* uparam(4) EPMX, 1e20 when unset              */
+  double sigmax;        /* uparam(5) SIGMX, 1e20 when unset             */
+} or_material;
+
+/* /PROP/SOLID values on the path (hm_read_prop14.F:338-361) */
+typedef struct {
+  double qa;            /* GEO(14), default 1.1   */
+  double qb;            /* GEO(15), default 0.05  */
+  double qh;            /* GEO(13), default 0.1   */
+} or_solid_prop;
+
+/* /PROP/SHELL values on the path (hm_read_prop01.F:141-317) */
+typedef struct {
+  double thk;           /* GEO(1) initial thickness (used where THKE is not given) */
+  int    npt;           /* integration points through the thickness, 1..10        */
+  int    ithk;          /* 1: element uses the current thickness (ITHK>0)         */
+  int    ipla;          /* 0: radial return (the only implemented IPLA)           */
+  double hm, hf, hr;    /* GEO(13..15) hourglass coefficients                     */
+  double shf;           /* shear factor SHF (5/6 for ISH=0)                       */
+  double pressure;      /* uniform /PLOAD-style pressure on the group, Pa (0=none)*/
+} or_shell_prop;
+
+/* time-step state of one part, in/out of or_ecycle_step (RESOL scalars) */
+typedef struct {
+  double tt;            /* TT      */
+  double dt1;           /* DT1     */
+  double dt2;           /* DT2     */
+  double dt12;          /* DT12    */
+  double dt2old;        /* DT2OLD  */
+  int    ncycle;        /* NCYCLE  */
+  int    ityptst;       /* ITYPTS  element type that set DT2 (1 solid, 3 shell) */
+  int    neltst;        /* NELTS   0-based element index in its part            */
+  int    pad;
+} or_ecycle_time;
+
+/* energies of one part, FP64 (ecrit.F:300-363, sbilan.F, cbilan.F, shvis3.F) */
+typedef struct {
+  double internal;      /* sum EINT*V0 (solids) + EINT(1)+EINT(2) (shells)  */
+  double kinetic;       /* 1/2 m |V + DT1/2 A|^2                            */
+  double kinetic_rot;   /* 1/2 I |VR + DT1/2 AR|^2                          */
+  double hourglass;     /* cumulative EHOUR                                 */
+  double plastic_work;  /* cumulative sum sigma_y * dpla * volume           */
+  double pad;
+} or_energies;
+
+/* --- lifecycle ---------------------------------------------------------- */
+/* replaces: coupling_adapter_create / configure (coupling_c_interface.h) */
+int  or_ecycle_create(const or_ecycle_config* cfg, or_ecycle** out);
+/* replaces: coupling_adapter_destroy */
+int  or_ecycle_destroy(or_ecycle* h);
+const char* or_ecycle_last_error(const or_ecycle* h);
+
+/* --- model upload (hot-path inputs stay resident in HBM) ----------------- */
+/* Adds a part; returns its index in *part.  Node arrays: X/V/VR (3,numnod),
+   MS/IN (numnod) from the starter (smass3.F:79, cinmas.F), ICODT/ICODR (numnod)
+   3-bit /BCS codes (bcs1.F:52-100; 4=x, 2=y, 1=z).  vr, in, icodr may be NULL. */
+int  or_ecycle_add_part(or_ecycle* h, int numnod, const double* x, const double* v,
+                        const double* vr, const double* ms, const double* in,
+                        const int* icodt, const int* icodr, int* part);
+
+/* Adds an 8-node 1-point hexa group (SFORC3, Isolid=1, Iframe=1, Ismstr=4).
+   ixs: 11 x nel (NIXS); vol0: GBUF%VOL initial volumes (may be NULL: computed). */
+int  or_ecycle_add_hex_group(or_ecycle* h, int part, int nel, const int* ixs,
+                             const or_material* mat, const or_solid_prop* prop,
+                             const double* vol0, int* group);
+
+/* Adds a 4-node Belytschko-Tsay shell group (CFORC3, Ishell 1, Ismstr 2).
+   ixc: 7 x nel (NIXC); thke: initial thickness per element (may be NULL). */
+int  or_ecycle_add_shell_group(or_ecycle* h, int part, int nel, const int* ixc,
+                               const or_material* mat, const or_shell_prop* prop,
+                               const double* thke, int* group);
+
+/* Per-element LAW2 yield stress A of a shell group (replaces uparam(1) per
+   element; used by the sensitivity workload).  jc_a: nel values, Pa. */
+int  or_ecycle_set_shell_yield(or_ecycle* h, int group, const double* jc_a);
+
+/* Builds the Parith/ON assembly tables (element_pon_: ADSKY/IADS/IADC) on the
+   device and allocates work buffers.  Must follow the last add_* call. */
+int  or_ecycle_finalize(or_ecycle* h);
+
+/* Restores nodes, element state and energy accumulators to the values given at
+   upload (the state after finalize), keeping the device layout; used to replay
+   a run (benchmarks, finite-difference sensitivity checks). */
+int  or_ecycle_reset(or_ecycle* h);
+
+/* --- the cycle ------------------------------------------------------------ */
+/* Runs ncycles explicit cycles for every part.  t: one or_ecycle_time per part,
+   read on entry and written on return.  Synchronous, bounded wait. */
+int  or_ecycle_step(or_ecycle* h, int ncycles, or_ecycle_time* t);
+
+/* --- download / upload for output and restart ---------------------------- */
+int  or_ecycle_get_nodes(or_ecycle* h, int part, double* x, double* d,
+                         double* v, double* vr);
+int  or_ecycle_set_nodes(or_ecycle* h, int part, const double* x, const double* d,
+                         const double* v, const double* vr);
+/* solid state: sig (nel x 6 component-major), eint (per initial volume), rho,
+   qvis, pla, epsd; any pointer may be NULL */
+int  or_ecycle_get_hex_state(or_ecycle* h, int group, double* sig, double* eint,
+                             double* rho, double* qvis, double* pla, double* epsd);
+/* shell state: sig (npt x 5 x nel), pla (npt x nel), thk, hourg (3 x nel
+   component-major), eint (2 x nel component-major); any pointer may be NULL */
+int  or_ecycle_get_shell_state(or_ecycle* h, int group, double* sig, double* pla,
+                               double* thk, double* hourg, double* eint);
+int  or_ecycle_energies(or_ecycle* h, int part, or_energies* e);
+
+/* --- diagnostics ----------------------------------------------------------- */
+/* Device error word of the last step: code (OR_E_*), element/node index. */
+int  or_ecycle_error_info(or_ecycle* h, int* code, int* index);
+/* Per-phase CUDA-event times of the last step, ms: [hex, shell, node, total]. */
+int  or_ecycle_phase_times(or_ecycle* h, double* ms4);
+/* Number of this library's kernel launches issued by the last step. */
+int  or_ecycle_launch_count(or_ecycle* h, long long* n);
+/* CUDA stream of the handle (cudaStream_t as void*), for event timing. */
+int  or_ecycle_stream(or_ecycle* h, void** stream);
+/* Bytes of device memory held by the handle. */
+int  or_ecycle_device_bytes(or_ecycle* h, long long* bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OR_ECYCLE_H */

@@ -1,0 +1,1148 @@
+// ecycle.cu -- host implementation of the C-ABI declared in include/or_ecycle.h.
+//
+// finalize() turns the uploaded groups into the device layout:
+//   * nodes of every part are concatenated, each part padded to NODE_TILE
+//     nodes, X stored as double4 (x, y, z, nodal mass), V / VR as R4
+//     (VR.w = rotational inertia), D as three FP64 planes, BCS codes as bytes;
+//   * every element group is reordered along a Morton curve of the element
+//     centroids and cut into patches of at most TILE elements; inside a patch
+//     the elements are greedily coloured (no shared node within a colour) and
+//     sorted by colour; connectivity becomes 16-bit patch-local node indices;
+//   * each (patch, node) pair owns one slot of a node-major skyline; a node's
+//     slots are ordered by patch number (element_pon_ ADSKY analogue).
+// step() launches hex, shell and node kernels per cycle, replayed through a
+// captured CUDA graph of GRAPH_CYCLES cycles.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/or_ecycle.h"
+#include "ecycle_kernels.cuh"
+
+using namespace orb;
+
+namespace {
+
+constexpr int NODE_TILE = 256;
+constexpr int GRAPH_CYCLES = 32;
+
+// through-thickness rules of COQINI (coqini.F:45-130), [npt-1][Z0 | WF | WM]
+const float ZW_TABLE[10][33] = {
+  {0.f, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0,  1.f, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0,  0.f, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0},
+  {-.5f, .5f, 0, 0, 0, 0, 0, 0, 0, 0, 0,  .5f, .5f, 0, 0, 0, 0, 0, 0, 0, 0, 0,  -.0833333f, .0833333f, 0, 0, 0, 0, 0, 0, 0, 0, 0},
+  {-.5f, 0.f, .5f, 0, 0, 0, 0, 0, 0, 0, 0,  .25f, .5f, .25f, 0, 0, 0, 0, 0, 0, 0, 0,  -.0833333f, 0.f, .0833333f, 0, 0, 0, 0, 0, 0, 0, 0},
+  {-.5f, -.1666667f, .1666667f, .5f, 0, 0, 0, 0, 0, 0, 0,  .1666667f, .3333333f, .3333333f, .1666667f, 0, 0, 0, 0, 0, 0, 0,
+   -.0648148f, -.0555556f, .0555556f, .0648148f, 0, 0, 0, 0, 0, 0, 0},
+  {-.5f, -.25f, 0.f, .25f, .5f, 0, 0, 0, 0, 0, 0,  .125f, .25f, .25f, .25f, .125f, 0, 0, 0, 0, 0, 0,
+   -.0520833f, -.0625f, 0.f, .0625f, .0520833f, 0, 0, 0, 0, 0, 0},
+  {-.5f, -.3f, -.1f, .1f, .3f, .5f, 0, 0, 0, 0, 0,  .1f, .2f, .2f, .2f, .2f, .1f, 0, 0, 0, 0, 0,
+   -.0433333f, -.06f, -.02f, .02f, .06f, .0433333f, 0, 0, 0, 0, 0},
+  {-.5f, -.3333333f, -.1666667f, 0.f, .1666667f, .3333333f, .5f, 0, 0, 0, 0,
+   .0833333f, .1666667f, .1666667f, .1666667f, .1666667f, .1666667f, .0833333f, 0, 0, 0, 0,
+   -.037037f, -.0555556f, -.0277778f, 0.f, .0277778f, .0555556f, .037037f, 0, 0, 0, 0},
+  {-.5f, -.3571429f, -.2142857f, -.0714286f, .0714286f, .2142857f, .3571429f, .5f, 0, 0, 0,
+   .0714286f, .1428571f, .1428571f, .1428571f, .1428571f, .1428571f, .1428571f, .0714286f, 0, 0, 0,
+   -.0323129f, -.0510204f, -.0306122f, -.0102041f, .0102041f, .0306122f, .0510204f, .0323129f, 0, 0, 0},
+  {-.5f, -.375f, -.25f, -.125f, 0.f, .125f, .25f, .375f, .5f, 0, 0,
+   .0625f, .125f, .125f, .125f, .125f, .125f, .125f, .125f, .0625f, 0, 0,
+   -.0286458f, -.046875f, -.03125f, -.015625f, 0.f, .015625f, .03125f, .046875f, .0286458f, 0, 0},
+  {-.5f, -.3888889f, -.2777778f, -.1666667f, -.0555555f, .0555555f, .1666667f, .2777778f, .3888889f, .5f, 0,
+   .0555556f, .1111111f, .1111111f, .1111111f, .1111111f, .1111111f, .1111111f, .1111111f, .1111111f, .0555556f, 0,
+   -.0257202f, -.0432099f, -.0308642f, -.0185185f, -.0061728f, .0061728f, .0185185f, .0308642f, .0432099f, .0257202f, 0},
+};
+
+// ----------------------------------------------------------------------------
+// host-side model as uploaded
+// ----------------------------------------------------------------------------
+struct HPart {
+  int numnod = 0;
+  std::vector<double> x, v, vr, ms, in;
+  std::vector<int> icodt, icodr;
+  int nel_solid = 0, nel_shell = 0;
+  bool has_rot = false;
+  int node_start = 0, node_pad = 0, tile_start = 0;
+};
+struct HHex {
+  int part = 0, nel = 0, gofs = 0;
+  std::vector<int> conn;            // 8*nel, part-local
+  or_material mat; or_solid_prop prop;
+  std::vector<double> vol0;
+  std::vector<int> internal;        // user element -> internal padded index
+};
+struct HShell {
+  int part = 0, nel = 0, gofs = 0;
+  std::vector<int> conn;            // 4*nel
+  or_material mat; or_shell_prop prop;
+  std::vector<double> thke, jca;
+  std::vector<int> internal;
+};
+
+template <class T> struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+};
+
+struct PatchSet {                   // host result of patch construction
+  std::vector<PatchInfo> info;
+  std::vector<int> nodes;           // global node ids, per patch contiguous
+  std::vector<int> slots;           // slot id of each (patch, node)
+  std::vector<int> elem_user;       // internal padded index -> (group, user index) encoded
+  std::vector<int> elem_group;
+  std::vector<uint16_t> local;      // internal padded index -> K local indices (+colour in corner 0)
+  int nelpad = 0, nlmax = 0;
+};
+
+}  // namespace
+
+struct or_ecycle {
+  or_ecycle_config cfg{};
+  std::string err;
+  cudaStream_t stream = nullptr;
+  std::vector<HPart> parts;
+  std::vector<HHex> hex;
+  std::vector<HShell> shell;
+  bool finalized = false;
+  int tile_hex = 256, tile_shell = 256, tile_node = NODE_TILE;
+  // device state
+  void* impl = nullptr;
+  double phase_ms[4] = {0, 0, 0, 0};
+  long long launches = 0;
+  long long dev_bytes = 0;
+  cudaGraphExec_t graph_exec = nullptr;
+  cudaGraph_t graph = nullptr;
+  int last_code = 0, last_index = -1;
+};
+
+namespace {
+
+int fail(or_ecycle* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+#define CK(call)                                                                  \
+  do {                                                                            \
+    cudaError_t e_ = (call);                                                      \
+    if (e_ != cudaSuccess)                                                        \
+      return fail(h, e_ == cudaErrorMemoryAllocation ? OR_E_NOMEM : OR_E_CUDA,    \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));            \
+  } while (0)
+
+template <class T>
+int dalloc(or_ecycle* h, DBuf<T>& b, size_t n) {
+  b.n = n;
+  if (n == 0) { b.p = nullptr; return OR_OK; }
+  CK(cudaMalloc((void**)&b.p, n * sizeof(T)));
+  h->dev_bytes += (long long)(n * sizeof(T));
+  return OR_OK;
+}
+template <class T>
+int dput(or_ecycle* h, DBuf<T>& b, const std::vector<T>& v) {
+  int rc = dalloc(h, b, v.size());
+  if (rc) return rc;
+  if (!v.empty()) CK(cudaMemcpy(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return OR_OK;
+}
+template <class T> void dfree(DBuf<T>& b) { if (b.p) cudaFree(b.p); b.p = nullptr; b.n = 0; }
+
+uint64_t morton3(uint32_t x, uint32_t y, uint32_t z) {
+  auto spread = [](uint64_t v) {
+    v &= 0x1fffff;
+    v = (v | v << 32) & 0x1f00000000ffffull;
+    v = (v | v << 16) & 0x1f0000ff0000ffull;
+    v = (v | v << 8) & 0x100f00f00f00f00full;
+    v = (v | v << 4) & 0x10c30c30c30c30c3ull;
+    v = (v | v << 2) & 0x1249249249249249ull;
+    return v;
+  };
+  return spread(x) | (spread(y) << 1) | (spread(z) << 2);
+}
+
+// Builds patches for a list of groups of K-node elements.  conn_of(g) gives the
+// part-local connectivity, node_base(g) the global node offset of the group's part.
+template <int K, class GroupT>
+int build_patches(or_ecycle* h, std::vector<GroupT>& groups, int tile, PatchSet& ps,
+                  std::vector<std::vector<std::pair<int, int>>>& node_patch, int patch_base) {
+  ps = PatchSet();
+  int elem0 = 0;
+  for (size_t gi = 0; gi < groups.size(); ++gi) {
+    GroupT& g = groups[gi];
+    const HPart& P = h->parts[g.part];
+    const int nel = g.nel;
+    // Morton order of centroids
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    std::vector<double> cen(3 * (size_t)nel);
+    for (int e = 0; e < nel; ++e)
+      for (int c = 0; c < 3; ++c) {
+        double s = 0;
+        for (int k = 0; k < K; ++k) s += P.x[3 * (size_t)g.conn[K * (size_t)e + k] + c];
+        s /= K;
+        cen[3 * (size_t)e + c] = s;
+        lo[c] = std::min(lo[c], s); hi[c] = std::max(hi[c], s);
+      }
+    std::vector<uint64_t> code(nel);
+    for (int e = 0; e < nel; ++e) {
+      uint32_t q[3];
+      for (int c = 0; c < 3; ++c) {
+        double span = hi[c] - lo[c];
+        double t = span > 0 ? (cen[3 * (size_t)e + c] - lo[c]) / span : 0.0;
+        q[c] = (uint32_t)std::min(2097151.0, std::max(0.0, t * 2097151.0));
+      }
+      code[e] = morton3(q[0], q[1], q[2]);
+    }
+    std::vector<int> order(nel);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return code[a] < code[b]; });
+    g.internal.assign(nel, -1);
+    const int node_base = P.node_start;
+    for (int s0 = 0; s0 < nel; s0 += tile) {
+      const int n = std::min(tile, nel - s0);
+      // unique nodes of the patch (sorted global ids)
+      std::vector<int> nodes;
+      nodes.reserve((size_t)n * K);
+      for (int t = 0; t < n; ++t)
+        for (int k = 0; k < K; ++k) nodes.push_back(node_base + g.conn[K * (size_t)order[s0 + t] + k]);
+      std::sort(nodes.begin(), nodes.end());
+      nodes.erase(std::unique(nodes.begin(), nodes.end()), nodes.end());
+      if ((int)nodes.size() > (int)LOCAL_MASK + 1)
+        return fail(h, OR_E_UNSUPPORTED, "patch has more than 2048 distinct nodes");
+      auto local_of = [&](int gid) { return (int)(std::lower_bound(nodes.begin(), nodes.end(), gid) - nodes.begin()); };
+      // greedy colouring in Morton order
+      std::vector<uint32_t> used(nodes.size(), 0u);
+      std::vector<int> col(n);
+      int ncol = 0;
+      for (int t = 0; t < n; ++t) {
+        uint32_t busy = 0;
+        int lcs[K];
+        for (int k = 0; k < K; ++k) { lcs[k] = local_of(node_base + g.conn[K * (size_t)order[s0 + t] + k]); busy |= used[lcs[k]]; }
+        int c = 0;
+        while (c < MAX_COLORS && (busy >> c & 1u)) ++c;
+        if (c >= MAX_COLORS) return fail(h, OR_E_UNSUPPORTED, "more than 32 colours in a patch");
+        col[t] = c;
+        ncol = std::max(ncol, c + 1);
+        for (int k = 0; k < K; ++k) used[lcs[k]] |= 1u << c;
+      }
+      std::vector<int> byc(n);
+      std::iota(byc.begin(), byc.end(), 0);
+      std::stable_sort(byc.begin(), byc.end(), [&](int a, int b) { return col[a] < col[b]; });
+      PatchInfo pi{};
+      pi.group = (int)gi; pi.nel = n; pi.node_ofs = (int)ps.nodes.size(); pi.nloc = (int)nodes.size();
+      pi.ncolor = ncol; pi.elem0 = elem0;
+      const int pid = (int)ps.info.size();
+      ps.info.push_back(pi);
+      ps.nlmax = std::max(ps.nlmax, (int)nodes.size());
+      for (size_t j = 0; j < nodes.size(); ++j) {
+        node_patch[nodes[j]].push_back({patch_base + pid, (int)(ps.nodes.size() + j)});
+      }
+      ps.nodes.insert(ps.nodes.end(), nodes.begin(), nodes.end());
+      ps.local.resize((size_t)(elem0 + tile) * K, 0);
+      ps.elem_user.resize(elem0 + tile, -1);
+      ps.elem_group.resize(elem0 + tile, -1);
+      for (int t = 0; t < n; ++t) {
+        const int ue = order[s0 + byc[t]];
+        const int ie = elem0 + t;
+        g.internal[ue] = ie;
+        ps.elem_user[ie] = ue;
+        ps.elem_group[ie] = (int)gi;
+        for (int k = 0; k < K; ++k) {
+          int l = local_of(node_base + g.conn[K * (size_t)ue + k]);
+          if (k == 0) l |= col[byc[t]] << COLOR_SHIFT;
+          ps.local[(size_t)ie * K + k] = (uint16_t)l;
+        }
+      }
+      elem0 += tile;
+    }
+  }
+  ps.nelpad = elem0;
+  ps.slots.assign(ps.nodes.size(), -1);
+  return OR_OK;
+}
+
+// ----------------------------------------------------------------------------
+// device model, templated on the element precision
+// ----------------------------------------------------------------------------
+template <class R>
+struct Impl {
+  typedef typename Vec4<R>::T R4;
+  int nnodpad = 0, ntiles = 0, nparts = 0, nslot = 0;
+  bool any_rot = false;
+  // nodes
+  DBuf<double4> X; DBuf<double> DX, DY, DZ; DBuf<R4> V, VR; DBuf<unsigned char> code;
+  DBuf<int> adsky, tile_part; DBuf<PartDesc> partd;
+  DBuf<R4> fslot, mslot;
+  DBuf<PartTime> time; DBuf<PartAcc> acc; DBuf<ErrorWord> err;
+  DBuf<double> ekin, ekinr;
+  // hexas
+  PatchSet hps;
+  DBuf<PatchInfo> hpatch; DBuf<HexGroupDesc> hdesc; DBuf<int> hnodes, hslots, helem; DBuf<uint4> hconn;
+  DBuf<R> hsig, heint, hrho, hqvis, hpla, hepsd, hvol0; DBuf<double> hvol0dp;
+  DBuf<double> hehour, hwpla;
+  // shells
+  PatchSet sps;
+  DBuf<PatchInfo> spatch; DBuf<ShellGroupDesc> sdesc; DBuf<int> snodes, sslots, selem, sdegen; DBuf<uint2> sconn;
+  DBuf<R> ssig, spla, sthk, sthke, shourg, seint, sjca;
+  DBuf<double> sehour, swpla;
+  DBuf<float> zw;
+  int maxnpt = 1;
+  std::vector<int> part_hex_patches, part_shell_patches;   // unused placeholders
+
+  HexArgs<R> hargs() {
+    HexArgs<R> a;
+    a.patch = hpatch.p; a.groups = hdesc.p; a.patch_nodes = hnodes.p; a.patch_slots = hslots.p;
+    a.conn = hconn.p; a.elem_id = helem.p; a.X = X.p; a.V = V.p;
+    a.sig = hsig.p; a.eint = heint.p; a.rho = hrho.p; a.qvis = hqvis.p; a.pla = hpla.p; a.epsd = hepsd.p;
+    a.vol0 = hvol0.p; a.vol0dp = hvol0dp.p; a.fslot = fslot.p; a.time = time.p; a.acc = acc.p;
+    a.blk_ehour = hehour.p; a.blk_wpla = hwpla.p; a.err = err.p;
+    a.nelpad = hps.nelpad; a.nparts = nparts; a.npatch = (int)hps.info.size();
+    return a;
+  }
+  ShellArgs<R> sargs() {
+    ShellArgs<R> a;
+    a.patch = spatch.p; a.groups = sdesc.p; a.patch_nodes = snodes.p; a.patch_slots = sslots.p;
+    a.conn = sconn.p; a.elem_id = selem.p; a.degen = sdegen.p; a.X = X.p; a.V = V.p; a.VR = VR.p;
+    a.sig = ssig.p; a.pla = spla.p; a.thk = sthk.p; a.thke = sthke.p; a.hourg = shourg.p; a.eint = seint.p;
+    a.jca = sjca.p; a.fslot = fslot.p; a.mslot = mslot.p; a.time = time.p; a.acc = acc.p;
+    a.blk_ehour = sehour.p; a.blk_wpla = swpla.p; a.err = err.p;
+    a.nelpad = sps.nelpad; a.nparts = nparts; a.npatch = (int)sps.info.size(); a.maxnpt = maxnpt;
+    return a;
+  }
+  NodeArgs<R> nargs(const or_ecycle* h) {
+    NodeArgs<R> a;
+    a.parts = partd.p; a.tile_part = tile_part.p; a.adsky = adsky.p; a.fslot = fslot.p; a.mslot = mslot.p;
+    a.X = X.p; a.DX = DX.p; a.DY = DY.p; a.DZ = DZ.p; a.V = V.p; a.VR = VR.p; a.code = code.p;
+    a.time = time.p; a.acc = acc.p; a.blk_ekin = ekin.p; a.blk_ekinr = ekinr.p; a.err = err.p;
+    a.growth = h->cfg.dt_growth; a.dtmx = h->cfg.dtmx; a.ntiles = ntiles; a.nparts = nparts;
+    a.split = sizeof(R) == 4;
+    return a;
+  }
+  void free_all() {
+    dfree(X); dfree(DX); dfree(DY); dfree(DZ); dfree(V); dfree(VR); dfree(code); dfree(adsky); dfree(tile_part);
+    dfree(partd); dfree(fslot); dfree(mslot); dfree(time); dfree(acc); dfree(err); dfree(ekin); dfree(ekinr);
+    dfree(hpatch); dfree(hdesc); dfree(hnodes); dfree(hslots); dfree(helem); dfree(hconn); dfree(hsig); dfree(heint);
+    dfree(hrho); dfree(hqvis); dfree(hpla); dfree(hepsd); dfree(hvol0); dfree(hvol0dp); dfree(hehour); dfree(hwpla);
+    dfree(spatch); dfree(sdesc); dfree(snodes); dfree(sslots); dfree(selem); dfree(sdegen); dfree(sconn);
+    dfree(ssig); dfree(spla); dfree(sthk); dfree(sthke); dfree(shourg); dfree(seint); dfree(sjca);
+    dfree(sehour); dfree(swpla); dfree(zw);
+  }
+};
+
+template <class R>
+size_t hex_smem(int nl) { return (size_t)nl * (3 * sizeof(double) + 6 * sizeof(R)); }
+template <class R>
+size_t shell_smem(int nl) { return (size_t)nl * (3 * sizeof(double) + 12 * sizeof(R)); }
+
+template <class R, int T>
+int launch_hex(or_ecycle* h, Impl<R>& m, int parity) {
+  if (m.hps.info.empty()) return OR_OK;
+  size_t sm = hex_smem<R>(m.hps.nlmax);
+  hex_patch_kernel<R, T><<<(unsigned)m.hps.info.size(), T, sm, h->stream>>>(m.hargs(), parity);
+  CK(cudaGetLastError());
+  h->launches++;
+  return OR_OK;
+}
+template <class R, int T>
+int launch_shell(or_ecycle* h, Impl<R>& m, int parity) {
+  if (m.sps.info.empty()) return OR_OK;
+  size_t sm = shell_smem<R>(m.sps.nlmax);
+  shell_patch_kernel<R, T><<<(unsigned)m.sps.info.size(), T, sm, h->stream>>>(m.sargs(), parity, m.zw.p);
+  CK(cudaGetLastError());
+  h->launches++;
+  return OR_OK;
+}
+template <class R>
+int launch_node(or_ecycle* h, Impl<R>& m, int parity) {
+  node_kernel<R, NODE_TILE><<<(unsigned)m.ntiles, NODE_TILE, 0, h->stream>>>(m.nargs(h), parity);
+  CK(cudaGetLastError());
+  h->launches++;
+  return OR_OK;
+}
+
+template <class R>
+int set_smem_attrs(or_ecycle* h, Impl<R>& m) {
+  int hs = (int)hex_smem<R>(m.hps.nlmax), ss = (int)shell_smem<R>(m.sps.nlmax);
+  CK(cudaFuncSetAttribute(hex_patch_kernel<R, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, hs));
+  CK(cudaFuncSetAttribute(hex_patch_kernel<R, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, hs));
+  CK(cudaFuncSetAttribute(shell_patch_kernel<R, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss));
+  CK(cudaFuncSetAttribute(shell_patch_kernel<R, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss));
+  if (hs > 200 * 1024 || ss > 200 * 1024) return fail(h, OR_E_UNSUPPORTED, "patch shared memory above 200 KB");
+  return OR_OK;
+}
+
+template <class R>
+int launch_cycle(or_ecycle* h, Impl<R>& m, int parity, cudaEvent_t* ev) {
+  int rc;
+  if (ev) CK(cudaEventRecord(ev[0], h->stream));
+  rc = h->tile_hex == 128 ? launch_hex<R, 128>(h, m, parity) : launch_hex<R, 256>(h, m, parity);
+  if (rc) return rc;
+  if (ev) CK(cudaEventRecord(ev[1], h->stream));
+  rc = h->tile_shell == 128 ? launch_shell<R, 128>(h, m, parity) : launch_shell<R, 256>(h, m, parity);
+  if (rc) return rc;
+  if (ev) CK(cudaEventRecord(ev[2], h->stream));
+  rc = launch_node<R>(h, m, parity);
+  if (rc) return rc;
+  if (ev) CK(cudaEventRecord(ev[3], h->stream));
+  return OR_OK;
+}
+
+template <class R>
+int reset_impl(or_ecycle* h);
+
+template <class R>
+int finalize_impl(or_ecycle* h) {
+  typedef typename Vec4<R>::T R4;
+  Impl<R>* mp = new Impl<R>();
+  h->impl = mp;
+  Impl<R>& m = *mp;
+  m.nparts = (int)h->parts.size();
+  // node layout
+  int nn = 0, nt = 0;
+  std::vector<int> tile_part;
+  for (auto& P : h->parts) {
+    P.node_start = nn;
+    P.tile_start = nt;
+    int pad = (P.numnod + NODE_TILE - 1) / NODE_TILE * NODE_TILE;
+    P.node_pad = pad;
+    for (int t = 0; t < pad / NODE_TILE; ++t) tile_part.push_back((int)(&P - &h->parts[0]));
+    nn += pad;
+    nt += pad / NODE_TILE;
+    m.any_rot = m.any_rot || P.has_rot;
+  }
+  m.nnodpad = nn;
+  m.ntiles = nt;
+  // patches
+  std::vector<std::vector<std::pair<int, int>>> node_patch(nn);
+  int rc = build_patches<8>(h, h->hex, h->tile_hex, m.hps, node_patch, 0);
+  if (rc) return rc;
+  const int nhp = (int)m.hps.info.size();
+  rc = build_patches<4>(h, h->shell, h->tile_shell, m.sps, node_patch, nhp);
+  if (rc) return rc;
+  // node-major slots: per node, its (patch) entries in ascending patch number
+  std::vector<int> adsky(nn + 1, 0);
+  for (int n = 0; n < nn; ++n) adsky[n + 1] = adsky[n] + (int)node_patch[n].size();
+  m.nslot = adsky[nn];
+  for (int n = 0; n < nn; ++n) {
+    auto& lst = node_patch[n];
+    std::sort(lst.begin(), lst.end());
+    for (size_t j = 0; j < lst.size(); ++j) {
+      const int pid = lst[j].first, pos = lst[j].second;
+      if (pid < nhp) m.hps.slots[pos] = adsky[n] + (int)j;
+      else m.sps.slots[pos] = adsky[n] + (int)j;
+    }
+  }
+  node_patch.clear();
+  node_patch.shrink_to_fit();
+  // node arrays
+  std::vector<double4> X(nn, make_double4(0, 0, 0, 0));
+  std::vector<R4> V(nn, mk4(R(0), R(0), R(0), R(0))), VR(m.any_rot ? nn : 0, mk4(R(0), R(0), R(0), R(0)));
+  std::vector<unsigned char> code(nn, 0);
+  std::vector<PartDesc> pd;
+  for (auto& P : h->parts) {
+    for (int i = 0; i < P.numnod; ++i) {
+      const int g = P.node_start + i;
+      X[g] = make_double4(P.x[3 * i], P.x[3 * i + 1], P.x[3 * i + 2], (double)(R)P.ms[i]);
+      V[g] = mk4(R(P.v[3 * i]), R(P.v[3 * i + 1]), R(P.v[3 * i + 2]), R(0));
+      if (m.any_rot) VR[g] = mk4(R(P.vr[3 * i]), R(P.vr[3 * i + 1]), R(P.vr[3 * i + 2]), R(P.in[i]));
+      code[g] = (unsigned char)((P.icodt[i] & 7) | ((P.icodr[i] & 7) << 3));
+    }
+    PartDesc d;
+    d.node_start = P.node_start; d.node_end = P.node_start + P.numnod; d.tile_start = P.tile_start;
+    d.has_rot = P.has_rot ? 1 : 0;
+    pd.push_back(d);
+  }
+  if ((rc = dput(h, m.X, X)) || (rc = dput(h, m.V, V)) || (rc = dput(h, m.VR, VR)) || (rc = dput(h, m.code, code)) ||
+      (rc = dput(h, m.adsky, adsky)) || (rc = dput(h, m.tile_part, tile_part)) || (rc = dput(h, m.partd, pd)))
+    return rc;
+  std::vector<double> zero(nn, 0.0);
+  if ((rc = dput(h, m.DX, zero)) || (rc = dput(h, m.DY, zero)) || (rc = dput(h, m.DZ, zero))) return rc;
+  if ((rc = dalloc(h, m.fslot, (size_t)m.nslot))) return rc;
+  CK(cudaMemset(m.fslot.p, 0, m.fslot.n * sizeof(R4)));
+  if (!h->shell.empty()) {
+    if ((rc = dalloc(h, m.mslot, (size_t)m.nslot))) return rc;
+    CK(cudaMemset(m.mslot.p, 0, m.mslot.n * sizeof(R4)));
+  }
+  if ((rc = dalloc(h, m.time, 2 * (size_t)m.nparts)) || (rc = dalloc(h, m.acc, 2 * (size_t)m.nparts)) ||
+      (rc = dalloc(h, m.err, 1)))
+    return rc;
+  CK(cudaMemset(m.err.p, 0, sizeof(ErrorWord)));
+  if ((rc = dput(h, m.ekin, std::vector<double>(m.ntiles, 0.0))) || (rc = dput(h, m.ekinr, std::vector<double>(m.ntiles, 0.0))))
+    return rc;
+  // hexas
+  if (!h->hex.empty()) {
+    PatchSet& ps = m.hps;
+    const int np = ps.nelpad;
+    std::vector<HexGroupDesc> desc;
+    for (auto& g : h->hex) {
+      HexGroupDesc d{};
+      d.part = g.part; d.law = g.mat.law; d.nel = g.nel;
+      d.rho0 = g.mat.rho0; d.shear = g.mat.shear; d.bulk = g.mat.bulk; d.jc_a = g.mat.jc_a; d.jc_b = g.mat.jc_b;
+      d.jc_n = g.mat.jc_n; d.epsmax = g.mat.epsmax; d.sigmax = g.mat.sigmax;
+      d.qa = g.prop.qa; d.qb = g.prop.qb; d.qh = g.prop.qh; d.dtfac = h->cfg.dtfac_solid; d.dtmin = h->cfg.dtmin_solid;
+      desc.push_back(d);
+    }
+    std::vector<uint4> conn(np, make_uint4(0, 0, 0, 0));
+    std::vector<int> elem(np, 0);
+    std::vector<R> rho(np, R(0)), vol0(np, R(0));
+    std::vector<double> vol0dp(np, 0.0);
+    for (int ie = 0; ie < np; ++ie) {
+      const int gi = ps.elem_group[ie];
+      if (gi < 0) continue;
+      const uint16_t* l = &ps.local[(size_t)ie * 8];
+      conn[ie] = make_uint4(l[0] | (unsigned)l[1] << 16, l[2] | (unsigned)l[3] << 16, l[4] | (unsigned)l[5] << 16,
+                            l[6] | (unsigned)l[7] << 16);
+      const HHex& g = h->hex[gi];
+      const int ue = ps.elem_user[ie];
+      elem[ie] = g.gofs + ue;
+      rho[ie] = R(g.mat.rho0);
+      vol0[ie] = R(g.vol0[ue]);
+      vol0dp[ie] = g.vol0[ue];
+    }
+    if ((rc = dput(h, m.hpatch, ps.info)) || (rc = dput(h, m.hdesc, desc)) || (rc = dput(h, m.hnodes, ps.nodes)) ||
+        (rc = dput(h, m.hslots, ps.slots)) || (rc = dput(h, m.helem, elem)) || (rc = dput(h, m.hconn, conn)) ||
+        (rc = dput(h, m.hrho, rho)) || (rc = dput(h, m.hvol0, vol0)) || (rc = dput(h, m.hvol0dp, vol0dp)))
+      return rc;
+    std::vector<R> z(np, R(0));
+    if ((rc = dput(h, m.heint, z)) || (rc = dput(h, m.hqvis, z)) || (rc = dput(h, m.hpla, z)) || (rc = dput(h, m.hepsd, z)))
+      return rc;
+    if ((rc = dalloc(h, m.hsig, 6 * (size_t)np))) return rc;
+    CK(cudaMemset(m.hsig.p, 0, m.hsig.n * sizeof(R)));
+    if ((rc = dput(h, m.hehour, std::vector<double>(ps.info.size(), 0.0))) ||
+        (rc = dput(h, m.hwpla, std::vector<double>(ps.info.size(), 0.0))))
+      return rc;
+  }
+  // shells
+  if (!h->shell.empty()) {
+    PatchSet& ps = m.sps;
+    const int np = ps.nelpad;
+    std::vector<ShellGroupDesc> desc;
+    bool any_jca = false;
+    for (auto& g : h->shell) {
+      ShellGroupDesc d{};
+      d.part = g.part; d.law = g.mat.law; d.nel = g.nel; d.npt = g.prop.npt; d.ithk = g.prop.ithk;
+      d.has_jca = g.jca.empty() ? 0 : 1;
+      any_jca = any_jca || !g.jca.empty();
+      d.rho0 = g.mat.rho0; d.young = g.mat.young; d.nu = g.mat.nu; d.shear = g.mat.shear; d.a11 = g.mat.a11;
+      d.a12 = g.mat.a12; d.ssp = g.mat.ssp_shell; d.jc_a = g.mat.jc_a; d.jc_b = g.mat.jc_b; d.jc_n = g.mat.jc_n;
+      d.sigmax = g.mat.sigmax; d.hm = g.prop.hm; d.hf = g.prop.hf; d.hr = g.prop.hr; d.shf = g.prop.shf;
+      d.pressure = g.prop.pressure; d.dtfac = h->cfg.dtfac_shell; d.dtmin = h->cfg.dtmin_shell;
+      desc.push_back(d);
+      m.maxnpt = std::max(m.maxnpt, g.prop.npt);
+    }
+    std::vector<uint2> conn(np, make_uint2(0, 0));
+    std::vector<int> elem(np, 0), degen(np, 0);
+    std::vector<R> thke(np, R(1)), jca(any_jca ? np : 0, R(0));
+    for (int ie = 0; ie < np; ++ie) {
+      const int gi = ps.elem_group[ie];
+      if (gi < 0) continue;
+      const uint16_t* l = &ps.local[(size_t)ie * 4];
+      conn[ie] = make_uint2(l[0] | (unsigned)l[1] << 16, l[2] | (unsigned)l[3] << 16);
+      const HShell& g = h->shell[gi];
+      const int ue = ps.elem_user[ie];
+      elem[ie] = g.gofs + ue;
+      degen[ie] = g.conn[4 * (size_t)ue + 2] == g.conn[4 * (size_t)ue + 3] ? 1 : 0;
+      thke[ie] = R(g.thke[ue]);
+      if (any_jca) jca[ie] = R(g.jca.empty() ? g.mat.jc_a : g.jca[ue]);
+    }
+    if ((rc = dput(h, m.spatch, ps.info)) || (rc = dput(h, m.sdesc, desc)) || (rc = dput(h, m.snodes, ps.nodes)) ||
+        (rc = dput(h, m.sslots, ps.slots)) || (rc = dput(h, m.selem, elem)) || (rc = dput(h, m.sdegen, degen)) ||
+        (rc = dput(h, m.sconn, conn)) || (rc = dput(h, m.sthke, thke)) || (rc = dput(h, m.sthk, thke)) ||
+        (rc = dput(h, m.sjca, jca)))
+      return rc;
+    if ((rc = dalloc(h, m.ssig, (size_t)m.maxnpt * 5 * np)) || (rc = dalloc(h, m.spla, (size_t)m.maxnpt * np)) ||
+        (rc = dalloc(h, m.shourg, 3 * (size_t)np)) || (rc = dalloc(h, m.seint, 2 * (size_t)np)))
+      return rc;
+    CK(cudaMemset(m.ssig.p, 0, m.ssig.n * sizeof(R)));
+    CK(cudaMemset(m.spla.p, 0, m.spla.n * sizeof(R)));
+    CK(cudaMemset(m.shourg.p, 0, m.shourg.n * sizeof(R)));
+    CK(cudaMemset(m.seint.p, 0, m.seint.n * sizeof(R)));
+    std::vector<float> zw(&ZW_TABLE[0][0], &ZW_TABLE[0][0] + 10 * 33);
+    if ((rc = dput(h, m.zw, zw))) return rc;
+    if ((rc = dput(h, m.sehour, std::vector<double>(ps.info.size(), 0.0))) ||
+        (rc = dput(h, m.swpla, std::vector<double>(ps.info.size(), 0.0))))
+      return rc;
+  }
+  rc = set_smem_attrs<R>(h, m);
+  if (rc) return rc;
+  CK(cudaDeviceSynchronize());
+  return OR_OK;
+}
+
+// Re-uploads the initial node arrays and re-initialises the element state.
+template <class R>
+int reset_impl(or_ecycle* h) {
+  typedef typename Vec4<R>::T R4;
+  Impl<R>& m = *(Impl<R>*)h->impl;
+  const int nn = m.nnodpad;
+  CK(cudaStreamSynchronize(h->stream));
+  std::vector<double4> X(nn, make_double4(0, 0, 0, 0));
+  std::vector<R4> V(nn, mk4(R(0), R(0), R(0), R(0))), VR(m.any_rot ? nn : 0, mk4(R(0), R(0), R(0), R(0)));
+  for (auto& P : h->parts)
+    for (int i = 0; i < P.numnod; ++i) {
+      const int g = P.node_start + i;
+      X[g] = make_double4(P.x[3 * i], P.x[3 * i + 1], P.x[3 * i + 2], (double)(R)P.ms[i]);
+      V[g] = mk4(R(P.v[3 * i]), R(P.v[3 * i + 1]), R(P.v[3 * i + 2]), R(0));
+      if (m.any_rot) VR[g] = mk4(R(P.vr[3 * i]), R(P.vr[3 * i + 1]), R(P.vr[3 * i + 2]), R(P.in[i]));
+    }
+  CK(cudaMemcpy(m.X.p, X.data(), X.size() * sizeof(double4), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(m.V.p, V.data(), V.size() * sizeof(R4), cudaMemcpyHostToDevice));
+  if (m.any_rot) CK(cudaMemcpy(m.VR.p, VR.data(), VR.size() * sizeof(R4), cudaMemcpyHostToDevice));
+  CK(cudaMemset(m.DX.p, 0, nn * sizeof(double)));
+  CK(cudaMemset(m.DY.p, 0, nn * sizeof(double)));
+  CK(cudaMemset(m.DZ.p, 0, nn * sizeof(double)));
+  if (!h->hex.empty()) {
+    const int np = m.hps.nelpad;
+    std::vector<R> rho(np, R(0));
+    for (int ie = 0; ie < np; ++ie) {
+      const int gi = m.hps.elem_group[ie];
+      if (gi >= 0) rho[ie] = R(h->hex[gi].mat.rho0);
+    }
+    CK(cudaMemcpy(m.hrho.p, rho.data(), np * sizeof(R), cudaMemcpyHostToDevice));
+    CK(cudaMemset(m.heint.p, 0, np * sizeof(R)));
+    CK(cudaMemset(m.hqvis.p, 0, np * sizeof(R)));
+    CK(cudaMemset(m.hpla.p, 0, np * sizeof(R)));
+    CK(cudaMemset(m.hepsd.p, 0, np * sizeof(R)));
+    CK(cudaMemset(m.hsig.p, 0, m.hsig.n * sizeof(R)));
+    CK(cudaMemset(m.hehour.p, 0, m.hehour.n * sizeof(double)));
+    CK(cudaMemset(m.hwpla.p, 0, m.hwpla.n * sizeof(double)));
+  }
+  if (!h->shell.empty()) {
+    CK(cudaMemcpy(m.sthk.p, m.sthke.p, m.sthk.n * sizeof(R), cudaMemcpyDeviceToDevice));
+    CK(cudaMemset(m.ssig.p, 0, m.ssig.n * sizeof(R)));
+    CK(cudaMemset(m.spla.p, 0, m.spla.n * sizeof(R)));
+    CK(cudaMemset(m.shourg.p, 0, m.shourg.n * sizeof(R)));
+    CK(cudaMemset(m.seint.p, 0, m.seint.n * sizeof(R)));
+    CK(cudaMemset(m.sehour.p, 0, m.sehour.n * sizeof(double)));
+    CK(cudaMemset(m.swpla.p, 0, m.swpla.n * sizeof(double)));
+  }
+  CK(cudaMemset(m.ekin.p, 0, m.ekin.n * sizeof(double)));
+  CK(cudaMemset(m.ekinr.p, 0, m.ekinr.n * sizeof(double)));
+  CK(cudaDeviceSynchronize());
+  return OR_OK;
+}
+
+int wait_stream(or_ecycle* h, cudaEvent_t ev) {
+  double limit = 3600.0;
+  if (const char* s = std::getenv("OR_ECYCLE_TIMEOUT_S")) limit = std::atof(s);
+  auto t0 = std::chrono::steady_clock::now();
+  for (;;) {
+    cudaError_t q = cudaEventQuery(ev);
+    if (q == cudaSuccess) return OR_OK;
+    if (q != cudaErrorNotReady) return fail(h, OR_E_CUDA, std::string("stream: ") + cudaGetErrorString(q));
+    double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (el > limit) return fail(h, OR_E_TIMEOUT, "bounded wait expired");
+    std::this_thread::sleep_for(std::chrono::microseconds(el < 0.01 ? 5 : 200));
+  }
+}
+
+template <class R>
+int step_impl(or_ecycle* h, int ncycles, or_ecycle_time* t) {
+  Impl<R>& m = *(Impl<R>*)h->impl;
+  const int np = m.nparts;
+  std::vector<PartTime> pt(np);
+  for (int p = 0; p < np; ++p) {
+    pt[p].tt = t[p].tt; pt[p].dt2 = t[p].dt2; pt[p].dt2old = t[p].dt2old; pt[p].dt1 = t[p].dt1;
+    pt[p].dt12 = t[p].dt12; pt[p].ncycle = t[p].ncycle; pt[p].ityptst = t[p].ityptst; pt[p].neltst = t[p].neltst;
+    pt[p].pad = 0;
+  }
+  std::vector<PartAcc> acc0(np);
+  for (auto& a : acc0) { a.dtkey = ~0ull; a.dtbits = ~0ull; }
+  h->launches = 0;
+  CK(cudaMemcpyAsync(m.time.p, pt.data(), np * sizeof(PartTime), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(m.acc.p, acc0.data(), np * sizeof(PartAcc), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemsetAsync(m.err.p, 0, sizeof(ErrorWord), h->stream));
+  int rc;
+  const bool use_graph = h->cfg.graph != 0;
+  int done = 0;
+  if (use_graph && ncycles >= GRAPH_CYCLES) {
+    if (!h->graph_exec) {
+      CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+      long long l0 = h->launches;
+      for (int c = 0; c < GRAPH_CYCLES; ++c) {
+        rc = launch_cycle<R>(h, m, c & 1, nullptr);
+        if (rc) { cudaGraph_t g; cudaStreamEndCapture(h->stream, &g); if (g) cudaGraphDestroy(g); return rc; }
+      }
+      CK(cudaStreamEndCapture(h->stream, &h->graph));
+      CK(cudaGraphInstantiate(&h->graph_exec, h->graph, 0));
+      h->launches = l0;
+    }
+    const long long per = (long long)GRAPH_CYCLES * ((m.hps.info.empty() ? 0 : 1) + (m.sps.info.empty() ? 0 : 1) + 1);
+    for (; done + GRAPH_CYCLES <= ncycles; done += GRAPH_CYCLES) {
+      CK(cudaGraphLaunch(h->graph_exec, h->stream));
+      h->launches += per;
+    }
+  }
+  cudaEvent_t ev[4];
+  const bool timing = !use_graph;
+  if (timing) {
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    for (double& x : h->phase_ms) x = 0;
+  }
+  for (; done < ncycles; ++done) {
+    rc = launch_cycle<R>(h, m, done & 1, timing ? ev : nullptr);
+    if (rc) return rc;
+    if (timing) {
+      CK(cudaEventSynchronize(ev[3]));
+      float a, b, c;
+      cudaEventElapsedTime(&a, ev[0], ev[1]);
+      cudaEventElapsedTime(&b, ev[1], ev[2]);
+      cudaEventElapsedTime(&c, ev[2], ev[3]);
+      h->phase_ms[0] += a; h->phase_ms[1] += b; h->phase_ms[2] += c; h->phase_ms[3] += a + b + c;
+    }
+  }
+  if (timing) for (auto& e : ev) cudaEventDestroy(e);
+  const int fin = ncycles & 1;
+  CK(cudaMemcpyAsync(pt.data(), m.time.p + fin * np, np * sizeof(PartTime), cudaMemcpyDeviceToHost, h->stream));
+  ErrorWord ew{};
+  CK(cudaMemcpyAsync(&ew, m.err.p, sizeof(ErrorWord), cudaMemcpyDeviceToHost, h->stream));
+  cudaEvent_t done_ev;
+  CK(cudaEventCreateWithFlags(&done_ev, cudaEventDisableTiming));
+  CK(cudaEventRecord(done_ev, h->stream));
+  rc = wait_stream(h, done_ev);
+  cudaEventDestroy(done_ev);
+  if (rc) return rc;
+  for (int p = 0; p < np; ++p) {
+    t[p].tt = pt[p].tt; t[p].dt1 = pt[p].dt1; t[p].dt2 = pt[p].dt2; t[p].dt12 = pt[p].dt12;
+    t[p].dt2old = pt[p].dt2old; t[p].ncycle = pt[p].ncycle; t[p].ityptst = pt[p].ityptst; t[p].neltst = pt[p].neltst;
+  }
+  h->last_code = ew.code;
+  h->last_index = ew.index;
+  if (ew.code) {
+    char buf[160];
+    snprintf(buf, sizeof buf, "device error %d at index %d", ew.code, ew.index);
+    return fail(h, ew.code, buf);
+  }
+  return OR_OK;
+}
+
+template <class R>
+int get_nodes_impl(or_ecycle* h, int part, double* x, double* d, double* v, double* vr) {
+  typedef typename Vec4<R>::T R4;
+  Impl<R>& m = *(Impl<R>*)h->impl;
+  const HPart& P = h->parts[part];
+  const int n = P.numnod, s = P.node_start;
+  CK(cudaStreamSynchronize(h->stream));
+  if (x) {
+    std::vector<double4> X(n);
+    CK(cudaMemcpy(X.data(), m.X.p + s, n * sizeof(double4), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n; ++i) { x[3 * i] = X[i].x; x[3 * i + 1] = X[i].y; x[3 * i + 2] = X[i].z; }
+  }
+  if (d) {
+    std::vector<double> a(n), b(n), c(n);
+    CK(cudaMemcpy(a.data(), m.DX.p + s, n * sizeof(double), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(b.data(), m.DY.p + s, n * sizeof(double), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(c.data(), m.DZ.p + s, n * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n; ++i) { d[3 * i] = a[i]; d[3 * i + 1] = b[i]; d[3 * i + 2] = c[i]; }
+  }
+  if (v) {
+    std::vector<R4> V(n);
+    CK(cudaMemcpy(V.data(), m.V.p + s, n * sizeof(R4), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n; ++i) { v[3 * i] = V[i].x; v[3 * i + 1] = V[i].y; v[3 * i + 2] = V[i].z; }
+  }
+  if (vr) {
+    if (m.VR.p) {
+      std::vector<R4> W(n);
+      CK(cudaMemcpy(W.data(), m.VR.p + s, n * sizeof(R4), cudaMemcpyDeviceToHost));
+      for (int i = 0; i < n; ++i) { vr[3 * i] = W[i].x; vr[3 * i + 1] = W[i].y; vr[3 * i + 2] = W[i].z; }
+    } else {
+      std::fill(vr, vr + 3 * (size_t)n, 0.0);
+    }
+  }
+  return OR_OK;
+}
+
+template <class R>
+int set_nodes_impl(or_ecycle* h, int part, const double* x, const double* d, const double* v, const double* vr) {
+  typedef typename Vec4<R>::T R4;
+  Impl<R>& m = *(Impl<R>*)h->impl;
+  const HPart& P = h->parts[part];
+  const int n = P.numnod, s = P.node_start;
+  CK(cudaStreamSynchronize(h->stream));
+  if (x) {
+    std::vector<double4> X(n);
+    CK(cudaMemcpy(X.data(), m.X.p + s, n * sizeof(double4), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n; ++i) { X[i].x = x[3 * i]; X[i].y = x[3 * i + 1]; X[i].z = x[3 * i + 2]; }
+    CK(cudaMemcpy(m.X.p + s, X.data(), n * sizeof(double4), cudaMemcpyHostToDevice));
+  }
+  if (d) {
+    std::vector<double> a(n), b(n), c(n);
+    for (int i = 0; i < n; ++i) { a[i] = d[3 * i]; b[i] = d[3 * i + 1]; c[i] = d[3 * i + 2]; }
+    CK(cudaMemcpy(m.DX.p + s, a.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(m.DY.p + s, b.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(m.DZ.p + s, c.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  if (v) {
+    std::vector<R4> V(n);
+    for (int i = 0; i < n; ++i) V[i] = mk4(R(v[3 * i]), R(v[3 * i + 1]), R(v[3 * i + 2]), R(0));
+    CK(cudaMemcpy(m.V.p + s, V.data(), n * sizeof(R4), cudaMemcpyHostToDevice));
+  }
+  if (vr && m.VR.p) {
+    std::vector<R4> W(n);
+    CK(cudaMemcpy(W.data(), m.VR.p + s, n * sizeof(R4), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n; ++i) { W[i].x = R(vr[3 * i]); W[i].y = R(vr[3 * i + 1]); W[i].z = R(vr[3 * i + 2]); }
+    CK(cudaMemcpy(m.VR.p + s, W.data(), n * sizeof(R4), cudaMemcpyHostToDevice));
+  }
+  return OR_OK;
+}
+
+template <class R>
+std::vector<R> d2h(const R* p, size_t n) {
+  std::vector<R> v(n);
+  if (n) cudaMemcpy(v.data(), p, n * sizeof(R), cudaMemcpyDeviceToHost);
+  return v;
+}
+
+template <class R>
+int hex_state_impl(or_ecycle* h, int gi, double* sig, double* eint, double* rho, double* qvis, double* pla, double* epsd) {
+  Impl<R>& m = *(Impl<R>*)h->impl;
+  const HHex& g = h->hex[gi];
+  const int np = m.hps.nelpad;
+  CK(cudaStreamSynchronize(h->stream));
+  if (sig) {
+    auto s = d2h(m.hsig.p, 6 * (size_t)np);
+    for (int c = 0; c < 6; ++c)
+      for (int i = 0; i < g.nel; ++i) sig[(size_t)c * g.nel + i] = s[(size_t)c * np + g.internal[i]];
+  }
+  auto one = [&](double* out, const DBuf<R>& b) {
+    if (!out) return;
+    auto s = d2h(b.p, (size_t)np);
+    for (int i = 0; i < g.nel; ++i) out[i] = s[g.internal[i]];
+  };
+  one(eint, m.heint); one(rho, m.hrho); one(qvis, m.hqvis); one(pla, m.hpla); one(epsd, m.hepsd);
+  CK(cudaGetLastError());
+  return OR_OK;
+}
+
+template <class R>
+int shell_state_impl(or_ecycle* h, int gi, double* sig, double* pla, double* thk, double* hourg, double* eint) {
+  Impl<R>& m = *(Impl<R>*)h->impl;
+  const HShell& g = h->shell[gi];
+  const int np = m.sps.nelpad, npt = g.prop.npt;
+  CK(cudaStreamSynchronize(h->stream));
+  if (sig) {
+    auto s = d2h(m.ssig.p, m.ssig.n);
+    for (int q = 0; q < npt * 5; ++q)
+      for (int i = 0; i < g.nel; ++i) sig[(size_t)q * g.nel + i] = s[(size_t)q * np + g.internal[i]];
+  }
+  if (pla) {
+    auto s = d2h(m.spla.p, m.spla.n);
+    for (int q = 0; q < npt; ++q)
+      for (int i = 0; i < g.nel; ++i) pla[(size_t)q * g.nel + i] = s[(size_t)q * np + g.internal[i]];
+  }
+  if (thk) {
+    auto s = d2h(m.sthk.p, (size_t)np);
+    for (int i = 0; i < g.nel; ++i) thk[i] = s[g.internal[i]];
+  }
+  if (hourg) {
+    auto s = d2h(m.shourg.p, 3 * (size_t)np);
+    for (int q = 0; q < 3; ++q)
+      for (int i = 0; i < g.nel; ++i) hourg[(size_t)q * g.nel + i] = s[(size_t)q * np + g.internal[i]];
+  }
+  if (eint) {
+    auto s = d2h(m.seint.p, 2 * (size_t)np);
+    for (int q = 0; q < 2; ++q)
+      for (int i = 0; i < g.nel; ++i) eint[(size_t)q * g.nel + i] = s[(size_t)q * np + g.internal[i]];
+  }
+  CK(cudaGetLastError());
+  return OR_OK;
+}
+
+template <class R>
+int energies_impl(or_ecycle* h, int part, or_energies* e) {
+  Impl<R>& m = *(Impl<R>*)h->impl;
+  CK(cudaStreamSynchronize(h->stream));
+  double ei = 0, eh = 0, wp = 0, ek = 0, ekr = 0;
+  if (!h->hex.empty()) {
+    auto eint = d2h(m.heint.p, m.heint.n);
+    auto vol0 = d2h(m.hvol0.p, m.hvol0.n);
+    auto ehour = d2h(m.hehour.p, m.hehour.n);
+    auto wpla = d2h(m.hwpla.p, m.hwpla.n);
+    for (size_t ie = 0; ie < eint.size(); ++ie) {
+      const int gi = m.hps.elem_group[ie];
+      if (gi >= 0 && h->hex[gi].part == part) ei += (double)eint[ie] * (double)vol0[ie];
+    }
+    for (size_t p = 0; p < m.hps.info.size(); ++p)
+      if (h->hex[m.hps.info[p].group].part == part) { eh += ehour[p]; wp += wpla[p]; }
+  }
+  if (!h->shell.empty()) {
+    auto eint = d2h(m.seint.p, m.seint.n);
+    auto ehour = d2h(m.sehour.p, m.sehour.n);
+    auto wpla = d2h(m.swpla.p, m.swpla.n);
+    const size_t np = m.sps.nelpad;
+    for (size_t ie = 0; ie < np; ++ie) {
+      const int gi = m.sps.elem_group[ie];
+      if (gi >= 0 && h->shell[gi].part == part) ei += (double)eint[ie] + (double)eint[np + ie];
+    }
+    for (size_t p = 0; p < m.sps.info.size(); ++p)
+      if (h->shell[m.sps.info[p].group].part == part) { eh += ehour[p]; wp += wpla[p]; }
+  }
+  auto ekin = d2h(m.ekin.p, m.ekin.n);
+  auto ekinr = d2h(m.ekinr.p, m.ekinr.n);
+  const HPart& P = h->parts[part];
+  for (int t = P.tile_start; t < P.tile_start + P.node_pad / NODE_TILE; ++t) { ek += ekin[t]; ekr += ekinr[t]; }
+  e->internal = ei; e->kinetic = ek; e->kinetic_rot = ekr; e->hourglass = eh; e->plastic_work = wp; e->pad = 0;
+  CK(cudaGetLastError());
+  return OR_OK;
+}
+
+template <class R>
+void destroy_impl(or_ecycle* h) {
+  if (!h->impl) return;
+  Impl<R>* m = (Impl<R>*)h->impl;
+  m->free_all();
+  delete m;
+  h->impl = nullptr;
+}
+
+#define DISPATCH(h, fn, ...) \
+  ((h)->cfg.precision == OR_PREC_SPLIT ? fn<float>(h, __VA_ARGS__) : fn<double>(h, __VA_ARGS__))
+
+bool bad_ptr(const void* p) { return p == nullptr; }
+
+}  // namespace
+
+extern "C" {
+
+int or_ecycle_create(const or_ecycle_config* cfg, or_ecycle** out) {
+  if (!cfg || !out) return OR_E_ARG;
+  if (cfg->precision != OR_PREC_FP64 && cfg->precision != OR_PREC_SPLIT) return OR_E_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return OR_E_CUDA;
+  if (cfg->device < 0 || cfg->device >= ndev) return OR_E_ARG;
+  or_ecycle* h = new or_ecycle();
+  h->cfg = *cfg;
+  if (h->cfg.dt_growth <= 0) h->cfg.dt_growth = (double)1.1f;
+  if (h->cfg.dtmx <= 0) h->cfg.dtmx = 1e20;
+  if (h->cfg.block_hex == 128 || h->cfg.block_hex == 256) h->tile_hex = h->cfg.block_hex;
+  if (h->cfg.block_shell == 128 || h->cfg.block_shell == 256) h->tile_shell = h->cfg.block_shell;
+  if (cudaSetDevice(cfg->device) != cudaSuccess || cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete h;
+    return OR_E_CUDA;
+  }
+  *out = h;
+  return OR_OK;
+}
+
+int or_ecycle_destroy(or_ecycle* h) {
+  if (!h) return OR_E_ARG;
+  cudaSetDevice(h->cfg.device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+  if (h->graph) cudaGraphDestroy(h->graph);
+  if (h->cfg.precision == OR_PREC_SPLIT) destroy_impl<float>(h); else destroy_impl<double>(h);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return OR_OK;
+}
+
+const char* or_ecycle_last_error(const or_ecycle* h) { return h ? h->err.c_str() : "null handle"; }
+
+int or_ecycle_add_part(or_ecycle* h, int numnod, const double* x, const double* v, const double* vr, const double* ms,
+                       const double* in, const int* icodt, const int* icodr, int* part) {
+  if (!h) return OR_E_ARG;
+  if (h->finalized) return fail(h, OR_E_STATE, "add_part after finalize");
+  if (numnod <= 0 || bad_ptr(x) || bad_ptr(v) || bad_ptr(ms) || bad_ptr(icodt) || bad_ptr(part))
+    return fail(h, OR_E_ARG, "add_part: null array or empty part");
+  HPart P;
+  P.numnod = numnod;
+  P.x.assign(x, x + 3 * (size_t)numnod);
+  P.v.assign(v, v + 3 * (size_t)numnod);
+  P.vr.assign(3 * (size_t)numnod, 0.0);
+  if (vr) P.vr.assign(vr, vr + 3 * (size_t)numnod);
+  P.ms.assign(ms, ms + numnod);
+  P.in.assign(numnod, 0.0);
+  if (in) P.in.assign(in, in + numnod);
+  P.icodt.assign(icodt, icodt + numnod);
+  P.icodr.assign(numnod, 0);
+  if (icodr) P.icodr.assign(icodr, icodr + numnod);
+  for (int i = 0; i < 3 * numnod; ++i)
+    if (!std::isfinite(P.x[i]) || !std::isfinite(P.v[i])) return fail(h, OR_E_ARG, "add_part: non-finite X or V");
+  h->parts.push_back(std::move(P));
+  *part = (int)h->parts.size() - 1;
+  return OR_OK;
+}
+
+int or_ecycle_add_hex_group(or_ecycle* h, int part, int nel, const int* ixs, const or_material* mat,
+                            const or_solid_prop* prop, const double* vol0, int* group) {
+  if (!h) return OR_E_ARG;
+  if (h->finalized) return fail(h, OR_E_STATE, "add_hex_group after finalize");
+  if (part < 0 || part >= (int)h->parts.size() || nel <= 0 || !ixs || !mat || !prop || !group)
+    return fail(h, OR_E_ARG, "add_hex_group: bad argument");
+  if (mat->law != OR_LAW_ELASTIC && mat->law != OR_LAW_JOHNSON_COOK) return fail(h, OR_E_UNSUPPORTED, "hex law");
+  HHex g;
+  g.part = part; g.nel = nel; g.mat = *mat; g.prop = *prop;
+  HPart& P = h->parts[part];
+  g.gofs = P.nel_solid;
+  g.conn.resize(8 * (size_t)nel);
+  for (int e = 0; e < nel; ++e)
+    for (int k = 0; k < 8; ++k) {
+      const int n = ixs[11 * (size_t)e + 1 + k] - 1;   // IXS rows 2..9, Fortran numbering
+      if (n < 0 || n >= P.numnod) return fail(h, OR_E_ARG, "add_hex_group: node index out of range in IXS");
+      g.conn[8 * (size_t)e + k] = n;
+    }
+  g.vol0.resize(nel);
+  for (int e = 0; e < nel; ++e) {
+    double v;
+    if (vol0) v = vol0[e];
+    else {
+      const int* c = &g.conn[8 * (size_t)e];
+      auto X = [&](int k, int q) { return P.x[3 * (size_t)c[k] + q]; };
+      double d[4][3];
+      const int pr[4][2] = {{6, 0}, {7, 1}, {4, 2}, {5, 3}};
+      for (int a = 0; a < 4; ++a) for (int q = 0; q < 3; ++q) d[a][q] = X(pr[a][0], q) - X(pr[a][1], q);
+      double j1[3], j4[3], j7[3];
+      for (int q = 0; q < 3; ++q) {
+        j1[q] = d[0][q] + d[1][q] - d[2][q] - d[3][q];
+        j4[q] = d[0][q] + d[3][q] + d[1][q] + d[2][q];
+        j7[q] = d[0][q] + d[3][q] - d[1][q] - d[2][q];
+      }
+      v = (j1[0] * (j4[1] * j7[2] - j4[2] * j7[1]) + j1[1] * (j4[2] * j7[0] - j4[0] * j7[2]) +
+           j1[2] * (j4[0] * j7[1] - j4[1] * j7[0])) / 64.0;
+    }
+    if (!(v > 0)) return fail(h, OR_E_NEGVOL, "add_hex_group: non-positive initial volume");
+    g.vol0[e] = v;
+  }
+  P.nel_solid += nel;
+  h->hex.push_back(std::move(g));
+  *group = (int)h->hex.size() - 1;
+  return OR_OK;
+}
+
+int or_ecycle_add_shell_group(or_ecycle* h, int part, int nel, const int* ixc, const or_material* mat,
+                              const or_shell_prop* prop, const double* thke, int* group) {
+  if (!h) return OR_E_ARG;
+  if (h->finalized) return fail(h, OR_E_STATE, "add_shell_group after finalize");
+  if (part < 0 || part >= (int)h->parts.size() || nel <= 0 || !ixc || !mat || !prop || !group)
+    return fail(h, OR_E_ARG, "add_shell_group: bad argument");
+  if (prop->npt < 1 || prop->npt > 10) return fail(h, OR_E_UNSUPPORTED, "shell npt outside 1..10");
+  if (prop->ipla != 0) return fail(h, OR_E_UNSUPPORTED, "shell IPLA other than radial return");
+  if (mat->law != OR_LAW_ELASTIC && mat->law != OR_LAW_JOHNSON_COOK) return fail(h, OR_E_UNSUPPORTED, "shell law");
+  HShell g;
+  g.part = part; g.nel = nel; g.mat = *mat; g.prop = *prop;
+  HPart& P = h->parts[part];
+  g.gofs = P.nel_shell;
+  g.conn.resize(4 * (size_t)nel);
+  for (int e = 0; e < nel; ++e)
+    for (int k = 0; k < 4; ++k) {
+      const int n = ixc[7 * (size_t)e + 1 + k] - 1;   // IXC rows 2..5
+      if (n < 0 || n >= P.numnod) return fail(h, OR_E_ARG, "add_shell_group: node index out of range in IXC");
+      g.conn[4 * (size_t)e + k] = n;
+    }
+  g.thke.resize(nel);
+  for (int e = 0; e < nel; ++e) {
+    g.thke[e] = thke ? thke[e] : prop->thk;
+    if (!(g.thke[e] > 0)) return fail(h, OR_E_ARG, "add_shell_group: non-positive thickness");
+  }
+  P.nel_shell += nel;
+  P.has_rot = true;
+  h->shell.push_back(std::move(g));
+  *group = (int)h->shell.size() - 1;
+  return OR_OK;
+}
+
+int or_ecycle_set_shell_yield(or_ecycle* h, int group, const double* jc_a) {
+  if (!h) return OR_E_ARG;
+  if (h->finalized) return fail(h, OR_E_STATE, "set_shell_yield after finalize");
+  if (group < 0 || group >= (int)h->shell.size() || !jc_a) return fail(h, OR_E_ARG, "set_shell_yield: bad argument");
+  HShell& g = h->shell[group];
+  g.jca.assign(jc_a, jc_a + g.nel);
+  return OR_OK;
+}
+
+int or_ecycle_finalize(or_ecycle* h) {
+  if (!h) return OR_E_ARG;
+  if (h->finalized) return fail(h, OR_E_STATE, "finalize called twice");
+  if (h->parts.empty()) return fail(h, OR_E_STATE, "finalize without parts");
+  if (cudaSetDevice(h->cfg.device) != cudaSuccess) return fail(h, OR_E_CUDA, "cudaSetDevice");
+  int rc = h->cfg.precision == OR_PREC_SPLIT ? finalize_impl<float>(h) : finalize_impl<double>(h);
+  if (rc) return rc;
+  h->finalized = true;
+  return OR_OK;
+}
+
+int or_ecycle_reset(or_ecycle* h) {
+  if (!h) return OR_E_ARG;
+  if (!h->finalized) return fail(h, OR_E_STATE, "reset before finalize");
+  cudaSetDevice(h->cfg.device);
+  return h->cfg.precision == OR_PREC_SPLIT ? reset_impl<float>(h) : reset_impl<double>(h);
+}
+
+int or_ecycle_step(or_ecycle* h, int ncycles, or_ecycle_time* t) {
+  if (!h) return OR_E_ARG;
+  if (!h->finalized) return fail(h, OR_E_STATE, "step before finalize");
+  if (ncycles < 0 || !t) return fail(h, OR_E_ARG, "step: bad argument");
+  if (ncycles == 0) return OR_OK;
+  cudaSetDevice(h->cfg.device);
+  return DISPATCH(h, step_impl, ncycles, t);
+}
+
+int or_ecycle_get_nodes(or_ecycle* h, int part, double* x, double* d, double* v, double* vr) {
+  if (!h || !h->finalized || part < 0 || part >= (int)h->parts.size()) return h ? fail(h, OR_E_ARG, "get_nodes") : OR_E_ARG;
+  cudaSetDevice(h->cfg.device);
+  return DISPATCH(h, get_nodes_impl, part, x, d, v, vr);
+}
+
+int or_ecycle_set_nodes(or_ecycle* h, int part, const double* x, const double* d, const double* v, const double* vr) {
+  if (!h || !h->finalized || part < 0 || part >= (int)h->parts.size()) return h ? fail(h, OR_E_ARG, "set_nodes") : OR_E_ARG;
+  cudaSetDevice(h->cfg.device);
+  return DISPATCH(h, set_nodes_impl, part, x, d, v, vr);
+}
+
+int or_ecycle_get_hex_state(or_ecycle* h, int group, double* sig, double* eint, double* rho, double* qvis, double* pla,
+                            double* epsd) {
+  if (!h || !h->finalized || group < 0 || group >= (int)h->hex.size()) return h ? fail(h, OR_E_ARG, "get_hex_state") : OR_E_ARG;
+  cudaSetDevice(h->cfg.device);
+  return DISPATCH(h, hex_state_impl, group, sig, eint, rho, qvis, pla, epsd);
+}
+
+int or_ecycle_get_shell_state(or_ecycle* h, int group, double* sig, double* pla, double* thk, double* hourg,
+                              double* eint) {
+  if (!h || !h->finalized || group < 0 || group >= (int)h->shell.size())
+    return h ? fail(h, OR_E_ARG, "get_shell_state") : OR_E_ARG;
+  cudaSetDevice(h->cfg.device);
+  return DISPATCH(h, shell_state_impl, group, sig, pla, thk, hourg, eint);
+}
+
+int or_ecycle_energies(or_ecycle* h, int part, or_energies* e) {
+  if (!h || !h->finalized || !e || part < 0 || part >= (int)h->parts.size()) return h ? fail(h, OR_E_ARG, "energies") : OR_E_ARG;
+  cudaSetDevice(h->cfg.device);
+  return DISPATCH(h, energies_impl, part, e);
+}
+
+int or_ecycle_error_info(or_ecycle* h, int* code, int* index) {
+  if (!h || !code || !index) return OR_E_ARG;
+  *code = h->last_code;
+  *index = h->last_index;
+  return OR_OK;
+}
+
+int or_ecycle_phase_times(or_ecycle* h, double* ms4) {
+  if (!h || !ms4) return OR_E_ARG;
+  for (int i = 0; i < 4; ++i) ms4[i] = h->phase_ms[i];
+  return OR_OK;
+}
+
+int or_ecycle_launch_count(or_ecycle* h, long long* n) {
+  if (!h || !n) return OR_E_ARG;
+  *n = h->launches;
+  return OR_OK;
+}
+
+int or_ecycle_stream(or_ecycle* h, void** stream) {
+  if (!h || !stream) return OR_E_ARG;
+  *stream = (void*)h->stream;
+  return OR_OK;
+}
+
+int or_ecycle_device_bytes(or_ecycle* h, long long* bytes) {
+  if (!h || !bytes) return OR_E_ARG;
+  *bytes = h->dev_bytes;
+  return OR_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,1035 @@
+// ecycle_kernels.cuh -- sm_100a kernels of the explicit element cycle.
+//
+// Three kernels per cycle:
+//   hex_patch_kernel    SFORC3 chain for 8-node 1-point hexas (+ LAW1/LAW2)
+//   shell_patch_kernel  CFORC3 chain for BT shells (+ LAW1/LAW2 plane stress)
+//   node_kernel         ASSPAR4 + dt logic + ACCELE + BCS10 + VELOCITY + DEPLA
+//
+// Elements are grouped into patches of at most TILE elements (one CTA each).
+// A patch lists its unique nodes; the CTA stages their coordinates and
+// velocities in shared memory, each thread computes one element, and the
+// corner forces are reduced into shared-memory node accumulators colour by
+// colour (no two elements of a colour share a node), so the sum order is fixed
+// and no float atomics are used.  Each (patch, node) partial sum is written to
+// one slot of a node-major skyline; the node kernel adds a node's slots in
+// ascending patch order (the Parith/ON idea of asspar4.F:160-175 applied to
+// patch partials instead of element corners).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace orb {
+
+constexpr double EM15 = 1e-15, EM20 = 1e-20, EM30 = 1e-30;
+constexpr int MAX_COLORS = 32;
+constexpr int COLOR_SHIFT = 11;            // local node index < 2048, colour in bits 11..15
+constexpr unsigned LOCAL_MASK = (1u << COLOR_SHIFT) - 1u;
+
+template <class R> struct Vec4;
+template <> struct Vec4<float> { typedef float4 T; };
+template <> struct Vec4<double> { typedef double4 T; };
+
+__host__ __device__ inline float4 mk4(float a, float b, float c, float d) { return make_float4(a, b, c, d); }
+__host__ __device__ inline double4 mk4(double a, double b, double c, double d) { return make_double4(a, b, c, d); }
+
+// ---------------------------------------------------------------------------
+// descriptors (built on the host at finalize, read-only on the device)
+// ---------------------------------------------------------------------------
+struct PatchInfo {
+  int group;      // group index (hex or shell table)
+  int nel;        // elements in this patch (<= TILE)
+  int node_ofs;   // offset into patch_nodes / patch_slots
+  int nloc;       // unique local nodes
+  int ncolor;     // colours used
+  int elem0;      // first element (padded internal index) of this patch
+  int pad0, pad1;
+};
+
+struct HexGroupDesc {
+  int part, law, nel, pad;
+  double rho0, shear, bulk, jc_a, jc_b, jc_n, epsmax, sigmax;
+  double qa, qb, qh, dtfac, dtmin;
+};
+
+struct ShellGroupDesc {
+  int part, law, nel, npt;
+  int ithk, has_jca, pad0, pad1;
+  double rho0, young, nu, shear, a11, a12, ssp, jc_a, jc_b, jc_n, sigmax;
+  double hm, hf, hr, shf, pressure, dtfac, dtmin;
+};
+
+struct PartDesc {
+  int node_start, node_end;  // padded global node range
+  int tile_start, has_rot;
+};
+
+// time state of a part at the START of a cycle (double-buffered by parity)
+struct PartTime {
+  double tt, dt2, dt2old, dt1, dt12;
+  int ncycle, ityptst, neltst, pad;
+};
+
+// per-part reduction targets of one cycle
+struct PartAcc {
+  unsigned long long dtkey;   // (float(dt) bits << 32) | (type<<31 | element), min
+  unsigned long long dtbits;  // exact dt bits (double), min
+};
+
+struct ErrorWord {
+  int code;
+  int index;
+};
+
+template <class R>
+struct HexArgs {
+  const PatchInfo* patch;
+  const HexGroupDesc* groups;
+  const int* patch_nodes;
+  const int* patch_slots;
+  const uint4* conn;          // 8 x uint16 local corners per element (colour in corner 0)
+  const int* elem_id;         // element number within its part (for NELTS)
+  const double4* X;           // x, y, z, nodal mass
+  const typename Vec4<R>::T* V;
+  R* sig;                     // 6 x nelpad component-major
+  R* eint; R* rho; R* qvis; R* pla; R* epsd;
+  const R* vol0; const double* vol0dp;
+  typename Vec4<R>::T* fslot;
+  const PartTime* time;       // [parity][part]
+  PartAcc* acc;               // [parity][part]
+  double* blk_ehour;          // per patch cumulative hourglass energy
+  double* blk_wpla;           // per patch cumulative plastic work
+  ErrorWord* err;
+  int nelpad, nparts, npatch;
+};
+
+template <class R>
+struct ShellArgs {
+  const PatchInfo* patch;
+  const ShellGroupDesc* groups;
+  const int* patch_nodes;
+  const int* patch_slots;
+  const uint2* conn;          // 4 x uint16 local corners per element (colour in corner 0)
+  const int* elem_id;
+  const int* degen;           // 1 if IXC(4)==IXC(5) (triangle stored as quad)
+  const double4* X;
+  const typename Vec4<R>::T* V;
+  const typename Vec4<R>::T* VR;
+  R* sig;                     // npt x 5 x nelpad
+  R* pla;                     // npt x nelpad
+  R* thk; const R* thke; R* hourg; R* eint; const R* jca;
+  typename Vec4<R>::T* fslot;
+  typename Vec4<R>::T* mslot;
+  const PartTime* time;
+  PartAcc* acc;
+  double* blk_ehour;
+  double* blk_wpla;
+  ErrorWord* err;
+  int nelpad, nparts, npatch, maxnpt;
+};
+
+template <class R>
+struct NodeArgs {
+  const PartDesc* parts;
+  const int* tile_part;
+  const int* adsky;           // nnodpad + 1
+  const typename Vec4<R>::T* fslot;
+  const typename Vec4<R>::T* mslot;   // may be null
+  double4* X;
+  double* DX; double* DY; double* DZ;
+  typename Vec4<R>::T* V;
+  typename Vec4<R>::T* VR;    // w = rotational inertia; may be null
+  const unsigned char* code;  // bits 0-2 ICODT, 3-5 ICODR
+  PartTime* time;
+  PartAcc* acc;
+  double* blk_ekin;           // per node tile, overwritten each cycle
+  double* blk_ekinr;
+  ErrorWord* err;
+  double growth, dtmx;
+  int ntiles, nparts, split;
+};
+
+// ---------------------------------------------------------------------------
+// helpers
+// ---------------------------------------------------------------------------
+__device__ inline void raise_error(ErrorWord* e, int code, int index) {
+  if (atomicCAS(&e->code, 0, code) == 0) e->index = index;
+}
+
+__device__ inline unsigned long long dt_key(double dt, int type, int elem) {
+  float f = (float)dt;
+  unsigned long long hi = (unsigned long long)__float_as_uint(f);
+  unsigned lo = (type == 3 ? 0u : 0x80000000u) | (unsigned)elem;
+  return (hi << 32) | lo;
+}
+
+template <class R> __device__ inline R rsqrt_(R x);
+template <class R> __device__ inline R ssqrt(R x) { return sqrt(x); }
+__device__ inline float ssqrt(float x) { return sqrtf(x); }
+
+template <class R> __device__ inline R cbrt_(R x) { return cbrt(x); }
+__device__ inline float cbrt_(float x) { return cbrtf(x); }
+template <class R> __device__ inline R pow_(R x, R y) { return pow(x, y); }
+__device__ inline float pow_(float x, float y) { return powf(x, y); }
+template <class R> __device__ inline R exp_(R x) { return exp(x); }
+__device__ inline float exp_(float x) { return expf(x); }
+template <class R> __device__ inline R log_(R x) { return log(x); }
+__device__ inline float log_(float x) { return logf(x); }
+
+// block-wide min of a 64-bit key and sums of two doubles (TILE threads)
+template <int TILE>
+__device__ inline void block_reduce(unsigned long long& key, unsigned long long& bits, double& s0, double& s1,
+                                    unsigned long long* skey, unsigned long long* sbits, double* ss0, double* ss1) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    unsigned long long k2 = __shfl_xor_sync(0xffffffffu, key, o);
+    unsigned long long b2 = __shfl_xor_sync(0xffffffffu, bits, o);
+    key = k2 < key ? k2 : key;
+    bits = b2 < bits ? b2 : bits;
+    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+  }
+  if (lane == 0) { skey[warp] = key; sbits[warp] = bits; ss0[warp] = s0; ss1[warp] = s1; }
+  __syncthreads();
+  if (warp == 0) {
+    constexpr int NW = TILE / 32;
+    key = lane < NW ? skey[lane] : ~0ull;
+    bits = lane < NW ? sbits[lane] : ~0ull;
+    s0 = lane < NW ? ss0[lane] : 0.0;
+    s1 = lane < NW ? ss1[lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      unsigned long long k2 = __shfl_xor_sync(0xffffffffu, key, o);
+      unsigned long long b2 = __shfl_xor_sync(0xffffffffu, bits, o);
+      key = k2 < key ? k2 : key;
+      bits = b2 < bits ? b2 : bits;
+      s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+      s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    }
+  }
+}
+
+// ===========================================================================
+// hexa patch kernel
+// ===========================================================================
+// Per element (thread): SCOOR3, SDERI3, SDLEN3, SDEFO3, SRHO3, SROTA3, MMAIN ->
+// M1LAW / M2LAW -> MQVISCB, SHVIS3, SFINT3; corner forces into shared memory.
+template <class R, int TILE>
+__global__ void __launch_bounds__(TILE)
+hex_patch_kernel(HexArgs<R> a, int parity) {
+  typedef typename Vec4<R>::T R4;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ unsigned long long s_key[TILE / 32], s_bits[TILE / 32];
+  __shared__ double s_s0[TILE / 32], s_s1[TILE / 32];
+  const int p = blockIdx.x;
+  const int tid = threadIdx.x;
+  const PatchInfo pi = a.patch[p];
+  const HexGroupDesc gd = a.groups[pi.group];
+  const int nl = pi.nloc;
+  // shared layout: x, y, z (double) | vx, vy, vz, fx, fy, fz (R)
+  double* sx = reinterpret_cast<double*>(smem_raw);
+  double* sy = sx + nl;
+  double* sz = sy + nl;
+  R* svx = reinterpret_cast<R*>(sz + nl);
+  R* svy = svx + nl;
+  R* svz = svy + nl;
+  R* sfx = svz + nl;
+  R* sfy = sfx + nl;
+  R* sfz = sfy + nl;
+  for (int j = tid; j < nl; j += TILE) {
+    const int g = a.patch_nodes[pi.node_ofs + j];
+    const double4 xx = a.X[g];
+    const R4 vv = a.V[g];
+    sx[j] = xx.x; sy[j] = xx.y; sz[j] = xx.z;
+    svx[j] = vv.x; svy[j] = vv.y; svz[j] = vv.z;
+    sfx[j] = R(0); sfy[j] = R(0); sfz[j] = R(0);
+  }
+  const PartTime& tm = a.time[parity * a.nparts + gd.part];
+  const R DT1 = R(tm.dt2);
+  const bool split = sizeof(R) == 4;
+  __syncthreads();
+
+  const bool active = tid < pi.nel;
+  const int e = pi.elem0 + tid;
+  const int nelpad = a.nelpad;
+  R F[3][8];
+  int lc[8];
+  int color = -1;
+  unsigned long long mykey = ~0ull, mybits = ~0ull;
+  double my_ehou = 0.0, my_wpla = 0.0;
+  if (active) {
+    const uint4 cw = a.conn[e];
+    lc[0] = cw.x & 0xffffu; lc[1] = cw.x >> 16; lc[2] = cw.y & 0xffffu; lc[3] = cw.y >> 16;
+    lc[4] = cw.z & 0xffffu; lc[5] = cw.z >> 16; lc[6] = cw.w & 0xffffu; lc[7] = cw.w >> 16;
+    color = lc[0] >> COLOR_SHIFT;
+    lc[0] &= LOCAL_MASK;
+    // ---- SDERI3 in FP64 (sderi3.F:103-149, 264-298) ----
+    double XD[8], YD[8], ZD[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) { XD[k] = sx[lc[k]]; YD[k] = sy[lc[k]]; ZD[k] = sz[lc[k]]; }
+    const double X17 = XD[6] - XD[0], X28 = XD[7] - XD[1], X35 = XD[4] - XD[2], X46 = XD[5] - XD[3];
+    const double Y17 = YD[6] - YD[0], Y28 = YD[7] - YD[1], Y35 = YD[4] - YD[2], Y46 = YD[5] - YD[3];
+    const double Z17 = ZD[6] - ZD[0], Z28 = ZD[7] - ZD[1], Z35 = ZD[4] - ZD[2], Z46 = ZD[5] - ZD[3];
+    const double J1 = X17 + X28 - X35 - X46, J2 = Y17 + Y28 - Y35 - Y46, J3 = Z17 + Z28 - Z35 - Z46;
+    const double xa = X17 + X46, xb = X28 + X35, ya = Y17 + Y46, yb = Y28 + Y35, za = Z17 + Z46, zb = Z28 + Z35;
+    const double J4 = xa + xb, J5 = ya + yb, J6 = za + zb, J7 = xa - xb, J8 = ya - yb, J9 = za - zb;
+    const double C1 = J5 * J9 - J6 * J8, C4 = J6 * J7 - J4 * J9, C7 = J4 * J8 - J5 * J7;
+    double det = (1.0 / 64.0) * (J1 * C1 + J2 * C4 + J3 * C7);
+    if (!(det > 0.0)) {   // SCHKJABT3: zero or negative volume stops the run
+      raise_error(a.err, 4, a.elem_id[e]);
+      det = 1.0;
+    }
+    const double dett = (1.0 / 64.0) / det;
+    const double I1 = dett * C1, I4 = dett * C4, I7 = dett * C7;
+    const double I2 = dett * (J3 * J8 - J2 * J9), I5 = dett * (J1 * J9 - J3 * J7), I8 = dett * (J2 * J7 - J1 * J8);
+    const double I3 = dett * (J2 * J6 - J3 * J5), I6 = dett * (J3 * J4 - J1 * J6), I9 = dett * (J1 * J5 - J2 * J4);
+    R PX[4], PY[4], PZ[4];
+    {
+      const double a12 = I1 + I2, a45 = I4 + I5, a78 = I7 + I8;
+      const double b12 = I1 - I2, b45 = I4 - I5, b78 = I7 - I8;
+      PX[0] = R(-a12 - I3); PY[0] = R(-a45 - I6); PZ[0] = R(-a78 - I9);
+      PX[1] = R(-a12 + I3); PY[1] = R(-a45 + I6); PZ[1] = R(-a78 + I9);
+      PX[2] = R(b12 + I3);  PY[2] = R(b45 + I6);  PZ[2] = R(b78 + I9);
+      PX[3] = R(b12 - I3);  PY[3] = R(b45 - I6);  PZ[3] = R(b78 - I9);
+    }
+    // hourglass projections PXiHj (sderi3.F:302-333): modes (+-+-+-+-), (++----++), (+--+-++-)
+    R PXH[4][3];
+    {
+      const double hx1 = XD[0] - XD[1] + XD[2] - XD[3] + XD[4] - XD[5] + XD[6] - XD[7];
+      const double hy1 = YD[0] - YD[1] + YD[2] - YD[3] + YD[4] - YD[5] + YD[6] - YD[7];
+      const double hz1 = ZD[0] - ZD[1] + ZD[2] - ZD[3] + ZD[4] - ZD[5] + ZD[6] - ZD[7];
+      const double hx2 = XD[0] + XD[1] - XD[2] - XD[3] - XD[4] - XD[5] + XD[6] + XD[7];
+      const double hy2 = YD[0] + YD[1] - YD[2] - YD[3] - YD[4] - YD[5] + YD[6] + YD[7];
+      const double hz2 = ZD[0] + ZD[1] - ZD[2] - ZD[3] - ZD[4] - ZD[5] + ZD[6] + ZD[7];
+      const double hx3 = XD[0] - XD[1] - XD[2] + XD[3] - XD[4] + XD[5] + XD[6] - XD[7];
+      const double hy3 = YD[0] - YD[1] - YD[2] + YD[3] - YD[4] + YD[5] + YD[6] - YD[7];
+      const double hz3 = ZD[0] - ZD[1] - ZD[2] + ZD[3] - ZD[4] + ZD[5] + ZD[6] - ZD[7];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        PXH[q][0] = PX[q] * R(hx1) + PY[q] * R(hy1) + PZ[q] * R(hz1);
+        PXH[q][1] = PX[q] * R(hx2) + PY[q] * R(hy2) + PZ[q] * R(hz2);
+        PXH[q][2] = PX[q] * R(hx3) + PY[q] * R(hy3) + PZ[q] * R(hz3);
+      }
+    }
+    const double VOLN_D = det;
+    const R VOLN = R(det);
+    // ---- SDLEN3 / SLEN (sdlen3.F:110-166): 4 V / sqrt(max face (E G - F^2)) ----
+    R AREAM = R(EM20);
+    {
+      const int FC[6][4] = {{0, 1, 2, 3}, {4, 5, 6, 7}, {0, 1, 5, 4}, {1, 2, 6, 5}, {2, 3, 7, 6}, {3, 0, 4, 7}};
+#pragma unroll
+      for (int f = 0; f < 6; ++f) {
+        const R x13 = R(XD[FC[f][2]] - XD[FC[f][0]]), x24 = R(XD[FC[f][3]] - XD[FC[f][1]]);
+        const R y13 = R(YD[FC[f][2]] - YD[FC[f][0]]), y24 = R(YD[FC[f][3]] - YD[FC[f][1]]);
+        const R z13 = R(ZD[FC[f][2]] - ZD[FC[f][0]]), z24 = R(ZD[FC[f][3]] - ZD[FC[f][1]]);
+        const R s1 = x13 - x24, t1 = x13 + x24, s2 = y13 - y24, t2 = y13 + y24, s3 = z13 - z24, t3 = z13 + z24;
+        const R E = s1 * s1 + s2 * s2 + s3 * s3, Fm = s1 * t1 + s2 * t2 + s3 * t3, G = t1 * t1 + t2 * t2 + t3 * t3;
+        const R ar = E * G - Fm * Fm;
+        AREAM = ar > AREAM ? ar : AREAM;
+      }
+    }
+    const R DELTAX = R(4) * VOLN / ssqrt(AREAM);
+    // ---- SDEFO3 (sdefo3.F:114-170, JHBE=1) ----
+    R VX[8], VY[8], VZ[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) { VX[k] = svx[lc[k]]; VY[k] = svy[lc[k]]; VZ[k] = svz[lc[k]]; }
+    const R vx17 = VX[0] - VX[6], vx28 = VX[1] - VX[7], vx35 = VX[2] - VX[4], vx46 = VX[3] - VX[5];
+    const R vy17 = VY[0] - VY[6], vy28 = VY[1] - VY[7], vy35 = VY[2] - VY[4], vy46 = VY[3] - VY[5];
+    const R vz17 = VZ[0] - VZ[6], vz28 = VZ[1] - VZ[7], vz35 = VZ[2] - VZ[4], vz46 = VZ[3] - VZ[5];
+    const R DXX = PX[0] * vx17 + PX[1] * vx28 + PX[2] * vx35 + PX[3] * vx46;
+    const R DYY = PY[0] * vy17 + PY[1] * vy28 + PY[2] * vy35 + PY[3] * vy46;
+    const R DZZ = PZ[0] * vz17 + PZ[1] * vz28 + PZ[2] * vz35 + PZ[3] * vz46;
+    const R DXY = PY[0] * vx17 + PY[1] * vx28 + PY[2] * vx35 + PY[3] * vx46;
+    const R DXZ = PZ[0] * vx17 + PZ[1] * vx28 + PZ[2] * vx35 + PZ[3] * vx46;
+    const R DYX = PX[0] * vy17 + PX[1] * vy28 + PX[2] * vy35 + PX[3] * vy46;
+    const R DYZ = PZ[0] * vy17 + PZ[1] * vy28 + PZ[2] * vy35 + PZ[3] * vy46;
+    const R DZX = PX[0] * vz17 + PX[1] * vz28 + PX[2] * vz35 + PX[3] * vz46;
+    const R DZY = PY[0] * vz17 + PY[1] * vz28 + PY[2] * vz35 + PY[3] * vz46;
+    const R DT1D2 = R(0.5) * DT1;
+    const R D4 = DXY + DYX, D5 = DYZ + DZY, D6 = DXZ + DZX;
+    const R WZZ = DT1D2 * (DYX - DXY), WYY = DT1D2 * (DXZ - DZX), WXX = DT1D2 * (DZY - DYZ);
+    // ---- SRHO3 (srho3.F:122-156; FP64 volume ratios in the split form, srho3.F:230-245) ----
+    const R RHO0 = R(gd.rho0);
+    const R rho_old = a.rho[e];
+    const R VOLO = a.vol0[e];
+    R DVOL, RHON, AMU;
+    if (split) {
+      const double v0 = a.vol0dp[e];
+      DVOL = R(VOLN_D - ((double)RHO0 / (double)rho_old) * v0);
+      RHON = R((double)RHO0 * (v0 / VOLN_D));
+      AMU = R(v0 / VOLN_D - 1.0);
+    } else {
+      DVOL = VOLN - (RHO0 / rho_old) * VOLO;
+      RHON = RHO0 * (VOLO / VOLN);
+      AMU = RHON / RHO0 - R(1);
+    }
+    R EINT = a.eint[e] * VOLO;
+    // ---- SROTA3 Jaumann rotation (srota3.F:81-91) ----
+    const R S1 = a.sig[0 * nelpad + e], S2 = a.sig[1 * nelpad + e], S3 = a.sig[2 * nelpad + e];
+    const R S4 = a.sig[3 * nelpad + e], S5 = a.sig[4 * nelpad + e], S6 = a.sig[5 * nelpad + e];
+    R SG[6];
+    {
+      const R q1 = R(2) * S4 * WZZ, q2 = R(2) * S6 * WYY, q3 = R(2) * S5 * WXX;
+      SG[0] = S1 - q1 + q2;
+      SG[1] = S2 + q1 - q3;
+      SG[2] = S3 - q2 + q3;
+      SG[3] = S4 + WZZ * (S1 - S2) + WYY * S5 - WXX * S6;
+      SG[4] = S5 + WXX * (S2 - S3) + WZZ * S6 - WYY * S4;
+      SG[5] = S6 + WYY * (S3 - S1) + WXX * S4 - WZZ * S5;
+    }
+    const R VOL_AVG = VOLN - R(0.5) * DVOL;
+    const R QOLD = a.qvis[e];
+    // ---- elastic predictor (m1law.F:124-140 / m2law.F:187-200) ----
+    const R OFF = R(1);
+    const R Gs = R(gd.shear) * OFF;
+    const R G1 = DT1 * Gs, G2 = R(2) * G1;
+    const R SSP = ssqrt((R(1.333) * Gs + R(gd.bulk)) / RHO0);
+    {
+      const R P = -R(1.0 / 3.0) * (SG[0] + SG[1] + SG[2]);
+      const R DAV = -R(1.0 / 3.0) * (DXX + DYY + DZZ);
+      SG[0] = SG[0] + P + G2 * (DXX + DAV);
+      SG[1] = SG[1] + P + G2 * (DYY + DAV);
+      SG[2] = SG[2] + P + G2 * (DZZ + DAV);
+      SG[3] = SG[3] + G1 * D4;
+      SG[4] = SG[4] + G1 * D5;
+      SG[5] = SG[5] + G1 * D6;
+    }
+    R DPLA = R(0), SIGY = R(0);
+    if (gd.law == 2) {
+      // ---- M2LAW radial return (m2law.F:197-352), CC=0, FISOKIN=0 ----
+      R AJ2 = R(0.5) * (SG[0] * SG[0] + SG[1] * SG[1] + SG[2] * SG[2]) + SG[3] * SG[3] + SG[4] * SG[4] + SG[5] * SG[5];
+      AJ2 = ssqrt(R(3) * AJ2);
+      {   // MSTRAIN_RATE, ISRATE = 0, total strain rate
+        const R e4 = R(0.5) * D4, e5 = R(0.5) * D5, e6 = R(0.5) * D6;
+        a.epsd[e] = ssqrt(DXX * DXX + DYY * DYY + DZZ * DZZ + R(2) * (e4 * e4 + e5 * e5 + e6 * e6));
+      }
+      const R CA = R(gd.jc_a), CB = R(gd.jc_b), CN = R(gd.jc_n);
+      R EPXE = a.pla[e];
+      R AK, QH;
+      if (CN == R(1)) { AK = CA + CB * EPXE; QH = CB; }
+      else if (EPXE > R(0)) {
+        AK = CA + CB * pow_(EPXE, CN);
+        QH = (CN > R(1)) ? CB * CN * pow_(EPXE, CN - R(1)) : CB * CN / pow_(EPXE, R(1) - CN);
+      } else { AK = CA; QH = R(0); }
+      if (R(gd.sigmax) < AK) { AK = R(gd.sigmax); QH = R(0); }
+      SIGY = AK;
+      if (EPXE > R(gd.epsmax)) { AK = R(0); QH = R(0); }
+      R SCALE = AK / (AJ2 > R(EM15) ? AJ2 : R(EM15));
+      SCALE = SCALE < R(1) ? SCALE : R(1);
+      const R den = R(3) * Gs + QH;
+      DPLA = (R(1) - SCALE) * AJ2 / (den > R(EM15) ? den : R(EM15));
+      AK = AK + DPLA * QH;
+      SCALE = AK / (AJ2 > R(EM15) ? AJ2 : R(EM15));
+      SCALE = SCALE < R(1) ? SCALE : R(1);
+#pragma unroll
+      for (int c = 0; c < 6; ++c) SG[c] = SCALE * SG[c];
+      a.pla[e] = EPXE + DPLA;
+      SIGY = SIGY > AK ? SIGY : AK;
+    }
+    // ---- MQVISCB (mqviscb.F:139-354) ----
+    R QNEW;
+    const R AL = VOLN > R(0) ? cbrt_(VOLN) : R(0);
+    {
+      const R DD = -DXX - DYY - DZZ;
+      const R AD = DD > R(0) ? DD : R(0);
+      const R QA = R(gd.qa), QB = R(gd.qb);
+      const R QAA = QA * QA * AD;
+      const R QX = QB * SSP + AL * QAA;
+      QNEW = RHON * AD * AL * (QAA * AL + QB * SSP);
+      R SSP_EQ = QX + ssqrt(QX * QX + SSP * SSP);
+      SSP_EQ = SSP_EQ > R(EM20) ? SSP_EQ : R(EM20);
+      const R DTX = R(gd.dtfac) * (DELTAX / SSP_EQ);
+      if ((double)DTX <= gd.dtmin) raise_error(a.err, 5, a.elem_id[e]);
+      const double dtd = (double)DTX;
+      mykey = dt_key(dtd, 1, a.elem_id[e]);
+      mybits = (unsigned long long)__double_as_longlong(dtd);
+    }
+    // ---- pressure and internal energy (m1law.F:172-190 / m2law.F:434-461) ----
+    const R PNEW = R(gd.bulk) * AMU;
+    SG[0] = (SG[0] - PNEW) * OFF; SG[1] = (SG[1] - PNEW) * OFF; SG[2] = (SG[2] - PNEW) * OFF;
+    SG[3] = SG[3] * OFF; SG[4] = SG[4] * OFF; SG[5] = SG[5] * OFF;
+    const R DTA = R(0.5) * DT1;
+    R EINC;
+    if (gd.law == 1) {
+      const R P2 = -(S1 + SG[0] + S2 + SG[1] + S3 + SG[2]) * R(1.0 / 3.0);
+      EINC = VOL_AVG * (DXX * (S1 + SG[0] + P2) + DYY * (S2 + SG[1] + P2) + DZZ * (S3 + SG[2] + P2) +
+                        D4 * (S4 + SG[3]) + D5 * (S5 + SG[4]) + D6 * (S6 + SG[5])) * DTA -
+             R(0.5) * DVOL * (QOLD + QNEW + P2);
+    } else {
+      EINC = VOL_AVG * (DXX * (S1 + SG[0]) + DYY * (S2 + SG[1]) + DZZ * (S3 + SG[2]) +
+                        D4 * (S4 + SG[3]) + D5 * (S5 + SG[4]) + D6 * (S6 + SG[5])) * DTA -
+             R(0.5) * DVOL * (QOLD + QNEW);
+      my_wpla = (double)SIGY * (double)DPLA * (double)VOLN;
+    }
+    const R vdiv = VOLO > R(EM15) ? VOLO : R(EM15);
+    EINT = (EINT + EINC * OFF) / vdiv;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) a.sig[c * nelpad + e] = SG[c];
+    a.eint[e] = EINT;
+    a.rho[e] = RHON;
+    a.qvis[e] = QNEW;
+    // ---- SHVIS3 Flanagan-Belytschko viscous hourglass (shvis3.F:156-424, JHBE>=1) ----
+    {
+      const R CAQ = R(0.25) * OFF * R(gd.qh);
+      R FCL = CAQ * RHON * (AL * AL);   // VOL**TWO_THIRD
+      const R FCQ = FCL * CAQ * R(100);
+      FCL = FCL * SSP;
+      // g-vectors of the three non-trivial modes; the 4th mode is the pure (+-+--+-+) vector
+      R Gv[3][8];
+      const int sgn[3][8] = {{1, -1, 1, -1, 1, -1, 1, -1}, {1, 1, -1, -1, -1, -1, 1, 1}, {1, -1, -1, 1, -1, 1, 1, -1}};
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        Gv[j][0] = R(sgn[j][0]) - PXH[0][j];
+        Gv[j][1] = R(sgn[j][1]) - PXH[1][j];
+        Gv[j][2] = R(sgn[j][2]) - PXH[2][j];
+        Gv[j][3] = R(sgn[j][3]) - PXH[3][j];
+        Gv[j][4] = R(sgn[j][4]) + PXH[2][j];
+        Gv[j][5] = R(sgn[j][5]) + PXH[3][j];
+        Gv[j][6] = R(sgn[j][6]) + PXH[0][j];
+        Gv[j][7] = R(sgn[j][7]) + PXH[1][j];
+      }
+      const int h4[8] = {1, -1, 1, -1, -1, 1, -1, 1};
+      R HGX[4], HGY[4], HGZ[4];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        R hx = R(0), hy = R(0), hz = R(0);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) { hx += Gv[j][k] * VX[k]; hy += Gv[j][k] * VY[k]; hz += Gv[j][k] * VZ[k]; }
+        HGX[j] = hx; HGY[j] = hy; HGZ[j] = hz;
+      }
+      HGX[3] = VX[0] - VX[1] + VX[2] - VX[3] - VX[4] + VX[5] - VX[6] + VX[7];
+      HGY[3] = VY[0] - VY[1] + VY[2] - VY[3] - VY[4] + VY[5] - VY[6] + VY[7];
+      HGZ[3] = VZ[0] - VZ[1] + VZ[2] - VZ[3] - VZ[4] + VZ[5] - VZ[6] + VZ[7];
+      R HX[4], HY[4], HZ[4];
+      R ehou = R(0);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        HX[j] = HGX[j] * (FCL + fabs(HGX[j]) * FCQ);
+        HY[j] = HGY[j] * (FCL + fabs(HGY[j]) * FCQ);
+        HZ[j] = HGZ[j] * (FCL + fabs(HGZ[j]) * FCQ);
+        ehou += HX[j] * HGX[j] + HY[j] * HGY[j] + HZ[j] * HGZ[j];
+      }
+      my_ehou = (double)(DT1 * ehou);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        F[0][k] = -Gv[0][k] * HX[0] - Gv[1][k] * HX[1] - Gv[2][k] * HX[2] - R(h4[k]) * HX[3];
+        F[1][k] = -Gv[0][k] * HY[0] - Gv[1][k] * HY[1] - Gv[2][k] * HY[2] - R(h4[k]) * HY[3];
+        F[2][k] = -Gv[0][k] * HZ[0] - Gv[1][k] * HZ[1] - Gv[2][k] * HZ[2] - R(h4[k]) * HZ[3];
+      }
+    }
+    // ---- SFINT3 (sfint3.F:256-321), antisymmetric pairs 1-7, 2-8, 3-5, 4-6 ----
+    {
+      const R s1 = (SG[0] - QNEW) * VOLN, s2 = (SG[1] - QNEW) * VOLN, s3 = (SG[2] - QNEW) * VOLN;
+      const R s4 = SG[3] * VOLN, s5 = SG[4] * VOLN, s6 = SG[5] * VOLN;
+      const int n1[4] = {0, 1, 2, 3}, n2[4] = {6, 7, 4, 5};
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        R f = s1 * PX[q] + s4 * PY[q] + s6 * PZ[q];
+        F[0][n1[q]] -= f; F[0][n2[q]] += f;
+        f = s2 * PY[q] + s4 * PX[q] + s5 * PZ[q];
+        F[1][n1[q]] -= f; F[1][n2[q]] += f;
+        f = s3 * PZ[q] + s6 * PX[q] + s5 * PY[q];
+        F[2][n1[q]] -= f; F[2][n2[q]] += f;
+      }
+    }
+  }
+  // ---- colour-ordered shared-memory assembly ----
+  for (int c = 0; c < pi.ncolor; ++c) {
+    if (color == c) {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const int l = lc[k];
+        sfx[l] += F[0][k]; sfy[l] += F[1][k]; sfz[l] += F[2][k];
+      }
+    }
+    __syncthreads();
+  }
+  for (int j = tid; j < nl; j += TILE) {
+    const int s = a.patch_slots[pi.node_ofs + j];
+    a.fslot[s] = mk4(sfx[j], sfy[j], sfz[j], R(0));
+  }
+  // ---- dt min-reduction and energy partials ----
+  block_reduce<TILE>(mykey, mybits, my_ehou, my_wpla, s_key, s_bits, s_s0, s_s1);
+  if (tid == 0) {
+    PartAcc* acc = &a.acc[parity * a.nparts + gd.part];
+    atomicMin(&acc->dtkey, mykey);
+    atomicMin(&acc->dtbits, mybits);
+    a.blk_ehour[p] += my_ehou;
+    a.blk_wpla[p] += my_wpla;
+  }
+}
+
+
+// ===========================================================================
+// shell patch kernel
+// ===========================================================================
+// Per element (thread): CCOOR3, CNVEC3, CDERI3, CCOEF3, CDLEN3, CDEFO3, CCURV3,
+// CSTRA3, MULAWC (SIGEPS01C / SIGEPS02C -> M2CPLR per integration point),
+// CHVIS3, CDT3, CFINT3; forces and moments into shared memory (CUPDT3P signs).
+template <class R, int TILE>
+__global__ void __launch_bounds__(TILE)
+shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
+  typedef typename Vec4<R>::T R4;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ unsigned long long s_key[TILE / 32], s_bits[TILE / 32];
+  __shared__ double s_s0[TILE / 32], s_s1[TILE / 32];
+  const int p = blockIdx.x;
+  const int tid = threadIdx.x;
+  const PatchInfo pi = a.patch[p];
+  const ShellGroupDesc gd = a.groups[pi.group];
+  const int nl = pi.nloc;
+  double* sx = reinterpret_cast<double*>(smem_raw);
+  double* sy = sx + nl;
+  double* sz = sy + nl;
+  R* sv = reinterpret_cast<R*>(sz + nl);   // vx vy vz rx ry rz fx fy fz mx my mz: 12 planes
+  for (int j = tid; j < nl; j += TILE) {
+    const int g = a.patch_nodes[pi.node_ofs + j];
+    const double4 xx = a.X[g];
+    const R4 vv = a.V[g];
+    const R4 rr = a.VR[g];
+    sx[j] = xx.x; sy[j] = xx.y; sz[j] = xx.z;
+    sv[0 * nl + j] = vv.x; sv[1 * nl + j] = vv.y; sv[2 * nl + j] = vv.z;
+    sv[3 * nl + j] = rr.x; sv[4 * nl + j] = rr.y; sv[5 * nl + j] = rr.z;
+#pragma unroll
+    for (int q = 6; q < 12; ++q) sv[q * nl + j] = R(0);
+  }
+  const PartTime& tm = a.time[parity * a.nparts + gd.part];
+  const R DT1 = R(tm.dt2);
+  __syncthreads();
+
+  const bool active = tid < pi.nel;
+  const int e = pi.elem0 + tid;
+  const int nelpad = a.nelpad;
+  int lc[4];
+  int color = -1;
+  R Fg[3][4], Mg[3][4];
+  unsigned long long mykey = ~0ull, mybits = ~0ull;
+  double my_ehou = 0.0, my_wpla = 0.0;
+  if (active) {
+    const uint2 cw = a.conn[e];
+    lc[0] = cw.x & 0xffffu; lc[1] = cw.x >> 16; lc[2] = cw.y & 0xffffu; lc[3] = cw.y >> 16;
+    color = lc[0] >> COLOR_SHIFT;
+    lc[0] &= LOCAL_MASK;
+    const R OFF = R(1);
+    // coordinate differences in FP64, cast to R (CNVEC3 / CDERI3 inputs)
+    const double x1 = sx[lc[0]], y1 = sy[lc[0]], z1 = sz[lc[0]];
+    const R X21 = R(sx[lc[1]] - x1), Y21 = R(sy[lc[1]] - y1), Z21 = R(sz[lc[1]] - z1);
+    const R X31 = R(sx[lc[2]] - x1), Y31 = R(sy[lc[2]] - y1), Z31 = R(sz[lc[2]] - z1);
+    const R X41 = R(sx[lc[3]] - x1), Y41 = R(sy[lc[3]] - y1), Z41 = R(sz[lc[3]] - z1);
+    const R X32 = R(sx[lc[2]] - sx[lc[1]]), Y32 = R(sy[lc[2]] - sy[lc[1]]), Z32 = R(sz[lc[2]] - sz[lc[1]]);
+    const R X34 = R(sx[lc[2]] - sx[lc[3]]), Y34 = R(sy[lc[2]] - sy[lc[3]]), Z34 = R(sz[lc[2]] - sz[lc[3]]);
+    // ---- CNVEC3, ISHFRAM = 0 (cnvec3.F:66-140) ----
+    R E1X = X21 + X34, E1Y = Y21 + Y34, E1Z = Z21 + Z34;
+    R E2X = X32 + X41, E2Y = Y32 + Y41, E2Z = Z32 + Z41;
+    R E3X = E1Y * E2Z - E1Z * E2Y, E3Y = E1Z * E2X - E1X * E2Z, E3Z = E1X * E2Y - E1Y * E2X;
+    {
+      R su = E3X * E3X + E3Y * E3Y + E3Z * E3Z;
+      su = ssqrt(su);
+      su = R(1) / (su > R(EM20) ? su : R(EM20));
+      E3X *= su; E3Y *= su; E3Z *= su;
+      const R q1 = E1X * E1X + E1Y * E1Y + E1Z * E1Z;
+      const R q2 = E2X * E2X + E2Y * E2Y + E2Z * E2Z;
+      su = ssqrt(q1 / q2);
+      E1X = E1X + (E2Y * E3Z - E2Z * E3Y) * su;
+      E1Y = E1Y + (E2Z * E3X - E2X * E3Z) * su;
+      E1Z = E1Z + (E2X * E3Y - E2Y * E3X) * su;
+      su = ssqrt(E1X * E1X + E1Y * E1Y + E1Z * E1Z);
+      su = R(1) / (su > R(EM20) ? su : R(EM20));
+      E1X *= su; E1Y *= su; E1Z *= su;
+      E2X = E3Y * E1Z - E3Z * E1Y; E2Y = E3Z * E1X - E3X * E1Z; E2Z = E3X * E1Y - E3Y * E1X;
+    }
+    // ---- CDERI3 (cderi3.F:87-190) ----
+    const R X2 = E1X * X21 + E1Y * Y21 + E1Z * Z21;
+    const R Y2 = E2X * X21 + E2Y * Y21 + E2Z * Z21;
+    const R Y3 = E2X * X31 + E2Y * Y31 + E2Z * Z31;
+    const R X3 = E1X * X31 + E1Y * Y31 + E1Z * Z31;
+    const R X4 = E1X * X41 + E1Y * Y41 + E1Z * Z41;
+    const R Y4 = E2X * X41 + E2Y * Y41 + E2Z * Z41;
+    const R PX1 = R(0.5) * (Y2 - Y4), PY1 = R(0.5) * (X4 - X2), PX2 = R(0.5) * Y3, PY2 = -R(0.5) * X3;
+    R AREA = R(2) * (PY2 * PX1 - PY1 * PX2);
+    AREA = AREA > R(EM20) ? AREA : R(EM20);
+    const R VHX = (-X2 + X3 - X4) / AREA, VHY = (-Y2 + Y3 - Y4) / AREA;
+    // ---- CCOEF3 (ccoef3.F:66-160) ----
+    const R THK0 = gd.ithk > 0 ? a.thk[e] : a.thke[e];
+    const R VOL0 = THK0 * AREA;
+    const R THK02 = THK0 * THK0;
+    const R RHO = R(gd.rho0), YM = R(gd.young), NU = R(gd.nu), GG = R(gd.shear);
+    const R A11 = R(gd.a11), A12 = R(gd.a12), SSP = R(gd.ssp);
+    const R H1 = R(gd.hm), H2 = R(gd.hf), H3 = R(gd.hr);
+    const int npt = gd.npt;
+    const R SHF = npt == 1 ? R(0) : R(gd.shf);
+    const R GS = GG * SHF;
+    // ---- CDLEN3 (cdlen3.F:69-121) ----
+    R ALDT;
+    {
+      const R AL1 = X2 * X2 + Y2 * Y2;
+      const R AL2 = (X3 - X2) * (X3 - X2) + (Y3 - Y2) * (Y3 - Y2);
+      const R AL6 = X3 * X3 + Y3 * Y3;
+      const R AL3 = (X4 - X3) * (X4 - X3) + (Y4 - Y3) * (Y4 - Y3);
+      const R AL4 = X4 * X4 + Y4 * Y4;
+      const R AL5 = (X4 - X2) * (X4 - X2) + (Y4 - Y2) * (Y4 - Y2);
+      R ALMIN = fmin(fmin(AL1, AL2), AL4);
+      const R ALQ = fmin(fmin(AL3, AL5), AL6);
+      if (AL3 != R(0)) ALMIN = fmin(ALMIN, ALQ);
+      R m56 = fmax(AL5, AL6);
+      m56 = m56 > R(EM20) ? m56 : R(EM20);
+      const R DTDYN = AREA * AREA / m56;
+      ALDT = fmax(DTDYN, ALMIN);
+      const R DTHOUR = R(0.5) * (ALMIN + ALDT) / fmax(H1, H2);
+      if (DTHOUR < ALDT) ALDT = DTHOUR;
+      ALDT = ssqrt(ALDT);
+    }
+    // ---- CDEFO3, IHBE <= 1 (cdefo3.F:84-131) ----
+    R VXl[4], VYl[4], VZl[4], RXl[4], RYl[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const R vx = sv[0 * nl + lc[k]], vy = sv[1 * nl + lc[k]], vz = sv[2 * nl + lc[k]];
+      VXl[k] = E1X * vx + E1Y * vy + E1Z * vz;
+      VYl[k] = E2X * vx + E2Y * vy + E2Z * vz;
+      VZl[k] = E3X * vx + E3Y * vy + E3Z * vz;
+      const R rx = sv[3 * nl + lc[k]], ry = sv[4 * nl + lc[k]], rz = sv[5 * nl + lc[k]];
+      RXl[k] = E1X * rx + E1Y * ry + E1Z * rz;
+      RYl[k] = E2X * rx + E2Y * ry + E2Z * rz;
+    }
+    R EXX, EYY, EXY, EXZ, EYZ, KXX, KYY, KXY;
+    {
+      const R VZ13 = VZl[0] - VZl[2], VZ24 = VZl[1] - VZl[3];
+      EYZ = PY1 * VZ13 + PY2 * VZ24;
+      EXZ = PX1 * VZ13 + PX2 * VZ24;
+      const R DT1V4 = R(0.25) * DT1;
+      const R t2a = PY2 + PY1;
+      const R t3a = copysign(fmax(fabs(t2a), R(EM20)), t2a);
+      const R t1a = DT1V4 * (VZ13 - VZ24) * (VZ13 - VZ24) / t3a;
+      const R VX13 = VXl[0] - VXl[2] - t1a, VX24 = VXl[1] - VXl[3] + t1a;
+      EXX = PX1 * VX13 + PX2 * VX24;
+      EXY = PY1 * VX13 + PY2 * VX24;
+      const R t1b = PX2 - PX1;
+      const R t3b = copysign(fmax(fabs(t1b), R(EM20)), t1b);
+      const R t2b = DT1V4 * (VZ13 + VZ24) * (VZ13 + VZ24) / t3b;
+      const R VY13 = VYl[0] - VYl[2] + t2b, VY24 = VYl[1] - VYl[3] + t2b;
+      EXY = EXY + PX1 * VY13 + PX2 * VY24;
+      EYY = PY1 * VY13 + PY2 * VY24;
+      // ---- CCURV3 (ccurv3.F:61-86) ----
+      const R RX13 = RXl[0] - RXl[2], RXAV = RXl[0] + RXl[1] + RXl[2] + RXl[3], RX24 = RXl[1] - RXl[3];
+      KYY = -PY1 * RX13 - PY2 * RX24;
+      R kxy = PX1 * RX13 + PX2 * RX24;
+      const R RY13 = RYl[0] - RYl[2], RYAV = RYl[0] + RYl[1] + RYl[2] + RYl[3], RY24 = RYl[1] - RYl[3];
+      KXX = PX1 * RY13 + PX2 * RY24;
+      KXY = PY1 * RY13 + PY2 * RY24 - kxy;
+      EXZ = EXZ + RYAV * (R(0.25) * AREA);
+      EYZ = EYZ - RXAV * (R(0.25) * AREA);
+      // ---- CSTRA3 (cstra3.F:91-101) ----
+      const R FAC1 = DT1 / AREA;
+      EXX *= FAC1; EYY *= FAC1; EXY *= FAC1; EYZ *= FAC1; EXZ *= FAC1;
+      KXX *= FAC1; KYY *= FAC1; KXY *= FAC1;
+    }
+    // ---- MULAWC layer loop (mulawc.F90:530-560, 596-1100, 2603-2620, 2930-2990) ----
+    const float* Z0 = zw + (npt - 1) * 33;      // [Z0 | WF | WM] of the npt-point rule
+    const float* WF = Z0 + 11;
+    const float* WM = Z0 + 22;
+    R FOR[5] = {R(0), R(0), R(0), R(0), R(0)}, MOM[3] = {R(0), R(0), R(0)};
+    R FOLD[5] = {R(0), R(0), R(0), R(0), R(0)}, MOLD[3] = {R(0), R(0), R(0)};
+    R THKN = a.thk[e];
+    const R CA = gd.has_jca ? a.jca[e] : R(gd.jc_a);
+    const R CB = R(gd.jc_b), CN = R(gd.jc_n), YMAX = R(gd.sigmax);
+    double wpla = 0.0;
+    for (int ip = 0; ip < npt; ++ip) {
+      const R wf = R(WF[ip]), wm = R(WM[ip]);
+      R SO[5], SN[5];
+#pragma unroll
+      for (int c = 0; c < 5; ++c) SO[c] = a.sig[(ip * 5 + c) * nelpad + e];
+#pragma unroll
+      for (int c = 0; c < 5; ++c) FOLD[c] = FOLD[c] + wf * SO[c];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) MOLD[c] = MOLD[c] + wm * SO[c];
+      const R THKLYL = wf * THK0;
+      const R ZT = R(Z0[ip]) * THK0;
+      const R DXX = EXX + ZT * KXX, DYY = EYY + ZT * KYY, DXY = EXY + ZT * KXY;
+      R EZZ = R(0);
+      if (gd.law == 1) {
+        // SIGEPS01C (sigeps01c.F:130-146)
+        SN[0] = SO[0] + A11 * DXX + A12 * DYY;
+        SN[1] = SO[1] + A12 * DXX + A11 * DYY;
+        SN[2] = SO[2] + GG * DXY;
+        SN[3] = SO[3] + GS * EYZ;
+        SN[4] = SO[4] + GS * EXZ;
+        EZZ = -NU * (DXX + DYY) / (R(1) - NU);
+      } else {
+        // SIGEPS02C -> M2CPLR, IPLA = 0 radial return (m2cplr.F:96-230)
+        const R A1 = YM / (R(1) - NU * NU), A2 = A1 * NU;
+        SN[0] = SO[0] + A1 * DXX + A2 * DYY;
+        SN[1] = SO[1] + A2 * DXX + A1 * DYY;
+        SN[2] = SO[2] + GG * DXY;
+        SN[3] = SO[3] + GS * EYZ;
+        SN[4] = SO[4] + GS * EXZ;
+        R PLA = a.pla[ip * nelpad + e];
+        R YLD = PLA == R(0) ? CA : CA + CB * exp_(CN * log_(PLA));
+        YLD = fmin(YLD, YMAX);
+        const R SVM = ssqrt(SN[0] * SN[0] + SN[1] * SN[1] - SN[0] * SN[1] + R(3) * SN[2] * SN[2]);
+        const R RR = fmin(R(1), YLD / (SVM + R(EM15)));
+        R DPLA = R(0);
+        if (RR < R(1)) {
+          SN[0] *= RR; SN[1] *= RR; SN[2] *= RR;
+          DPLA = OFF * fmax(R(0), (SVM - YLD) / YM);
+          EZZ = DPLA * (R(0.5) * (SN[0] + SN[1])) / YLD;
+          PLA = PLA + DPLA;
+          a.pla[ip * nelpad + e] = PLA;
+        }
+        EZZ = -(DXX + DYY) * NU - (R(1) - R(2) * NU) * EZZ;   // sigeps02c.F:215-224
+        EZZ = EZZ / (R(1) - NU);
+        wpla += (double)YLD * (double)DPLA * (double)AREA * (double)THKLYL;
+      }
+      THKN = THKN + EZZ * THKLYL * OFF;
+#pragma unroll
+      for (int c = 0; c < 5; ++c) a.sig[(ip * 5 + c) * nelpad + e] = SN[c];
+#pragma unroll
+      for (int c = 0; c < 5; ++c) FOR[c] = FOR[c] + wf * SN[c];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) MOM[c] = MOM[c] + wm * SN[c];
+    }
+    my_wpla = wpla;
+    a.thk[e] = THKN > R(EM30) ? THKN : R(EM30);
+    {
+      const R DEGMB = FOLD[0] * EXX + FOLD[1] * EYY + FOLD[2] * EXY + FOLD[3] * EYZ + FOLD[4] * EXZ +
+                      (FOR[0] * EXX + FOR[1] * EYY + FOR[2] * EXY + FOR[3] * EYZ + FOR[4] * EXZ);
+      const R DEGFX = MOLD[0] * KXX + MOLD[1] * KYY + MOLD[2] * KXY +
+                      (MOM[0] * KXX + MOM[1] * KYY + MOM[2] * KXY);
+      const R VOL2 = R(0.5) * VOL0;
+      a.eint[0 * nelpad + e] = a.eint[0 * nelpad + e] + DEGMB * VOL2;
+      a.eint[1 * nelpad + e] = a.eint[1 * nelpad + e] + DEGFX * THK0 * VOL2;
+    }
+    // ---- CHVIS3, ISMSTR = 2, IHBE = 1, HELAS = HVISC = 1/2, HVLIN = 0 (chvis3.F:116-300) ----
+    R H1j[3], H2j[3], H3j[3], HOUR4, HOUR5;
+    {
+      const R px1v = PX1 * VHX, px2v = PX2 * VHX, py1v = PY1 * VHY, py2v = PY2 * VHY;
+      R GAMA[4];
+      GAMA[0] = OFF * (R(1) - px1v - py1v);
+      GAMA[2] = OFF * (R(1) + px1v + py1v);
+      GAMA[1] = OFF * (-R(1) - px2v - py2v);
+      GAMA[3] = OFF * (-R(1) + px2v + py2v);
+      const R SHFPR3 = SHF / (R(3) * (R(1) + NU));
+      const R R1 = R(0.25) * RHO * R(100);
+      const R A1c = R1 * (R(0.5) * H1);
+      const R A3c = R1 * (R(0.5) * H2) * ssqrt(SHFPR3);
+      const R A5c = R(0.5) * H3 * R1 * R(0.072169);
+      const R R0e = R(0.25) * YM * R(0.5);
+      const R A7c = H1 * R0e, A8c = H2 * R0e * SHFPR3;
+      const R T2A = THK02 * AREA;
+      R H1Q = A1c * ssqrt(T2A), H2Q = A3c * THK02, H3Q = A5c * T2A;
+      const R TD = THK0 * DT1;
+      R HH1 = A7c * TD;
+      const R B1 = PX1 * PX1 + PY1 * PY1, B2 = PX2 * PX2 + PY2 * PY2;
+      R HH2 = A8c * THK02 * TD / (B1 + B2);
+      if (a.degen[e]) { H1Q = H2Q = H3Q = HH1 = HH2 = R(0); }
+      R HG1 = VXl[0] * GAMA[0] + VXl[1] * GAMA[1] + VXl[2] * GAMA[2] + VXl[3] * GAMA[3];
+      R HG2 = VYl[0] * GAMA[0] + VYl[1] * GAMA[1] + VYl[2] * GAMA[2] + VYl[3] * GAMA[3];
+      const R hour1 = a.hourg[0 * nelpad + e] + HG1 * HH1;
+      const R hour2 = a.hourg[1 * nelpad + e] + HG2 * HH1;
+      const R HOUR1A = hour1 + HG1 * (H1Q * fabs(HG1));
+      const R HOUR2A = hour2 + HG2 * (H1Q * fabs(HG2));
+#pragma unroll
+      for (int k = 0; k < 3; ++k) { H1j[k] = HOUR1A * GAMA[k]; H2j[k] = HOUR2A * GAMA[k]; }
+      R EHOU = HOUR1A * HG1 + HOUR2A * HG2;
+      HG1 = VZl[0] * GAMA[0] + VZl[1] * GAMA[1] + VZl[2] * GAMA[2] + VZl[3] * GAMA[3];
+      const R hour3 = a.hourg[2 * nelpad + e] + HG1 * HH2;
+      const R HOUR3A = hour3 + HG1 * (H2Q * fabs(HG1));
+#pragma unroll
+      for (int k = 0; k < 3; ++k) H3j[k] = HOUR3A * GAMA[k];
+      EHOU = EHOU + HOUR3A * HG1;
+      HG1 = RXl[0] - RXl[1] + RXl[2] - RXl[3];
+      HG2 = RYl[0] - RYl[1] + RYl[2] - RYl[3];
+      HOUR4 = HG1 * (H3Q * fabs(HG1));
+      HOUR5 = HG2 * (H3Q * fabs(HG2));
+      EHOU = EHOU + HOUR4 * HG1 + HOUR5 * HG2;
+      my_ehou = (double)(DT1 * EHOU * OFF);
+      a.hourg[0 * nelpad + e] = hour1; a.hourg[1 * nelpad + e] = hour2; a.hourg[2 * nelpad + e] = hour3;
+    }
+    // ---- CDT3 (cdt3.F:110-115, 203-214) ----
+    {
+      const R DT = R(gd.dtfac) * ALDT / SSP;
+      if ((double)DT <= gd.dtmin) raise_error(a.err, 5, a.elem_id[e]);
+      mykey = dt_key((double)DT, 3, a.elem_id[e]);
+      mybits = (unsigned long long)__double_as_longlong((double)DT);
+    }
+    // ---- CFINT3, ISIGI = 0 (cfint3.F:173-260) ----
+    {
+      const R F1A = FOR[0] * THK0, F2A = FOR[1] * THK0, F3A = FOR[2] * THK0, F4A = FOR[3] * THK0, F5A = FOR[4] * THK0;
+      const R M4 = R(0.25) * (F4A * AREA), M5 = R(0.25) * (F5A * AREA);
+      const R F12 = F1A * PX2 + F3A * PY2, F22 = F2A * PY2 + F3A * PX2, F32 = F5A * PX2 + F4A * PY2;
+      const R F11 = F1A * PX1 + F3A * PY1, F21 = F2A * PY1 + F3A * PX1, F31 = F5A * PX1 + F4A * PY1;
+      const R Gc[3][3] = {{F11 + H1j[0], F12 + H1j[1], H1j[2] - F11},
+                          {F21 + H2j[0], F22 + H2j[1], H2j[2] - F21},
+                          {F31 + H3j[0], F32 + H3j[1], H3j[2] - F31}};
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        Fg[0][k] = E1X * Gc[0][k] + E2X * Gc[1][k] + E3X * Gc[2][k];
+        Fg[1][k] = E1Y * Gc[0][k] + E2Y * Gc[1][k] + E3Y * Gc[2][k];
+        Fg[2][k] = E1Z * Gc[0][k] + E2Z * Gc[1][k] + E3Z * Gc[2][k];
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) Fg[c][3] = -Fg[c][0] - Fg[c][1] - Fg[c][2];
+      const R M1A = MOM[0] * THK02, M2A = MOM[1] * THK02, M3A = MOM[2] * THK02;
+      const R M11 = -M2A * PY1 - M3A * PX1, M21 = M1A * PX1 + M3A * PY1;
+      const R M12 = -M2A * PY2 - M3A * PX2, M22 = M1A * PX2 + M3A * PY2;
+      const R G1m[4] = {M11 - M4 + HOUR4 * OFF, M12 - M4 - HOUR4 * OFF, -M11 - M4 + HOUR4 * OFF, -M12 - M4 - HOUR4 * OFF};
+      const R G2m[4] = {M21 + M5 + HOUR5 * OFF, M22 + M5 - HOUR5 * OFF, -M21 + M5 + HOUR5 * OFF, -M22 + M5 - HOUR5 * OFF};
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        Mg[0][k] = E1X * G1m[k] + E2X * G2m[k];
+        Mg[1][k] = E1Y * G1m[k] + E2Y * G2m[k];
+        Mg[2][k] = E1Z * G1m[k] + E2Z * G2m[k];
+      }
+    }
+    // ---- uniform pressure (load_pressure.F:201-207): F = -p N / 8, N = x13 x x24 ----
+    R PF[3] = {R(0), R(0), R(0)};
+    if (gd.pressure != 0.0) {
+      const double ax = sx[lc[2]] - x1, ay = sy[lc[2]] - y1, az = sz[lc[2]] - z1;
+      const double bx = sx[lc[3]] - sx[lc[1]], by = sy[lc[3]] - sy[lc[1]], bz = sz[lc[3]] - sz[lc[1]];
+      const R NX = R(ay * bz - az * by), NY = R(az * bx - ax * bz), NZ = R(ax * by - ay * bx);
+      const R AA = -R(gd.pressure) * R(0.125);
+      PF[0] = AA * NX; PF[1] = AA * NY; PF[2] = AA * NZ;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      Fg[0][k] = -Fg[0][k] + PF[0]; Fg[1][k] = -Fg[1][k] + PF[1]; Fg[2][k] = -Fg[2][k] + PF[2];
+      Mg[0][k] = -Mg[0][k]; Mg[1][k] = -Mg[1][k]; Mg[2][k] = -Mg[2][k];
+    }
+  }
+  // ---- colour-ordered shared-memory assembly ----
+  R* sf = sv + 6 * nl;
+  for (int c = 0; c < pi.ncolor; ++c) {
+    if (color == c) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int l = lc[k];
+        sf[0 * nl + l] += Fg[0][k]; sf[1 * nl + l] += Fg[1][k]; sf[2 * nl + l] += Fg[2][k];
+        sf[3 * nl + l] += Mg[0][k]; sf[4 * nl + l] += Mg[1][k]; sf[5 * nl + l] += Mg[2][k];
+      }
+    }
+    __syncthreads();
+  }
+  for (int j = tid; j < nl; j += TILE) {
+    const int s = a.patch_slots[pi.node_ofs + j];
+    a.fslot[s] = mk4(sf[0 * nl + j], sf[1 * nl + j], sf[2 * nl + j], R(0));
+    a.mslot[s] = mk4(sf[3 * nl + j], sf[4 * nl + j], sf[5 * nl + j], R(0));
+  }
+  block_reduce<TILE>(mykey, mybits, my_ehou, my_wpla, s_key, s_bits, s_s0, s_s1);
+  if (tid == 0) {
+    PartAcc* acc = &a.acc[parity * a.nparts + gd.part];
+    atomicMin(&acc->dtkey, mykey);
+    atomicMin(&acc->dtbits, mybits);
+    a.blk_ehour[p] += my_ehou;
+    a.blk_wpla[p] += my_wpla;
+  }
+}
+
+// ===========================================================================
+// node kernel: ASSPAR4 + dt (resol.F:5853-6226) + ACCELE + BCS10 + VELOCITY + DEPLA
+// ===========================================================================
+template <class R, int TILE>
+__global__ void __launch_bounds__(TILE)
+node_kernel(NodeArgs<R> a, int parity) {
+  typedef typename Vec4<R>::T R4;
+  __shared__ double s_e0[TILE / 32], s_e1[TILE / 32];
+  for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
+    const int part = a.tile_part[tile];
+    const PartDesc pd = a.parts[part];
+    const PartTime t0 = a.time[parity * a.nparts + part];
+    const PartAcc ac = a.acc[parity * a.nparts + part];
+    // dt logic, identical in every thread
+    double dt2t = __longlong_as_double((long long)ac.dtbits);
+    double DT2 = 1e6;                                  // EP06
+    int ityp = t0.ityptst, nelt = t0.neltst;
+    if (ac.dtbits != ~0ull && dt2t < DT2) {
+      DT2 = dt2t;
+      ityp = (ac.dtkey & 0x80000000ull) ? 1 : 3;
+      nelt = (int)(ac.dtkey & 0x7fffffffull);
+    }
+    const double cap = a.growth * t0.dt2old;
+    DT2 = DT2 < cap ? DT2 : cap;
+    DT2 = DT2 < a.dtmx ? DT2 : a.dtmx;
+    if (a.split) DT2 = (double)(float)DT2;
+    const double DT1 = t0.dt2;
+    const double DT12 = 0.5 * (DT1 + DT2);
+    if (tile == pd.tile_start && threadIdx.x == 0) {
+      PartTime t1;
+      t1.tt = t0.tt + DT2; t1.dt2 = DT2; t1.dt2old = DT2; t1.dt1 = DT1; t1.dt12 = DT12;
+      t1.ncycle = t0.ncycle + 1; t1.ityptst = ityp; t1.neltst = nelt; t1.pad = 0;
+      a.time[(1 - parity) * a.nparts + part] = t1;
+      PartAcc r; r.dtkey = ~0ull; r.dtbits = ~0ull;
+      a.acc[(1 - parity) * a.nparts + part] = r;
+    }
+    const int n = tile * TILE + threadIdx.x;
+    double ek = 0.0, ekr = 0.0;
+    if (n < pd.node_end) {
+      R ax = R(0), ay = R(0), az = R(0), rx = R(0), ry = R(0), rz = R(0);
+      const int k0 = a.adsky[n], k1 = a.adsky[n + 1];
+      for (int k = k0; k < k1; ++k) {
+        const R4 f = a.fslot[k];
+        ax += f.x; ay += f.y; az += f.z;
+      }
+      const double4 xm = a.X[n];
+      R4 v = a.V[n];
+      const unsigned char code = a.code[n];
+      // ACCELE (accele.F:63-80)
+      const R ms = R(xm.w);
+      if (ms > R(0)) { const R r = R(1) / ms; ax *= r; ay *= r; az *= r; }
+      else { ax = ay = az = R(0); }
+      if (!isfinite((double)ax + (double)ay + (double)az)) raise_error(a.err, 6, n);
+      // BCS10 (bcs1.F:52-100)
+      if (code & 4) { v.x = R(0); ax = R(0); }
+      if (code & 2) { v.y = R(0); ay = R(0); }
+      if (code & 1) { v.z = R(0); az = R(0); }
+      const double dt05 = 0.5 * DT1;
+      {
+        const double wx = (double)v.x + dt05 * (double)ax, wy = (double)v.y + dt05 * (double)ay,
+                     wz = (double)v.z + dt05 * (double)az;
+        ek = (wx * wx + wy * wy + wz * wz) * 0.5 * (double)ms;
+      }
+      // VELOCITY (velocity.F:56-62)
+      const R dt12 = R(DT12);
+      v.x = v.x + dt12 * ax; v.y = v.y + dt12 * ay; v.z = v.z + dt12 * az;
+      a.V[n] = v;
+      // DEPLA (displacement.F:69-100), FP64 accumulation
+      const double ux = DT2 * (double)v.x, uy = DT2 * (double)v.y, uz = DT2 * (double)v.z;
+      a.DX[n] += ux; a.DY[n] += uy; a.DZ[n] += uz;
+      a.X[n] = make_double4(xm.x + ux, xm.y + uy, xm.z + uz, xm.w);
+      if (pd.has_rot) {
+        for (int k = k0; k < k1; ++k) {
+          const R4 m = a.mslot[k];
+          rx += m.x; ry += m.y; rz += m.z;
+        }
+        R4 w = a.VR[n];
+        const R in = w.w;
+        if (in > R(0)) { const R r = R(1) / in; rx *= r; ry *= r; rz *= r; }
+        else { rx = ry = rz = R(0); }
+        if (code & 32) { w.x = R(0); rx = R(0); }
+        if (code & 16) { w.y = R(0); ry = R(0); }
+        if (code & 8)  { w.z = R(0); rz = R(0); }
+        const double wx = (double)w.x + dt05 * (double)rx, wy = (double)w.y + dt05 * (double)ry,
+                     wz = (double)w.z + dt05 * (double)rz;
+        ekr = (wx * wx + wy * wy + wz * wz) * 0.5 * (double)in;
+        w.x = w.x + dt12 * rx; w.y = w.y + dt12 * ry; w.z = w.z + dt12 * rz;
+        a.VR[n] = w;
+      }
+    }
+    // per-tile kinetic energy partials (fixed tree order -> deterministic)
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      ek += __shfl_xor_sync(0xffffffffu, ek, o);
+      ekr += __shfl_xor_sync(0xffffffffu, ekr, o);
+    }
+    if (lane == 0) { s_e0[warp] = ek; s_e1[warp] = ekr; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s0 = 0.0, s1 = 0.0;
+      for (int w = 0; w < TILE / 32; ++w) { s0 += s_e0[w]; s1 += s_e1[w]; }
+      a.blk_ekin[tile] = s0;
+      a.blk_ekinr[tile] = s1;
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace orb

@@ -1,0 +1,224 @@
+"""Parity of the sm_100a path (through the C-ABI) against the CPU oracle.
+
+Tolerances (written here on purpose):
+* plain FP64 form: 1e-10 relative, normwise  max|gpu - oracle| / max|oracle|
+  for nodal displacements, velocities, element stresses, plastic strain,
+  thickness and the internal / kinetic / hourglass energies;
+* split form: 1e-5 relative nodal-displacement error against the FP64 oracle.
+"""
+import numpy as np
+import pytest
+
+from openradioss_b200 import abi, decks
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-10
+SPLIT_TOL = 1e-5
+
+
+def rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    s = max(np.abs(b).max(), 1e-300)
+    return np.abs(a - b).max() / s
+
+
+@pytest.fixture(scope="module")
+def lib():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from openradioss_b200 import build
+    build.build()
+    from openradioss_b200.ecycle import load_library
+    return load_library()
+
+
+def run_pair(deck, ncycles, precision=abi.OR_PREC_FP64, oracle_precision=abi.OR_PREC_FP64, **kw):
+    from openradioss_b200.ecycle import ECycle
+    from oracle.oracle import Oracle
+    g = ECycle(deck, precision=precision, **kw)
+    o = Oracle(deck, precision=oracle_precision, nthreads=8)
+    g.step(ncycles)
+    o.step(ncycles)
+    return g, o
+
+
+def check_nodes(g, o, tol, parts=None):
+    for p in range(g.nparts) if parts is None else parts:
+        a, b = g.get_nodes(p), o.get_nodes(p)
+        for k in ("d", "v"):
+            assert rel(a[k], b[k]) < tol, (p, k, rel(a[k], b[k]))
+        if np.abs(b["vr"]).max() > 0:
+            assert rel(a["vr"], b["vr"]) < tol, (p, "vr", rel(a["vr"], b["vr"]))
+        ta, tb = g.time(p), o.time(p)
+        assert abs(ta["dt2"] - tb["dt2"]) <= tol * tb["dt2"]
+        assert abs(ta["tt"] - tb["tt"]) <= tol * tb["tt"]
+        assert ta["ncycle"] == tb["ncycle"]
+
+
+def check_hex(g, o, tol):
+    for gi in range(len(g.hex_groups)):
+        a, b = g.hex_state(gi), o.hex_state(gi)
+        for k in ("sig", "eint", "rho", "qvis", "pla", "epsd"):
+            if np.abs(b[k]).max() > 0:
+                assert rel(a[k], b[k]) < tol, (gi, k, rel(a[k], b[k]))
+
+
+def check_shell(g, o, tol):
+    for gi in range(len(g.shell_groups)):
+        a, b = g.shell_state(gi), o.shell_state(gi)
+        for k in ("sig", "pla", "thk", "hourg", "eint"):
+            if np.abs(b[k]).max() > 0:
+                assert rel(a[k], b[k]) < tol, (gi, k, rel(a[k], b[k]))
+
+
+def check_energies(g, o, tol, part=0):
+    ea, eb = g.energies(part), o.energies(part)
+    for k in ("internal", "kinetic", "kinetic_rot", "hourglass", "plastic_work"):
+        if abs(eb[k]) > 0:
+            assert abs(ea[k] - eb[k]) <= tol * abs(eb[k]) + 1e-300, (k, ea[k], eb[k])
+
+
+def test_hex_law1_fp64(lib):
+    d = decks.c1_hex_block(nx=6, ny=5, nz=12)
+    g, o = run_pair(d, 300)
+    check_nodes(g, o, FP64_TOL)
+    check_hex(g, o, FP64_TOL)
+    check_energies(g, o, FP64_TOL)
+
+
+def test_hex_law2_fp64(lib):
+    d = decks.c1_hex_block(nx=4, ny=4, nz=10, law=decks.LAW_JOHNSON_COOK, vz=-60.0)
+    g, o = run_pair(d, 250)
+    assert o.hex_state(0)["pla"].max() > 0       # plastic flow happened
+    check_nodes(g, o, FP64_TOL)
+    check_hex(g, o, FP64_TOL)
+    check_energies(g, o, FP64_TOL)
+
+
+def test_shell_law2_plate_fp64(lib):
+    d = decks.c2_shell_plate(n=20, size=0.02, pressure=2e7)
+    g, o = run_pair(d, 400)
+    assert o.shell_state(0)["pla"].max() > 0
+    check_nodes(g, o, FP64_TOL)
+    check_shell(g, o, FP64_TOL)
+    check_energies(g, o, FP64_TOL)
+
+
+def test_shell_law1_plate_fp64(lib):
+    d = decks.c2_shell_plate(n=12, size=0.012, law=decks.LAW_ELASTIC, npt=3)
+    g, o = run_pair(d, 200)
+    check_nodes(g, o, FP64_TOL)
+    check_shell(g, o, FP64_TOL)
+
+
+def test_mixed_mesh_fp64(lib):
+    d = decks.c4_mixed_mesh(nx=4, ny=5, nz=8)
+    g, o = run_pair(d, 150)
+    check_nodes(g, o, FP64_TOL)
+    check_hex(g, o, FP64_TOL)
+    check_shell(g, o, FP64_TOL)
+    check_energies(g, o, FP64_TOL)
+
+
+def test_batched_parts_own_dt(lib):
+    d = decks.c3_batched_parts(nparts=6, seed=3, scale=0.01)
+    g, o = run_pair(d, 120)
+    check_nodes(g, o, FP64_TOL)
+    dts = {g.time(p)["dt2"] for p in range(g.nparts)}
+    assert len(dts) > 1                          # every part keeps its own time step
+    for p in range(g.nparts):
+        check_energies(g, o, FP64_TOL, part=p)
+
+
+def test_per_element_yield_and_thickness(lib):
+    d = decks.c5_adjoint_plate(n=12, ncycles=100, size=0.012, pressure=3e7)
+    g, o = run_pair(d, 200)
+    check_nodes(g, o, FP64_TOL)
+    check_shell(g, o, FP64_TOL)
+
+
+def test_split_plate_within_1e5(lib):
+    d = decks.c2_shell_plate(n=24, size=0.024)
+    g, o = run_pair(d, 400, precision=abi.OR_PREC_SPLIT)
+    a, b = g.get_nodes(), o.get_nodes()
+    assert rel(a["d"], b["d"]) < SPLIT_TOL, rel(a["d"], b["d"])
+
+
+def test_split_hex_within_1e5(lib):
+    d = decks.c1_hex_block(nx=5, ny=5, nz=12)
+    g, o = run_pair(d, 300, precision=abi.OR_PREC_SPLIT)
+    a, b = g.get_nodes(), o.get_nodes()
+    assert rel(a["d"], b["d"]) < SPLIT_TOL, rel(a["d"], b["d"])
+
+
+def test_split_matches_split_oracle(lib):
+    d = decks.c4_mixed_mesh(nx=3, ny=3, nz=6)
+    g, o = run_pair(d, 100, precision=abi.OR_PREC_SPLIT, oracle_precision=abi.OR_PREC_SPLIT)
+    check_nodes(g, o, 1e-5)
+
+
+def test_graph_equals_eager_bitwise(lib):
+    from openradioss_b200.ecycle import ECycle
+    d = decks.c4_mixed_mesh(nx=3, ny=4, nz=6)
+    a = ECycle(d, graph=1)
+    b = ECycle(d, graph=0)
+    a.step(70)
+    b.step(70)
+    na, nb = a.get_nodes(), b.get_nodes()
+    assert np.array_equal(na["d"], nb["d"]) and np.array_equal(na["v"], nb["v"])
+    assert a.energies() == b.energies()
+
+
+def test_deterministic_repeat(lib):
+    from openradioss_b200.ecycle import ECycle
+    d = decks.c2_shell_plate(n=16, size=0.016, pressure=2e7)
+    r = []
+    for _ in range(2):
+        g = ECycle(d, precision=abi.OR_PREC_SPLIT)
+        g.step(96)
+        r.append(g.get_nodes()["d"])
+    assert np.array_equal(r[0], r[1])
+
+
+def test_step_in_pieces_equals_one_call(lib):
+    from openradioss_b200.ecycle import ECycle
+    d = decks.c1_hex_block(nx=3, ny=3, nz=6, law=decks.LAW_JOHNSON_COOK, vz=-40.0)
+    a = ECycle(d)
+    b = ECycle(d)
+    a.step(77)
+    for n in (1, 32, 7, 37):
+        b.step(n)
+    assert np.array_equal(a.get_nodes()["d"], b.get_nodes()["d"])
+    assert a.time() == b.time()
+
+
+def test_tile_shapes_agree(lib):
+    from openradioss_b200.ecycle import ECycle
+    d = decks.c4_mixed_mesh(nx=4, ny=4, nz=8)
+    a = ECycle(d, block_hex=128, block_shell=128)
+    b = ECycle(d, block_hex=256, block_shell=256)
+    a.step(64)
+    b.step(64)
+    assert rel(a.get_nodes()["d"], b.get_nodes()["d"]) < FP64_TOL
+
+
+def test_negative_volume_reports_element(lib):
+    from openradioss_b200.ecycle import ECycle, ECycleError
+    d = decks.c1_hex_block(nx=2, ny=2, nz=2)
+    p = d["parts"][0]
+    # crush one element: node of element 5 pushed through its opposite face
+    ixs = p["hex"][0]["ixs"]
+    n7 = ixs[5, 7] - 1
+    p["v"][:] = 0.0
+    p["v"][n7] = (-3e4, -3e4, -3e4)
+    p["icodt"][:] = 0
+    g = ECycle(d)
+    with pytest.raises(ECycleError) as ei:
+        g.step(40)
+    code, idx = g.error_info()
+    assert code == abi.OR_E_NEGVOL
+    assert ei.value.code == abi.OR_E_NEGVOL
+    assert 0 <= idx < ixs.shape[0]
