@@ -627,7 +627,7 @@ int reset_impl(or_ecycle* h) {
 }
 
 int wait_stream(or_ecycle* h, cudaEvent_t ev) {
-  double limit = 3600.0;
+  double limit = 900.0;
   if (const char* s = std::getenv("OR_ECYCLE_TIMEOUT_S")) limit = std::atof(s);
   auto t0 = std::chrono::steady_clock::now();
   for (;;) {
