@@ -234,7 +234,10 @@ def c3_batched_parts(nparts=64, seed=0, ncycles=500, scale=1.0):
         law = LAW_ELASTIC if rng.random() < 0.5 else LAW_JOHNSON_COOK
         vmag = rng.uniform(1.0, 20.0)
         if is_hex:
-            nx = max(1, int(round((nel / 4.0) ** (1.0 / 3.0))))
+            # at least 3 elements across: a 1-element-wide column of 1-point hexas is
+            # unstable at the element time step (its volumetric mode, omega^2 = 12 K / rho h^2,
+            # is above the Courant estimate of sdlen3.F / mqviscb.F)
+            nx = max(3, int(round((nel / 4.0) ** (1.0 / 3.0))))
             x, conn = hex_block(nx, nx, 4 * nx, 1e-3)
             p = new_part(x)
             add_hex(p, conn, steel_elastic() if law == LAW_ELASTIC else steel_jc(), solid_prop())
@@ -244,7 +247,7 @@ def c3_batched_parts(nparts=64, seed=0, ncycles=500, scale=1.0):
             p["icodt"][base] = 7
             p["v"][~base] = vmag * d
         else:
-            n = max(2, int(round(math.sqrt(nel))))
+            n = max(4, int(round(math.sqrt(nel))))
             x, conn, edge = quad_plate(n, n * 1e-3, jitter=0.05, seed=int(rng.integers(1 << 30)))
             p = new_part(x)
             mat = aluminium_jc() if law == LAW_JOHNSON_COOK else material(LAW_ELASTIC, 2700.0, 70e9, 0.33)

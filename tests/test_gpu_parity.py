@@ -99,7 +99,7 @@ def test_hex_law2_fp64(lib):
 
 
 def test_shell_law2_plate_fp64(lib):
-    d = decks.c2_shell_plate(n=20, size=0.02, pressure=2e7)
+    d = decks.c2_shell_plate(n=20, size=0.02, pressure=5e6)
     g, o = run_pair(d, 400)
     assert o.shell_state(0)["pla"].max() > 0
     check_nodes(g, o, FP64_TOL)
@@ -134,8 +134,9 @@ def test_batched_parts_own_dt(lib):
 
 
 def test_per_element_yield_and_thickness(lib):
-    d = decks.c5_adjoint_plate(n=12, ncycles=100, size=0.012, pressure=3e7)
+    d = decks.c5_adjoint_plate(n=12, ncycles=100, size=0.012, pressure=6e6)
     g, o = run_pair(d, 200)
+    assert o.shell_state(0)["pla"].max() > 0
     check_nodes(g, o, FP64_TOL)
     check_shell(g, o, FP64_TOL)
 
@@ -174,7 +175,7 @@ def test_graph_equals_eager_bitwise(lib):
 
 def test_deterministic_repeat(lib):
     from openradioss_b200.ecycle import ECycle
-    d = decks.c2_shell_plate(n=16, size=0.016, pressure=2e7)
+    d = decks.c2_shell_plate(n=16, size=0.016, pressure=5e6)
     r = []
     for _ in range(2):
         g = ECycle(d, precision=abi.OR_PREC_SPLIT)
@@ -209,16 +210,14 @@ def test_negative_volume_reports_element(lib):
     from openradioss_b200.ecycle import ECycle, ECycleError
     d = decks.c1_hex_block(nx=2, ny=2, nz=2)
     p = d["parts"][0]
-    # crush one element: node of element 5 pushed through its opposite face
+    # element 5 with its bottom and top faces swapped: inverted Jacobian, while the
+    # host-side V0 stays positive, so only the device-side SCHKJABT3 check can see it
     ixs = p["hex"][0]["ixs"]
-    n7 = ixs[5, 7] - 1
-    p["v"][:] = 0.0
-    p["v"][n7] = (-3e4, -3e4, -3e4)
-    p["icodt"][:] = 0
+    ixs[5, 1:9] = np.concatenate([ixs[5, 5:9], ixs[5, 1:5]]).copy()
     g = ECycle(d)
     with pytest.raises(ECycleError) as ei:
-        g.step(40)
+        g.step(3)
     code, idx = g.error_info()
     assert code == abi.OR_E_NEGVOL
     assert ei.value.code == abi.OR_E_NEGVOL
-    assert 0 <= idx < ixs.shape[0]
+    assert idx == 5
