@@ -15,6 +15,11 @@ pytestmark = pytest.mark.gpu
 
 FP64_TOL = 1e-10
 SPLIT_TOL = 1e-5
+# Integration-point state of plastically flowing shells: the radial return near the
+# yield surface amplifies round-off differences (FMA contraction on the device,
+# patch-partial vs element-slot assembly order) by about E/H; nodal quantities of
+# the same runs stay within FP64_TOL.
+FP64_PLASTIC_IP_TOL = 1e-9
 
 
 def rel(a, b):
@@ -103,7 +108,7 @@ def test_shell_law2_plate_fp64(lib):
     g, o = run_pair(d, 400)
     assert o.shell_state(0)["pla"].max() > 0
     check_nodes(g, o, FP64_TOL)
-    check_shell(g, o, FP64_TOL)
+    check_shell(g, o, FP64_PLASTIC_IP_TOL)
     check_energies(g, o, FP64_TOL)
 
 
