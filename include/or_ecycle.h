@@ -210,6 +210,30 @@ int  or_ecycle_stream(or_ecycle* h, void** stream);
 /* Bytes of device memory held by the handle. */
 int  or_ecycle_device_bytes(or_ecycle* h, long long* bytes);
 
+/* --- entry point that allocates nothing ---------------------------------- */
+/* No counterpart in the reference.  For callers that cannot let this library
+   allocate device memory (for example an engine that reserves one device pool
+   at start-up and must keep its footprint fixed through the time loop): runs
+   ncycles of one FP64 hexa group (LAW1/LAW2) of one part on caller-owned
+   device arrays, with the reference's own Parith/ON tables (iads: skyline slot
+   of each of the 8 corners, adsky: node -> slot CSR, numnod+1 entries), and
+   keeps its only scratch, the FSKY force skyline, in a static device array of
+   OR_NOALLOC_MAX_SLOTS slots (8 MB, held by every GPU that loads the library).
+   Larger groups are rejected with OR_E_ARG.  No cudaMalloc / cudaFree or other
+   allocating call is made.  The first call on a device looks up the scratch
+   address with that device current; make it before any stream capture.  All
+   calls share the scratch: calls that overlap on the GPU race.
+   Arrays: x, d, v 3 x numnod; ms, icodt numnod; conn, iads 8 x nel (0-based);
+   sig 6 x nel component-major; eint, rho, qvis, pla, epsd, vol0 nel.
+   stream: a cudaStream_t (NULL = legacy default stream). */
+#define OR_NOALLOC_MAX_SLOTS 262144
+int  or_ecycle_hex_step_noalloc(int device, void* stream, int ncycles, or_ecycle_time* t,
+                                int numnod, double* x, double* d, double* v, const double* ms,
+                                const int* icodt, int nel, const int* conn, const int* iads,
+                                const int* adsky, const or_material* mat, const or_solid_prop* prop,
+                                double dtfac, double dtmx, double dt_growth, double* sig, double* eint,
+                                double* rho, double* qvis, double* pla, double* epsd, const double* vol0);
+
 #ifdef __cplusplus
 }
 #endif

@@ -9,7 +9,7 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRC = [os.path.join(HERE, "csrc", "ecycle.cu")]
+SRC = [os.path.join(HERE, "csrc", "ecycle.cu"), os.path.join(HERE, "csrc", "ecycle_noalloc.cu")]
 DEPS = SRC + [os.path.join(HERE, "csrc", "ecycle_kernels.cuh"),
               os.path.join(HERE, "..", "include", "or_ecycle.h")]
 OUT = os.path.join(HERE, "libor_ecycle.so")
