@@ -125,7 +125,7 @@ def cpu_baseline(deck, cycles, budget_s, fast=True):
     o.step(n)
     dt = time.perf_counter() - t0
     return {"value": nel * n / dt, "unit": "element-updates/s", "cores": nthreads, "kind": "port",
-            "sample": f"first {n + 2} of {cycles} cycles of the same deck (2 untimed), FP64, "
+            "sample": f"{n} timed cycles (after 2 untimed) of the {cycles}-cycle deck, FP64, "
                       f"C++ restatement of the reference CPU path, OpenMP {nthreads} threads"}
 
 
@@ -216,8 +216,13 @@ def main():
                 launches += h.launch_count()
         return ms, launches
 
+    # ---- tile shapes from the autotuner (timed on this GPU, cached) ----
+    from openradioss_b200 import autotune
+    bh_s, bs_s, tune_s = autotune.tune(deck, abi.OR_PREC_SPLIT, device=local)
+    bh_d, bs_d, tune_d = autotune.tune(deck, abi.OR_PREC_FP64, device=local)
+
     # ---- split form (the headline) ----
-    hs = ECycle(deck, precision=abi.OR_PREC_SPLIT, device=local, graph=1)
+    hs = ECycle(deck, precision=abi.OR_PREC_SPLIT, device=local, graph=1, block_hex=bh_s, block_shell=bs_s)
     timed_runs(hs, 0, 1)                      # graph capture + first-touch outside timing
     sampler = ClockSampler(local)
     sampler.start()
@@ -227,7 +232,7 @@ def main():
     d_split = hs.get_nodes()["d"]
 
     # ---- plain FP64 form ----
-    hd = ECycle(deck, precision=abi.OR_PREC_FP64, device=local, graph=1)
+    hd = ECycle(deck, precision=abi.OR_PREC_FP64, device=local, graph=1, block_hex=bh_d, block_shell=bs_d)
     timed_runs(hd, 0, 1)
     nfp = max(2, args.steps // 2)
     ms_fp64, _ = timed_runs(hd, nfp, 1)
@@ -245,7 +250,7 @@ def main():
     value_fp64 = world * nel * cycles / (t_fp64 * 1e-3)
 
     # ---- per-kernel device times (eager launches with CUDA events on the handle's stream) ----
-    hp = ECycle(deck, precision=abi.OR_PREC_SPLIT, device=local, graph=0)
+    hp = ECycle(deck, precision=abi.OR_PREC_SPLIT, device=local, graph=0, block_hex=bh_s, block_shell=bs_s)
     kcyc = min(cycles, 200)
     hp.step(kcyc)
     hp.reset()
@@ -320,8 +325,9 @@ def main():
                        "elements_per_gpu": nel, "nodes_per_gpu": nnod, "cycles_per_step": cycles,
                        "precision": "split: FP32 element/material math, FP64 X/D/volumes/energies",
                        "l2": "256 MB buffer written before every timed step",
-                       "cuda_graph_cycles": 32, "tile_hex": 256, "tile_shell": 256},
-            "fp64": {"value": value_fp64, "ms_per_step": t_fp64, "dtype": "f64"},
+                       "cuda_graph_cycles": 32, "tile_hex": bh_s, "tile_shell": bs_s,
+                       "autotune_ms_per_cycle": {"split": tune_s, "fp64": tune_d}},
+            "fp64": {"value": value_fp64, "ms_per_step": t_fp64, "dtype": "f64", "tile_hex": bh_d, "tile_shell": bs_d},
             "split_over_fp64": value / value_fp64,
             "split_rel_disp_error_vs_fp64": split_err,
             "roofline": {"bound": "hbm", "kernel": f"{dom}_patch_kernel" if dom != "node" else "node_kernel",

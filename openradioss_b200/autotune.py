@@ -1,0 +1,92 @@
+"""Tile-shape autotuner for the patch kernels.
+
+For a deck and precision, builds one handle per candidate tile (elements per
+patch = threads per CTA of the hexa and shell kernels), times a few hundred
+graph-replayed cycles with CUDA events on the handle's stream, and returns the
+fastest.  Results are cached per (deck name, element count, precision, GPU) in
+``autotune_cache.json`` beside this file.
+
+    python -m openradioss_b200.autotune --workload shell_plate
+"""
+from __future__ import annotations
+
+import json
+import os
+
+from . import abi, decks
+
+CANDIDATES = (64, 128, 256)
+CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "autotune_cache.json")
+
+
+def _key(deck, precision, gpu):
+    return f"{deck.get('name', 'deck')}|{decks.num_elements(deck)}|{precision}|{gpu}"
+
+
+def _time_cycles(h, ncycles):
+    import torch
+    s = torch.cuda.ExternalStream(h.stream())
+    h.step(min(ncycles, 64))          # first replay captures the graph
+    h.reset()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(s)
+    h.step(ncycles)
+    e1.record(s)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / ncycles
+
+
+def tune(deck, precision=abi.OR_PREC_SPLIT, ncycles=256, use_cache=True, device=0, verbose=False):
+    """Returns (block_hex, block_shell, {candidate: ms per cycle})."""
+    import torch
+    from .ecycle import ECycle
+    gpu = torch.cuda.get_device_name(device)
+    key = _key(deck, precision, gpu)
+    cache = {}
+    if use_cache and os.path.exists(CACHE):
+        try:
+            cache = json.load(open(CACHE))
+        except (OSError, ValueError):
+            cache = {}
+    if use_cache and key in cache:
+        c = cache[key]
+        return c["block_hex"], c["block_shell"], c["ms_per_cycle"]
+    has_hex = any(p["hex"] for p in deck["parts"])
+    has_shell = any(p["shell"] for p in deck["parts"])
+    timings = {}
+    for t in CANDIDATES:
+        h = ECycle(deck, precision=precision, device=device, graph=1, block_hex=t, block_shell=t)
+        timings[t] = _time_cycles(h, ncycles)
+        h.close()
+        if verbose:
+            print(f"tile {t}: {timings[t] * 1e3:.2f} us/cycle", flush=True)
+    best = min(timings, key=timings.get)
+    bh = best if has_hex else 256
+    bs = best if has_shell else 256
+    cache[key] = {"block_hex": bh, "block_shell": bs, "ms_per_cycle": {str(k): v for k, v in timings.items()}}
+    try:
+        json.dump(cache, open(CACHE, "w"), indent=1, sort_keys=True)
+    except OSError:
+        pass
+    return bh, bs, cache[key]["ms_per_cycle"]
+
+
+def main():
+    import argparse
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="shell_plate",
+                    choices=["shell_plate", "hex_block", "mixed_mesh", "batched_parts"])
+    ap.add_argument("--precision", default="split", choices=["split", "fp64"])
+    ap.add_argument("--cycles", type=int, default=256)
+    a = ap.parse_args()
+    from . import build
+    build.build()
+    fac = {"shell_plate": decks.c2_shell_plate, "hex_block": decks.c1_hex_block,
+           "mixed_mesh": decks.c4_mixed_mesh, "batched_parts": decks.c3_batched_parts}[a.workload]
+    prec = abi.OR_PREC_SPLIT if a.precision == "split" else abi.OR_PREC_FP64
+    print(tune(fac(), prec, a.cycles, use_cache=False, verbose=True))
+
+
+if __name__ == "__main__":
+    main()

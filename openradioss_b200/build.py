@@ -15,7 +15,10 @@ DEPS = SRC + [os.path.join(HERE, "csrc", "ecycle_kernels.cuh"),
 OUT = os.path.join(HERE, "libor_ecycle.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
-         "-Xcompiler", "-fPIC", "-shared", "--expt-relaxed-constexpr"]
+         "-Xcompiler", "-fPIC", "-shared", "--expt-relaxed-constexpr",
+         # single precision only (the split form's FP32 kernels): fast sqrt/div/exp/log,
+         # FP32 denormals flushed; FP64 arithmetic is unaffected
+         "--use_fast_math"]
 
 
 def needs_build():

@@ -30,7 +30,7 @@ using namespace orb;
 
 namespace {
 
-constexpr int NODE_TILE = 256;
+constexpr int NODE_TILE = 128;
 constexpr int GRAPH_CYCLES = 32;
 
 // through-thickness rules of COQINI (coqini.F:45-130), [npt-1][Z0 | WF | WM]
@@ -291,7 +291,7 @@ struct Impl {
   DBuf<double> sehour, swpla;
   DBuf<float> zw;
   int maxnpt = 1;
-  std::vector<int> part_hex_patches, part_shell_patches;   // unused placeholders
+  int uniform_npt = 0;       // npt shared by every shell group, 0 if they differ
 
   HexArgs<R> hargs() {
     HexArgs<R> a;
@@ -347,14 +347,18 @@ int launch_hex(or_ecycle* h, Impl<R>& m, int parity) {
   h->launches++;
   return OR_OK;
 }
-template <class R, int T>
+template <class R, int T, int NPT>
 int launch_shell(or_ecycle* h, Impl<R>& m, int parity) {
   if (m.sps.info.empty()) return OR_OK;
   size_t sm = shell_smem<R>(m.sps.nlmax);
-  shell_patch_kernel<R, T><<<(unsigned)m.sps.info.size(), T, sm, h->stream>>>(m.sargs(), parity, m.zw.p);
+  shell_patch_kernel<R, T, NPT><<<(unsigned)m.sps.info.size(), T, sm, h->stream>>>(m.sargs(), parity, m.zw.p);
   CK(cudaGetLastError());
   h->launches++;
   return OR_OK;
+}
+template <class R, int T>
+int launch_shell_npt(or_ecycle* h, Impl<R>& m, int parity) {
+  return m.uniform_npt == 5 ? launch_shell<R, T, 5>(h, m, parity) : launch_shell<R, T, 0>(h, m, parity);
 }
 template <class R>
 int launch_node(or_ecycle* h, Impl<R>& m, int parity) {
@@ -364,14 +368,24 @@ int launch_node(or_ecycle* h, Impl<R>& m, int parity) {
   return OR_OK;
 }
 
+template <class F>
+cudaError_t set_smem(F* f, int bytes) {
+  return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
 template <class R>
 int set_smem_attrs(or_ecycle* h, Impl<R>& m) {
   int hs = (int)hex_smem<R>(m.hps.nlmax), ss = (int)shell_smem<R>(m.sps.nlmax);
-  CK(cudaFuncSetAttribute(hex_patch_kernel<R, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, hs));
-  CK(cudaFuncSetAttribute(hex_patch_kernel<R, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, hs));
-  CK(cudaFuncSetAttribute(shell_patch_kernel<R, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss));
-  CK(cudaFuncSetAttribute(shell_patch_kernel<R, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss));
   if (hs > 200 * 1024 || ss > 200 * 1024) return fail(h, OR_E_UNSUPPORTED, "patch shared memory above 200 KB");
+  CK(set_smem(hex_patch_kernel<R, 64>, hs));
+  CK(set_smem(hex_patch_kernel<R, 128>, hs));
+  CK(set_smem(hex_patch_kernel<R, 256>, hs));
+  CK(set_smem(shell_patch_kernel<R, 64, 0>, ss));
+  CK(set_smem(shell_patch_kernel<R, 128, 0>, ss));
+  CK(set_smem(shell_patch_kernel<R, 256, 0>, ss));
+  CK(set_smem(shell_patch_kernel<R, 64, 5>, ss));
+  CK(set_smem(shell_patch_kernel<R, 128, 5>, ss));
+  CK(set_smem(shell_patch_kernel<R, 256, 5>, ss));
   return OR_OK;
 }
 
@@ -379,10 +393,12 @@ template <class R>
 int launch_cycle(or_ecycle* h, Impl<R>& m, int parity, cudaEvent_t* ev) {
   int rc;
   if (ev) CK(cudaEventRecord(ev[0], h->stream));
-  rc = h->tile_hex == 128 ? launch_hex<R, 128>(h, m, parity) : launch_hex<R, 256>(h, m, parity);
+  rc = h->tile_hex == 64 ? launch_hex<R, 64>(h, m, parity)
+       : h->tile_hex == 128 ? launch_hex<R, 128>(h, m, parity) : launch_hex<R, 256>(h, m, parity);
   if (rc) return rc;
   if (ev) CK(cudaEventRecord(ev[1], h->stream));
-  rc = h->tile_shell == 128 ? launch_shell<R, 128>(h, m, parity) : launch_shell<R, 256>(h, m, parity);
+  rc = h->tile_shell == 64 ? launch_shell_npt<R, 64>(h, m, parity)
+       : h->tile_shell == 128 ? launch_shell_npt<R, 128>(h, m, parity) : launch_shell_npt<R, 256>(h, m, parity);
   if (rc) return rc;
   if (ev) CK(cudaEventRecord(ev[2], h->stream));
   rc = launch_node<R>(h, m, parity);
@@ -534,6 +550,9 @@ int finalize_impl(or_ecycle* h) {
       desc.push_back(d);
       m.maxnpt = std::max(m.maxnpt, g.prop.npt);
     }
+    m.uniform_npt = h->shell[0].prop.npt;
+    for (auto& g : h->shell)
+      if (g.prop.npt != m.uniform_npt) m.uniform_npt = 0;
     std::vector<uint2> conn(np, make_uint2(0, 0));
     std::vector<int> elem(np, 0), degen(np, 0);
     std::vector<R> thke(np, R(1)), jca(any_jca ? np : 0, R(0));
@@ -918,8 +937,9 @@ int or_ecycle_create(const or_ecycle_config* cfg, or_ecycle** out) {
   h->cfg = *cfg;
   if (h->cfg.dt_growth <= 0) h->cfg.dt_growth = (double)1.1f;
   if (h->cfg.dtmx <= 0) h->cfg.dtmx = 1e20;
-  if (h->cfg.block_hex == 128 || h->cfg.block_hex == 256) h->tile_hex = h->cfg.block_hex;
-  if (h->cfg.block_shell == 128 || h->cfg.block_shell == 256) h->tile_shell = h->cfg.block_shell;
+  auto tile_ok = [](int b) { return b == 64 || b == 128 || b == 256; };
+  if (tile_ok(h->cfg.block_hex)) h->tile_hex = h->cfg.block_hex;
+  if (tile_ok(h->cfg.block_shell)) h->tile_shell = h->cfg.block_shell;
   if (cudaSetDevice(cfg->device) != cudaSuccess || cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
     delete h;
     return OR_E_CUDA;

@@ -236,6 +236,27 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
   R* sfx = svz + nl;
   R* sfy = sfx + nl;
   R* sfz = sfy + nl;
+  const bool active = tid < pi.nel;
+  const int e = pi.elem0 + tid;
+  const int nelpad = a.nelpad;
+  // issue every per-element load before the staging barrier so that they are in
+  // flight together with the node gathers
+  uint4 cw = make_uint4(0, 0, 0, 0);
+  R st_sig[6], st_eint = R(0), st_rho = R(1), st_qvis = R(0), st_vol0 = R(1), st_pla = R(0);
+  double st_vol0dp = 1.0;
+  int st_eid = 0;
+  if (active) {
+    cw = a.conn[e];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) st_sig[c] = a.sig[c * nelpad + e];
+    st_eint = a.eint[e];
+    st_rho = a.rho[e];
+    st_qvis = a.qvis[e];
+    st_vol0 = a.vol0[e];
+    if (sizeof(R) == 4) st_vol0dp = a.vol0dp[e];
+    if (gd.law == 2) st_pla = a.pla[e];
+    st_eid = a.elem_id[e];
+  }
   for (int j = tid; j < nl; j += TILE) {
     const int g = a.patch_nodes[pi.node_ofs + j];
     const double4 xx = a.X[g];
@@ -249,16 +270,12 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
   const bool split = sizeof(R) == 4;
   __syncthreads();
 
-  const bool active = tid < pi.nel;
-  const int e = pi.elem0 + tid;
-  const int nelpad = a.nelpad;
   R F[3][8];
   int lc[8];
   int color = -1;
   unsigned long long mykey = ~0ull, mybits = ~0ull;
   double my_ehou = 0.0, my_wpla = 0.0;
   if (active) {
-    const uint4 cw = a.conn[e];
     lc[0] = cw.x & 0xffffu; lc[1] = cw.x >> 16; lc[2] = cw.y & 0xffffu; lc[3] = cw.y >> 16;
     lc[4] = cw.z & 0xffffu; lc[5] = cw.z >> 16; lc[6] = cw.w & 0xffffu; lc[7] = cw.w >> 16;
     color = lc[0] >> COLOR_SHIFT;
@@ -276,7 +293,7 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
     const double C1 = J5 * J9 - J6 * J8, C4 = J6 * J7 - J4 * J9, C7 = J4 * J8 - J5 * J7;
     double det = (1.0 / 64.0) * (J1 * C1 + J2 * C4 + J3 * C7);
     if (!(det > 0.0)) {   // SCHKJABT3: zero or negative volume stops the run
-      raise_error(a.err, 4, a.elem_id[e]);
+      raise_error(a.err, 4, st_eid);
       det = 1.0;
     }
     const double dett = (1.0 / 64.0) / det;
@@ -350,11 +367,11 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
     const R WZZ = DT1D2 * (DYX - DXY), WYY = DT1D2 * (DXZ - DZX), WXX = DT1D2 * (DZY - DYZ);
     // ---- SRHO3 (srho3.F:122-156; FP64 volume ratios in the split form, srho3.F:230-245) ----
     const R RHO0 = R(gd.rho0);
-    const R rho_old = a.rho[e];
-    const R VOLO = a.vol0[e];
+    const R rho_old = st_rho;
+    const R VOLO = st_vol0;
     R DVOL, RHON, AMU;
     if (split) {
-      const double v0 = a.vol0dp[e];
+      const double v0 = st_vol0dp;
       DVOL = R(VOLN_D - ((double)RHO0 / (double)rho_old) * v0);
       RHON = R((double)RHO0 * (v0 / VOLN_D));
       AMU = R(v0 / VOLN_D - 1.0);
@@ -363,10 +380,10 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
       RHON = RHO0 * (VOLO / VOLN);
       AMU = RHON / RHO0 - R(1);
     }
-    R EINT = a.eint[e] * VOLO;
+    R EINT = st_eint * VOLO;
     // ---- SROTA3 Jaumann rotation (srota3.F:81-91) ----
-    const R S1 = a.sig[0 * nelpad + e], S2 = a.sig[1 * nelpad + e], S3 = a.sig[2 * nelpad + e];
-    const R S4 = a.sig[3 * nelpad + e], S5 = a.sig[4 * nelpad + e], S6 = a.sig[5 * nelpad + e];
+    const R S1 = st_sig[0], S2 = st_sig[1], S3 = st_sig[2];
+    const R S4 = st_sig[3], S5 = st_sig[4], S6 = st_sig[5];
     R SG[6];
     {
       const R q1 = R(2) * S4 * WZZ, q2 = R(2) * S6 * WYY, q3 = R(2) * S5 * WXX;
@@ -378,7 +395,7 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
       SG[5] = S6 + WYY * (S3 - S1) + WXX * S4 - WZZ * S5;
     }
     const R VOL_AVG = VOLN - R(0.5) * DVOL;
-    const R QOLD = a.qvis[e];
+    const R QOLD = st_qvis;
     // ---- elastic predictor (m1law.F:124-140 / m2law.F:187-200) ----
     const R OFF = R(1);
     const R Gs = R(gd.shear) * OFF;
@@ -404,7 +421,7 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
         a.epsd[e] = ssqrt(DXX * DXX + DYY * DYY + DZZ * DZZ + R(2) * (e4 * e4 + e5 * e5 + e6 * e6));
       }
       const R CA = R(gd.jc_a), CB = R(gd.jc_b), CN = R(gd.jc_n);
-      R EPXE = a.pla[e];
+      R EPXE = st_pla;
       R AK, QH;
       if (CN == R(1)) { AK = CA + CB * EPXE; QH = CB; }
       else if (EPXE > R(0)) {
@@ -439,9 +456,9 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
       R SSP_EQ = QX + ssqrt(QX * QX + SSP * SSP);
       SSP_EQ = SSP_EQ > R(EM20) ? SSP_EQ : R(EM20);
       const R DTX = R(gd.dtfac) * (DELTAX / SSP_EQ);
-      if ((double)DTX <= gd.dtmin) raise_error(a.err, 5, a.elem_id[e]);
+      if ((double)DTX <= gd.dtmin) raise_error(a.err, 5, st_eid);
       const double dtd = (double)DTX;
-      mykey = dt_key(dtd, 1, a.elem_id[e]);
+      mykey = dt_key(dtd, 1, st_eid);
       mybits = (unsigned long long)__double_as_longlong(dtd);
     }
     // ---- pressure and internal energy (m1law.F:172-190 / m2law.F:434-461) ----
@@ -566,7 +583,9 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
 // Per element (thread): CCOOR3, CNVEC3, CDERI3, CCOEF3, CDLEN3, CDEFO3, CCURV3,
 // CSTRA3, MULAWC (SIGEPS01C / SIGEPS02C -> M2CPLR per integration point),
 // CHVIS3, CDT3, CFINT3; forces and moments into shared memory (CUPDT3P signs).
-template <class R, int TILE>
+// NPT > 0: every group of the launch has NPT integration points and the
+// integration-point state is loaded up front; NPT = 0: generic 1..10 points.
+template <class R, int TILE, int NPT>
 __global__ void __launch_bounds__(TILE)
 shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
   typedef typename Vec4<R>::T R4;
@@ -582,6 +601,34 @@ shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
   double* sy = sx + nl;
   double* sz = sy + nl;
   R* sv = reinterpret_cast<R*>(sz + nl);   // vx vy vz rx ry rz fx fy fz mx my mz: 12 planes
+  const bool active = tid < pi.nel;
+  const int e = pi.elem0 + tid;
+  const int nelpad = a.nelpad;
+  // per-element loads issued before the staging barrier (overlap with the gathers)
+  constexpr int NP = NPT > 0 ? NPT : 1;
+  uint2 cw = make_uint2(0, 0);
+  R st_thk = R(1), st_thke = R(1), st_h0 = R(0), st_h1 = R(0), st_h2 = R(0), st_e0 = R(0), st_e1 = R(0);
+  R st_jca = R(0);
+  R st_sig[NP][5], st_pla[NP];
+  int st_degen = 0, st_eid = 0;
+  if (active) {
+    cw = a.conn[e];
+    st_thk = a.thk[e];
+    st_thke = a.thke[e];
+    st_h0 = a.hourg[0 * nelpad + e]; st_h1 = a.hourg[1 * nelpad + e]; st_h2 = a.hourg[2 * nelpad + e];
+    st_e0 = a.eint[0 * nelpad + e]; st_e1 = a.eint[1 * nelpad + e];
+    if (gd.has_jca) st_jca = a.jca[e];
+    st_degen = a.degen[e];
+    st_eid = a.elem_id[e];
+    if (NPT > 0) {
+#pragma unroll
+      for (int ip = 0; ip < NP; ++ip) {
+#pragma unroll
+        for (int c = 0; c < 5; ++c) st_sig[ip][c] = a.sig[(ip * 5 + c) * nelpad + e];
+        st_pla[ip] = gd.law == 2 ? a.pla[ip * nelpad + e] : R(0);
+      }
+    }
+  }
   for (int j = tid; j < nl; j += TILE) {
     const int g = a.patch_nodes[pi.node_ofs + j];
     const double4 xx = a.X[g];
@@ -597,16 +644,12 @@ shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
   const R DT1 = R(tm.dt2);
   __syncthreads();
 
-  const bool active = tid < pi.nel;
-  const int e = pi.elem0 + tid;
-  const int nelpad = a.nelpad;
   int lc[4];
   int color = -1;
   R Fg[3][4], Mg[3][4];
   unsigned long long mykey = ~0ull, mybits = ~0ull;
   double my_ehou = 0.0, my_wpla = 0.0;
   if (active) {
-    const uint2 cw = a.conn[e];
     lc[0] = cw.x & 0xffffu; lc[1] = cw.x >> 16; lc[2] = cw.y & 0xffffu; lc[3] = cw.y >> 16;
     color = lc[0] >> COLOR_SHIFT;
     lc[0] &= LOCAL_MASK;
@@ -650,13 +693,13 @@ shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
     AREA = AREA > R(EM20) ? AREA : R(EM20);
     const R VHX = (-X2 + X3 - X4) / AREA, VHY = (-Y2 + Y3 - Y4) / AREA;
     // ---- CCOEF3 (ccoef3.F:66-160) ----
-    const R THK0 = gd.ithk > 0 ? a.thk[e] : a.thke[e];
+    const R THK0 = gd.ithk > 0 ? st_thk : st_thke;
     const R VOL0 = THK0 * AREA;
     const R THK02 = THK0 * THK0;
     const R RHO = R(gd.rho0), YM = R(gd.young), NU = R(gd.nu), GG = R(gd.shear);
     const R A11 = R(gd.a11), A12 = R(gd.a12), SSP = R(gd.ssp);
     const R H1 = R(gd.hm), H2 = R(gd.hf), H3 = R(gd.hr);
-    const int npt = gd.npt;
+    const int npt = NPT > 0 ? NPT : gd.npt;
     const R SHF = npt == 1 ? R(0) : R(gd.shf);
     const R GS = GG * SHF;
     // ---- CDLEN3 (cdlen3.F:69-121) ----
@@ -729,15 +772,22 @@ shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
     const float* WM = Z0 + 22;
     R FOR[5] = {R(0), R(0), R(0), R(0), R(0)}, MOM[3] = {R(0), R(0), R(0)};
     R FOLD[5] = {R(0), R(0), R(0), R(0), R(0)}, MOLD[3] = {R(0), R(0), R(0)};
-    R THKN = a.thk[e];
-    const R CA = gd.has_jca ? a.jca[e] : R(gd.jc_a);
+    R THKN = st_thk;
+    const R CA = gd.has_jca ? st_jca : R(gd.jc_a);
     const R CB = R(gd.jc_b), CN = R(gd.jc_n), YMAX = R(gd.sigmax);
     double wpla = 0.0;
-    for (int ip = 0; ip < npt; ++ip) {
+#pragma unroll
+    for (int ip = 0; ip < (NPT > 0 ? NPT : 10); ++ip) {
+      if (NPT == 0 && ip >= npt) break;
       const R wf = R(WF[ip]), wm = R(WM[ip]);
       R SO[5], SN[5];
+      if (NPT > 0) {
 #pragma unroll
-      for (int c = 0; c < 5; ++c) SO[c] = a.sig[(ip * 5 + c) * nelpad + e];
+        for (int c = 0; c < 5; ++c) SO[c] = st_sig[NPT > 0 ? ip : 0][c];
+      } else {
+#pragma unroll
+        for (int c = 0; c < 5; ++c) SO[c] = a.sig[(ip * 5 + c) * nelpad + e];
+      }
 #pragma unroll
       for (int c = 0; c < 5; ++c) FOLD[c] = FOLD[c] + wf * SO[c];
 #pragma unroll
@@ -762,7 +812,7 @@ shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
         SN[2] = SO[2] + GG * DXY;
         SN[3] = SO[3] + GS * EYZ;
         SN[4] = SO[4] + GS * EXZ;
-        R PLA = a.pla[ip * nelpad + e];
+        R PLA = NPT > 0 ? st_pla[NPT > 0 ? ip : 0] : a.pla[ip * nelpad + e];
         R YLD = PLA == R(0) ? CA : CA + CB * exp_(CN * log_(PLA));
         YLD = fmin(YLD, YMAX);
         const R SVM = ssqrt(SN[0] * SN[0] + SN[1] * SN[1] - SN[0] * SN[1] + R(3) * SN[2] * SN[2]);
@@ -795,8 +845,8 @@ shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
       const R DEGFX = MOLD[0] * KXX + MOLD[1] * KYY + MOLD[2] * KXY +
                       (MOM[0] * KXX + MOM[1] * KYY + MOM[2] * KXY);
       const R VOL2 = R(0.5) * VOL0;
-      a.eint[0 * nelpad + e] = a.eint[0 * nelpad + e] + DEGMB * VOL2;
-      a.eint[1 * nelpad + e] = a.eint[1 * nelpad + e] + DEGFX * THK0 * VOL2;
+      a.eint[0 * nelpad + e] = st_e0 + DEGMB * VOL2;
+      a.eint[1 * nelpad + e] = st_e1 + DEGFX * THK0 * VOL2;
     }
     // ---- CHVIS3, ISMSTR = 2, IHBE = 1, HELAS = HVISC = 1/2, HVLIN = 0 (chvis3.F:116-300) ----
     R H1j[3], H2j[3], H3j[3], HOUR4, HOUR5;
@@ -820,18 +870,18 @@ shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
       R HH1 = A7c * TD;
       const R B1 = PX1 * PX1 + PY1 * PY1, B2 = PX2 * PX2 + PY2 * PY2;
       R HH2 = A8c * THK02 * TD / (B1 + B2);
-      if (a.degen[e]) { H1Q = H2Q = H3Q = HH1 = HH2 = R(0); }
+      if (st_degen) { H1Q = H2Q = H3Q = HH1 = HH2 = R(0); }
       R HG1 = VXl[0] * GAMA[0] + VXl[1] * GAMA[1] + VXl[2] * GAMA[2] + VXl[3] * GAMA[3];
       R HG2 = VYl[0] * GAMA[0] + VYl[1] * GAMA[1] + VYl[2] * GAMA[2] + VYl[3] * GAMA[3];
-      const R hour1 = a.hourg[0 * nelpad + e] + HG1 * HH1;
-      const R hour2 = a.hourg[1 * nelpad + e] + HG2 * HH1;
+      const R hour1 = st_h0 + HG1 * HH1;
+      const R hour2 = st_h1 + HG2 * HH1;
       const R HOUR1A = hour1 + HG1 * (H1Q * fabs(HG1));
       const R HOUR2A = hour2 + HG2 * (H1Q * fabs(HG2));
 #pragma unroll
       for (int k = 0; k < 3; ++k) { H1j[k] = HOUR1A * GAMA[k]; H2j[k] = HOUR2A * GAMA[k]; }
       R EHOU = HOUR1A * HG1 + HOUR2A * HG2;
       HG1 = VZl[0] * GAMA[0] + VZl[1] * GAMA[1] + VZl[2] * GAMA[2] + VZl[3] * GAMA[3];
-      const R hour3 = a.hourg[2 * nelpad + e] + HG1 * HH2;
+      const R hour3 = st_h2 + HG1 * HH2;
       const R HOUR3A = hour3 + HG1 * (H2Q * fabs(HG1));
 #pragma unroll
       for (int k = 0; k < 3; ++k) H3j[k] = HOUR3A * GAMA[k];
@@ -847,8 +897,8 @@ shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
     // ---- CDT3 (cdt3.F:110-115, 203-214) ----
     {
       const R DT = R(gd.dtfac) * ALDT / SSP;
-      if ((double)DT <= gd.dtmin) raise_error(a.err, 5, a.elem_id[e]);
-      mykey = dt_key((double)DT, 3, a.elem_id[e]);
+      if ((double)DT <= gd.dtmin) raise_error(a.err, 5, st_eid);
+      mykey = dt_key((double)DT, 3, st_eid);
       mybits = (unsigned long long)__double_as_longlong((double)DT);
     }
     // ---- CFINT3, ISIGI = 0 (cfint3.F:173-260) ----
@@ -931,13 +981,38 @@ __global__ void __launch_bounds__(TILE)
 node_kernel(NodeArgs<R> a, int parity) {
   typedef typename Vec4<R>::T R4;
   __shared__ double s_e0[TILE / 32], s_e1[TILE / 32];
+  const int* __restrict__ adsky = a.adsky;
+  const R4* __restrict__ fslot = a.fslot;
+  const R4* __restrict__ mslot = a.mslot;
+  double4* __restrict__ X = a.X;
+  R4* __restrict__ V = a.V;
+  R4* __restrict__ VR = a.VR;
+  double* __restrict__ DX = a.DX;
+  double* __restrict__ DY = a.DY;
+  double* __restrict__ DZ = a.DZ;
+  const unsigned char* __restrict__ codes = a.code;
   for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
     const int part = a.tile_part[tile];
     const PartDesc pd = a.parts[part];
+    const int n = tile * TILE + threadIdx.x;
+    const bool valid = n < pd.node_end;
+    // node loads first: independent of the dt logic below
+    int k0 = 0, k1 = 0;
+    double4 xm = make_double4(0, 0, 0, 0);
+    R4 v = mk4(R(0), R(0), R(0), R(0));
+    double dx = 0, dy = 0, dz = 0;
+    unsigned char code = 0;
+    if (valid) {
+      k0 = adsky[n]; k1 = adsky[n + 1];
+      xm = X[n]; v = V[n]; code = codes[n];
+      dx = DX[n]; dy = DY[n]; dz = DZ[n];
+    }
+    R4 f0 = mk4(R(0), R(0), R(0), R(0));
+    if (valid && k1 > k0) f0 = fslot[k0];
     const PartTime t0 = a.time[parity * a.nparts + part];
     const PartAcc ac = a.acc[parity * a.nparts + part];
-    // dt logic, identical in every thread
-    double dt2t = __longlong_as_double((long long)ac.dtbits);
+    // dt logic (resol.F:5853-5858, 6080, 6224-6226), identical in every thread
+    const double dt2t = __longlong_as_double((long long)ac.dtbits);
     double DT2 = 1e6;                                  // EP06
     int ityp = t0.ityptst, nelt = t0.neltst;
     if (ac.dtbits != ~0ull && dt2t < DT2) {
@@ -951,26 +1026,14 @@ node_kernel(NodeArgs<R> a, int parity) {
     if (a.split) DT2 = (double)(float)DT2;
     const double DT1 = t0.dt2;
     const double DT12 = 0.5 * (DT1 + DT2);
-    if (tile == pd.tile_start && threadIdx.x == 0) {
-      PartTime t1;
-      t1.tt = t0.tt + DT2; t1.dt2 = DT2; t1.dt2old = DT2; t1.dt1 = DT1; t1.dt12 = DT12;
-      t1.ncycle = t0.ncycle + 1; t1.ityptst = ityp; t1.neltst = nelt; t1.pad = 0;
-      a.time[(1 - parity) * a.nparts + part] = t1;
-      PartAcc r; r.dtkey = ~0ull; r.dtbits = ~0ull;
-      a.acc[(1 - parity) * a.nparts + part] = r;
-    }
-    const int n = tile * TILE + threadIdx.x;
     double ek = 0.0, ekr = 0.0;
-    if (n < pd.node_end) {
-      R ax = R(0), ay = R(0), az = R(0), rx = R(0), ry = R(0), rz = R(0);
-      const int k0 = a.adsky[n], k1 = a.adsky[n + 1];
-      for (int k = k0; k < k1; ++k) {
-        const R4 f = a.fslot[k];
+    if (valid) {
+      // ASSPAR4: the node's patch partials in ascending patch order
+      R ax = f0.x, ay = f0.y, az = f0.z;
+      for (int k = k0 + 1; k < k1; ++k) {
+        const R4 f = fslot[k];
         ax += f.x; ay += f.y; az += f.z;
       }
-      const double4 xm = a.X[n];
-      R4 v = a.V[n];
-      const unsigned char code = a.code[n];
       // ACCELE (accele.F:63-80)
       const R ms = R(xm.w);
       if (ms > R(0)) { const R r = R(1) / ms; ax *= r; ay *= r; az *= r; }
@@ -989,17 +1052,18 @@ node_kernel(NodeArgs<R> a, int parity) {
       // VELOCITY (velocity.F:56-62)
       const R dt12 = R(DT12);
       v.x = v.x + dt12 * ax; v.y = v.y + dt12 * ay; v.z = v.z + dt12 * az;
-      a.V[n] = v;
+      V[n] = v;
       // DEPLA (displacement.F:69-100), FP64 accumulation
       const double ux = DT2 * (double)v.x, uy = DT2 * (double)v.y, uz = DT2 * (double)v.z;
-      a.DX[n] += ux; a.DY[n] += uy; a.DZ[n] += uz;
-      a.X[n] = make_double4(xm.x + ux, xm.y + uy, xm.z + uz, xm.w);
+      DX[n] = dx + ux; DY[n] = dy + uy; DZ[n] = dz + uz;
+      X[n] = make_double4(xm.x + ux, xm.y + uy, xm.z + uz, xm.w);
       if (pd.has_rot) {
+        R4 w = VR[n];
+        R rx = R(0), ry = R(0), rz = R(0);
         for (int k = k0; k < k1; ++k) {
-          const R4 m = a.mslot[k];
+          const R4 m = mslot[k];
           rx += m.x; ry += m.y; rz += m.z;
         }
-        R4 w = a.VR[n];
         const R in = w.w;
         if (in > R(0)) { const R r = R(1) / in; rx *= r; ry *= r; rz *= r; }
         else { rx = ry = rz = R(0); }
@@ -1010,7 +1074,7 @@ node_kernel(NodeArgs<R> a, int parity) {
                      wz = (double)w.z + dt05 * (double)rz;
         ekr = (wx * wx + wy * wy + wz * wz) * 0.5 * (double)in;
         w.x = w.x + dt12 * rx; w.y = w.y + dt12 * ry; w.z = w.z + dt12 * rz;
-        a.VR[n] = w;
+        VR[n] = w;
       }
     }
     // per-tile kinetic energy partials (fixed tree order -> deterministic)
@@ -1027,6 +1091,14 @@ node_kernel(NodeArgs<R> a, int parity) {
       for (int w = 0; w < TILE / 32; ++w) { s0 += s_e0[w]; s1 += s_e1[w]; }
       a.blk_ekin[tile] = s0;
       a.blk_ekinr[tile] = s1;
+      if (tile == pd.tile_start) {
+        PartTime t1;
+        t1.tt = t0.tt + DT2; t1.dt2 = DT2; t1.dt2old = DT2; t1.dt1 = DT1; t1.dt12 = DT12;
+        t1.ncycle = t0.ncycle + 1; t1.ityptst = ityp; t1.neltst = nelt; t1.pad = 0;
+        a.time[(1 - parity) * a.nparts + part] = t1;
+        PartAcc r; r.dtkey = ~0ull; r.dtbits = ~0ull;
+        a.acc[(1 - parity) * a.nparts + part] = r;
+      }
     }
     __syncthreads();
   }
