@@ -210,12 +210,44 @@ __device__ inline void block_reduce(unsigned long long& key, unsigned long long&
 }
 
 // ===========================================================================
+// register budgets of the patch kernels
+// ===========================================================================
+// Resident 128-thread CTAs per SM each patch kernel is compiled for (the
+// minimum-blocks argument of __launch_bounds__, scaled to the tile).  The
+// kernels are issue/latency-bound with ~170-255 live registers unbounded, so
+// more resident warps pay for the spilled registers (which stay in L1); the
+// defaults are the fastest caps of a sweep on B200: hexa FP32 6 CTAs (80
+// registers), shell FP32 3 (168), hexa FP64 4 (128), shell FP64 3 (168).
+#ifndef ORB_HEX_CTAS_F32
+#define ORB_HEX_CTAS_F32 6
+#endif
+#ifndef ORB_SHELL_CTAS_F32
+#define ORB_SHELL_CTAS_F32 3
+#endif
+#ifndef ORB_HEX_CTAS_F64
+#define ORB_HEX_CTAS_F64 4
+#endif
+#ifndef ORB_SHELL_CTAS_F64
+#define ORB_SHELL_CTAS_F64 3
+#endif
+template <class R> struct Occupancy;
+template <> struct Occupancy<float> {
+  static constexpr int hex = ORB_HEX_CTAS_F32, shell = ORB_SHELL_CTAS_F32;
+};
+template <> struct Occupancy<double> {
+  static constexpr int hex = ORB_HEX_CTAS_F64, shell = ORB_SHELL_CTAS_F64;
+};
+__host__ __device__ constexpr int min_blocks(int ctas128, int tile) {
+  return ctas128 * 128 / tile > 0 ? ctas128 * 128 / tile : 1;
+}
+
+// ===========================================================================
 // hexa patch kernel
 // ===========================================================================
 // Per element (thread): SCOOR3, SDERI3, SDLEN3, SDEFO3, SRHO3, SROTA3, MMAIN ->
 // M1LAW / M2LAW -> MQVISCB, SHVIS3, SFINT3; corner forces into shared memory.
 template <class R, int TILE>
-__global__ void __launch_bounds__(TILE)
+__global__ void __launch_bounds__(TILE, min_blocks(Occupancy<R>::hex, TILE))
 hex_patch_kernel(HexArgs<R> a, int parity) {
   typedef typename Vec4<R>::T R4;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -586,7 +618,7 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
 // NPT > 0: every group of the launch has NPT integration points and the
 // integration-point state is loaded up front; NPT = 0: generic 1..10 points.
 template <class R, int TILE, int NPT>
-__global__ void __launch_bounds__(TILE)
+__global__ void __launch_bounds__(TILE, min_blocks(Occupancy<R>::shell, TILE))
 shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
   typedef typename Vec4<R>::T R4;
   extern __shared__ __align__(16) unsigned char smem_raw[];
