@@ -1,7 +1,7 @@
 """Runs a workload for a few eager cycles (one launch per kernel per cycle, no
 CUDA graph) and prints per-phase device times; the command profiled by ncu.
 
-    python -m openradioss_b200.profile_run --workload shell_plate --cycles 20 [--n 600]
+    python -m openradioss_b200.profile_run --workload shell_plate --cycles 20 [--n 600] [--tile 128]
 """
 from __future__ import annotations
 
@@ -25,11 +25,13 @@ def main():
     ap.add_argument("--n", type=int, default=0, help="mesh size parameter (0 = workload default)")
     ap.add_argument("--cycles", type=int, default=20)
     ap.add_argument("--precision", default="split", choices=["split", "fp64"])
+    ap.add_argument("--tile", type=int, default=0, help="elements per patch (0 = library default)")
     a = ap.parse_args()
     build.build()
     d = FACTORIES[a.workload](a.n)
     prec = abi.OR_PREC_SPLIT if a.precision == "split" else abi.OR_PREC_FP64
-    h = ECycle(d, precision=prec, graph=0)
+    tiles = dict(block_hex=a.tile, block_shell=a.tile) if a.tile else {}
+    h = ECycle(d, precision=prec, graph=0, **tiles)
     h.step(a.cycles)
     print(json.dumps({"workload": a.workload, "elements": decks.num_elements(d), "cycles": a.cycles,
                       "phase_ms": h.phase_times(), "launches": h.launch_count(), "time": h.time()}))
