@@ -210,6 +210,38 @@ int  or_ecycle_stream(or_ecycle* h, void** stream);
 /* Bytes of device memory held by the handle. */
 int  or_ecycle_device_bytes(or_ecycle* h, long long* bytes);
 
+/* --- adjoint (design sensitivities) -------------------------------------- */
+/* Response of or_ecycle_adjoint:
+     J = w_disp * D(comp) of node `node` of part `part` after the call's cycles
+       + w_plastic * plastic work accumulated by all shell elements over them. */
+typedef struct {
+  int    part;          /* part of the response node                                  */
+  int    node;          /* 0-based node index within the part; < 0: no displacement   */
+  int    comp;          /* 0 = x, 1 = y, 2 = z                                        */
+  int    checkpoint;    /* cycles between state checkpoints (<= 0: 50)                */
+  double w_disp;
+  double w_plastic;
+} or_adjoint_response;
+
+/* Runs ncycles from the current state exactly like or_ecycle_step (the handle
+   ends in the same state, t is updated the same way), then the hand-written
+   reverse of those cycles, and returns J and its gradient with respect to
+   - dJ_dA:   the Johnson-Cook yield A of every shell element (shell groups in
+              add order, elements in IXC order; 0 for LAW1 groups),
+   - dJ_dthk: the thickness of every shell element at the start of the call
+              (the THK state, and THKE where ITHK = 0 makes THKE the one used),
+   - dJ_dms, dJ_din: the nodal masses and rotational inertias (parts in add
+              order, nodes in part order), so that a caller whose masses depend
+              on the thickness adds that chain itself.
+   The time-step sequence of the forward run is held fixed: the gradient is
+   exact when dt does not depend on the parameters, e.g. when DTMX is below
+   every element time step.  The reverse recomputes each segment of
+   r->checkpoint cycles from a stored state.  FP64 handles with shell groups
+   only (OR_E_UNSUPPORTED otherwise).  Any output pointer may be NULL.
+   No counterpart in the reference, which has no adjoint. */
+int  or_ecycle_adjoint(or_ecycle* h, int ncycles, const or_adjoint_response* r, or_ecycle_time* t,
+                       double* J, double* dJ_dA, double* dJ_dthk, double* dJ_dms, double* dJ_din);
+
 /* --- entry point that allocates nothing ---------------------------------- */
 /* No counterpart in the reference.  For callers that cannot let this library
    allocate device memory (for example an engine that reserves one device pool

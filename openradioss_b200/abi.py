@@ -62,6 +62,11 @@ class Energies(C.Structure):
                 ("hourglass", C.c_double), ("plastic_work", C.c_double), ("pad", C.c_double)]
 
 
+class AdjointResponse(C.Structure):
+    _fields_ = [("part", C.c_int), ("node", C.c_int), ("comp", C.c_int), ("checkpoint", C.c_int),
+                ("w_disp", C.c_double), ("w_plastic", C.c_double)]
+
+
 # the growth factor of resol.F:6080 is the default-REAL literal 1.1
 DT_GROWTH_REF = float(__import__("numpy").float32(1.1))
 

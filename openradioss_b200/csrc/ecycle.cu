@@ -25,6 +25,8 @@
 
 #include "../../include/or_ecycle.h"
 #include "ecycle_kernels.cuh"
+#include "adjoint_kernels.cuh"
+#include "coqini_table.h"
 
 using namespace orb;
 
@@ -33,30 +35,6 @@ namespace {
 constexpr int NODE_TILE = 128;
 constexpr int GRAPH_CYCLES = 32;
 
-// through-thickness rules of COQINI (coqini.F:45-130), [npt-1][Z0 | WF | WM]
-const float ZW_TABLE[10][33] = {
-  {0.f, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0,  1.f, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0,  0.f, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0},
-  {-.5f, .5f, 0, 0, 0, 0, 0, 0, 0, 0, 0,  .5f, .5f, 0, 0, 0, 0, 0, 0, 0, 0, 0,  -.0833333f, .0833333f, 0, 0, 0, 0, 0, 0, 0, 0, 0},
-  {-.5f, 0.f, .5f, 0, 0, 0, 0, 0, 0, 0, 0,  .25f, .5f, .25f, 0, 0, 0, 0, 0, 0, 0, 0,  -.0833333f, 0.f, .0833333f, 0, 0, 0, 0, 0, 0, 0, 0},
-  {-.5f, -.1666667f, .1666667f, .5f, 0, 0, 0, 0, 0, 0, 0,  .1666667f, .3333333f, .3333333f, .1666667f, 0, 0, 0, 0, 0, 0, 0,
-   -.0648148f, -.0555556f, .0555556f, .0648148f, 0, 0, 0, 0, 0, 0, 0},
-  {-.5f, -.25f, 0.f, .25f, .5f, 0, 0, 0, 0, 0, 0,  .125f, .25f, .25f, .25f, .125f, 0, 0, 0, 0, 0, 0,
-   -.0520833f, -.0625f, 0.f, .0625f, .0520833f, 0, 0, 0, 0, 0, 0},
-  {-.5f, -.3f, -.1f, .1f, .3f, .5f, 0, 0, 0, 0, 0,  .1f, .2f, .2f, .2f, .2f, .1f, 0, 0, 0, 0, 0,
-   -.0433333f, -.06f, -.02f, .02f, .06f, .0433333f, 0, 0, 0, 0, 0},
-  {-.5f, -.3333333f, -.1666667f, 0.f, .1666667f, .3333333f, .5f, 0, 0, 0, 0,
-   .0833333f, .1666667f, .1666667f, .1666667f, .1666667f, .1666667f, .0833333f, 0, 0, 0, 0,
-   -.037037f, -.0555556f, -.0277778f, 0.f, .0277778f, .0555556f, .037037f, 0, 0, 0, 0},
-  {-.5f, -.3571429f, -.2142857f, -.0714286f, .0714286f, .2142857f, .3571429f, .5f, 0, 0, 0,
-   .0714286f, .1428571f, .1428571f, .1428571f, .1428571f, .1428571f, .1428571f, .0714286f, 0, 0, 0,
-   -.0323129f, -.0510204f, -.0306122f, -.0102041f, .0102041f, .0306122f, .0510204f, .0323129f, 0, 0, 0},
-  {-.5f, -.375f, -.25f, -.125f, 0.f, .125f, .25f, .375f, .5f, 0, 0,
-   .0625f, .125f, .125f, .125f, .125f, .125f, .125f, .125f, .0625f, 0, 0,
-   -.0286458f, -.046875f, -.03125f, -.015625f, 0.f, .015625f, .03125f, .046875f, .0286458f, 0, 0},
-  {-.5f, -.3888889f, -.2777778f, -.1666667f, -.0555555f, .0555555f, .1666667f, .2777778f, .3888889f, .5f, 0,
-   .0555556f, .1111111f, .1111111f, .1111111f, .1111111f, .1111111f, .1111111f, .1111111f, .1111111f, .0555556f, 0,
-   -.0257202f, -.0432099f, -.0308642f, -.0185185f, -.0061728f, .0061728f, .0185185f, .0308642f, .0432099f, .0257202f, 0},
-};
 
 // ----------------------------------------------------------------------------
 // host-side model as uploaded
@@ -112,6 +90,7 @@ struct or_ecycle {
   int tile_hex = 256, tile_shell = 256, tile_node = NODE_TILE;
   // device state
   void* impl = nullptr;
+  void* adj = nullptr;               // adjoint workspace, allocated by the first or_ecycle_adjoint
   double phase_ms[4] = {0, 0, 0, 0};
   long long launches = 0;
   long long dev_bytes = 0;
@@ -921,6 +900,336 @@ void destroy_impl(or_ecycle* h) {
 #define DISPATCH(h, fn, ...) \
   ((h)->cfg.precision == OR_PREC_SPLIT ? fn<float>(h, __VA_ARGS__) : fn<double>(h, __VA_ARGS__))
 
+// ----------------------------------------------------------------------------
+// adjoint of the shell cycle (FP64 handles): checkpointed forward sweep, then
+// per segment a recompute that stores every cycle's start state, then the
+// reverse cycles of the segment from last to first
+// ----------------------------------------------------------------------------
+struct AdjField {
+  void* p;
+  size_t bytes, off;
+};
+
+struct AdjWork {
+  DBuf<AdjGroup> groups; DBuf<int> egroup; DBuf<int4> enodes; DBuf<int> csr_ofs, csr_ent;
+  DBuf<double4> lamX, lamD, lamV, lamVR, lamF, lamM, cX, cV, cR;
+  DBuf<double> dms, din, lsig, lpla, lthk, lhourg, dA, dthke;
+  DBuf<PartTime> tlog;
+  DBuf<unsigned char> ckpt, seg, fin;
+  std::vector<AdjField> full, slot;
+  size_t full_bytes = 0, slot_bytes = 0;
+  int ncap = -1, nck_cap = 0, kcap = 0;
+  void free_all() {
+    dfree(groups); dfree(egroup); dfree(enodes); dfree(csr_ofs); dfree(csr_ent);
+    dfree(lamX); dfree(lamD); dfree(lamV); dfree(lamVR); dfree(lamF); dfree(lamM); dfree(cX); dfree(cV); dfree(cR);
+    dfree(dms); dfree(din); dfree(lsig); dfree(lpla); dfree(lthk); dfree(lhourg); dfree(dA); dfree(dthke);
+    dfree(tlog); dfree(ckpt); dfree(seg); dfree(fin);
+  }
+};
+
+size_t layout_fields(std::vector<AdjField>& f) {
+  size_t off = 0;
+  for (auto& x : f) { x.off = off; off += (x.bytes + 255) / 256 * 256; }
+  return off;
+}
+
+int adj_save(or_ecycle* h, const std::vector<AdjField>& f, unsigned char* buf) {
+  for (const auto& x : f)
+    if (x.bytes) CK(cudaMemcpyAsync(buf + x.off, x.p, x.bytes, cudaMemcpyDeviceToDevice, h->stream));
+  return OR_OK;
+}
+int adj_restore(or_ecycle* h, const std::vector<AdjField>& f, const unsigned char* buf) {
+  for (const auto& x : f)
+    if (x.bytes) CK(cudaMemcpyAsync(x.p, buf + x.off, x.bytes, cudaMemcpyDeviceToDevice, h->stream));
+  return OR_OK;
+}
+
+// device tables and buffers of the adjoint, sized for ncycles / checkpoint
+int adj_prepare(or_ecycle* h, Impl<double>& m, int ncycles, int K) {
+  if (!h->adj) h->adj = new AdjWork();
+  AdjWork& w = *(AdjWork*)h->adj;
+  int rc;
+  const int nn = m.nnodpad, np = m.sps.nelpad;
+  if (!w.groups.p) {
+    std::vector<AdjGroup> gr;
+    for (auto& g : h->shell) {
+      AdjGroup a{};
+      orb_adj::ShellParams& P = a.P;
+      P.law = g.mat.law; P.npt = g.prop.npt; P.ithk = g.prop.ithk; P.degen = 0;
+      P.rho = g.mat.rho0; P.young = g.mat.young; P.nu = g.mat.nu; P.shear = g.mat.shear; P.a11 = g.mat.a11;
+      P.a12 = g.mat.a12; P.jc_b = g.mat.jc_b; P.jc_n = g.mat.jc_n; P.sigmax = g.mat.sigmax;
+      P.hm = g.prop.hm; P.hf = g.prop.hf; P.hr = g.prop.hr; P.shf = g.prop.shf; P.pressure = g.prop.pressure;
+      a.part = g.part; a.has_jca = g.jca.empty() ? 0 : 1; a.jc_a = g.mat.jc_a;
+      gr.push_back(a);
+    }
+    // global corner nodes of each internal element, and the node -> corner CSR
+    std::vector<int4> en(np, make_int4(0, 0, 0, 0));
+    std::vector<int> cnt(nn + 1, 0);
+    for (const PatchInfo& pi : m.sps.info)
+      for (int t = 0; t < pi.nel; ++t) {
+        const int ie = pi.elem0 + t;
+        int g[4];
+        for (int k = 0; k < 4; ++k) {
+          const int l = m.sps.local[(size_t)ie * 4 + k] & LOCAL_MASK;
+          if (l >= pi.nloc) return fail(h, OR_E_STATE, "adjoint: corner outside its patch");
+          g[k] = m.sps.nodes[pi.node_ofs + l];
+          if (g[k] < 0 || g[k] >= nn) return fail(h, OR_E_STATE, "adjoint: corner node out of range");
+          cnt[g[k] + 1]++;
+        }
+        en[ie] = make_int4(g[0], g[1], g[2], g[3]);
+      }
+    for (int n = 0; n < nn; ++n) cnt[n + 1] += cnt[n];
+    std::vector<int> ent(cnt[nn]), nxt(cnt.begin(), cnt.end() - 1);
+    for (int ie = 0; ie < np; ++ie) {
+      if (m.sps.elem_group[ie] < 0) continue;
+      const int g[4] = {en[ie].x, en[ie].y, en[ie].z, en[ie].w};
+      for (int k = 0; k < 4; ++k) ent[nxt[g[k]]++] = 4 * ie + k;
+    }
+    if ((rc = dput(h, w.groups, gr)) || (rc = dput(h, w.egroup, m.sps.elem_group)) || (rc = dput(h, w.enodes, en)) ||
+        (rc = dput(h, w.csr_ofs, cnt)) || (rc = dput(h, w.csr_ent, ent)))
+      return rc;
+    const size_t n4 = (size_t)nn, c4 = 4 * (size_t)np;
+    if ((rc = dalloc(h, w.lamX, n4)) || (rc = dalloc(h, w.lamD, n4)) || (rc = dalloc(h, w.lamV, n4)) ||
+        (rc = dalloc(h, w.lamVR, n4)) || (rc = dalloc(h, w.lamF, n4)) || (rc = dalloc(h, w.lamM, n4)) ||
+        (rc = dalloc(h, w.cX, c4)) || (rc = dalloc(h, w.cV, c4)) || (rc = dalloc(h, w.cR, c4)) ||
+        (rc = dalloc(h, w.dms, n4)) || (rc = dalloc(h, w.din, n4)) || (rc = dalloc(h, w.lsig, m.ssig.n)) ||
+        (rc = dalloc(h, w.lpla, m.spla.n)) || (rc = dalloc(h, w.lthk, (size_t)np)) ||
+        (rc = dalloc(h, w.lhourg, 3 * (size_t)np)) || (rc = dalloc(h, w.dA, (size_t)np)) ||
+        (rc = dalloc(h, w.dthke, (size_t)np)))
+      return rc;
+    // the full state (checkpoints, end state) and the per-cycle slot state
+    w.full = {{m.X.p, m.X.n * sizeof(double4), 0}, {m.DX.p, m.DX.n * sizeof(double), 0},
+              {m.DY.p, m.DY.n * sizeof(double), 0}, {m.DZ.p, m.DZ.n * sizeof(double), 0},
+              {m.V.p, m.V.n * sizeof(double4), 0}, {m.VR.p, m.VR.n * sizeof(double4), 0},
+              {m.ssig.p, m.ssig.n * sizeof(double), 0}, {m.spla.p, m.spla.n * sizeof(double), 0},
+              {m.sthk.p, m.sthk.n * sizeof(double), 0}, {m.shourg.p, m.shourg.n * sizeof(double), 0},
+              {m.seint.p, m.seint.n * sizeof(double), 0}, {m.sehour.p, m.sehour.n * sizeof(double), 0},
+              {m.swpla.p, m.swpla.n * sizeof(double), 0}, {m.ekin.p, m.ekin.n * sizeof(double), 0},
+              {m.ekinr.p, m.ekinr.n * sizeof(double), 0}};
+    w.slot = {{m.X.p, m.X.n * sizeof(double4), 0}, {m.V.p, m.V.n * sizeof(double4), 0},
+              {m.VR.p, m.VR.n * sizeof(double4), 0}, {m.ssig.p, m.ssig.n * sizeof(double), 0},
+              {m.spla.p, m.spla.n * sizeof(double), 0}, {m.sthk.p, m.sthk.n * sizeof(double), 0},
+              {m.shourg.p, m.shourg.n * sizeof(double), 0}};
+    w.full_bytes = layout_fields(w.full);
+    w.slot_bytes = layout_fields(w.slot);
+    if ((rc = dalloc(h, w.fin, w.full_bytes))) return rc;
+  }
+  const int nck = (ncycles + K - 1) / K;
+  if (ncycles > w.ncap) {
+    dfree(w.tlog);
+    if ((rc = dalloc(h, w.tlog, (size_t)(ncycles + 1) * m.nparts))) return rc;
+    w.ncap = ncycles;
+  }
+  if (nck > w.nck_cap) {
+    dfree(w.ckpt);
+    if ((rc = dalloc(h, w.ckpt, (size_t)nck * w.full_bytes))) return rc;
+    w.nck_cap = nck;
+  }
+  if (K > w.kcap) {
+    dfree(w.seg);
+    if ((rc = dalloc(h, w.seg, (size_t)(K + 1) * w.slot_bytes))) return rc;
+    w.kcap = K;
+  }
+  return OR_OK;
+}
+
+int adj_check_error(or_ecycle* h, Impl<double>& m) {
+  ErrorWord ew{};
+  CK(cudaMemcpyAsync(&ew, m.err.p, sizeof(ErrorWord), cudaMemcpyDeviceToHost, h->stream));
+  cudaEvent_t ev;
+  CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  CK(cudaEventRecord(ev, h->stream));
+  int rc = wait_stream(h, ev);
+  cudaEventDestroy(ev);
+  if (rc) return rc;
+  h->last_code = ew.code;
+  h->last_index = ew.index;
+  if (ew.code) {
+    char buf[160];
+    snprintf(buf, sizeof buf, "device error %d at index %d", ew.code, ew.index);
+    return fail(h, ew.code, buf);
+  }
+  return OR_OK;
+}
+
+double adj_plastic_work(or_ecycle* h) {
+  double s = 0.0;
+  for (int p = 0; p < (int)h->parts.size(); ++p) {
+    or_energies e{};
+    if (energies_impl<double>(h, p, &e) == OR_OK) s += e.plastic_work;
+  }
+  return s;
+}
+
+template <int NP>
+int launch_adj_shell(or_ecycle* h, const AdjShellArgs& a) {
+  adj_shell_kernel<NP><<<(unsigned)((a.nelpad + 127) / 128), 128, 0, h->stream>>>(a);
+  CK(cudaGetLastError());
+  h->launches++;
+  return OR_OK;
+}
+
+int adjoint_impl(or_ecycle* h, int N, const or_adjoint_response* r, or_ecycle_time* t, double* J, double* dJ_dA,
+                 double* dJ_dthk, double* dJ_dms, double* dJ_din) {
+  Impl<double>& m = *(Impl<double>*)h->impl;
+  const int K = r->checkpoint > 0 ? r->checkpoint : 50;
+  int rc = adj_prepare(h, m, N, K);
+  if (rc) return rc;
+  AdjWork& w = *(AdjWork*)h->adj;
+  const int np = m.nparts, nn = m.nnodpad, nelpad = m.sps.nelpad;
+  int gnode = -1;
+  if (r->node >= 0) gnode = h->parts[r->part].node_start + r->node;
+  // ---- forward sweep with checkpoints ----
+  std::vector<PartTime> pt(np);
+  for (int p = 0; p < np; ++p) {
+    pt[p].tt = t[p].tt; pt[p].dt2 = t[p].dt2; pt[p].dt2old = t[p].dt2old; pt[p].dt1 = t[p].dt1;
+    pt[p].dt12 = t[p].dt12; pt[p].ncycle = t[p].ncycle; pt[p].ityptst = t[p].ityptst; pt[p].neltst = t[p].neltst;
+    pt[p].pad = 0;
+  }
+  const double wp0 = adj_plastic_work(h);
+  h->launches = 0;
+  CK(cudaMemcpyAsync(m.time.p, pt.data(), np * sizeof(PartTime), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(w.tlog.p, pt.data(), np * sizeof(PartTime), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemsetAsync(m.acc.p, 0xff, np * sizeof(PartAcc), h->stream));
+  CK(cudaMemsetAsync(m.err.p, 0, sizeof(ErrorWord), h->stream));
+  for (int c = 0; c < N; ++c) {
+    if (c % K == 0 && (rc = adj_save(h, w.full, w.ckpt.p + (size_t)(c / K) * w.full_bytes))) return rc;
+    if ((rc = launch_cycle<double>(h, m, c & 1, nullptr))) return rc;
+    CK(cudaMemcpyAsync(w.tlog.p + (size_t)(c + 1) * np, m.time.p + ((c + 1) & 1) * np, np * sizeof(PartTime),
+                       cudaMemcpyDeviceToDevice, h->stream));
+  }
+  if ((rc = adj_save(h, w.full, w.fin.p))) return rc;
+  if ((rc = adj_check_error(h, m))) return rc;
+  const double wp1 = adj_plastic_work(h);
+  double dval = 0.0;
+  if (gnode >= 0) {
+    const double* D = r->comp == 0 ? m.DX.p : r->comp == 1 ? m.DY.p : m.DZ.p;
+    CK(cudaMemcpy(&dval, D + gnode, sizeof(double), cudaMemcpyDeviceToHost));
+  }
+  const double Jval = r->w_disp * dval + r->w_plastic * (wp1 - wp0);
+  // ---- adjoint state at the end ----
+  CK(cudaMemsetAsync(w.lamX.p, 0, nn * sizeof(double4), h->stream));
+  CK(cudaMemsetAsync(w.lamD.p, 0, nn * sizeof(double4), h->stream));
+  CK(cudaMemsetAsync(w.lamV.p, 0, nn * sizeof(double4), h->stream));
+  CK(cudaMemsetAsync(w.lamVR.p, 0, nn * sizeof(double4), h->stream));
+  CK(cudaMemsetAsync(w.dms.p, 0, nn * sizeof(double), h->stream));
+  CK(cudaMemsetAsync(w.din.p, 0, nn * sizeof(double), h->stream));
+  CK(cudaMemsetAsync(w.lsig.p, 0, w.lsig.n * sizeof(double), h->stream));
+  CK(cudaMemsetAsync(w.lpla.p, 0, w.lpla.n * sizeof(double), h->stream));
+  CK(cudaMemsetAsync(w.lthk.p, 0, w.lthk.n * sizeof(double), h->stream));
+  CK(cudaMemsetAsync(w.lhourg.p, 0, w.lhourg.n * sizeof(double), h->stream));
+  CK(cudaMemsetAsync(w.dA.p, 0, w.dA.n * sizeof(double), h->stream));
+  CK(cudaMemsetAsync(w.dthke.p, 0, w.dthke.n * sizeof(double), h->stream));
+  if (gnode >= 0) {
+    const double wd = r->w_disp;
+    CK(cudaMemcpyAsync((double*)(w.lamD.p + gnode) + r->comp, &wd, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));      // wd is a host local
+  }
+  // ---- reverse, segment by segment ----
+  const int nseg = (N + K - 1) / K;
+  const unsigned nb_node = (unsigned)((nn + 127) / 128);
+  const AdjField& fX = w.slot[0];
+  const AdjField& fV = w.slot[1];
+  const AdjField& fVR = w.slot[2];
+  const AdjField& fS = w.slot[3];
+  const AdjField& fP = w.slot[4];
+  const AdjField& fT = w.slot[5];
+  const AdjField& fH = w.slot[6];
+  for (int sg = nseg - 1; sg >= 0; --sg) {
+    const int c0 = sg * K, c1 = std::min(N, c0 + K);
+    if ((rc = adj_restore(h, w.full, w.ckpt.p + (size_t)sg * w.full_bytes))) return rc;
+    CK(cudaMemcpyAsync(m.time.p + (c0 & 1) * np, w.tlog.p + (size_t)c0 * np, np * sizeof(PartTime),
+                       cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemsetAsync(m.acc.p + (c0 & 1) * np, 0xff, np * sizeof(PartAcc), h->stream));
+    for (int c = c0; c < c1; ++c) {
+      if ((rc = adj_save(h, w.slot, w.seg.p + (size_t)(c - c0) * w.slot_bytes))) return rc;
+      if ((rc = launch_cycle<double>(h, m, c & 1, nullptr))) return rc;
+    }
+    if ((rc = adj_save(h, w.slot, w.seg.p + (size_t)(c1 - c0) * w.slot_bytes))) return rc;
+    for (int c = c1 - 1; c >= c0; --c) {
+      unsigned char* s0 = w.seg.p + (size_t)(c - c0) * w.slot_bytes;
+      unsigned char* s1 = s0 + w.slot_bytes;
+      AdjNodeArgs na;
+      na.parts = m.partd.p; na.tile_part = m.tile_part.p; na.code = m.code.p;
+      na.Xn = (const double4*)(s0 + fX.off); na.Vn = (const double4*)(s0 + fV.off);
+      na.Vn1 = (const double4*)(s1 + fV.off); na.VRn = (const double4*)(s0 + fVR.off);
+      na.VRn1 = (const double4*)(s1 + fVR.off); na.tnext = w.tlog.p + (size_t)(c + 1) * np;
+      na.lamX = w.lamX.p; na.lamD = w.lamD.p; na.lamV = w.lamV.p; na.lamVR = w.lamVR.p;
+      na.lamF = w.lamF.p; na.lamM = w.lamM.p; na.dms = w.dms.p; na.din = w.din.p;
+      na.nnodpad = nn; na.node_tile = NODE_TILE;
+      adj_node_pre_kernel<<<nb_node, 128, 0, h->stream>>>(na);
+      CK(cudaGetLastError());
+      AdjShellArgs sa;
+      sa.groups = w.groups.p; sa.egroup = w.egroup.p; sa.enodes = w.enodes.p; sa.degen = m.sdegen.p;
+      sa.Xn = na.Xn; sa.Vn = na.Vn; sa.VRn = na.VRn;
+      sa.sig = (const double*)(s0 + fS.off); sa.pla = (const double*)(s0 + fP.off);
+      sa.thk = (const double*)(s0 + fT.off); sa.thke = m.sthke.p; sa.hourg = (const double*)(s0 + fH.off);
+      sa.jca = m.sjca.p; sa.tcur = w.tlog.p + (size_t)c * np; sa.lamF = w.lamF.p; sa.lamM = w.lamM.p;
+      sa.lsig = w.lsig.p; sa.lpla = w.lpla.p; sa.lthk = w.lthk.p; sa.lhourg = w.lhourg.p; sa.dA = w.dA.p;
+      sa.dthke = w.dthke.p; sa.cX = w.cX.p; sa.cV = w.cV.p; sa.cR = w.cR.p; sa.zw = m.zw.p;
+      sa.w_plastic = r->w_plastic; sa.nelpad = nelpad;
+      rc = m.uniform_npt == 5 ? launch_adj_shell<5>(h, sa) : launch_adj_shell<10>(h, sa);
+      if (rc) return rc;
+      AdjPostArgs pa;
+      pa.ofs = w.csr_ofs.p; pa.ent = w.csr_ent.p; pa.cX = w.cX.p; pa.cV = w.cV.p; pa.cR = w.cR.p;
+      pa.lamX = w.lamX.p; pa.lamV = w.lamV.p; pa.lamVR = w.lamVR.p; pa.nnodpad = nn;
+      adj_node_post_kernel<<<nb_node, 128, 0, h->stream>>>(pa);
+      CK(cudaGetLastError());
+      h->launches += 3;
+    }
+  }
+  // ---- back to the end state of the forward sweep ----
+  if ((rc = adj_restore(h, w.full, w.fin.p))) return rc;
+  CK(cudaMemcpyAsync(m.time.p + (N & 1) * np, w.tlog.p + (size_t)N * np, np * sizeof(PartTime),
+                     cudaMemcpyDeviceToDevice, h->stream));
+  if ((rc = adj_check_error(h, m))) return rc;
+  // ---- outputs in user order ----
+  std::vector<PartTime> tend(np);
+  CK(cudaMemcpy(tend.data(), w.tlog.p + (size_t)N * np, np * sizeof(PartTime), cudaMemcpyDeviceToHost));
+  if (dJ_dA || dJ_dthk) {
+    auto dA = d2h(w.dA.p, (size_t)nelpad);
+    auto dte = d2h(w.dthke.p, (size_t)nelpad);
+    auto lth = d2h(w.lthk.p, (size_t)nelpad);
+    size_t o = 0;
+    for (auto& g : h->shell) {
+      for (int ue = 0; ue < g.nel; ++ue) {
+        const int ie = g.internal[ue];
+        if (dJ_dA) dJ_dA[o + ue] = g.mat.law == OR_LAW_JOHNSON_COOK ? dA[ie] : 0.0;
+        if (dJ_dthk) dJ_dthk[o + ue] = lth[ie] + dte[ie];
+      }
+      o += g.nel;
+    }
+  }
+  if (dJ_dms || dJ_din) {
+    auto dm = d2h(w.dms.p, (size_t)nn);
+    auto di = d2h(w.din.p, (size_t)nn);
+    size_t o = 0;
+    for (auto& P : h->parts) {
+      for (int i = 0; i < P.numnod; ++i) {
+        if (dJ_dms) dJ_dms[o + i] = dm[P.node_start + i];
+        if (dJ_din) dJ_din[o + i] = di[P.node_start + i];
+      }
+      o += P.numnod;
+    }
+  }
+  CK(cudaGetLastError());
+  for (int p = 0; p < np; ++p) {
+    t[p].tt = tend[p].tt; t[p].dt1 = tend[p].dt1; t[p].dt2 = tend[p].dt2; t[p].dt12 = tend[p].dt12;
+    t[p].dt2old = tend[p].dt2old; t[p].ncycle = tend[p].ncycle; t[p].ityptst = tend[p].ityptst;
+    t[p].neltst = tend[p].neltst;
+  }
+  if (J) *J = Jval;
+  return OR_OK;
+}
+
+void adj_destroy(or_ecycle* h) {
+  if (!h->adj) return;
+  AdjWork* w = (AdjWork*)h->adj;
+  w->free_all();
+  delete w;
+  h->adj = nullptr;
+}
+
 bool bad_ptr(const void* p) { return p == nullptr; }
 
 }  // namespace
@@ -954,6 +1263,7 @@ int or_ecycle_destroy(or_ecycle* h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
   if (h->graph) cudaGraphDestroy(h->graph);
+  adj_destroy(h);
   if (h->cfg.precision == OR_PREC_SPLIT) destroy_impl<float>(h); else destroy_impl<double>(h);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
@@ -1099,6 +1409,22 @@ int or_ecycle_step(or_ecycle* h, int ncycles, or_ecycle_time* t) {
   if (ncycles == 0) return OR_OK;
   cudaSetDevice(h->cfg.device);
   return DISPATCH(h, step_impl, ncycles, t);
+}
+
+int or_ecycle_adjoint(or_ecycle* h, int ncycles, const or_adjoint_response* r, or_ecycle_time* t, double* J,
+                      double* dJ_dA, double* dJ_dthk, double* dJ_dms, double* dJ_din) {
+  if (!h) return OR_E_ARG;
+  if (!h->finalized) return fail(h, OR_E_STATE, "adjoint before finalize");
+  if (ncycles <= 0 || !r || !t) return fail(h, OR_E_ARG, "adjoint: bad argument");
+  if (h->cfg.precision != OR_PREC_FP64) return fail(h, OR_E_UNSUPPORTED, "adjoint: FP64 handles only");
+  if (!h->hex.empty() || h->shell.empty()) return fail(h, OR_E_UNSUPPORTED, "adjoint: shell groups only");
+  if (r->node >= 0) {
+    if (r->part < 0 || r->part >= (int)h->parts.size() || r->node >= h->parts[r->part].numnod || r->comp < 0 ||
+        r->comp > 2)
+      return fail(h, OR_E_ARG, "adjoint: response node out of range");
+  }
+  cudaSetDevice(h->cfg.device);
+  return adjoint_impl(h, ncycles, r, t, J, dJ_dA, dJ_dthk, dJ_dms, dJ_din);
 }
 
 int or_ecycle_get_nodes(or_ecycle* h, int part, double* x, double* d, double* v, double* vr) {

@@ -44,7 +44,7 @@ EXPORTS = [
     "or_ecycle_finalize", "or_ecycle_reset", "or_ecycle_step", "or_ecycle_get_nodes", "or_ecycle_set_nodes",
     "or_ecycle_get_hex_state", "or_ecycle_get_shell_state", "or_ecycle_energies",
     "or_ecycle_error_info", "or_ecycle_phase_times", "or_ecycle_launch_count",
-    "or_ecycle_stream", "or_ecycle_device_bytes",
+    "or_ecycle_stream", "or_ecycle_device_bytes", "or_ecycle_adjoint", "or_ecycle_hex_step_noalloc",
 ]
 
 
@@ -75,6 +75,8 @@ def _declare(lib):
         "or_ecycle_launch_count": ([P, C.POINTER(C.c_longlong)], C.c_int),
         "or_ecycle_stream": ([P, C.POINTER(C.c_void_p)], C.c_int),
         "or_ecycle_device_bytes": ([P, C.POINTER(C.c_longlong)], C.c_int),
+        "or_ecycle_adjoint": ([P, C.c_int, C.POINTER(abi.AdjointResponse), C.POINTER(abi.Time), dp, dp, dp, dp, dp],
+                              C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -244,6 +246,25 @@ class ECycle(_DeckModel):
         n = C.c_longlong()
         self._call("device_bytes", C.byref(n))
         return n.value
+
+    def adjoint(self, ncycles, node=-1, comp=2, part=0, w_disp=1.0, w_plastic=0.0, checkpoint=50):
+        """Runs ``ncycles`` like :meth:`step` and the reverse of those cycles
+        (or_ecycle_adjoint).  Returns J = w_disp * D[node, comp] (end of the
+        run) + w_plastic * (plastic work of the run) and its gradient with
+        respect to the shell elements' Johnson-Cook A and initial thickness
+        (one array per shell group) and the nodal masses and rotational
+        inertias (one array per part), the dt sequence held fixed."""
+        nsh = sum(g[1] for g in self.shell_groups)
+        nno = sum(self.numnod(p) for p in range(self.nparts))
+        dA, dthk, dms, din = np.zeros(nsh), np.zeros(nsh), np.zeros(nno), np.zeros(nno)
+        J = C.c_double()
+        r = abi.AdjointResponse(part, node, comp, checkpoint, w_disp, w_plastic)
+        self._call("adjoint", int(ncycles), C.byref(r), self.times, C.byref(J),
+                   *(abi.ptr(a, C.c_double) for a in (dA, dthk, dms, din)))
+        gsplit = np.cumsum([g[1] for g in self.shell_groups])[:-1]
+        nsplit = np.cumsum([self.numnod(p) for p in range(self.nparts)])[:-1]
+        return dict(J=J.value, dA=np.split(dA, gsplit), dthk=np.split(dthk, gsplit),
+                    dms=np.split(dms, nsplit), din=np.split(din, nsplit))
 
     def close(self):
         if getattr(self, "h", None):
