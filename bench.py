@@ -5,10 +5,12 @@
 
 One step = one complete run of the workload (all its cycles) from the uploaded
 initial state; the state is reset between steps outside the timed region and
-L2 is flushed (a 256 MB write) before every timed step.  Under torchrun each
-rank runs its own replica of the workload (independent decks: weak scaling,
-no data-path collective); timing is the max over ranks of device time.
-Prints one JSON line on rank 0.
+L2 is flushed (a 256 MB write) before every timed step.  Under torchrun a deck
+of several independent parts (batched_parts) is sharded: each rank runs its
+share of the parts (largest-first on element count, openradioss_b200/shard.py),
+strong scaling over the fixed deck; a single-mesh deck is replicated, one copy
+per rank (weak scaling).  Neither needs a data-path collective.  Timing is the
+max over ranks of device time.  Prints one JSON line on rank 0.
 """
 from __future__ import annotations
 
@@ -168,6 +170,34 @@ def reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def adjoint_timing(device, ncycles=500, checkpoint=50, reps=3):
+    """Wall time of or_ecycle_adjoint (forward sweep, recompute, reverse) on the
+    C5 plate, and of the same cycles forward only, both FP64 and synchronous."""
+    from openradioss_b200 import abi, adjoint, decks
+    from openradioss_b200.ecycle import ECycle
+    deck = decks.c5_adjoint_plate(ncycles=ncycles)
+    deck["dtmx"] = 1.4e-7                     # dt below every element's: the dt sequence is fixed
+    node = adjoint.centre_node(deck)
+    h = ECycle(deck, precision=abi.OR_PREC_FP64, device=device, graph=1)
+    h.adjoint(ncycles, node=node, w_disp=1.0, w_plastic=1.0, checkpoint=checkpoint)   # allocation, warm-up
+    ta, tf = [], []
+    for _ in range(reps):
+        h.reset()
+        t0 = time.perf_counter()
+        h.adjoint(ncycles, node=node, w_disp=1.0, w_plastic=1.0, checkpoint=checkpoint)
+        ta.append(time.perf_counter() - t0)
+        h.reset()
+        t0 = time.perf_counter()
+        h.step(ncycles)
+        tf.append(time.perf_counter() - t0)
+    nel = decks.num_elements(deck)
+    a, f = min(ta), min(tf)
+    return {"workload": f"C5 plate 200x200, per-element A and thickness, {ncycles} cycles, FP64, "
+                        f"checkpoint every {checkpoint} cycles, responses w(T) + plastic work",
+            "adjoint_ms": a * 1e3, "forward_ms": f * 1e3, "adjoint_over_forward": a / f,
+            "element_cycles_per_s_adjoint": nel * ncycles / a}
+
+
 # ---------------------------------------------------------------------------
 def main():
     args = parse()
@@ -184,13 +214,17 @@ def main():
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
 
-    from openradioss_b200 import abi, build, decks, roofline
+    from openradioss_b200 import abi, build, decks, roofline, shard
     from openradioss_b200.ecycle import ECycle
     build.build()
-    deck = make_deck(args.workload)
+    full = make_deck(args.workload)
+    sharded = world > 1 and len(full["parts"]) > 1
+    deck = shard.rank_deck(full, rank, world) if sharded else full
     cycles = args.cycles or WORKLOADS[args.workload][1]
     nel = decks.num_elements(deck)
     nnod = decks.num_nodes(deck)
+    # element-updates of one step over all ranks
+    nel_job = decks.num_elements(full) if sharded else world * nel
 
     def barrier():
         if world > 1:
@@ -246,23 +280,20 @@ def main():
     if world > 1:
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
     t_split, t_fp64 = float(tt[0]), float(tt[1])
-    value = world * nel * cycles / (t_split * 1e-3)
-    value_fp64 = world * nel * cycles / (t_fp64 * 1e-3)
+    value = nel_job * cycles / (t_split * 1e-3)
+    value_fp64 = nel_job * cycles / (t_fp64 * 1e-3)
 
-    # ---- per-kernel device times (eager launches with CUDA events on the handle's stream) ----
-    hp = ECycle(deck, precision=abi.OR_PREC_SPLIT, device=local, graph=0, block_hex=bh_s, block_shell=bs_s)
-    kcyc = min(cycles, 200)
-    hp.step(kcyc)
-    hp.reset()
-    hp.step(kcyc)
-    ph = hp.phase_times()
-    del hp
+    # ---- per-kernel device times: each phase kernel launched back to back from a
+    # graph on the state a full run leaves, CUDA events on the handle's stream ----
+    hs.reset()
+    hs.step(cycles)
+    kt = hs.kernel_times(reps=64)            # microseconds per launch; resets the handle
     s = 4
     eb_hex = sum(g["ixs"].shape[0] * roofline.hex_bytes(s, g["mat"]["law"]) for p in deck["parts"] for g in p["hex"])
     eb_shell = sum(g["ixc"].shape[0] * roofline.shell_bytes(s, g["prop"]["npt"]) for p in deck["parts"] for g in p["shell"])
     eb, nb, _ = roofline.deck_bytes(deck, s)
     peak, peak_src = roofline.measured_peak()
-    kern = {"hex": (ph["hex"] / kcyc, eb_hex), "shell": (ph["shell"] / kcyc, eb_shell), "node": (ph["node"] / kcyc, nb)}
+    kern = {"hex": (kt["hex"] * 1e-3, eb_hex), "shell": (kt["shell"] * 1e-3, eb_shell), "node": (kt["node"] * 1e-3, nb)}
     dom = max(kern, key=lambda k: kern[k][0])
     dom_ms, dom_bytes = kern[dom]
     traffic = None
@@ -309,7 +340,12 @@ def main():
     te = torch.tensor([sum(e2e_t) / len(e2e_t)], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * nel * cycles / float(te[0])
+    e2e_value = nel_job * cycles / float(te[0])
+
+    # ---- C5: the adjoint on the sensitivity plate (FP64), next to its forward ----
+    adj = None
+    if world == 1 and args.workload == "shell_plate":
+        adj = adjoint_timing(local)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -319,10 +355,13 @@ def main():
         line = {
             "metric": "element-updates/s", "value": value, "unit": "element-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_split, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+            "scaling": "strong" if sharded else "weak", "vs_baseline": None, "dtype": "f32+f64",
             "data": "synthetic (seeded numpy decks with the workload's shapes)",
             "config": {"workload": args.workload, "description": WORKLOADS[args.workload][2],
                        "elements_per_gpu": nel, "nodes_per_gpu": nnod, "cycles_per_step": cycles,
+                       "elements_per_step_all_ranks": nel_job,
+                       "parallelism": (f"parts sharded over {world} ranks" if sharded
+                                       else f"{world} independent replica(s)"),
                        "precision": "split: FP32 element/material math, FP64 X/D/volumes/energies",
                        "l2": "256 MB buffer written before every timed step",
                        "cuda_graph_cycles": 32, "tile_hex": bh_s, "tile_shell": bs_s,
@@ -344,6 +383,8 @@ def main():
             "clocks": clocks,
             "gpu_launches": launches,
         }
+        if adj is not None:
+            line["adjoint"] = adj
         print(json.dumps(line), flush=True)
     del hs
     if world > 1:

@@ -203,6 +203,12 @@ int  or_ecycle_energies(or_ecycle* h, int part, or_energies* e);
 int  or_ecycle_error_info(or_ecycle* h, int* code, int* index);
 /* Per-phase CUDA-event times of the last step, ms: [hex, shell, node, total]. */
 int  or_ecycle_phase_times(or_ecycle* h, double* ms4);
+/* Device time of one launch of each phase kernel, microseconds: [hex, shell,
+   node] (0 for a phase without work).  Each kernel is launched `reps` times
+   back to back from a CUDA graph, replayed between two events, on the state the
+   last step left; the handle is then reset to its uploaded state, as by
+   or_ecycle_reset.  For roofline measurement; no counterpart in the reference. */
+int  or_ecycle_kernel_times(or_ecycle* h, int reps, double* us3);
 /* Number of this library's kernel launches issued by the last step. */
 int  or_ecycle_launch_count(or_ecycle* h, long long* n);
 /* CUDA stream of the handle (cudaStream_t as void*), for event timing. */

@@ -97,6 +97,7 @@ struct or_ecycle {
   cudaGraphExec_t graph_exec = nullptr;
   cudaGraph_t graph = nullptr;
   int last_code = 0, last_index = -1;
+  int next_parity = 0;                // time-buffer parity of the state after the last step
 };
 
 namespace {
@@ -675,26 +676,37 @@ int step_impl(or_ecycle* h, int ncycles, or_ecycle_time* t) {
       h->launches += per;
     }
   }
-  cudaEvent_t ev[4];
+  // eager cycles; without a graph each phase is bracketed by events, read back
+  // once per chunk of cycles so that the host keeps the launch queue full
+  constexpr int TCHUNK = 64;
   const bool timing = !use_graph;
+  std::vector<cudaEvent_t> ev;
   if (timing) {
+    ev.resize(4 * (size_t)std::min(TCHUNK, std::max(1, ncycles - done)));
     for (auto& e : ev) CK(cudaEventCreate(&e));
     for (double& x : h->phase_ms) x = 0;
   }
-  for (; done < ncycles; ++done) {
-    rc = launch_cycle<R>(h, m, done & 1, timing ? ev : nullptr);
-    if (rc) return rc;
-    if (timing) {
-      CK(cudaEventSynchronize(ev[3]));
-      float a, b, c;
-      cudaEventElapsedTime(&a, ev[0], ev[1]);
-      cudaEventElapsedTime(&b, ev[1], ev[2]);
-      cudaEventElapsedTime(&c, ev[2], ev[3]);
-      h->phase_ms[0] += a; h->phase_ms[1] += b; h->phase_ms[2] += c; h->phase_ms[3] += a + b + c;
+  while (done < ncycles) {
+    const int nc = timing ? std::min(TCHUNK, ncycles - done) : ncycles - done;
+    for (int c = 0; c < nc; ++c) {
+      rc = launch_cycle<R>(h, m, (done + c) & 1, timing ? &ev[4 * (size_t)c] : nullptr);
+      if (rc) return rc;
     }
+    if (timing) {
+      CK(cudaEventSynchronize(ev[4 * (size_t)(nc - 1) + 3]));
+      for (int c = 0; c < nc; ++c) {
+        float a, b, d;
+        cudaEventElapsedTime(&a, ev[4 * c], ev[4 * c + 1]);
+        cudaEventElapsedTime(&b, ev[4 * c + 1], ev[4 * c + 2]);
+        cudaEventElapsedTime(&d, ev[4 * c + 2], ev[4 * c + 3]);
+        h->phase_ms[0] += a; h->phase_ms[1] += b; h->phase_ms[2] += d; h->phase_ms[3] += a + b + d;
+      }
+    }
+    done += nc;
   }
-  if (timing) for (auto& e : ev) cudaEventDestroy(e);
+  for (auto& e : ev) cudaEventDestroy(e);
   const int fin = ncycles & 1;
+  h->next_parity = fin;
   CK(cudaMemcpyAsync(pt.data(), m.time.p + fin * np, np * sizeof(PartTime), cudaMemcpyDeviceToHost, h->stream));
   ErrorWord ew{};
   CK(cudaMemcpyAsync(&ew, m.err.p, sizeof(ErrorWord), cudaMemcpyDeviceToHost, h->stream));
@@ -716,6 +728,55 @@ int step_impl(or_ecycle* h, int ncycles, or_ecycle_time* t) {
     return fail(h, ew.code, buf);
   }
   return OR_OK;
+}
+
+// Device time of one launch of each phase kernel: `reps` launches of the same
+// kernel captured back to back in a graph, replayed once between two events
+// on the handle's stream.  The repeated launches advance the state, which is
+// then reset to the uploaded one.
+template <class R>
+int kernel_times_impl(or_ecycle* h, int reps, double* us) {
+  Impl<R>& m = *(Impl<R>*)h->impl;
+  const int parity = h->next_parity;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  int rc = OR_OK;
+  for (int ph = 0; ph < 3 && rc == OR_OK; ++ph) {
+    us[ph] = 0.0;
+    if ((ph == 0 && m.hps.info.empty()) || (ph == 1 && m.sps.info.empty())) continue;
+    auto launch = [&]() -> int {
+      if (ph == 0)
+        return h->tile_hex == 64 ? launch_hex<R, 64>(h, m, parity)
+               : h->tile_hex == 128 ? launch_hex<R, 128>(h, m, parity) : launch_hex<R, 256>(h, m, parity);
+      if (ph == 1)
+        return h->tile_shell == 64 ? launch_shell_npt<R, 64>(h, m, parity)
+               : h->tile_shell == 128 ? launch_shell_npt<R, 128>(h, m, parity) : launch_shell_npt<R, 256>(h, m, parity);
+      return launch_node<R>(h, m, parity);
+    };
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ge = nullptr;
+    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    for (int i = 0; i < reps && rc == OR_OK; ++i) rc = launch();
+    cudaError_t ec = cudaStreamEndCapture(h->stream, &g);
+    if (rc == OR_OK && ec != cudaSuccess) rc = fail(h, OR_E_CUDA, cudaGetErrorString(ec));
+    if (rc == OR_OK && (ec = cudaGraphInstantiate(&ge, g, 0)) != cudaSuccess) rc = fail(h, OR_E_CUDA, cudaGetErrorString(ec));
+    if (rc == OR_OK) {
+      float ms = 0.f;
+      if (cudaGraphLaunch(ge, h->stream) != cudaSuccess || cudaEventRecord(e0, h->stream) != cudaSuccess ||
+          cudaGraphLaunch(ge, h->stream) != cudaSuccess || cudaEventRecord(e1, h->stream) != cudaSuccess ||
+          cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
+        rc = fail(h, OR_E_CUDA, "kernel timing replay");
+      us[ph] = 1e3 * (double)ms / reps;
+    }
+    if (ge) cudaGraphExecDestroy(ge);
+    if (g) cudaGraphDestroy(g);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  h->next_parity = 0;
+  return reset_impl<R>(h);
 }
 
 template <class R>
@@ -1399,6 +1460,7 @@ int or_ecycle_reset(or_ecycle* h) {
   if (!h) return OR_E_ARG;
   if (!h->finalized) return fail(h, OR_E_STATE, "reset before finalize");
   cudaSetDevice(h->cfg.device);
+  h->next_parity = 0;
   return h->cfg.precision == OR_PREC_SPLIT ? reset_impl<float>(h) : reset_impl<double>(h);
 }
 
@@ -1471,6 +1533,14 @@ int or_ecycle_phase_times(or_ecycle* h, double* ms4) {
   if (!h || !ms4) return OR_E_ARG;
   for (int i = 0; i < 4; ++i) ms4[i] = h->phase_ms[i];
   return OR_OK;
+}
+
+int or_ecycle_kernel_times(or_ecycle* h, int reps, double* us3) {
+  if (!h || !us3) return OR_E_ARG;
+  if (!h->finalized) return fail(h, OR_E_STATE, "kernel_times before finalize");
+  if (reps <= 0 || reps > 4096) return fail(h, OR_E_ARG, "kernel_times: reps outside 1..4096");
+  cudaSetDevice(h->cfg.device);
+  return DISPATCH(h, kernel_times_impl, reps, us3);
 }
 
 int or_ecycle_launch_count(or_ecycle* h, long long* n) {

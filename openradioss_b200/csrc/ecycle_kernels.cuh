@@ -1039,8 +1039,12 @@ node_kernel(NodeArgs<R> a, int parity) {
       xm = X[n]; v = V[n]; code = codes[n];
       dx = DX[n]; dy = DY[n]; dz = DZ[n];
     }
-    R4 f0 = mk4(R(0), R(0), R(0), R(0));
+    R4 f0 = mk4(R(0), R(0), R(0), R(0)), m0 = f0, w0 = f0;
     if (valid && k1 > k0) f0 = fslot[k0];
+    if (valid && pd.has_rot) {            // rotational loads issued with the others
+      w0 = VR[n];
+      if (k1 > k0) m0 = mslot[k0];
+    }
     const PartTime t0 = a.time[parity * a.nparts + part];
     const PartAcc ac = a.acc[parity * a.nparts + part];
     // dt logic (resol.F:5853-5858, 6080, 6224-6226), identical in every thread
@@ -1090,9 +1094,9 @@ node_kernel(NodeArgs<R> a, int parity) {
       DX[n] = dx + ux; DY[n] = dy + uy; DZ[n] = dz + uz;
       X[n] = make_double4(xm.x + ux, xm.y + uy, xm.z + uz, xm.w);
       if (pd.has_rot) {
-        R4 w = VR[n];
-        R rx = R(0), ry = R(0), rz = R(0);
-        for (int k = k0; k < k1; ++k) {
+        R4 w = w0;
+        R rx = m0.x, ry = m0.y, rz = m0.z;
+        for (int k = k0 + 1; k < k1; ++k) {
           const R4 m = mslot[k];
           rx += m.x; ry += m.y; rz += m.z;
         }

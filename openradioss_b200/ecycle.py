@@ -45,6 +45,7 @@ EXPORTS = [
     "or_ecycle_get_hex_state", "or_ecycle_get_shell_state", "or_ecycle_energies",
     "or_ecycle_error_info", "or_ecycle_phase_times", "or_ecycle_launch_count",
     "or_ecycle_stream", "or_ecycle_device_bytes", "or_ecycle_adjoint", "or_ecycle_hex_step_noalloc",
+    "or_ecycle_kernel_times",
 ]
 
 
@@ -73,6 +74,7 @@ def _declare(lib):
         "or_ecycle_error_info": ([P, ip, ip], C.c_int),
         "or_ecycle_phase_times": ([P, dp], C.c_int),
         "or_ecycle_launch_count": ([P, C.POINTER(C.c_longlong)], C.c_int),
+        "or_ecycle_kernel_times": ([P, C.c_int, dp], C.c_int),
         "or_ecycle_stream": ([P, C.POINTER(C.c_void_p)], C.c_int),
         "or_ecycle_device_bytes": ([P, C.POINTER(C.c_longlong)], C.c_int),
         "or_ecycle_adjoint": ([P, C.c_int, C.POINTER(abi.AdjointResponse), C.POINTER(abi.Time), dp, dp, dp, dp, dp],
@@ -231,6 +233,16 @@ class ECycle(_DeckModel):
         a = np.zeros(4)
         self._call("phase_times", abi.ptr(a, C.c_double))
         return dict(hex=a[0], shell=a[1], node=a[2], total=a[3])
+
+    def kernel_times(self, reps=64):
+        """Device microseconds of one launch of each phase kernel (hex, shell,
+        node), from graph-replayed back-to-back launches on the current state;
+        the handle is reset afterwards."""
+        a = np.zeros(3)
+        self._call("kernel_times", int(reps), abi.ptr(a, C.c_double))
+        for p in range(self.nparts):
+            self.times[p] = abi.initial_time()
+        return dict(hex=a[0], shell=a[1], node=a[2])
 
     def launch_count(self):
         n = C.c_longlong()

@@ -226,3 +226,19 @@ def test_negative_volume_reports_element(lib):
     assert code == abi.OR_E_NEGVOL
     assert ei.value.code == abi.OR_E_NEGVOL
     assert idx == 5
+
+
+def test_kernel_times_then_reset(lib):
+    """or_ecycle_kernel_times times each phase present in the deck and leaves the
+    handle in its uploaded state: a run after it equals a fresh handle's run."""
+    from openradioss_b200.ecycle import ECycle
+    d = decks.c2_shell_plate(n=16, size=0.016, pressure=5e6)
+    a = ECycle(d, precision=abi.OR_PREC_SPLIT)
+    a.step(40)
+    kt = a.kernel_times(reps=8)
+    assert kt["hex"] == 0.0 and kt["shell"] > 0.0 and kt["node"] > 0.0
+    a.step(40)
+    b = ECycle(d, precision=abi.OR_PREC_SPLIT)
+    b.step(40)
+    assert np.array_equal(a.get_nodes()["d"], b.get_nodes()["d"])
+    assert a.time() == b.time()
