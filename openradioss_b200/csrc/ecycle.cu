@@ -132,6 +132,15 @@ int dput(or_ecycle* h, DBuf<T>& b, const std::vector<T>& v) {
 }
 template <class T> void dfree(DBuf<T>& b) { if (b.p) cudaFree(b.p); b.p = nullptr; b.n = 0; }
 
+// check the kernels' compile-time 5-point rule against the shared table
+constexpr bool coq5_matches_table() {
+  for (int q = 0; q < 3; ++q)
+    for (int ip = 0; ip < 5; ++ip)
+      if (coq5(q, ip) != ZW_TABLE[4][11 * q + ip]) return false;
+  return true;
+}
+static_assert(coq5_matches_table(), "5-point rule constants differ from COQINI's table");
+
 uint64_t morton3(uint32_t x, uint32_t y, uint32_t z) {
   auto spread = [](uint64_t v) {
     v &= 0x1fffff;
@@ -245,6 +254,22 @@ int build_patches(or_ecycle* h, std::vector<GroupT>& groups, int tile, PatchSet&
   return OR_OK;
 }
 
+// Patch node and slot lists at a fixed stride of nlmax entries per patch; the
+// padding repeats the patch's first node (a valid address) with slot -1.
+void padded_lists(const PatchSet& ps, std::vector<int>& nodes, std::vector<int>& slots) {
+  const size_t np = ps.info.size(), L = (size_t)ps.nlmax;
+  nodes.assign(np * L, 0);
+  slots.assign(np * L, -1);
+  for (size_t p = 0; p < np; ++p) {
+    const PatchInfo& pi = ps.info[p];
+    for (int j = 0; j < (int)L; ++j) {
+      const int src = pi.node_ofs + (j < pi.nloc ? j : 0);
+      nodes[p * L + j] = ps.nodes[src];
+      if (j < pi.nloc) slots[p * L + j] = ps.slots[src];
+    }
+  }
+}
+
 // ----------------------------------------------------------------------------
 // device model, templated on the element precision
 // ----------------------------------------------------------------------------
@@ -280,7 +305,7 @@ struct Impl {
     a.sig = hsig.p; a.eint = heint.p; a.rho = hrho.p; a.qvis = hqvis.p; a.pla = hpla.p; a.epsd = hepsd.p;
     a.vol0 = hvol0.p; a.vol0dp = hvol0dp.p; a.fslot = fslot.p; a.time = time.p; a.acc = acc.p;
     a.blk_ehour = hehour.p; a.blk_wpla = hwpla.p; a.err = err.p;
-    a.nelpad = hps.nelpad; a.nparts = nparts; a.npatch = (int)hps.info.size();
+    a.nelpad = hps.nelpad; a.nparts = nparts; a.npatch = (int)hps.info.size(); a.nlmax = hps.nlmax;
     return a;
   }
   ShellArgs<R> sargs() {
@@ -291,6 +316,7 @@ struct Impl {
     a.jca = sjca.p; a.fslot = fslot.p; a.mslot = mslot.p; a.time = time.p; a.acc = acc.p;
     a.blk_ehour = sehour.p; a.blk_wpla = swpla.p; a.err = err.p;
     a.nelpad = sps.nelpad; a.nparts = nparts; a.npatch = (int)sps.info.size(); a.maxnpt = maxnpt;
+    a.nlmax = sps.nlmax;
     return a;
   }
   NodeArgs<R> nargs(const or_ecycle* h) {
@@ -499,8 +525,10 @@ int finalize_impl(or_ecycle* h) {
       vol0[ie] = R(g.vol0[ue]);
       vol0dp[ie] = g.vol0[ue];
     }
-    if ((rc = dput(h, m.hpatch, ps.info)) || (rc = dput(h, m.hdesc, desc)) || (rc = dput(h, m.hnodes, ps.nodes)) ||
-        (rc = dput(h, m.hslots, ps.slots)) || (rc = dput(h, m.helem, elem)) || (rc = dput(h, m.hconn, conn)) ||
+    std::vector<int> pn, pslot;
+    padded_lists(ps, pn, pslot);
+    if ((rc = dput(h, m.hpatch, ps.info)) || (rc = dput(h, m.hdesc, desc)) || (rc = dput(h, m.hnodes, pn)) ||
+        (rc = dput(h, m.hslots, pslot)) || (rc = dput(h, m.helem, elem)) || (rc = dput(h, m.hconn, conn)) ||
         (rc = dput(h, m.hrho, rho)) || (rc = dput(h, m.hvol0, vol0)) || (rc = dput(h, m.hvol0dp, vol0dp)))
       return rc;
     std::vector<R> z(np, R(0));
@@ -548,8 +576,10 @@ int finalize_impl(or_ecycle* h) {
       thke[ie] = R(g.thke[ue]);
       if (any_jca) jca[ie] = R(g.jca.empty() ? g.mat.jc_a : g.jca[ue]);
     }
-    if ((rc = dput(h, m.spatch, ps.info)) || (rc = dput(h, m.sdesc, desc)) || (rc = dput(h, m.snodes, ps.nodes)) ||
-        (rc = dput(h, m.sslots, ps.slots)) || (rc = dput(h, m.selem, elem)) || (rc = dput(h, m.sdegen, degen)) ||
+    std::vector<int> pn, pslot;
+    padded_lists(ps, pn, pslot);
+    if ((rc = dput(h, m.spatch, ps.info)) || (rc = dput(h, m.sdesc, desc)) || (rc = dput(h, m.snodes, pn)) ||
+        (rc = dput(h, m.sslots, pslot)) || (rc = dput(h, m.selem, elem)) || (rc = dput(h, m.sdegen, degen)) ||
         (rc = dput(h, m.sconn, conn)) || (rc = dput(h, m.sthke, thke)) || (rc = dput(h, m.sthk, thke)) ||
         (rc = dput(h, m.sjca, jca)))
       return rc;

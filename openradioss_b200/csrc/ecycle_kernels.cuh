@@ -84,8 +84,8 @@ template <class R>
 struct HexArgs {
   const PatchInfo* patch;
   const HexGroupDesc* groups;
-  const int* patch_nodes;
-  const int* patch_slots;
+  const int* patch_nodes;     // nlmax per patch; padding repeats a node of the patch
+  const int* patch_slots;     // nlmax per patch; padding -1
   const uint4* conn;          // 8 x uint16 local corners per element (colour in corner 0)
   const int* elem_id;         // element number within its part (for NELTS)
   const double4* X;           // x, y, z, nodal mass
@@ -100,14 +100,15 @@ struct HexArgs {
   double* blk_wpla;           // per patch cumulative plastic work
   ErrorWord* err;
   int nelpad, nparts, npatch;
+  int nlmax;                  // stride of patch_nodes / patch_slots (padded per patch)
 };
 
 template <class R>
 struct ShellArgs {
   const PatchInfo* patch;
   const ShellGroupDesc* groups;
-  const int* patch_nodes;
-  const int* patch_slots;
+  const int* patch_nodes;     // nlmax per patch; padding repeats a node of the patch
+  const int* patch_slots;     // nlmax per patch; padding -1
   const uint2* conn;          // 4 x uint16 local corners per element (colour in corner 0)
   const int* elem_id;
   const int* degen;           // 1 if IXC(4)==IXC(5) (triangle stored as quad)
@@ -125,6 +126,7 @@ struct ShellArgs {
   double* blk_wpla;
   ErrorWord* err;
   int nelpad, nparts, npatch, maxnpt;
+  int nlmax;                  // stride of patch_nodes / patch_slots (padded per patch)
 };
 
 template <class R>
@@ -230,6 +232,15 @@ __device__ inline void block_reduce(unsigned long long& key, unsigned long long&
 #ifndef ORB_SHELL_CTAS_F64
 #define ORB_SHELL_CTAS_F64 3
 #endif
+// The 5-point rule of COQINI (coqini.F:45-130) as compile-time constants for the
+// NPT = 5 shell kernels (row 0: Z0, 1: WF, 2: WM); the host build checks them
+// against the shared table of coqini_table.h.
+__host__ __device__ constexpr float coq5(int row, int ip) {
+  return row == 0 ? (ip == 0 ? -.5f : ip == 1 ? -.25f : ip == 2 ? 0.f : ip == 3 ? .25f : .5f)
+         : row == 1 ? (ip == 0 || ip == 4 ? .125f : .25f)
+                    : (ip == 0 ? -.0520833f : ip == 1 ? -.0625f : ip == 2 ? 0.f : ip == 3 ? .0625f : .0520833f);
+}
+
 template <class R> struct Occupancy;
 template <> struct Occupancy<float> {
   static constexpr int hex = ORB_HEX_CTAS_F32, shell = ORB_SHELL_CTAS_F32;
@@ -255,21 +266,22 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
   __shared__ double s_s0[TILE / 32], s_s1[TILE / 32];
   const int p = blockIdx.x;
   const int tid = threadIdx.x;
+  // Patches are padded to TILE elements and their node lists to nlmax entries,
+  // so every address below follows from (p, tid) alone: the per-element loads
+  // and the node gathers are issued without waiting for the patch descriptor.
+  const int NLM = a.nlmax;
+  const int e = p * TILE + tid;
   const PatchInfo pi = a.patch[p];
-  const HexGroupDesc gd = a.groups[pi.group];
-  const int nl = pi.nloc;
-  // shared layout: x, y, z (double) | vx, vy, vz, fx, fy, fz (R)
+  // shared layout, planes of NLM: x, y, z (double) | vx, vy, vz, fx, fy, fz (R)
   double* sx = reinterpret_cast<double*>(smem_raw);
-  double* sy = sx + nl;
-  double* sz = sy + nl;
-  R* svx = reinterpret_cast<R*>(sz + nl);
-  R* svy = svx + nl;
-  R* svz = svy + nl;
-  R* sfx = svz + nl;
-  R* sfy = sfx + nl;
-  R* sfz = sfy + nl;
-  const bool active = tid < pi.nel;
-  const int e = pi.elem0 + tid;
+  double* sy = sx + NLM;
+  double* sz = sy + NLM;
+  R* svx = reinterpret_cast<R*>(sz + NLM);
+  R* svy = svx + NLM;
+  R* svz = svy + NLM;
+  R* sfx = svz + NLM;
+  R* sfy = sfx + NLM;
+  R* sfz = sfy + NLM;
   const int nelpad = a.nelpad;
   // issue every per-element load before the staging barrier so that they are in
   // flight together with the node gathers
@@ -277,7 +289,7 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
   R st_sig[6], st_eint = R(0), st_rho = R(1), st_qvis = R(0), st_vol0 = R(1), st_pla = R(0);
   double st_vol0dp = 1.0;
   int st_eid = 0;
-  if (active) {
+  {   // padding elements (tid >= nel) hold valid zero state: load unconditionally
     cw = a.conn[e];
 #pragma unroll
     for (int c = 0; c < 6; ++c) st_sig[c] = a.sig[c * nelpad + e];
@@ -286,17 +298,20 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
     st_qvis = a.qvis[e];
     st_vol0 = a.vol0[e];
     if (sizeof(R) == 4) st_vol0dp = a.vol0dp[e];
-    if (gd.law == 2) st_pla = a.pla[e];
+    st_pla = a.pla[e];
     st_eid = a.elem_id[e];
   }
-  for (int j = tid; j < nl; j += TILE) {
-    const int g = a.patch_nodes[pi.node_ofs + j];
+  for (int j = tid; j < NLM; j += TILE) {
+    const int g = a.patch_nodes[p * NLM + j];
     const double4 xx = a.X[g];
     const R4 vv = a.V[g];
     sx[j] = xx.x; sy[j] = xx.y; sz[j] = xx.z;
     svx[j] = vv.x; svy[j] = vv.y; svz[j] = vv.z;
     sfx[j] = R(0); sfy[j] = R(0); sfz[j] = R(0);
   }
+  const HexGroupDesc gd = a.groups[pi.group];
+  const bool active = tid < pi.nel;
+  const int nl = pi.nloc;
   const PartTime& tm = a.time[parity * a.nparts + gd.part];
   const R DT1 = R(tm.dt2);
   const bool split = sizeof(R) == 4;
@@ -594,7 +609,7 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
     __syncthreads();
   }
   for (int j = tid; j < nl; j += TILE) {
-    const int s = a.patch_slots[pi.node_ofs + j];
+    const int s = a.patch_slots[p * NLM + j];
     a.fslot[s] = mk4(sfx[j], sfy[j], sfz[j], R(0));
   }
   // ---- dt min-reduction and energy partials ----
@@ -626,15 +641,15 @@ shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
   __shared__ double s_s0[TILE / 32], s_s1[TILE / 32];
   const int p = blockIdx.x;
   const int tid = threadIdx.x;
+  // element index and node-list slots follow from (p, tid) alone (patches padded
+  // to TILE elements and nlmax nodes): loads start before the descriptors arrive
+  const int NLM = a.nlmax;
+  const int e = p * TILE + tid;
   const PatchInfo pi = a.patch[p];
-  const ShellGroupDesc gd = a.groups[pi.group];
-  const int nl = pi.nloc;
   double* sx = reinterpret_cast<double*>(smem_raw);
-  double* sy = sx + nl;
-  double* sz = sy + nl;
-  R* sv = reinterpret_cast<R*>(sz + nl);   // vx vy vz rx ry rz fx fy fz mx my mz: 12 planes
-  const bool active = tid < pi.nel;
-  const int e = pi.elem0 + tid;
+  double* sy = sx + NLM;
+  double* sz = sy + NLM;
+  R* sv = reinterpret_cast<R*>(sz + NLM);   // vx vy vz rx ry rz fx fy fz mx my mz: 12 planes of NLM
   const int nelpad = a.nelpad;
   // per-element loads issued before the staging barrier (overlap with the gathers)
   constexpr int NP = NPT > 0 ? NPT : 1;
@@ -643,13 +658,13 @@ shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
   R st_jca = R(0);
   R st_sig[NP][5], st_pla[NP];
   int st_degen = 0, st_eid = 0;
-  if (active) {
+  {   // padding elements (tid >= nel) hold valid state: load unconditionally
     cw = a.conn[e];
     st_thk = a.thk[e];
     st_thke = a.thke[e];
     st_h0 = a.hourg[0 * nelpad + e]; st_h1 = a.hourg[1 * nelpad + e]; st_h2 = a.hourg[2 * nelpad + e];
     st_e0 = a.eint[0 * nelpad + e]; st_e1 = a.eint[1 * nelpad + e];
-    if (gd.has_jca) st_jca = a.jca[e];
+    if (a.jca) st_jca = a.jca[e];
     st_degen = a.degen[e];
     st_eid = a.elem_id[e];
     if (NPT > 0) {
@@ -657,21 +672,24 @@ shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
       for (int ip = 0; ip < NP; ++ip) {
 #pragma unroll
         for (int c = 0; c < 5; ++c) st_sig[ip][c] = a.sig[(ip * 5 + c) * nelpad + e];
-        st_pla[ip] = gd.law == 2 ? a.pla[ip * nelpad + e] : R(0);
+        st_pla[ip] = a.pla[ip * nelpad + e];
       }
     }
   }
-  for (int j = tid; j < nl; j += TILE) {
-    const int g = a.patch_nodes[pi.node_ofs + j];
+  for (int j = tid; j < NLM; j += TILE) {
+    const int g = a.patch_nodes[p * NLM + j];
     const double4 xx = a.X[g];
     const R4 vv = a.V[g];
     const R4 rr = a.VR[g];
     sx[j] = xx.x; sy[j] = xx.y; sz[j] = xx.z;
-    sv[0 * nl + j] = vv.x; sv[1 * nl + j] = vv.y; sv[2 * nl + j] = vv.z;
-    sv[3 * nl + j] = rr.x; sv[4 * nl + j] = rr.y; sv[5 * nl + j] = rr.z;
+    sv[0 * NLM + j] = vv.x; sv[1 * NLM + j] = vv.y; sv[2 * NLM + j] = vv.z;
+    sv[3 * NLM + j] = rr.x; sv[4 * NLM + j] = rr.y; sv[5 * NLM + j] = rr.z;
 #pragma unroll
-    for (int q = 6; q < 12; ++q) sv[q * nl + j] = R(0);
+    for (int q = 6; q < 12; ++q) sv[q * NLM + j] = R(0);
   }
+  const ShellGroupDesc gd = a.groups[pi.group];
+  const bool active = tid < pi.nel;
+  const int nl = pi.nloc;
   const PartTime& tm = a.time[parity * a.nparts + gd.part];
   const R DT1 = R(tm.dt2);
   __syncthreads();
@@ -758,11 +776,11 @@ shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
     R VXl[4], VYl[4], VZl[4], RXl[4], RYl[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      const R vx = sv[0 * nl + lc[k]], vy = sv[1 * nl + lc[k]], vz = sv[2 * nl + lc[k]];
+      const R vx = sv[0 * NLM + lc[k]], vy = sv[1 * NLM + lc[k]], vz = sv[2 * NLM + lc[k]];
       VXl[k] = E1X * vx + E1Y * vy + E1Z * vz;
       VYl[k] = E2X * vx + E2Y * vy + E2Z * vz;
       VZl[k] = E3X * vx + E3Y * vy + E3Z * vz;
-      const R rx = sv[3 * nl + lc[k]], ry = sv[4 * nl + lc[k]], rz = sv[5 * nl + lc[k]];
+      const R rx = sv[3 * NLM + lc[k]], ry = sv[4 * NLM + lc[k]], rz = sv[5 * NLM + lc[k]];
       RXl[k] = E1X * rx + E1Y * ry + E1Z * rz;
       RYl[k] = E2X * rx + E2Y * ry + E2Z * rz;
     }
@@ -811,7 +829,7 @@ shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
 #pragma unroll
     for (int ip = 0; ip < (NPT > 0 ? NPT : 10); ++ip) {
       if (NPT == 0 && ip >= npt) break;
-      const R wf = R(WF[ip]), wm = R(WM[ip]);
+      const R wf = R(NPT == 5 ? coq5(1, ip) : WF[ip]), wm = R(NPT == 5 ? coq5(2, ip) : WM[ip]);
       R SO[5], SN[5];
       if (NPT > 0) {
 #pragma unroll
@@ -825,7 +843,7 @@ shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) MOLD[c] = MOLD[c] + wm * SO[c];
       const R THKLYL = wf * THK0;
-      const R ZT = R(Z0[ip]) * THK0;
+      const R ZT = R(NPT == 5 ? coq5(0, ip) : Z0[ip]) * THK0;
       const R DXX = EXX + ZT * KXX, DYY = EYY + ZT * KYY, DXY = EXY + ZT * KXY;
       R EZZ = R(0);
       if (gd.law == 1) {
@@ -978,22 +996,22 @@ shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
     }
   }
   // ---- colour-ordered shared-memory assembly ----
-  R* sf = sv + 6 * nl;
+  R* sf = sv + 6 * NLM;
   for (int c = 0; c < pi.ncolor; ++c) {
     if (color == c) {
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         const int l = lc[k];
-        sf[0 * nl + l] += Fg[0][k]; sf[1 * nl + l] += Fg[1][k]; sf[2 * nl + l] += Fg[2][k];
-        sf[3 * nl + l] += Mg[0][k]; sf[4 * nl + l] += Mg[1][k]; sf[5 * nl + l] += Mg[2][k];
+        sf[0 * NLM + l] += Fg[0][k]; sf[1 * NLM + l] += Fg[1][k]; sf[2 * NLM + l] += Fg[2][k];
+        sf[3 * NLM + l] += Mg[0][k]; sf[4 * NLM + l] += Mg[1][k]; sf[5 * NLM + l] += Mg[2][k];
       }
     }
     __syncthreads();
   }
   for (int j = tid; j < nl; j += TILE) {
-    const int s = a.patch_slots[pi.node_ofs + j];
-    a.fslot[s] = mk4(sf[0 * nl + j], sf[1 * nl + j], sf[2 * nl + j], R(0));
-    a.mslot[s] = mk4(sf[3 * nl + j], sf[4 * nl + j], sf[5 * nl + j], R(0));
+    const int s = a.patch_slots[p * NLM + j];
+    a.fslot[s] = mk4(sf[0 * NLM + j], sf[1 * NLM + j], sf[2 * NLM + j], R(0));
+    a.mslot[s] = mk4(sf[3 * NLM + j], sf[4 * NLM + j], sf[5 * NLM + j], R(0));
   }
   block_reduce<TILE>(mykey, mybits, my_ehou, my_wpla, s_key, s_bits, s_s0, s_s1);
   if (tid == 0) {
