@@ -223,7 +223,7 @@ int build_patches(or_ecycle* h, std::vector<GroupT>& groups, int tile, PatchSet&
       std::stable_sort(byc.begin(), byc.end(), [&](int a, int b) { return col[a] < col[b]; });
       PatchInfo pi{};
       pi.group = (int)gi; pi.nel = n; pi.node_ofs = (int)ps.nodes.size(); pi.nloc = (int)nodes.size();
-      pi.ncolor = ncol; pi.elem0 = elem0;
+      pi.ncolor = ncol; pi.elem0 = elem0; pi.part = g.part;
       const int pid = (int)ps.info.size();
       ps.info.push_back(pi);
       ps.nlmax = std::max(ps.nlmax, (int)nodes.size());

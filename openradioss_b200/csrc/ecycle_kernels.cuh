@@ -42,7 +42,8 @@ struct PatchInfo {
   int nloc;       // unique local nodes
   int ncolor;     // colours used
   int elem0;      // first element (padded internal index) of this patch
-  int pad0, pad1;
+  int part;       // part of the patch's group (time state, dt reduction target)
+  int pad1;
 };
 
 struct HexGroupDesc {
@@ -272,6 +273,12 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
   const int NLM = a.nlmax;
   const int e = p * TILE + tid;
   const PatchInfo pi = a.patch[p];
+  // issued now, used at the end: the patch's slot numbers (up to two per thread)
+  // and its cumulative energy partials
+  const int slot0 = tid < NLM ? a.patch_slots[p * NLM + tid] : -1;
+  const int slot1 = tid + TILE < NLM ? a.patch_slots[p * NLM + tid + TILE] : -1;
+  double pre_ehour = 0.0, pre_wpla = 0.0;
+  if (tid == 0) { pre_ehour = a.blk_ehour[p]; pre_wpla = a.blk_wpla[p]; }
   // shared layout, planes of NLM: x, y, z (double) | vx, vy, vz, fx, fy, fz (R)
   double* sx = reinterpret_cast<double*>(smem_raw);
   double* sy = sx + NLM;
@@ -312,7 +319,7 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
   const HexGroupDesc gd = a.groups[pi.group];
   const bool active = tid < pi.nel;
   const int nl = pi.nloc;
-  const PartTime& tm = a.time[parity * a.nparts + gd.part];
+  const PartTime& tm = a.time[parity * a.nparts + pi.part];
   const R DT1 = R(tm.dt2);
   const bool split = sizeof(R) == 4;
   __syncthreads();
@@ -609,17 +616,17 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
     __syncthreads();
   }
   for (int j = tid; j < nl; j += TILE) {
-    const int s = a.patch_slots[p * NLM + j];
+    const int s = j == tid ? slot0 : j == tid + TILE ? slot1 : a.patch_slots[p * NLM + j];
     a.fslot[s] = mk4(sfx[j], sfy[j], sfz[j], R(0));
   }
   // ---- dt min-reduction and energy partials ----
   block_reduce<TILE>(mykey, mybits, my_ehou, my_wpla, s_key, s_bits, s_s0, s_s1);
   if (tid == 0) {
-    PartAcc* acc = &a.acc[parity * a.nparts + gd.part];
+    PartAcc* acc = &a.acc[parity * a.nparts + pi.part];
     atomicMin(&acc->dtkey, mykey);
     atomicMin(&acc->dtbits, mybits);
-    a.blk_ehour[p] += my_ehou;
-    a.blk_wpla[p] += my_wpla;
+    a.blk_ehour[p] = pre_ehour + my_ehou;
+    a.blk_wpla[p] = pre_wpla + my_wpla;
   }
 }
 
@@ -646,6 +653,12 @@ shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
   const int NLM = a.nlmax;
   const int e = p * TILE + tid;
   const PatchInfo pi = a.patch[p];
+  // issued now, used at the end: the patch's slot numbers (up to two per thread)
+  // and its cumulative energy partials
+  const int slot0 = tid < NLM ? a.patch_slots[p * NLM + tid] : -1;
+  const int slot1 = tid + TILE < NLM ? a.patch_slots[p * NLM + tid + TILE] : -1;
+  double pre_ehour = 0.0, pre_wpla = 0.0;
+  if (tid == 0) { pre_ehour = a.blk_ehour[p]; pre_wpla = a.blk_wpla[p]; }
   double* sx = reinterpret_cast<double*>(smem_raw);
   double* sy = sx + NLM;
   double* sz = sy + NLM;
@@ -690,7 +703,7 @@ shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
   const ShellGroupDesc gd = a.groups[pi.group];
   const bool active = tid < pi.nel;
   const int nl = pi.nloc;
-  const PartTime& tm = a.time[parity * a.nparts + gd.part];
+  const PartTime& tm = a.time[parity * a.nparts + pi.part];
   const R DT1 = R(tm.dt2);
   __syncthreads();
 
@@ -1009,17 +1022,17 @@ shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
     __syncthreads();
   }
   for (int j = tid; j < nl; j += TILE) {
-    const int s = a.patch_slots[p * NLM + j];
+    const int s = j == tid ? slot0 : j == tid + TILE ? slot1 : a.patch_slots[p * NLM + j];
     a.fslot[s] = mk4(sf[0 * NLM + j], sf[1 * NLM + j], sf[2 * NLM + j], R(0));
     a.mslot[s] = mk4(sf[3 * NLM + j], sf[4 * NLM + j], sf[5 * NLM + j], R(0));
   }
   block_reduce<TILE>(mykey, mybits, my_ehou, my_wpla, s_key, s_bits, s_s0, s_s1);
   if (tid == 0) {
-    PartAcc* acc = &a.acc[parity * a.nparts + gd.part];
+    PartAcc* acc = &a.acc[parity * a.nparts + pi.part];
     atomicMin(&acc->dtkey, mykey);
     atomicMin(&acc->dtbits, mybits);
-    a.blk_ehour[p] += my_ehou;
-    a.blk_wpla[p] += my_wpla;
+    a.blk_ehour[p] = pre_ehour + my_ehou;
+    a.blk_wpla[p] = pre_wpla + my_wpla;
   }
 }
 
