@@ -350,36 +350,45 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
       raise_error(a.err, 4, st_eid);
       det = 1.0;
     }
-    const double dett = (1.0 / 64.0) / det;
-    const double I1 = dett * C1, I4 = dett * C4, I7 = dett * C7;
-    const double I2 = dett * (J3 * J8 - J2 * J9), I5 = dett * (J1 * J9 - J3 * J7), I8 = dett * (J2 * J7 - J1 * J8);
-    const double I3 = dett * (J2 * J6 - J3 * J5), I6 = dett * (J3 * J4 - J1 * J6), I9 = dett * (J1 * J5 - J2 * J4);
+    // Beyond the determinant nothing here needs FP64 (the reference's -prec=sp
+    // build forms the inverse Jacobian, the hourglass vectors and SDLEN3 in
+    // my_real): they use R, with coordinates relative to corner 1 (differences
+    // taken in FP64, then rounded), so the 24 FP64 coordinates die here.
+    R xr[8], yr[8], zr[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) { xr[k] = R(XD[k] - XD[0]); yr[k] = R(YD[k] - YD[0]); zr[k] = R(ZD[k] - ZD[0]); }
+    const R j1 = R(J1), j2 = R(J2), j3 = R(J3), j4 = R(J4), j5 = R(J5), j6 = R(J6), j7 = R(J7), j8 = R(J8), j9 = R(J9);
+    const R dett = R(1.0 / 64.0) / R(det);
+    const R I1 = dett * R(C1), I4 = dett * R(C4), I7 = dett * R(C7);
+    const R I2 = dett * (j3 * j8 - j2 * j9), I5 = dett * (j1 * j9 - j3 * j7), I8 = dett * (j2 * j7 - j1 * j8);
+    const R I3 = dett * (j2 * j6 - j3 * j5), I6 = dett * (j3 * j4 - j1 * j6), I9 = dett * (j1 * j5 - j2 * j4);
     R PX[4], PY[4], PZ[4];
     {
-      const double a12 = I1 + I2, a45 = I4 + I5, a78 = I7 + I8;
-      const double b12 = I1 - I2, b45 = I4 - I5, b78 = I7 - I8;
-      PX[0] = R(-a12 - I3); PY[0] = R(-a45 - I6); PZ[0] = R(-a78 - I9);
-      PX[1] = R(-a12 + I3); PY[1] = R(-a45 + I6); PZ[1] = R(-a78 + I9);
-      PX[2] = R(b12 + I3);  PY[2] = R(b45 + I6);  PZ[2] = R(b78 + I9);
-      PX[3] = R(b12 - I3);  PY[3] = R(b45 - I6);  PZ[3] = R(b78 - I9);
+      const R a12 = I1 + I2, a45 = I4 + I5, a78 = I7 + I8;
+      const R b12 = I1 - I2, b45 = I4 - I5, b78 = I7 - I8;
+      PX[0] = -a12 - I3; PY[0] = -a45 - I6; PZ[0] = -a78 - I9;
+      PX[1] = -a12 + I3; PY[1] = -a45 + I6; PZ[1] = -a78 + I9;
+      PX[2] = b12 + I3;  PY[2] = b45 + I6;  PZ[2] = b78 + I9;
+      PX[3] = b12 - I3;  PY[3] = b45 - I6;  PZ[3] = b78 - I9;
     }
-    // hourglass projections PXiHj (sderi3.F:302-333): modes (+-+-+-+-), (++----++), (+--+-++-)
+    // hourglass projections PXiHj (sderi3.F:302-333): modes (+-+-+-+-), (++----++), (+--+-++-);
+    // the mode vectors sum to zero, so relative coordinates give the same products
     R PXH[4][3];
     {
-      const double hx1 = XD[0] - XD[1] + XD[2] - XD[3] + XD[4] - XD[5] + XD[6] - XD[7];
-      const double hy1 = YD[0] - YD[1] + YD[2] - YD[3] + YD[4] - YD[5] + YD[6] - YD[7];
-      const double hz1 = ZD[0] - ZD[1] + ZD[2] - ZD[3] + ZD[4] - ZD[5] + ZD[6] - ZD[7];
-      const double hx2 = XD[0] + XD[1] - XD[2] - XD[3] - XD[4] - XD[5] + XD[6] + XD[7];
-      const double hy2 = YD[0] + YD[1] - YD[2] - YD[3] - YD[4] - YD[5] + YD[6] + YD[7];
-      const double hz2 = ZD[0] + ZD[1] - ZD[2] - ZD[3] - ZD[4] - ZD[5] + ZD[6] + ZD[7];
-      const double hx3 = XD[0] - XD[1] - XD[2] + XD[3] - XD[4] + XD[5] + XD[6] - XD[7];
-      const double hy3 = YD[0] - YD[1] - YD[2] + YD[3] - YD[4] + YD[5] + YD[6] - YD[7];
-      const double hz3 = ZD[0] - ZD[1] - ZD[2] + ZD[3] - ZD[4] + ZD[5] + ZD[6] - ZD[7];
+      const R hx1 = xr[0] - xr[1] + xr[2] - xr[3] + xr[4] - xr[5] + xr[6] - xr[7];
+      const R hy1 = yr[0] - yr[1] + yr[2] - yr[3] + yr[4] - yr[5] + yr[6] - yr[7];
+      const R hz1 = zr[0] - zr[1] + zr[2] - zr[3] + zr[4] - zr[5] + zr[6] - zr[7];
+      const R hx2 = xr[0] + xr[1] - xr[2] - xr[3] - xr[4] - xr[5] + xr[6] + xr[7];
+      const R hy2 = yr[0] + yr[1] - yr[2] - yr[3] - yr[4] - yr[5] + yr[6] + yr[7];
+      const R hz2 = zr[0] + zr[1] - zr[2] - zr[3] - zr[4] - zr[5] + zr[6] + zr[7];
+      const R hx3 = xr[0] - xr[1] - xr[2] + xr[3] - xr[4] + xr[5] + xr[6] - xr[7];
+      const R hy3 = yr[0] - yr[1] - yr[2] + yr[3] - yr[4] + yr[5] + yr[6] - yr[7];
+      const R hz3 = zr[0] - zr[1] - zr[2] + zr[3] - zr[4] + zr[5] + zr[6] - zr[7];
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        PXH[q][0] = PX[q] * R(hx1) + PY[q] * R(hy1) + PZ[q] * R(hz1);
-        PXH[q][1] = PX[q] * R(hx2) + PY[q] * R(hy2) + PZ[q] * R(hz2);
-        PXH[q][2] = PX[q] * R(hx3) + PY[q] * R(hy3) + PZ[q] * R(hz3);
+        PXH[q][0] = PX[q] * hx1 + PY[q] * hy1 + PZ[q] * hz1;
+        PXH[q][1] = PX[q] * hx2 + PY[q] * hy2 + PZ[q] * hz2;
+        PXH[q][2] = PX[q] * hx3 + PY[q] * hy3 + PZ[q] * hz3;
       }
     }
     const double VOLN_D = det;
@@ -390,9 +399,9 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
       const int FC[6][4] = {{0, 1, 2, 3}, {4, 5, 6, 7}, {0, 1, 5, 4}, {1, 2, 6, 5}, {2, 3, 7, 6}, {3, 0, 4, 7}};
 #pragma unroll
       for (int f = 0; f < 6; ++f) {
-        const R x13 = R(XD[FC[f][2]] - XD[FC[f][0]]), x24 = R(XD[FC[f][3]] - XD[FC[f][1]]);
-        const R y13 = R(YD[FC[f][2]] - YD[FC[f][0]]), y24 = R(YD[FC[f][3]] - YD[FC[f][1]]);
-        const R z13 = R(ZD[FC[f][2]] - ZD[FC[f][0]]), z24 = R(ZD[FC[f][3]] - ZD[FC[f][1]]);
+        const R x13 = xr[FC[f][2]] - xr[FC[f][0]], x24 = xr[FC[f][3]] - xr[FC[f][1]];
+        const R y13 = yr[FC[f][2]] - yr[FC[f][0]], y24 = yr[FC[f][3]] - yr[FC[f][1]];
+        const R z13 = zr[FC[f][2]] - zr[FC[f][0]], z24 = zr[FC[f][3]] - zr[FC[f][1]];
         const R s1 = x13 - x24, t1 = x13 + x24, s2 = y13 - y24, t2 = y13 + y24, s3 = z13 - z24, t3 = z13 + z24;
         const R E = s1 * s1 + s2 * s2 + s3 * s3, Fm = s1 * t1 + s2 * t2 + s3 * t3, G = t1 * t1 + t2 * t2 + t3 * t3;
         const R ar = E * G - Fm * Fm;
