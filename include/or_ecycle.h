@@ -216,6 +216,35 @@ int  or_ecycle_stream(or_ecycle* h, void** stream);
 /* Bytes of device memory held by the handle. */
 int  or_ecycle_device_bytes(or_ecycle* h, long long* bytes);
 
+/* --- domain decomposition (one part split over ranks) ---------------------- */
+/* The reference's SPMD cycle on one mesh: each rank runs a handle with its
+   share of the elements and the nodes they touch (full nodal masses); per
+   cycle, the ranks exchange the partial force/moment sums of the nodes they
+   share (SPMD_EXCH_A, resol.F after FORINT) and take the minimum of their
+   element time steps (SPMD_GLOB_MIN5).  The exchange itself is the caller's
+   (NCCL all-gather over NVLink, or any transport):
+     or_ecycle_spmd_begin(h, t)
+     per cycle: or_ecycle_spmd_elements(h, my_buf)      element kernels + pack
+                all-gather my_buf of every rank into bufs, rank order
+                or_ecycle_spmd_nodes(h, bufs, nranks)    nodal phase
+     or_ecycle_spmd_end(h, t)
+   A shared node's force is the sum of every rank's partial in rank order, so
+   every rank computes the same nodal update.  Buffers are device memory of
+   or_ecycle_spmd_buffer_bytes each, on the handle's device; the per-cycle
+   calls are asynchronous on the handle's stream, begin and end synchronous.
+   or_ecycle_set_halo: the part's nodes shared with other ranks, as nloc
+   (part-local node, global halo slot in [0, nhalo)) pairs; count_ke[i] = 0 when
+   another rank counts the node's kinetic energy (NULL: all counted).
+   One part per handle.  No counterpart in the reference's C interfaces: the
+   reference does this exchange in Fortran over MPI. */
+int  or_ecycle_set_halo(or_ecycle* h, int part, int nloc, const int* local_node, const int* halo_slot,
+                        const int* count_ke, int nhalo);
+int  or_ecycle_spmd_buffer_bytes(or_ecycle* h, long long* bytes);
+int  or_ecycle_spmd_begin(or_ecycle* h, or_ecycle_time* t);
+int  or_ecycle_spmd_elements(or_ecycle* h, void* dev_buf);
+int  or_ecycle_spmd_nodes(or_ecycle* h, const void* dev_bufs, int nranks);
+int  or_ecycle_spmd_end(or_ecycle* h, or_ecycle_time* t);
+
 /* --- adjoint (design sensitivities) -------------------------------------- */
 /* Response of or_ecycle_adjoint:
      J = w_disp * D(comp) of node `node` of part `part` after the call's cycles

@@ -97,6 +97,7 @@ struct or_ecycle {
   cudaGraphExec_t graph_exec = nullptr;
   cudaGraph_t graph = nullptr;
   int last_code = 0, last_index = -1;
+  int spmd_k = -1;                    // cycle index of a running domain-decomposed step, -1 outside one
   int next_parity = 0;                // time-buffer parity of the state after the last step
 };
 
@@ -297,6 +298,9 @@ struct Impl {
   DBuf<float> zw;
   int maxnpt = 1;
   int uniform_npt = 0;       // npt shared by every shell group, 0 if they differ
+  // domain decomposition: halo nodes of this rank's part
+  DBuf<int> halo_slot, halo_node; DBuf<unsigned char> halo_ke;
+  int nhalo = -1;            // -1: no halo set
 
   HexArgs<R> hargs() {
     HexArgs<R> a;
@@ -326,6 +330,7 @@ struct Impl {
     a.time = time.p; a.acc = acc.p; a.blk_ekin = ekin.p; a.blk_ekinr = ekinr.p; a.err = err.p;
     a.growth = h->cfg.dt_growth; a.dtmx = h->cfg.dtmx; a.ntiles = ntiles; a.nparts = nparts;
     a.split = sizeof(R) == 4;
+    a.halo_slot = nullptr; a.halo_ke = nullptr; a.xbuf = nullptr; a.xbytes = 0; a.nranks = 0; a.nhalo = 0;
     return a;
   }
   void free_all() {
@@ -336,6 +341,7 @@ struct Impl {
     dfree(spatch); dfree(sdesc); dfree(snodes); dfree(sslots); dfree(selem); dfree(sdegen); dfree(sconn);
     dfree(ssig); dfree(spla); dfree(sthk); dfree(sthke); dfree(shourg); dfree(seint); dfree(sjca);
     dfree(sehour); dfree(swpla); dfree(zw);
+    dfree(halo_slot); dfree(halo_node); dfree(halo_ke);
   }
 };
 
@@ -988,6 +994,124 @@ void destroy_impl(or_ecycle* h) {
   h->impl = nullptr;
 }
 
+// ----------------------------------------------------------------------------
+// domain decomposition: one part split over ranks, one boundary-force exchange
+// and one time-step minimum per cycle (the reference's SPMD_EXCH_A and
+// SPMD_GLOB_MIN5), the exchange itself left to the caller (NCCL, gloo, MPI)
+// ----------------------------------------------------------------------------
+template <class R>
+int set_halo_impl(or_ecycle* h, int nloc, const int* local_node, const int* slot, const int* count_ke, int nhalo) {
+  Impl<R>& m = *(Impl<R>*)h->impl;
+  const HPart& P = h->parts[0];
+  std::vector<int> hs(m.nnodpad, -1), hn(std::max(nhalo, 1), -1);
+  std::vector<unsigned char> ke(m.nnodpad, 1);
+  for (int i = 0; i < nloc; ++i) {
+    const int n = local_node[i], q = slot[i];
+    if (n < 0 || n >= P.numnod || q < 0 || q >= nhalo) return fail(h, OR_E_ARG, "set_halo: node or slot out of range");
+    if (hn[q] >= 0) return fail(h, OR_E_ARG, "set_halo: slot given twice");
+    const int g = P.node_start + n;
+    hs[g] = q;
+    hn[q] = g;
+    ke[g] = count_ke ? (count_ke[i] ? 1 : 0) : 1;
+  }
+  dfree(m.halo_slot); dfree(m.halo_node); dfree(m.halo_ke);
+  int rc;
+  if ((rc = dput(h, m.halo_slot, hs)) || (rc = dput(h, m.halo_node, hn)) || (rc = dput(h, m.halo_ke, ke))) return rc;
+  m.nhalo = nhalo;
+  return OR_OK;
+}
+
+template <class R>
+int spmd_begin_impl(or_ecycle* h, or_ecycle_time* t) {
+  Impl<R>& m = *(Impl<R>*)h->impl;
+  PartTime pt{};
+  pt.tt = t->tt; pt.dt2 = t->dt2; pt.dt2old = t->dt2old; pt.dt1 = t->dt1; pt.dt12 = t->dt12;
+  pt.ncycle = t->ncycle; pt.ityptst = t->ityptst; pt.neltst = t->neltst;
+  PartAcc a0;
+  a0.dtkey = ~0ull; a0.dtbits = ~0ull;
+  CK(cudaMemcpyAsync(m.time.p, &pt, sizeof(PartTime), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(m.acc.p, &a0, sizeof(PartAcc), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemsetAsync(m.err.p, 0, sizeof(ErrorWord), h->stream));
+  CK(cudaStreamSynchronize(h->stream));      // pt and a0 are host locals
+  h->spmd_k = 0;
+  h->launches = 0;
+  return OR_OK;
+}
+
+template <class R>
+int spmd_elements_impl(or_ecycle* h, void* buf) {
+  Impl<R>& m = *(Impl<R>*)h->impl;
+  const int parity = h->spmd_k & 1;
+  int rc = h->tile_hex == 64 ? launch_hex<R, 64>(h, m, parity)
+           : h->tile_hex == 128 ? launch_hex<R, 128>(h, m, parity) : launch_hex<R, 256>(h, m, parity);
+  if (rc) return rc;
+  rc = h->tile_shell == 64 ? launch_shell_npt<R, 64>(h, m, parity)
+       : h->tile_shell == 128 ? launch_shell_npt<R, 128>(h, m, parity) : launch_shell_npt<R, 256>(h, m, parity);
+  if (rc) return rc;
+  halo_pack_kernel<R><<<(unsigned)std::max(1, (m.nhalo + 127) / 128), 128, 0, h->stream>>>(
+      m.halo_node.p, m.adsky.p, m.fslot.p, m.mslot.p, m.acc.p + parity, (unsigned char*)buf, m.nhalo);
+  CK(cudaGetLastError());
+  h->launches++;
+  return OR_OK;
+}
+
+template <class R>
+int spmd_nodes_impl(or_ecycle* h, const void* bufs, int nranks) {
+  Impl<R>& m = *(Impl<R>*)h->impl;
+  const int parity = h->spmd_k & 1;
+  NodeArgs<R> a = m.nargs(h);
+  a.halo_slot = m.halo_slot.p; a.halo_ke = m.halo_ke.p; a.xbuf = (const unsigned char*)bufs;
+  a.xbytes = halo_buffer_bytes<R>(m.nhalo); a.nranks = nranks; a.nhalo = m.nhalo;
+  node_kernel<R, NODE_TILE><<<(unsigned)m.ntiles, NODE_TILE, 0, h->stream>>>(a, parity);
+  CK(cudaGetLastError());
+  h->launches++;
+  h->spmd_k++;
+  return OR_OK;
+}
+
+template <class R>
+int spmd_end_impl(or_ecycle* h, or_ecycle_time* t) {
+  Impl<R>& m = *(Impl<R>*)h->impl;
+  const int fin = h->spmd_k & 1;
+  PartTime pt{};
+  ErrorWord ew{};
+  CK(cudaMemcpyAsync(&pt, m.time.p + fin, sizeof(PartTime), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(&ew, m.err.p, sizeof(ErrorWord), cudaMemcpyDeviceToHost, h->stream));
+  cudaEvent_t ev;
+  CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  CK(cudaEventRecord(ev, h->stream));
+  int rc = wait_stream(h, ev);
+  cudaEventDestroy(ev);
+  if (rc) return rc;
+  t->tt = pt.tt; t->dt1 = pt.dt1; t->dt2 = pt.dt2; t->dt12 = pt.dt12; t->dt2old = pt.dt2old;
+  t->ncycle = pt.ncycle; t->ityptst = pt.ityptst; t->neltst = pt.neltst;
+  h->next_parity = fin;
+  h->spmd_k = -1;
+  h->last_code = ew.code;
+  h->last_index = ew.index;
+  if (ew.code) {
+    char b[160];
+    snprintf(b, sizeof b, "device error %d at index %d", ew.code, ew.index);
+    return fail(h, ew.code, b);
+  }
+  return OR_OK;
+}
+
+int spmd_nhalo(const or_ecycle* h) {
+  return h->cfg.precision == OR_PREC_SPLIT ? ((const Impl<float>*)h->impl)->nhalo
+                                           : ((const Impl<double>*)h->impl)->nhalo;
+}
+
+int spmd_ready(or_ecycle* h, bool running) {
+  if (!h) return OR_E_ARG;
+  if (!h->finalized) return fail(h, OR_E_STATE, "spmd call before finalize");
+  if (spmd_nhalo(h) < 0) return fail(h, OR_E_STATE, "spmd call before set_halo");
+  if (running != (h->spmd_k >= 0))
+    return fail(h, OR_E_STATE, running ? "spmd cycle outside spmd_begin/end" : "spmd_begin twice");
+  cudaSetDevice(h->cfg.device);
+  return OR_OK;
+}
+
 #define DISPATCH(h, fn, ...) \
   ((h)->cfg.precision == OR_PREC_SPLIT ? fn<float>(h, __VA_ARGS__) : fn<double>(h, __VA_ARGS__))
 
@@ -1517,6 +1641,55 @@ int or_ecycle_adjoint(or_ecycle* h, int ncycles, const or_adjoint_response* r, o
   }
   cudaSetDevice(h->cfg.device);
   return adjoint_impl(h, ncycles, r, t, J, dJ_dA, dJ_dthk, dJ_dms, dJ_din);
+}
+
+int or_ecycle_set_halo(or_ecycle* h, int part, int nloc, const int* local_node, const int* halo_slot,
+                       const int* count_ke, int nhalo) {
+  if (!h) return OR_E_ARG;
+  if (!h->finalized) return fail(h, OR_E_STATE, "set_halo before finalize");
+  if (h->parts.size() != 1 || part != 0) return fail(h, OR_E_UNSUPPORTED, "set_halo: one part per handle");
+  if (h->spmd_k >= 0) return fail(h, OR_E_STATE, "set_halo inside spmd_begin/end");
+  if (nloc < 0 || nhalo < 0 || nloc > nhalo || (nloc > 0 && (!local_node || !halo_slot)))
+    return fail(h, OR_E_ARG, "set_halo: bad argument");
+  cudaSetDevice(h->cfg.device);
+  return DISPATCH(h, set_halo_impl, nloc, local_node, halo_slot, count_ke, nhalo);
+}
+
+int or_ecycle_spmd_buffer_bytes(or_ecycle* h, long long* bytes) {
+  if (!h || !bytes) return OR_E_ARG;
+  if (!h->finalized) return fail(h, OR_E_STATE, "spmd_buffer_bytes before finalize");
+  const int nh = spmd_nhalo(h);
+  if (nh < 0) return fail(h, OR_E_STATE, "spmd_buffer_bytes before set_halo");
+  *bytes = (long long)(h->cfg.precision == OR_PREC_SPLIT ? halo_buffer_bytes<float>(nh) : halo_buffer_bytes<double>(nh));
+  return OR_OK;
+}
+
+int or_ecycle_spmd_begin(or_ecycle* h, or_ecycle_time* t) {
+  int rc = spmd_ready(h, false);
+  if (rc) return rc;
+  if (!t) return fail(h, OR_E_ARG, "spmd_begin: null time");
+  return DISPATCH(h, spmd_begin_impl, t);
+}
+
+int or_ecycle_spmd_elements(or_ecycle* h, void* dev_buf) {
+  int rc = spmd_ready(h, true);
+  if (rc) return rc;
+  if (!dev_buf) return fail(h, OR_E_ARG, "spmd_elements: null buffer");
+  return DISPATCH(h, spmd_elements_impl, dev_buf);
+}
+
+int or_ecycle_spmd_nodes(or_ecycle* h, const void* dev_bufs, int nranks) {
+  int rc = spmd_ready(h, true);
+  if (rc) return rc;
+  if (!dev_bufs || nranks < 1) return fail(h, OR_E_ARG, "spmd_nodes: bad argument");
+  return DISPATCH(h, spmd_nodes_impl, dev_bufs, nranks);
+}
+
+int or_ecycle_spmd_end(or_ecycle* h, or_ecycle_time* t) {
+  int rc = spmd_ready(h, true);
+  if (rc) return rc;
+  if (!t) return fail(h, OR_E_ARG, "spmd_end: null time");
+  return DISPATCH(h, spmd_end_impl, t);
 }
 
 int or_ecycle_get_nodes(or_ecycle* h, int part, double* x, double* d, double* v, double* vr) {

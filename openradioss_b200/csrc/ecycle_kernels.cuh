@@ -149,7 +149,23 @@ struct NodeArgs {
   ErrorWord* err;
   double growth, dtmx;
   int ntiles, nparts, split;
+  // Domain decomposition (one part split over ranks); halo_slot is null otherwise.
+  // A node shared with other ranks takes its force and moment as the sum of every
+  // rank's partial sum, rank by rank, from the gathered exchange buffers; the
+  // time step is the minimum of every rank's reduction.
+  const int* halo_slot;            // per node: its slot in the exchange buffers, or -1
+  const unsigned char* halo_ke;    // per node: 0 if another rank counts its kinetic energy
+  const unsigned char* xbuf;       // nranks exchange buffers, xbytes each (halo_pack_kernel layout)
+  size_t xbytes;
+  int nranks, nhalo;
 };
+
+// Exchange buffer of one rank: nhalo force sums (R4), nhalo moment sums (R4),
+// then the rank's PartAcc of the cycle.
+template <class R>
+__host__ __device__ inline size_t halo_buffer_bytes(int nhalo) {
+  return 2 * (size_t)nhalo * sizeof(typename Vec4<R>::T) + sizeof(PartAcc);
+}
 
 // ---------------------------------------------------------------------------
 // helpers
@@ -1086,7 +1102,14 @@ node_kernel(NodeArgs<R> a, int parity) {
       if (k1 > k0) m0 = mslot[k0];
     }
     const PartTime t0 = a.time[parity * a.nparts + part];
-    const PartAcc ac = a.acc[parity * a.nparts + part];
+    PartAcc ac = a.acc[parity * a.nparts + part];
+    if (a.halo_slot) {   // SPMD: time step = min over every rank's reduction (SPMD_GLOB_MIN5)
+      for (int r = 0; r < a.nranks; ++r) {
+        const PartAcc o = *reinterpret_cast<const PartAcc*>(a.xbuf + (size_t)r * a.xbytes + 2 * (size_t)a.nhalo * sizeof(R4));
+        ac.dtkey = o.dtkey < ac.dtkey ? o.dtkey : ac.dtkey;
+        ac.dtbits = o.dtbits < ac.dtbits ? o.dtbits : ac.dtbits;
+      }
+    }
     // dt logic (resol.F:5853-5858, 6080, 6224-6226), identical in every thread
     const double dt2t = __longlong_as_double((long long)ac.dtbits);
     double DT2 = 1e6;                                  // EP06
@@ -1109,6 +1132,14 @@ node_kernel(NodeArgs<R> a, int parity) {
       for (int k = k0 + 1; k < k1; ++k) {
         const R4 f = fslot[k];
         ax += f.x; ay += f.y; az += f.z;
+      }
+      const int hs = a.halo_slot ? a.halo_slot[n] : -1;
+      if (hs >= 0) {       // SPMD_EXCH_A: every rank's partial, in rank order
+        for (int r = 0; r < a.nranks; ++r) {
+          const R4 f = reinterpret_cast<const R4*>(a.xbuf + (size_t)r * a.xbytes)[hs];
+          if (r == 0) { ax = f.x; ay = f.y; az = f.z; }
+          else { ax += f.x; ay += f.y; az += f.z; }
+        }
       }
       // ACCELE (accele.F:63-80)
       const R ms = R(xm.w);
@@ -1140,6 +1171,13 @@ node_kernel(NodeArgs<R> a, int parity) {
           const R4 m = mslot[k];
           rx += m.x; ry += m.y; rz += m.z;
         }
+        if (hs >= 0) {
+          for (int r = 0; r < a.nranks; ++r) {
+            const R4 m = reinterpret_cast<const R4*>(a.xbuf + (size_t)r * a.xbytes)[a.nhalo + hs];
+            if (r == 0) { rx = m.x; ry = m.y; rz = m.z; }
+            else { rx += m.x; ry += m.y; rz += m.z; }
+          }
+        }
         const R in = w.w;
         if (in > R(0)) { const R r = R(1) / in; rx *= r; ry *= r; rz *= r; }
         else { rx = ry = rz = R(0); }
@@ -1153,6 +1191,7 @@ node_kernel(NodeArgs<R> a, int parity) {
         VR[n] = w;
       }
     }
+    if (valid && a.halo_slot && !a.halo_ke[n]) { ek = 0.0; ekr = 0.0; }   // counted by another rank
     // per-tile kinetic energy partials (fixed tree order -> deterministic)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -1178,6 +1217,41 @@ node_kernel(NodeArgs<R> a, int parity) {
     }
     __syncthreads();
   }
+}
+
+// ===========================================================================
+// halo pack (domain decomposition): this rank's partial force and moment sums of
+// every halo node it holds (its slots in ascending order, as the node kernel adds
+// them), zero for halo nodes it does not hold, and its reduction of the cycle
+// ===========================================================================
+template <class R>
+__global__ void __launch_bounds__(128)
+halo_pack_kernel(const int* __restrict__ halo_node, const int* __restrict__ adsky,
+                 const typename Vec4<R>::T* __restrict__ fslot, const typename Vec4<R>::T* __restrict__ mslot,
+                 const PartAcc* __restrict__ acc, unsigned char* buf, int nhalo) {
+  typedef typename Vec4<R>::T R4;
+  R4* F = reinterpret_cast<R4*>(buf);
+  R4* M = F + nhalo;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) *reinterpret_cast<PartAcc*>(M + nhalo) = acc[0];
+  if (i >= nhalo) return;
+  const int n = halo_node[i];
+  R4 f = mk4(R(0), R(0), R(0), R(0)), m = f;
+  if (n >= 0) {
+    const int k0 = adsky[n], k1 = adsky[n + 1];
+    if (k1 > k0) {
+      f = fslot[k0];
+      if (mslot) m = mslot[k0];
+    }
+    for (int k = k0 + 1; k < k1; ++k) {
+      const R4 a = fslot[k];
+      f.x += a.x; f.y += a.y; f.z += a.z;
+      if (mslot) { const R4 b = mslot[k]; m.x += b.x; m.y += b.y; m.z += b.z; }
+    }
+    f.w = R(0); m.w = R(0);
+  }
+  F[i] = f;
+  M[i] = m;
 }
 
 }  // namespace orb

@@ -45,7 +45,8 @@ EXPORTS = [
     "or_ecycle_get_hex_state", "or_ecycle_get_shell_state", "or_ecycle_energies",
     "or_ecycle_error_info", "or_ecycle_phase_times", "or_ecycle_launch_count",
     "or_ecycle_stream", "or_ecycle_device_bytes", "or_ecycle_adjoint", "or_ecycle_hex_step_noalloc",
-    "or_ecycle_kernel_times",
+    "or_ecycle_kernel_times", "or_ecycle_set_halo", "or_ecycle_spmd_buffer_bytes", "or_ecycle_spmd_begin",
+    "or_ecycle_spmd_elements", "or_ecycle_spmd_nodes", "or_ecycle_spmd_end",
 ]
 
 
@@ -75,6 +76,12 @@ def _declare(lib):
         "or_ecycle_phase_times": ([P, dp], C.c_int),
         "or_ecycle_launch_count": ([P, C.POINTER(C.c_longlong)], C.c_int),
         "or_ecycle_kernel_times": ([P, C.c_int, dp], C.c_int),
+        "or_ecycle_set_halo": ([P, C.c_int, C.c_int, ip, ip, ip, C.c_int], C.c_int),
+        "or_ecycle_spmd_buffer_bytes": ([P, C.POINTER(C.c_longlong)], C.c_int),
+        "or_ecycle_spmd_begin": ([P, C.POINTER(abi.Time)], C.c_int),
+        "or_ecycle_spmd_elements": ([P, P], C.c_int),
+        "or_ecycle_spmd_nodes": ([P, P, C.c_int], C.c_int),
+        "or_ecycle_spmd_end": ([P, C.POINTER(abi.Time)], C.c_int),
         "or_ecycle_stream": ([P, C.POINTER(C.c_void_p)], C.c_int),
         "or_ecycle_device_bytes": ([P, C.POINTER(C.c_longlong)], C.c_int),
         "or_ecycle_adjoint": ([P, C.c_int, C.POINTER(abi.AdjointResponse), C.POINTER(abi.Time), dp, dp, dp, dp, dp],
