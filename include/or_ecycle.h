@@ -110,6 +110,8 @@ typedef struct {
   int    npt;           /* integration points through the thickness, 1..10        */
   int    ithk;          /* 1: element uses the current thickness (ITHK>0)         */
   int    ipla;          /* 0: radial return (the only implemented IPLA)           */
+  int    ishfram;       /* local frame: 0 (default) or 2 (/SHFRA/V4, contrl.F:478-486;
+                           cnvec3.F:82-106)                                        */
   double hm, hf, hr;    /* GEO(13..15) hourglass coefficients                     */
   double shf;           /* shear factor SHF (5/6 for ISH=0)                       */
   double pressure;      /* uniform /PLOAD-style pressure on the group, Pa (0=none)*/
@@ -168,6 +170,20 @@ int  or_ecycle_add_shell_group(or_ecycle* h, int part, int nel, const int* ixc,
 /* Per-element LAW2 yield stress A of a shell group (replaces uparam(1) per
    element; used by the sensitivity workload).  jc_a: nel values, Pa. */
 int  or_ecycle_set_shell_yield(or_ecycle* h, int group, const double* jc_a);
+
+/* Rigid velocity link of the engine's /VEL/TRA and /VEL/ROT cards (frelnk.F:75-101,
+   RLINK10 rlink10.F:60-90, RLINK1 rlink1.F): after ACCELE and BCS10, every node of
+   the link takes the mass-weighted mean acceleration of the link's nodes in the
+   directions of ic (4=x, 2=y, 1=z; weights MS) and the inertia-weighted mean
+   rotational acceleration in the directions of icr (weights IN); BCS10 is then
+   applied again (resol.F:7022, :7053, :7458).  nodes: nnod 1-based node numbers
+   of the part; a node belongs to one link at most; global axes only (no skew).
+   Before finalize; returns the link's index in *link. */
+int  or_ecycle_add_rlink(or_ecycle* h, int part, int nnod, const int* nodes,
+                         int ic, int icr, int* link);
+/* Changes the directions of a link between steps (an engine file that no longer
+   lists it: ic = icr = 0). */
+int  or_ecycle_set_rlink(or_ecycle* h, int link, int ic, int icr);
 
 /* Builds the Parith/ON assembly tables (element_pon_: ADSKY/IADS/IADC) on the
    device and allocates work buffers.  Must follow the last add_* call. */

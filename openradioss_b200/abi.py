@@ -47,7 +47,7 @@ class SolidProp(C.Structure):
 
 class ShellProp(C.Structure):
     _fields_ = [("thk", C.c_double), ("npt", C.c_int), ("ithk", C.c_int), ("ipla", C.c_int),
-                ("hm", C.c_double), ("hf", C.c_double), ("hr", C.c_double), ("shf", C.c_double),
+                ("ishfram", C.c_int), ("hm", C.c_double), ("hf", C.c_double), ("hr", C.c_double), ("shf", C.c_double),
                 ("pressure", C.c_double)]
 
 
@@ -88,8 +88,8 @@ def make_solid_prop(p: dict) -> SolidProp:
 
 
 def make_shell_prop(p: dict) -> ShellProp:
-    return ShellProp(p["thk"], int(p["npt"]), int(p["ithk"]), int(p["ipla"]), p["hm"], p["hf"],
-                     p["hr"], p["shf"], p["pressure"])
+    return ShellProp(p["thk"], int(p["npt"]), int(p["ithk"]), int(p["ipla"]), int(p.get("ishfram", 0)),
+                     p["hm"], p["hf"], p["hr"], p["shf"], p["pressure"])
 
 
 def initial_time(dt2old=1e30):

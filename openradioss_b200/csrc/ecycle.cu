@@ -47,6 +47,10 @@ struct HPart {
   bool has_rot = false;
   int node_start = 0, node_pad = 0, tile_start = 0;
 };
+struct HLink {
+  int part = 0, ic = 0, icr = 0;
+  std::vector<int> nodes;           // part-local, 0-based
+};
 struct HHex {
   int part = 0, nel = 0, gofs = 0;
   std::vector<int> conn;            // 8*nel, part-local
@@ -86,6 +90,7 @@ struct or_ecycle {
   std::vector<HPart> parts;
   std::vector<HHex> hex;
   std::vector<HShell> shell;
+  std::vector<HLink> links;
   bool finalized = false;
   int tile_hex = 256, tile_shell = 256, tile_node = NODE_TILE;
   // device state
@@ -301,6 +306,9 @@ struct Impl {
   // domain decomposition: halo nodes of this rank's part
   DBuf<int> halo_slot, halo_node; DBuf<unsigned char> halo_ke;
   int nhalo = -1;            // -1: no halo set
+  // rigid links
+  DBuf<LinkDesc> linkd; DBuf<int> link_nodes, link_of; DBuf<LinkMean> link_mean;
+  int nlinks = 0;
 
   HexArgs<R> hargs() {
     HexArgs<R> a;
@@ -331,6 +339,7 @@ struct Impl {
     a.growth = h->cfg.dt_growth; a.dtmx = h->cfg.dtmx; a.ntiles = ntiles; a.nparts = nparts;
     a.split = sizeof(R) == 4;
     a.halo_slot = nullptr; a.halo_ke = nullptr; a.xbuf = nullptr; a.xbytes = 0; a.nranks = 0; a.nhalo = 0;
+    a.link_of = nlinks ? link_of.p : nullptr; a.link_mean = nlinks ? link_mean.p : nullptr;
     return a;
   }
   void free_all() {
@@ -342,6 +351,7 @@ struct Impl {
     dfree(ssig); dfree(spla); dfree(sthk); dfree(sthke); dfree(shourg); dfree(seint); dfree(sjca);
     dfree(sehour); dfree(swpla); dfree(zw);
     dfree(halo_slot); dfree(halo_node); dfree(halo_ke);
+    dfree(linkd); dfree(link_nodes); dfree(link_of); dfree(link_mean);
   }
 };
 
@@ -371,6 +381,15 @@ int launch_shell(or_ecycle* h, Impl<R>& m, int parity) {
 template <class R, int T>
 int launch_shell_npt(or_ecycle* h, Impl<R>& m, int parity) {
   return m.uniform_npt == 5 ? launch_shell<R, T, 5>(h, m, parity) : launch_shell<R, T, 0>(h, m, parity);
+}
+template <class R>
+int launch_link(or_ecycle* h, Impl<R>& m) {
+  if (!m.nlinks) return OR_OK;
+  link_kernel<R><<<(unsigned)m.nlinks, LINK_THREADS, 0, h->stream>>>(
+      m.linkd.p, m.link_nodes.p, m.adsky.p, m.fslot.p, m.mslot.p, m.X.p, m.VR.p, m.code.p, m.link_mean.p);
+  CK(cudaGetLastError());
+  h->launches++;
+  return OR_OK;
 }
 template <class R>
 int launch_node(or_ecycle* h, Impl<R>& m, int parity) {
@@ -413,6 +432,8 @@ int launch_cycle(or_ecycle* h, Impl<R>& m, int parity, cudaEvent_t* ev) {
        : h->tile_shell == 128 ? launch_shell_npt<R, 128>(h, m, parity) : launch_shell_npt<R, 256>(h, m, parity);
   if (rc) return rc;
   if (ev) CK(cudaEventRecord(ev[2], h->stream));
+  rc = launch_link<R>(h, m);
+  if (rc) return rc;
   rc = launch_node<R>(h, m, parity);
   if (rc) return rc;
   if (ev) CK(cudaEventRecord(ev[3], h->stream));
@@ -483,6 +504,27 @@ int finalize_impl(or_ecycle* h) {
     d.node_start = P.node_start; d.node_end = P.node_start + P.numnod; d.tile_start = P.tile_start;
     d.has_rot = P.has_rot ? 1 : 0;
     pd.push_back(d);
+  }
+  // rigid links: node lists in global padded numbering, code bit 6 on their nodes
+  if (!h->links.empty()) {
+    std::vector<LinkDesc> ld;
+    std::vector<int> ln, lof(nn, -1);
+    for (auto& L : h->links) {
+      LinkDesc d;
+      d.first = (int)ln.size(); d.count = (int)L.nodes.size(); d.ic = L.ic; d.icr = L.icr;
+      const int base = h->parts[L.part].node_start;
+      for (int n : L.nodes) {
+        ln.push_back(base + n);
+        lof[base + n] = (int)ld.size();
+        code[base + n] |= 64;
+      }
+      ld.push_back(d);
+    }
+    m.nlinks = (int)ld.size();
+    if ((rc = dput(h, m.linkd, ld)) || (rc = dput(h, m.link_nodes, ln)) || (rc = dput(h, m.link_of, lof)) ||
+        (rc = dalloc(h, m.link_mean, ld.size())))
+      return rc;
+    CK(cudaMemset(m.link_mean.p, 0, m.link_mean.n * sizeof(LinkMean)));
   }
   if ((rc = dput(h, m.X, X)) || (rc = dput(h, m.V, V)) || (rc = dput(h, m.VR, VR)) || (rc = dput(h, m.code, code)) ||
       (rc = dput(h, m.adsky, adsky)) || (rc = dput(h, m.tile_part, tile_part)) || (rc = dput(h, m.partd, pd)))
@@ -555,6 +597,7 @@ int finalize_impl(or_ecycle* h) {
     for (auto& g : h->shell) {
       ShellGroupDesc d{};
       d.part = g.part; d.law = g.mat.law; d.nel = g.nel; d.npt = g.prop.npt; d.ithk = g.prop.ithk;
+      d.ishfram = g.prop.ishfram;
       d.has_jca = g.jca.empty() ? 0 : 1;
       any_jca = any_jca || !g.jca.empty();
       d.rho0 = g.mat.rho0; d.young = g.mat.young; d.nu = g.mat.nu; d.shear = g.mat.shear; d.a11 = g.mat.a11;
@@ -1566,6 +1609,7 @@ int or_ecycle_add_shell_group(or_ecycle* h, int part, int nel, const int* ixc, c
     return fail(h, OR_E_ARG, "add_shell_group: bad argument");
   if (prop->npt < 1 || prop->npt > 10) return fail(h, OR_E_UNSUPPORTED, "shell npt outside 1..10");
   if (prop->ipla != 0) return fail(h, OR_E_UNSUPPORTED, "shell IPLA other than radial return");
+  if (prop->ishfram != 0 && prop->ishfram != 2) return fail(h, OR_E_UNSUPPORTED, "shell ISHFRAM other than 0 or 2");
   if (mat->law != OR_LAW_ELASTIC && mat->law != OR_LAW_JOHNSON_COOK) return fail(h, OR_E_UNSUPPORTED, "shell law");
   HShell g;
   g.part = part; g.nel = nel; g.mat = *mat; g.prop = *prop;
@@ -1596,6 +1640,48 @@ int or_ecycle_set_shell_yield(or_ecycle* h, int group, const double* jc_a) {
   if (group < 0 || group >= (int)h->shell.size() || !jc_a) return fail(h, OR_E_ARG, "set_shell_yield: bad argument");
   HShell& g = h->shell[group];
   g.jca.assign(jc_a, jc_a + g.nel);
+  return OR_OK;
+}
+
+int or_ecycle_add_rlink(or_ecycle* h, int part, int nnod, const int* nodes, int ic, int icr, int* link) {
+  if (!h) return OR_E_ARG;
+  if (h->finalized) return fail(h, OR_E_STATE, "add_rlink after finalize");
+  if (part < 0 || part >= (int)h->parts.size() || nnod < 1 || !nodes || ic < 0 || ic > 7 || icr < 0 || icr > 7)
+    return fail(h, OR_E_ARG, "add_rlink: bad argument");
+  HLink L;
+  L.part = part; L.ic = ic; L.icr = icr;
+  std::vector<char> seen(h->parts[part].numnod, 0);
+  for (auto& o : h->links)
+    if (o.part == part) for (int n : o.nodes) seen[n] = 1;
+  for (int i = 0; i < nnod; ++i) {
+    const int n = nodes[i] - 1;
+    if (n < 0 || n >= h->parts[part].numnod) return fail(h, OR_E_ARG, "add_rlink: node number out of range");
+    if (seen[n]) return fail(h, OR_E_UNSUPPORTED, "add_rlink: node already in a rigid link");
+    seen[n] = 1;
+    L.nodes.push_back(n);
+  }
+  if (icr && !h->parts[part].has_rot) return fail(h, OR_E_ARG, "add_rlink: rotations on a part without them");
+  h->links.push_back(std::move(L));
+  if (link) *link = (int)h->links.size() - 1;
+  return OR_OK;
+}
+
+int or_ecycle_set_rlink(or_ecycle* h, int link, int ic, int icr) {
+  if (!h) return OR_E_ARG;
+  if (link < 0 || link >= (int)h->links.size() || ic < 0 || ic > 7 || icr < 0 || icr > 7)
+    return fail(h, OR_E_ARG, "set_rlink: bad argument");
+  HLink& L = h->links[link];
+  if (icr && !h->parts[L.part].has_rot) return fail(h, OR_E_ARG, "set_rlink: rotations on a part without them");
+  L.ic = ic; L.icr = icr;
+  if (!h->finalized) return OR_OK;
+  cudaSetDevice(h->cfg.device);
+  int first = 0;
+  for (int l = 0; l < link; ++l) first += (int)h->links[l].nodes.size();
+  LinkDesc d;
+  d.first = first; d.count = (int)L.nodes.size(); d.ic = ic; d.icr = icr;
+  LinkDesc* dst = h->cfg.precision == OR_PREC_SPLIT ? ((Impl<float>*)h->impl)->linkd.p : ((Impl<double>*)h->impl)->linkd.p;
+  CK(cudaMemcpyAsync(dst + link, &d, sizeof(LinkDesc), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
   return OR_OK;
 }
 
@@ -1634,6 +1720,9 @@ int or_ecycle_adjoint(or_ecycle* h, int ncycles, const or_adjoint_response* r, o
   if (ncycles <= 0 || !r || !t) return fail(h, OR_E_ARG, "adjoint: bad argument");
   if (h->cfg.precision != OR_PREC_FP64) return fail(h, OR_E_UNSUPPORTED, "adjoint: FP64 handles only");
   if (!h->hex.empty() || h->shell.empty()) return fail(h, OR_E_UNSUPPORTED, "adjoint: shell groups only");
+  if (!h->links.empty()) return fail(h, OR_E_UNSUPPORTED, "adjoint: rigid links");
+  for (auto& g : h->shell)
+    if (g.prop.ishfram != 0) return fail(h, OR_E_UNSUPPORTED, "adjoint: ISHFRAM 0 only");
   if (r->node >= 0) {
     if (r->part < 0 || r->part >= (int)h->parts.size() || r->node >= h->parts[r->part].numnod || r->comp < 0 ||
         r->comp > 2)
@@ -1648,6 +1737,7 @@ int or_ecycle_set_halo(or_ecycle* h, int part, int nloc, const int* local_node, 
   if (!h) return OR_E_ARG;
   if (!h->finalized) return fail(h, OR_E_STATE, "set_halo before finalize");
   if (h->parts.size() != 1 || part != 0) return fail(h, OR_E_UNSUPPORTED, "set_halo: one part per handle");
+  if (!h->links.empty()) return fail(h, OR_E_UNSUPPORTED, "set_halo: rigid links across domains");
   if (h->spmd_k >= 0) return fail(h, OR_E_STATE, "set_halo inside spmd_begin/end");
   if (nloc < 0 || nhalo < 0 || nloc > nhalo || (nloc > 0 && (!local_node || !halo_slot)))
     return fail(h, OR_E_ARG, "set_halo: bad argument");

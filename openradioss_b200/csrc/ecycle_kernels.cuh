@@ -54,7 +54,7 @@ struct HexGroupDesc {
 
 struct ShellGroupDesc {
   int part, law, nel, npt;
-  int ithk, has_jca, pad0, pad1;
+  int ithk, has_jca, ishfram, pad1;
   double rho0, young, nu, shear, a11, a12, ssp, jc_a, jc_b, jc_n, sigmax;
   double hm, hf, hr, shf, pressure, dtfac, dtmin;
 };
@@ -74,6 +74,17 @@ struct PartTime {
 struct PartAcc {
   unsigned long long dtkey;   // (float(dt) bits << 32) | (type<<31 | element), min
   unsigned long long dtbits;  // exact dt bits (double), min
+};
+
+// rigid velocity link (/VEL/TRA, /VEL/ROT; rlink1.F): its nodes and directions
+struct LinkDesc {
+  int first, count;     // node range in link_nodes (global padded node numbers)
+  int ic, icr;          // translation / rotation directions, 4=x 2=y 1=z, 0 = off
+};
+// mean accelerations of one link in the current cycle (link_kernel)
+struct LinkMean {
+  double a[3], ar[3];
+  int ic, icr;          // directions applied: 0 where the link's mass (inertia) is zero
 };
 
 struct ErrorWord {
@@ -158,6 +169,10 @@ struct NodeArgs {
   const unsigned char* xbuf;       // nranks exchange buffers, xbytes each (halo_pack_kernel layout)
   size_t xbytes;
   int nranks, nhalo;
+  // rigid links: for a node with code bit 6, link_mean[link_of[n]] replaces its
+  // acceleration in the link's directions; null without links
+  const int* link_of;
+  const LinkMean* link_mean;
 };
 
 // Exchange buffer of one rank: nhalo force sums (R4), nhalo moment sums (R4),
@@ -749,11 +764,26 @@ shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
     const R X41 = R(sx[lc[3]] - x1), Y41 = R(sy[lc[3]] - y1), Z41 = R(sz[lc[3]] - z1);
     const R X32 = R(sx[lc[2]] - sx[lc[1]]), Y32 = R(sy[lc[2]] - sy[lc[1]]), Z32 = R(sz[lc[2]] - sz[lc[1]]);
     const R X34 = R(sx[lc[2]] - sx[lc[3]]), Y34 = R(sy[lc[2]] - sy[lc[3]]), Z34 = R(sz[lc[2]] - sz[lc[3]]);
-    // ---- CNVEC3, ISHFRAM = 0 (cnvec3.F:66-140) ----
+    // ---- CNVEC3, ISHFRAM = 0 (cnvec3.F:66-81) or 2 (cnvec3.F:82-106) ----
     R E1X = X21 + X34, E1Y = Y21 + Y34, E1Z = Z21 + Z34;
     R E2X = X32 + X41, E2Y = Y32 + Y41, E2Z = Z32 + Z41;
     R E3X = E1Y * E2Z - E1Z * E2Y, E3Y = E1Z * E2X - E1X * E2Z, E3Z = E1X * E2Y - E1Y * E2X;
-    {
+    if (gd.ishfram == 2) {
+      R su = E2X * E2X + E2Y * E2Y + E2Z * E2Z;
+      E1X = E1X * su + E2Y * E3Z - E2Z * E3Y;
+      E1Y = E1Y * su + E2Z * E3X - E2X * E3Z;
+      E1Z = E1Z * su + E2X * E3Y - E2Y * E3X;
+      su = ssqrt(E1X * E1X + E1Y * E1Y + E1Z * E1Z);
+      su = R(1) / (su > R(EM20) ? su : R(EM20));
+      E1X *= su; E1Y *= su; E1Z *= su;
+      su = ssqrt(E3X * E3X + E3Y * E3Y + E3Z * E3Z);
+      su = R(1) / (su > R(EM20) ? su : R(EM20));
+      E3X *= su; E3Y *= su; E3Z *= su;
+      E2X = E3Y * E1Z - E3Z * E1Y; E2Y = E3Z * E1X - E3X * E1Z; E2Z = E3X * E1Y - E3Y * E1X;
+      su = ssqrt(E2X * E2X + E2Y * E2Y + E2Z * E2Z);
+      su = R(1) / (su > R(EM20) ? su : R(EM20));
+      E2X *= su; E2Y *= su; E2Z *= su;
+    } else {
       R su = E3X * E3X + E3Y * E3Y + E3Z * E3Z;
       su = ssqrt(su);
       su = R(1) / (su > R(EM20) ? su : R(EM20));
@@ -1150,6 +1180,16 @@ node_kernel(NodeArgs<R> a, int parity) {
       if (code & 4) { v.x = R(0); ax = R(0); }
       if (code & 2) { v.y = R(0); ay = R(0); }
       if (code & 1) { v.z = R(0); az = R(0); }
+      if (code & 64) {      // RLINK10 (resol.F:7053), then BCS10 again (resol.F:7458)
+        const LinkMean* lm = &a.link_mean[a.link_of[n]];
+        const int ic = lm->ic;
+        if (ic & 4) ax = R(lm->a[0]);
+        if (ic & 2) ay = R(lm->a[1]);
+        if (ic & 1) az = R(lm->a[2]);
+        if (code & 4) ax = R(0);
+        if (code & 2) ay = R(0);
+        if (code & 1) az = R(0);
+      }
       const double dt05 = 0.5 * DT1;
       {
         const double wx = (double)v.x + dt05 * (double)ax, wy = (double)v.y + dt05 * (double)ay,
@@ -1184,6 +1224,16 @@ node_kernel(NodeArgs<R> a, int parity) {
         if (code & 32) { w.x = R(0); rx = R(0); }
         if (code & 16) { w.y = R(0); ry = R(0); }
         if (code & 8)  { w.z = R(0); rz = R(0); }
+        if (code & 64) {
+          const LinkMean* lm = &a.link_mean[a.link_of[n]];
+          const int icr = lm->icr;
+          if (icr & 4) rx = R(lm->ar[0]);
+          if (icr & 2) ry = R(lm->ar[1]);
+          if (icr & 1) rz = R(lm->ar[2]);
+          if (code & 32) rx = R(0);
+          if (code & 16) ry = R(0);
+          if (code & 8)  rz = R(0);
+        }
         const double wx = (double)w.x + dt05 * (double)rx, wy = (double)w.y + dt05 * (double)ry,
                      wz = (double)w.z + dt05 * (double)rz;
         ekr = (wx * wx + wy * wy + wz * wz) * 0.5 * (double)in;
@@ -1216,6 +1266,79 @@ node_kernel(NodeArgs<R> a, int parity) {
       }
     }
     __syncthreads();
+  }
+}
+
+// ===========================================================================
+// rigid links (RLINK1, rlink1.F): per link (one block), MASS = sum MS and
+// AX = sum MS*A over its nodes after ACCELE and BCS10 (the node kernel's
+// ASSPAR4 order), sums in FP64 in a fixed order; mean = AX / MASS.  Same for
+// the rotations with IN.  Runs between the element kernels and the node kernel.
+// ===========================================================================
+constexpr int LINK_THREADS = 128;
+
+template <class R>
+__global__ void __launch_bounds__(LINK_THREADS)
+link_kernel(const LinkDesc* __restrict__ links, const int* __restrict__ link_nodes, const int* __restrict__ adsky,
+            const typename Vec4<R>::T* __restrict__ fslot, const typename Vec4<R>::T* __restrict__ mslot,
+            const double4* __restrict__ X, const typename Vec4<R>::T* __restrict__ VR,
+            const unsigned char* __restrict__ codes, LinkMean* __restrict__ out) {
+  typedef typename Vec4<R>::T R4;
+  __shared__ double s_sum[8][LINK_THREADS / 32];
+  const LinkDesc L = links[blockIdx.x];
+  double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (L.ic | L.icr) {
+    for (int j = threadIdx.x; j < L.count; j += LINK_THREADS) {
+      const int n = link_nodes[L.first + j];
+      const int k0 = adsky[n], k1 = adsky[n + 1];
+      const unsigned char code = codes[n];
+      R ax = R(0), ay = R(0), az = R(0);
+      if (k1 > k0) { const R4 f = fslot[k0]; ax = f.x; ay = f.y; az = f.z; }
+      for (int k = k0 + 1; k < k1; ++k) { const R4 f = fslot[k]; ax += f.x; ay += f.y; az += f.z; }
+      const R ms = R(X[n].w);
+      if (ms > R(0)) { const R r = R(1) / ms; ax *= r; ay *= r; az *= r; }
+      else { ax = ay = az = R(0); }
+      if (code & 4) ax = R(0);
+      if (code & 2) ay = R(0);
+      if (code & 1) az = R(0);
+      s[0] += (double)ms; s[1] += (double)(ms * ax); s[2] += (double)(ms * ay); s[3] += (double)(ms * az);
+      if (VR && mslot && L.icr) {
+        R rx = R(0), ry = R(0), rz = R(0);
+        if (k1 > k0) { const R4 m = mslot[k0]; rx = m.x; ry = m.y; rz = m.z; }
+        for (int k = k0 + 1; k < k1; ++k) { const R4 m = mslot[k]; rx += m.x; ry += m.y; rz += m.z; }
+        const R in = VR[n].w;
+        if (in > R(0)) { const R r = R(1) / in; rx *= r; ry *= r; rz *= r; }
+        else { rx = ry = rz = R(0); }
+        if (code & 32) rx = R(0);
+        if (code & 16) ry = R(0);
+        if (code & 8)  rz = R(0);
+        s[4] += (double)in; s[5] += (double)(in * rx); s[6] += (double)(in * ry); s[7] += (double)(in * rz);
+      }
+    }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s[q] += __shfl_xor_sync(0xffffffffu, s[q], o);
+    if (lane == 0) s_sum[q][warp] = s[q];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      t[q] = 0.0;
+      for (int w = 0; w < LINK_THREADS / 32; ++w) t[q] += s_sum[q][w];
+    }
+    LinkMean r;
+    r.ic = t[0] != 0.0 ? L.ic : 0;        // rlink1.F: IF(MASS==ZERO)GOTO 250
+    r.icr = t[4] != 0.0 ? L.icr : 0;      // IF(INER==ZERO)RETURN
+    for (int c = 0; c < 3; ++c) {
+      r.a[c] = r.ic ? t[1 + c] / t[0] : 0.0;
+      r.ar[c] = r.icr ? t[5 + c] / t[4] : 0.0;
+    }
+    out[blockIdx.x] = r;
   }
 }
 

@@ -62,8 +62,8 @@ def solid_prop(qa=1.1, qb=0.05, qh=0.1):
     return dict(qa=qa, qb=qb, qh=qh)
 
 
-def shell_prop(thk, npt=5, ithk=1, hm=0.01, hf=0.01, hr=0.01, shf=5.0 / 6.0, pressure=0.0):
-    return dict(thk=thk, npt=npt, ithk=ithk, ipla=0, hm=hm, hf=hf, hr=hr, shf=shf,
+def shell_prop(thk, npt=5, ithk=1, hm=0.01, hf=0.01, hr=0.01, shf=5.0 / 6.0, pressure=0.0, ishfram=0):
+    return dict(thk=thk, npt=npt, ithk=ithk, ipla=0, ishfram=ishfram, hm=hm, hf=hf, hr=hr, shf=shf,
                 pressure=pressure)
 
 
@@ -302,3 +302,50 @@ def c5_adjoint_plate(n=200, ncycles=500, seed=1, **kw):
     jc_a = rng.uniform(300e6, 400e6, nel)
     thke = rng.uniform(0.9e-3, 1.1e-3, nel)
     return c2_shell_plate(n=n, ncycles=ncycles, jc_a=jc_a, thke=thke, **kw)
+
+
+def hat_rail(length=0.3, wall=0.03, top=0.05, h=5e-3, kink=(0.1, 0.2), offset=0.03, thk=1.5e-3,
+             mass=500.0, v0=10.0, npt=3, sigmax=600e6, ncycles=400):
+    """Crash rail: a hat section (two walls of height ``wall`` joined by a top
+    of width ``top``) swept along x over ``length``, the section moving by
+    ``offset`` along y on a linear S-ramp between x = kink[0] and kink[1]; BT
+    shells of edge ~h, LAW2 steel with a yield cap, 3 integration points,
+    /SHFRA/V4 element frames (ISHFRAM 2).  The end x = 0 is one rigid link
+    (x, y, z) carrying an added ``mass`` at its first node, all its nodes
+    starting at v0 along x; the end x = length is held along x; free wall
+    edges and both ends are held along z, with the rotations of the ends and
+    the x/y rotations of the wall edges fixed."""
+    nw, nt = int(round(wall / h)), int(round(top / h))
+    nc = int(round(length / h))
+    # section rows: wall 1 at y = top (z up), top at z = wall, wall 2 at y = 0 (z down)
+    rows = [(top, wall * k / nw) for k in range(nw)] + \
+           [(top - top * k / nt, wall) for k in range(nt)] + \
+           [(0.0, wall - wall * k / nw) for k in range(nw + 1)]
+    nr = len(rows) - 1
+    xc = np.linspace(0.0, length, nc + 1)
+    ramp = offset * np.clip((xc - kink[0]) / (kink[1] - kink[0]), 0.0, 1.0)
+    x = np.zeros(((nr + 1) * (nc + 1), 3))
+    nid = lambda r, c: r * (nc + 1) + c
+    for r, (y0, z) in enumerate(rows):
+        x[nid(r, 0):nid(r, nc) + 1, 0] = xc
+        x[nid(r, 0):nid(r, nc) + 1, 1] = y0 - ramp
+        x[nid(r, 0):nid(r, nc) + 1, 2] = z
+    R, Cc = np.meshgrid(np.arange(nr), np.arange(nc), indexing="ij")
+    R, Cc = R.ravel(), Cc.ravel()
+    conn = np.stack([nid(R, Cc), nid(R, Cc + 1), nid(R + 1, Cc + 1), nid(R + 1, Cc)], axis=1).astype(np.int64)
+    p = new_part(x)
+    mat = material(LAW_JOHNSON_COOK, 7850.0, 210e9, 0.3, 350e6, 275e6, 0.36, sigmax=sigmax)
+    add_shell(p, conn, mat, shell_prop(thk, npt=npt, ithk=0, hr=1e-5, ishfram=2))
+    left = np.array([nid(r, 0) for r in range(nr + 1)])
+    right = np.array([nid(r, nc) for r in range(nr + 1)])
+    edges = np.concatenate([np.arange(nid(0, 0), nid(0, nc) + 1), np.arange(nid(nr, 0), nid(nr, nc) + 1)])
+    p["icodt"][edges] |= 1
+    p["icodr"][edges] |= 6
+    p["icodt"][left] |= 1
+    p["icodr"][left] |= 7
+    p["icodt"][right] |= 5
+    p["icodr"][right] |= 7
+    p["v"][left, 0] = v0
+    p["ms"][left[0]] += mass
+    p["rlinks"] = [dict(nodes=left, ic=7, icr=0)]
+    return deck([p], ncycles=ncycles, name=f"hat_rail_{nr}x{nc}")

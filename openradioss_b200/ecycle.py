@@ -46,7 +46,8 @@ EXPORTS = [
     "or_ecycle_error_info", "or_ecycle_phase_times", "or_ecycle_launch_count",
     "or_ecycle_stream", "or_ecycle_device_bytes", "or_ecycle_adjoint", "or_ecycle_hex_step_noalloc",
     "or_ecycle_kernel_times", "or_ecycle_set_halo", "or_ecycle_spmd_buffer_bytes", "or_ecycle_spmd_begin",
-    "or_ecycle_spmd_elements", "or_ecycle_spmd_nodes", "or_ecycle_spmd_end",
+    "or_ecycle_spmd_elements", "or_ecycle_spmd_nodes", "or_ecycle_spmd_end", "or_ecycle_add_rlink",
+    "or_ecycle_set_rlink",
 ]
 
 
@@ -64,6 +65,8 @@ def _declare(lib):
         "or_ecycle_add_shell_group": ([P, C.c_int, C.c_int, ip, C.POINTER(abi.Material),
                                        C.POINTER(abi.ShellProp), dp, ip], C.c_int),
         "or_ecycle_set_shell_yield": ([P, C.c_int, dp], C.c_int),
+        "or_ecycle_add_rlink": ([P, C.c_int, C.c_int, ip, C.c_int, C.c_int, ip], C.c_int),
+        "or_ecycle_set_rlink": ([P, C.c_int, C.c_int, C.c_int], C.c_int),
         "or_ecycle_finalize": ([P], C.c_int),
         "or_ecycle_reset": ([P], C.c_int),
         "or_ecycle_step": ([P, C.c_int, C.POINTER(abi.Time)], C.c_int),
@@ -135,8 +138,15 @@ class _DeckModel:
                 if g.get("jc_a") is not None:
                     self._call("set_shell_yield", gi, abi.ptr(_f64(g["jc_a"]), C.c_double))
                 self.shell_groups.append((part, ixc.shape[0], int(g["prop"]["npt"])))
+            for rl in p.get("rlinks", []):
+                nodes = _i32(np.asarray(rl["nodes"]) + 1)
+                self._add_rlink(part, nodes.size, nodes, int(rl.get("ic", 7)), int(rl.get("icr", 0)))
         self._call("finalize")
         self.times = (abi.Time * self.nparts)(*[abi.initial_time() for _ in range(self.nparts)])
+
+    def set_rlink(self, link, ic, icr=0):
+        """New directions of rigid link ``link`` (0 and 0 switch it off)."""
+        self._call("set_rlink", int(link), int(ic), int(icr))
 
     # --- accessors -----------------------------------------------------------
     def numnod(self, part=0):
@@ -221,6 +231,11 @@ class ECycle(_DeckModel):
         self._call("add_shell_group", part, nel, abi.ptr(ixc, C.c_int), C.byref(mat), C.byref(prop),
                    abi.ptr(thke, C.c_double), C.byref(g))
         return g.value
+
+    def _add_rlink(self, part, n, nodes, ic, icr):
+        li = C.c_int()
+        self._call("add_rlink", part, n, abi.ptr(nodes, C.c_int), ic, icr, C.byref(li))
+        return li.value
 
     def step(self, ncycles):
         self._call("step", int(ncycles), self.times)

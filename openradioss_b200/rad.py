@@ -1,0 +1,350 @@
+"""Reader of Radioss block-format input decks for the element-cycle path.
+
+A reference run is a starter deck (``<run>_0000.rad``) followed by one or more
+engine decks (``<run>_0001.rad``, ...).  This module reads the keywords that
+define what the element cycle computes and turns them into the deck dict of
+:mod:`openradioss_b200.decks` (one part holding every node), with the starter's
+nodal masses and inertias:
+
+starter keywords
+  /BEGIN (input version >= 2017: 20-character real fields), /NODE,
+  /SHELL/<part>, /PART, /PROP/SHELL (TYPE1), /MAT/PLAS_JOHNS (LAW2, Iflag 0),
+  /MAT/ELAST (LAW1), /DEF_SHELL, /SHFRA/V4, /BCS (no skew), /GRNOD/NODE,
+  /INIVEL/TRA (no skew), /ADMAS/0
+engine keywords
+  /RUN (final time), /VEL/TRA and /VEL/ROT (rigid velocity links, no skew)
+
+Keywords that only request output (/TITLE, /TH, /ANIM, /PRINT, ...) are
+skipped; any other keyword raises :class:`RadError`, so a deck is never run
+with part of its physics silently dropped.
+
+Starter semantics restated here (the reference starter is not on the path):
+
+* /PROP/SHELL flags fall back to /DEF_SHELL, then to the built-in defaults
+  Ishell 1, Ismstr 2, Ithick 0, Iplas 0 (hm_read_prop01.F:112-272,
+  defaults_mod.F90:160-165); hm = hf = hr = 0.01 when zero and shear factor
+  5/6 (hm_read_prop01.F:204-240);
+* global integration N = 0 with LAW2 becomes 3 integration points
+  (cgrtails.F:795-806, warning 1912); LAW1 keeps N = 0 only with the
+  resultant law, which the element cycle does not implement;
+* shell nodal mass rho t A / 4 and inertia EMS (A / 9 + t^2 / 12), with A the
+  CEVECI area 1/2 |(x3 - x1) x (x4 - x2)| (cinmas.F:369, :703; ceveci.F);
+  /ADMAS type 0 adds its mass to every node of the group;
+* LAW2: G = E / 2(1 + nu), A11 = E / (1 - nu^2), shell sound speed
+  sqrt(E / rho) (hm_read_mat02_jc.F90); SIG_max0 = 0 and EPS_p_max = 0 mean
+  no limit.
+"""
+from __future__ import annotations
+
+import math
+import os
+
+import numpy as np
+
+from . import decks
+
+
+class RadError(ValueError):
+    """Deck outside what the reader (and the element cycle) implements."""
+
+
+# keywords that only steer output, restart files or the reference's own
+# parallel setup; they do not change the element cycle
+_IGNORED_STARTER = {"TITLE", "ANALY", "IOFLAG", "SPMD", "TH", "END", "RANDOM"}
+_IGNORED_ENGINE = {"ANIM", "PRINT", "TFILE", "MON", "VERS", "PROC", "H3D", "OUTP", "RFILE", "PARITH",
+                   "STOP", "TITLE", "END"}
+
+
+def _int(line, col, width=10, default=0):
+    s = line[col:col + width].strip()
+    return int(s) if s else default
+
+
+def _real(line, col, width=20, default=0.0):
+    s = line[col:col + width].strip()
+    if not s:
+        return default
+    s = s.replace("D", "E").replace("d", "e")
+    # Fortran reals may omit the exponent letter: "1.5-3"
+    for i in range(1, len(s)):
+        if s[i] in "+-" and s[i - 1] not in "eE" and s[i - 1].isdigit():
+            s = s[:i] + "e" + s[i:]
+            break
+    return float(s)
+
+
+def _blocks(path):
+    """(keyword fields, data lines, line number) of every block of a deck;
+    comment lines (#, $) dropped, ``#include`` followed relative to the deck."""
+    base = os.path.dirname(os.path.abspath(path))
+    out = []
+    cur = None
+
+    def feed(p):
+        nonlocal cur
+        with open(p, "r", errors="replace") as f:
+            for ln, raw in enumerate(f, 1):
+                line = raw.rstrip("\n\r")
+                if line.startswith("#include"):
+                    feed(os.path.join(base, line.split(None, 1)[1].strip()))
+                    continue
+                if not line.strip() or line[0] in "#$":
+                    continue
+                if line[0] == "/":
+                    cur = ([k for k in line.strip()[1:].split("/") if k != ""], [], (p, ln))
+                    out.append(cur)
+                elif cur is not None:
+                    cur[1].append(line)
+
+    feed(path)
+    return out
+
+
+def _node_list(lines):
+    ids = []
+    for line in lines:
+        for c in range(0, len(line), 10):
+            s = line[c:c + 10].strip()
+            if s:
+                ids.append(int(s))
+    return ids
+
+
+class StarterDeck:
+    """Content of a starter deck: the keywords listed in the module docstring."""
+
+    def __init__(self, path):
+        self.path = path
+        self.title = ""
+        self.invers = 0
+        self.nodes = {}            # id -> (x, y, z), file order
+        self.shells = {}           # part id -> list of (elem id, n1, n2, n3, n4)
+        self.parts = {}            # id -> (prop id, mat id)
+        self.props = {}            # id -> dict
+        self.mats = {}             # id -> dict
+        self.grnod = {}            # id -> list of node ids
+        self.bcs = []              # (tra code, rot code, grnod id)
+        self.inivel = []           # (vx, vy, vz, grnod id)
+        self.admas = []            # (mass, grnod id)
+        self.def_shell = dict(ishell=0, ismstr=0, ithick=0, iplas=0)
+        self.ishfram = 0
+        for key, lines, where in _blocks(path):
+            self._block(key, lines, where)
+
+    def _block(self, key, L, where):
+        k0 = key[0].upper()
+        if k0 == "BEGIN":
+            self.title = L[0].strip() if L else ""
+            self.invers = _int(L[1], 0) if len(L) > 1 else 0
+            if self.invers < 2017:
+                raise RadError(f"{where}: input version {self.invers}: only the 2017+ block format is read")
+        elif k0 in _IGNORED_STARTER:
+            if k0 == "RANDOM" and L and _real(L[0], 0) != 0.0:
+                raise RadError(f"{where}: /RANDOM noise is not implemented")
+        elif k0 == "NODE":
+            for line in L:
+                self.nodes[_int(line, 0)] = (_real(line, 10), _real(line, 30), _real(line, 50))
+        elif k0 == "SHELL":
+            part = int(key[1])
+            rows = self.shells.setdefault(part, [])
+            for line in L:
+                rows.append(tuple(_int(line, 10 * c) for c in range(5)))
+        elif k0 == "PART":
+            self.parts[int(key[1])] = (_int(L[1], 0), _int(L[1], 10))
+        elif k0 == "PROP":
+            if key[1].upper() not in ("SHELL", "TYPE1"):
+                raise RadError(f"{where}: /PROP/{key[1]} is not on the element-cycle path")
+            pid = int(key[2])
+            self.props[pid] = dict(
+                ishell=_int(L[1], 0), ismstr=_int(L[1], 10), ish3n=_int(L[1], 20), idrill=_int(L[1], 30),
+                hm=_real(L[2], 0), hf=_real(L[2], 20), hr=_real(L[2], 40), dm=_real(L[2], 60), dn=_real(L[2], 80),
+                n=_int(L[3], 0), istrain=_int(L[3], 10), thick=_real(L[3], 20), ashear=_real(L[3], 40),
+                ithick=_int(L[3], 60), iplas=_int(L[3], 70))
+        elif k0 == "MAT":
+            law = key[1].upper()
+            mid = int(key[2])
+            if law in ("PLAS_JOHNS", "LAW2"):
+                if _int(L[2], 40) != 0:
+                    raise RadError(f"{where}: /MAT/PLAS_JOHNS Iflag != 0 is not implemented")
+                c = _real(L[4], 0) if len(L) > 4 else 0.0
+                m = _real(L[5], 0) if len(L) > 5 else 0.0
+                if c != 0.0 or m != 0.0:
+                    raise RadError(f"{where}: strain-rate or thermal Johnson-Cook terms are not implemented")
+                self.mats[mid] = dict(law=2, rho=_real(L[1], 0), E=_real(L[2], 0), nu=_real(L[2], 20),
+                                      a=_real(L[3], 0), b=_real(L[3], 20), n=_real(L[3], 40),
+                                      epsmax=_real(L[3], 60), sigmax=_real(L[3], 80))
+            elif law in ("ELAST", "LAW1"):
+                self.mats[mid] = dict(law=1, rho=_real(L[1], 0), E=_real(L[2], 0), nu=_real(L[2], 20))
+            else:
+                raise RadError(f"{where}: /MAT/{key[1]} is not on the element-cycle path")
+        elif k0 == "DEF_SHELL":
+            self.def_shell = dict(ishell=_int(L[0], 0), ismstr=_int(L[0], 10), ithick=_int(L[0], 20),
+                                  iplas=_int(L[0], 30))
+        elif k0 == "SHFRA":
+            if len(key) < 2 or key[1].upper() != "V4":
+                raise RadError(f"{where}: /SHFRA only as /SHFRA/V4")
+            self.ishfram = 2           # contrl.F:478-486
+        elif k0 == "BCS":
+            line = L[1]
+            tra, rot = line[3:6], line[7:10]
+            if _int(line, 10) != 0:
+                raise RadError(f"{where}: /BCS with a skew frame is not implemented")
+            code = lambda s: sum(b for ch, b in zip(s.replace(" ", "0"), (4, 2, 1)) if ch == "1")
+            self.bcs.append((code(tra), code(rot), _int(line, 20)))
+        elif k0 == "GRNOD":
+            if key[1].upper() != "NODE":
+                raise RadError(f"{where}: /GRNOD/{key[1]} is not implemented")
+            self.grnod[int(key[2])] = _node_list(L[1:])
+        elif k0 == "INIVEL":
+            if key[1].upper() != "TRA":
+                raise RadError(f"{where}: /INIVEL/{key[1]} is not implemented")
+            line = L[1]
+            if _int(line, 70) != 0:
+                raise RadError(f"{where}: /INIVEL with a skew frame is not implemented")
+            self.inivel.append((_real(line, 0), _real(line, 20), _real(line, 40), _int(line, 60)))
+        elif k0 == "ADMAS":
+            if int(key[1]) != 0:
+                raise RadError(f"{where}: /ADMAS type {key[1]} is not implemented")
+            self.admas.append((_real(L[1], 0), _int(L[1], 20)))
+        else:
+            raise RadError(f"{where}: keyword /{'/'.join(key)} is not implemented")
+
+
+class EngineDeck:
+    """Content of one engine deck: final time and rigid velocity links."""
+
+    def __init__(self, path):
+        self.path = path
+        self.tstop = None
+        self.rlinks = []            # dict(ic, icr, nodes=[ids])
+        for key, lines, where in _blocks(path):
+            k0 = key[0].upper()
+            if k0 == "RUN":
+                self.tstop = _real(lines[0], 0)
+            elif k0 == "VEL":
+                kind = key[1].upper()
+                dirs = key[2].upper() if len(key) > 2 else "XYZ"
+                if len(key) > 3 and int(key[3]) != 0:
+                    raise RadError(f"{where}: /VEL with a skew frame is not implemented")
+                if kind not in ("TRA", "ROT"):
+                    raise RadError(f"{where}: /VEL/{key[1]} is not implemented")
+                ic = sum(b for ch, b in (("X", 4), ("Y", 2), ("Z", 1)) if ch in dirs)
+                self.rlinks.append(dict(ic=ic if kind == "TRA" else 0, icr=ic if kind == "ROT" else 0,
+                                        nodes=_node_list(lines)))
+            elif k0 in _IGNORED_ENGINE:
+                pass
+            else:
+                raise RadError(f"{where}: engine keyword /{'/'.join(key)} is not implemented")
+        if self.tstop is None:
+            raise RadError(f"{path}: no /RUN card")
+
+
+def _shell_flags(sd, prop):
+    """IHBE, ISMSTR, ITHK, IPLA and NPT after the starter's defaults."""
+    ds = sd.def_shell
+    ihbe = prop["ishell"] or ds["ishell"] or 1
+    ismstr = prop["ismstr"] or ds["ismstr"] or 2
+    ithk = prop["ithick"] or ds["ithick"]
+    ipla = prop["iplas"] or ds["iplas"]
+    return ihbe, ismstr, ithk, ipla
+
+
+def to_deck(sd: StarterDeck, name=None):
+    """The element-cycle deck of a starter deck: one part with every node (in
+    the order of /NODE), one shell group per /PART in ascending part id, and
+    ``ids`` (node ids) / ``elem_ids`` (element ids per group) for reporting."""
+    ids = np.array(list(sd.nodes.keys()), np.int64)
+    x = np.array(list(sd.nodes.values()), np.float64)
+    index = {int(i): k for k, i in enumerate(ids)}
+    part = decks.new_part(x)
+    elem_ids = []
+    for pid in sorted(sd.shells):
+        if pid not in sd.parts:
+            raise RadError(f"/SHELL/{pid}: no /PART/{pid}")
+        prop_id, mat_id = sd.parts[pid]
+        prop, mat = sd.props[prop_id], sd.mats[mat_id]
+        ihbe, ismstr, ithk, ipla = _shell_flags(sd, prop)
+        if ihbe != 1 or ismstr != 2:
+            raise RadError(f"/PROP/SHELL/{prop_id}: Ishell {ihbe} / Ismstr {ismstr}; the element cycle "
+                           "implements Ishell 1 with Ismstr 2")
+        if ipla not in (0, 2):
+            raise RadError(f"/PROP/SHELL/{prop_id}: Iplas {ipla} (iterative return) is not implemented")
+        if prop["dm"] != 0.0:
+            raise RadError(f"/PROP/SHELL/{prop_id}: membrane damping dm is not implemented")
+        npt = prop["n"]
+        if npt == 0:
+            if mat["law"] == 2:
+                npt = 3                     # cgrtails.F:795-806
+            else:
+                raise RadError(f"/PROP/SHELL/{prop_id}: global integration (N = 0) with LAW1")
+        if not 1 <= npt <= 10:
+            raise RadError(f"/PROP/SHELL/{prop_id}: N = {npt}")
+        rows = sorted(sd.shells[pid])
+        conn = np.array([[index[n] for n in r[1:]] for r in rows], np.int64)
+        if mat["law"] == 2:
+            m = decks.material(decks.LAW_JOHNSON_COOK, mat["rho"], mat["E"], mat["nu"], jc_a=mat["a"],
+                               jc_b=mat["b"], jc_n=mat["n"],
+                               epsmax=mat["epsmax"] if mat["epsmax"] > 0.0 else 1e20,
+                               sigmax=mat["sigmax"] if mat["sigmax"] > 0.0 else 1e20)
+        else:
+            m = decks.material(decks.LAW_ELASTIC, mat["rho"], mat["E"], mat["nu"])
+        p = decks.shell_prop(prop["thick"], npt=npt, ithk=1 if ithk > 0 else 0,
+                             hm=prop["hm"] or 0.01, hf=prop["hf"] or 0.01, hr=prop["hr"] or 0.01,
+                             ishfram=sd.ishfram)
+        if prop["ashear"] != 0.0:
+            p["shf"] = prop["ashear"]
+        if npt == 1:
+            p["shf"] = 0.0
+        decks.add_shell(part, conn, m, p)
+        elem_ids.append(np.array([r[0] for r in rows], np.int64))
+    for tra, rot, g in sd.bcs:
+        for n in sd.grnod[g]:
+            part["icodt"][index[n]] |= tra
+            part["icodr"][index[n]] |= rot
+    for vx, vy, vz, g in sd.inivel:
+        for n in sd.grnod[g]:
+            part["v"][index[n]] = (vx, vy, vz)
+    for mass, g in sd.admas:
+        for n in sd.grnod[g]:
+            part["ms"][index[n]] += mass
+    part["ids"] = ids
+    part["elem_ids"] = elem_ids
+    d = decks.deck([part], name=name or sd.title or "rad")
+    return d
+
+
+def add_engine(deck, ed: EngineDeck):
+    """The rigid links of an engine deck, as ``rlinks`` of the deck's part
+    (node ids mapped to 0-based node indices)."""
+    part = deck["parts"][0]
+    index = {int(i): k for k, i in enumerate(part["ids"])}
+    part["rlinks"] = [dict(ic=r["ic"], icr=r["icr"], nodes=np.array([index[n] for n in r["nodes"]], np.int64))
+                      for r in ed.rlinks]
+    return deck
+
+
+def element_id(deck, ityptst, neltst):
+    """User id of the element that set the time step (shell groups only)."""
+    if ityptst != 3 or neltst < 0:
+        return None
+    for ids in deck["parts"][0]["elem_ids"]:
+        if neltst < ids.size:
+            return int(ids[neltst])
+        neltst -= ids.size
+    return None
+
+
+def part_masses(deck):
+    """Structural mass of each shell group (rho t A), as the starter's
+    PART MASS table prints it."""
+    part = deck["parts"][0]
+    out = []
+    for g in part["shell"]:
+        conn = g["ixc"][:, 1:5] - 1
+        area = decks.shell_areas(part["x"], conn)
+        out.append(float(np.sum(g["mat"]["rho0"] * g["thke"] * area)))
+    return out
+
+
+def total_mass(deck):
+    return float(np.sum(deck["parts"][0]["ms"]))

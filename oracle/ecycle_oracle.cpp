@@ -3,10 +3,15 @@
 // baseline).  Nothing in the product links or calls this file.
 //
 // Parity status: the reference (Fortran, no compiler in this container) cannot
-// be run here; this restatement is pinned by hand-derived known-answer tests
-// (tests/test_oracle_known_answers.py) and by the reference's own miniqa
-// energy tolerances where applicable.  Parity against the reference binary is
-// unpinned.
+// be run here.  This restatement is pinned against the reference engine's own
+// output: on the reference's QA case miniqa/RESTART/cra2 (BT shells, LAW2
+// with a yield cap, 3 integration points, ISHFRAM 2, /BCS, /ADMAS, /INIVEL,
+// a /VEL/TRA rigid link, two engine runs, 3375 cycles) it reproduces every
+// printed digit of the listing's time, time step, time-step element,
+// internal and kinetic energies (tests/test_oracle_cra2.py, fixture
+// tests/golden/cra2_listing.json).  The solid path is pinned by hand-derived
+// known-answer tests (tests/test_oracle_known_answers.py); no reference
+// listing exercises it.
 //
 // Each routine follows the reference routine cited beside it, in the same
 // operation order, with "my_real" = R (double for the FP64 form, float for the
@@ -25,6 +30,7 @@
 #include <vector>
 #include <string>
 #include <algorithm>
+#include <array>
 #include <omp.h>
 #include "../include/or_ecycle.h"
 
@@ -110,12 +116,19 @@ struct PartData {
   double ekin = 0, ekinr = 0;
 };
 
+// rigid velocity link (/VEL/TRA, /VEL/ROT): frelnk.F:75-101, rlink1.F
+struct RLink {
+  int part, ic, icr;
+  std::vector<int> nodes;     // 0-based, in the card's order
+};
+
 template <class R>
 struct Model {
   or_ecycle_config cfg;
   std::vector<PartData<R>> parts;
   std::vector<HexGroup<R>> hex;
   std::vector<ShellGroup<R>> shell;
+  std::vector<RLink> rlinks;
   bool finalized = false;
   std::string err;
   int errcode = 0, errindex = -1;
@@ -485,7 +498,7 @@ int hex_element(const Model<R>& m, HexGroup<R>& g, PartData<R>& P, int i, double
 }
 
 // ----------------------------------------------------------------------------
-// CFORC3 chain for one 4-node BT shell, Ishell=1 (IHBE=1), ISMSTR=2, ISHFRAM=0.
+// CFORC3 chain for one 4-node BT shell, Ishell=1 (IHBE=1), ISMSTR=2, ISHFRAM=0 or 2.
 // ----------------------------------------------------------------------------
 template <class R>
 int shell_element(const Model<R>& m, ShellGroup<R>& g, PartData<R>& P, int i, double dt1d,
@@ -508,7 +521,7 @@ int shell_element(const Model<R>& m, ShellGroup<R>& g, PartData<R>& P, int i, do
   const R OFF = std::min(R(1), R(1));   // OFFG = 1 (no deletion on the path)
   // coordinate differences: my_real in the reference; FP64 then cast in the split form
   auto dif = [&](const double* a, int p, int q) -> R { return split ? R(a[p] - a[q]) : R(R(a[p]) - R(a[q])); };
-  // CNVEC3 (cnvec3.F:66-140), ISHFRAM=0
+  // CNVEC3 (cnvec3.F:66-140), ISHFRAM=0 or 2
   R E1X, E1Y, E1Z, E2X, E2Y, E2Z, E3X, E3Y, E3Z;
   {
     R X21 = dif(XG, 1, 0), X32 = dif(XG, 2, 1), X34 = dif(XG, 2, 3), X41 = dif(XG, 3, 0);
@@ -517,6 +530,23 @@ int shell_element(const Model<R>& m, ShellGroup<R>& g, PartData<R>& P, int i, do
     E1X = X21 + X34; E1Y = Y21 + Y34; E1Z = Z21 + Z34;
     E2X = X32 + X41; E2Y = Y32 + Y41; E2Z = Z32 + Z41;
     E3X = E1Y * E2Z - E1Z * E2Y; E3Y = E1Z * E2X - E1X * E2Z; E3Z = E1X * E2Y - E1Y * E2X;
+    if (pr.ishfram == 2) {
+      // cnvec3.F:82-106: E1 = |E2|^2 E1 + E2 x E3 (E3 not yet normalised)
+      R SUMA = E2X * E2X + E2Y * E2Y + E2Z * E2Z;
+      E1X = E1X * SUMA + E2Y * E3Z - E2Z * E3Y;
+      E1Y = E1Y * SUMA + E2Z * E3X - E2X * E3Z;
+      E1Z = E1Z * SUMA + E2X * E3Y - E2Y * E3X;
+      SUMA = E1X * E1X + E1Y * E1Y + E1Z * E1Z;
+      SUMA = R(1) / std::max(std::sqrt(SUMA), R(EM20));
+      E1X *= SUMA; E1Y *= SUMA; E1Z *= SUMA;
+      SUMA = E3X * E3X + E3Y * E3Y + E3Z * E3Z;
+      SUMA = R(1) / std::max(std::sqrt(SUMA), R(EM20));
+      E3X *= SUMA; E3Y *= SUMA; E3Z *= SUMA;
+      E2X = E3Y * E1Z - E3Z * E1Y; E2Y = E3Z * E1X - E3X * E1Z; E2Z = E3X * E1Y - E3Y * E1X;
+      SUMA = E2X * E2X + E2Y * E2Y + E2Z * E2Z;
+      SUMA = R(1) / std::max(std::sqrt(SUMA), R(EM20));
+      E2X *= SUMA; E2Y *= SUMA; E2Z *= SUMA;
+    } else {
     R SUMA = E3X * E3X + E3Y * E3Y + E3Z * E3Z;
     SUMA = R(1) / std::max(std::sqrt(SUMA), R(EM20));
     E3X *= SUMA; E3Y *= SUMA; E3Z *= SUMA;
@@ -530,6 +560,7 @@ int shell_element(const Model<R>& m, ShellGroup<R>& g, PartData<R>& P, int i, do
     SUMA = R(1) / std::max(std::sqrt(SUMA), R(EM20));
     E1X *= SUMA; E1Y *= SUMA; E1Z *= SUMA;
     E2X = E3Y * E1Z - E3Z * E1Y; E2Y = E3Z * E1X - E3X * E1Z; E2Z = E3X * E1Y - E3Y * E1X;
+    }
   }
   // CDERI3 (cderi3.F:87-190)
   R X2, X3, X4, Y2, Y3, Y4, Z2;
@@ -884,36 +915,88 @@ int cycle(Model<R>& m, int p, or_ecycle_time& t, int nthreads, bool last) {
   t.dt2old = DT2;
   t.dt12 = 0.5 * (t.dt1 + t.dt2);
   const R DT12 = R(t.dt12);
-  // ASSPAR4 + ACCELE + BCS10 + (energies) + VELOCITY + DEPLA, per node
-  const int N = P.numnod;
-  std::vector<double> ek(last ? N : 0), ekr(last ? N : 0);
-  int nan_node = -1;
-#pragma omp parallel for num_threads(nthreads) schedule(static)
-  for (int n = 0; n < N; ++n) {
-    R a[3] = {0, 0, 0}, ar[3] = {0, 0, 0};
+  // ASSPAR4 + ACCELE (accele.F:63-123) + the acceleration part of BCS10 for node n
+  auto node_acc = [&P](int n, R* a, R* ar) {
+    a[0] = a[1] = a[2] = ar[0] = ar[1] = ar[2] = R(0);
     for (long k = P.adsky[n]; k < P.adsky[n + 1]; ++k) {
       const R* f = &P.fsky[8 * k];
       a[0] = a[0] + f[0]; a[1] = a[1] + f[1]; a[2] = a[2] + f[2];
       ar[0] = ar[0] + f[3]; ar[1] = ar[1] + f[4]; ar[2] = ar[2] + f[5];
     }
-    // ACCELE (accele.F:63-123)
     R msn = P.ms[n];
     if (msn > R(0)) { R r = R(1) / msn; a[0] *= r; a[1] *= r; a[2] *= r; }
     else { a[0] = a[1] = a[2] = 0; }
     R inn = P.in[n];
     if (inn > R(0)) { R r = R(1) / inn; ar[0] *= r; ar[1] *= r; ar[2] *= r; }
     else { ar[0] = ar[1] = ar[2] = 0; }
+  };
+  auto bcs_acc = [](int ct, int cr, R* a, R* ar) {
+    if (ct & 4) a[0] = 0;
+    if (ct & 2) a[1] = 0;
+    if (ct & 1) a[2] = 0;
+    if (cr & 4) ar[0] = 0;
+    if (cr & 2) ar[1] = 0;
+    if (cr & 1) ar[2] = 0;
+  };
+  // RLINK10 / RLINK1 (resol.F:7053, rlink1.F): per link, MASS = sum MS, AX = sum MS*A
+  // over its nodes after ACCELE and BCS10 (FRL6 sums in DOUBLE PRECISION), mean = AX/MASS
+  const int N = P.numnod;
+  std::vector<int> link_of;
+  std::vector<std::array<double, 6>> link_mean;
+  std::vector<std::array<int, 2>> link_dirs;
+  for (auto& L : m.rlinks) {
+    if (L.part != p || (L.ic == 0 && L.icr == 0)) continue;
+    if (link_of.empty()) link_of.assign(N, -1);
+    const int li = (int)link_mean.size();
+    double S[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int n : L.nodes) {
+      R a[3], ar[3];
+      node_acc(n, a, ar);
+      bcs_acc(P.icodt[n], P.icodr[n], a, ar);
+      const R msn = P.ms[n], inn = P.in[n];
+      S[0] += double(msn); S[1] += double(msn * a[0]); S[2] += double(msn * a[1]); S[3] += double(msn * a[2]);
+      S[4] += double(inn); S[5] += double(inn * ar[0]); S[6] += double(inn * ar[1]); S[7] += double(inn * ar[2]);
+      link_of[n] = li;
+    }
+    int ic = L.ic, icr = L.icr;
+    if (S[0] == 0.0) ic = 0;          // rlink1.F: IF(MASS==ZERO)GOTO 250
+    if (S[4] == 0.0) icr = 0;         // IF(INER==ZERO)RETURN
+    link_mean.push_back({ic ? S[1] / S[0] : 0.0, ic ? S[2] / S[0] : 0.0, ic ? S[3] / S[0] : 0.0,
+                         icr ? S[5] / S[4] : 0.0, icr ? S[6] / S[4] : 0.0, icr ? S[7] / S[4] : 0.0});
+    link_dirs.push_back({ic, icr});
+  }
+  // ASSPAR4 + ACCELE + BCS10 + RLINK10 + BCS10 + (energies) + VELOCITY + DEPLA, per node
+  std::vector<double> ek(last ? N : 0), ekr(last ? N : 0);
+  int nan_node = -1;
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+  for (int n = 0; n < N; ++n) {
+    R a[3], ar[3];
+    node_acc(n, a, ar);
+    const R msn = P.ms[n], inn = P.in[n];
     if (!std::isfinite(double(a[0]) + double(a[1]) + double(a[2]))) nan_node = n;
     R* v = &P.v[3 * n];
     R* vr = &P.vr[3 * n];
     // BCS10 / BCS1V (bcs1.F:52-100): bit 4 = x, 2 = y, 1 = z
     int ct = P.icodt[n], cr = P.icodr[n];
-    if (ct & 4) { v[0] = 0; a[0] = 0; }
-    if (ct & 2) { v[1] = 0; a[1] = 0; }
-    if (ct & 1) { v[2] = 0; a[2] = 0; }
-    if (cr & 4) { vr[0] = 0; ar[0] = 0; }
-    if (cr & 2) { vr[1] = 0; ar[1] = 0; }
-    if (cr & 1) { vr[2] = 0; ar[2] = 0; }
+    if (ct & 4) v[0] = 0;
+    if (ct & 2) v[1] = 0;
+    if (ct & 1) v[2] = 0;
+    if (cr & 4) vr[0] = 0;
+    if (cr & 2) vr[1] = 0;
+    if (cr & 1) vr[2] = 0;
+    bcs_acc(ct, cr, a, ar);
+    if (!link_of.empty() && link_of[n] >= 0) {
+      const int li = link_of[n];
+      const auto& mu = link_mean[li];
+      const int ic = link_dirs[li][0], icr = link_dirs[li][1];
+      if (ic & 4) a[0] = R(mu[0]);
+      if (ic & 2) a[1] = R(mu[1]);
+      if (ic & 1) a[2] = R(mu[2]);
+      if (icr & 4) ar[0] = R(mu[3]);
+      if (icr & 2) ar[1] = R(mu[4]);
+      if (icr & 1) ar[2] = R(mu[5]);
+      bcs_acc(ct, cr, a, ar);         // resol.F:7458 reimposes the BCS
+    }
     if (last) {   // ECRIT (ecrit.F:262-268, 315-322): DT05 = DT1/2
       double dt05 = 0.5 * DT1;
       double vx = double(v[0]) + dt05 * double(a[0]), vy = double(v[1]) + dt05 * double(a[1]), vz = double(v[2]) + dt05 * double(a[2]);
@@ -1006,6 +1089,7 @@ template <class R>
 int add_shell(Model<R>& m, int part, int nel, const int* ixc, const or_material* mat,
               const or_shell_prop* prop, const double* thke) {
   if (prop->npt < 1 || prop->npt > 10 || prop->ipla != 0) return OR_E_UNSUPPORTED;
+  if (prop->ishfram != 0 && prop->ishfram != 2) return OR_E_UNSUPPORTED;
   ShellGroup<R> g;
   g.part = part; g.nel = nel; g.mat = *mat; g.prop = *prop;
   g.gofs = m.parts[part].nel_shell;
@@ -1053,6 +1137,29 @@ int oracle_set_shell_yield(void* hh, int gi, const double* jc_a) {
     auto& g = m.shell[gi];
     g.jca.resize(g.nel);
     for (int i = 0; i < g.nel; ++i) g.jca[i] = jc_a[i];
+    return (int)OR_OK;
+  });
+}
+int oracle_add_rlink(void* hh, int part, int nnod, const int* nodes, int ic, int icr) {
+  Handle* h = (Handle*)hh;
+  return h->with([&](auto& m) {
+    if (part < 0 || part >= (int)m.parts.size() || nnod < 1 || !nodes || ic < 0 || ic > 7 || icr < 0 || icr > 7)
+      return (int)OR_E_ARG;
+    RLink L;
+    L.part = part; L.ic = ic; L.icr = icr;
+    for (int i = 0; i < nnod; ++i) {
+      if (nodes[i] < 1 || nodes[i] > m.parts[part].numnod) return (int)OR_E_ARG;
+      L.nodes.push_back(nodes[i] - 1);
+    }
+    m.rlinks.push_back(std::move(L));
+    return (int)OR_OK;
+  });
+}
+int oracle_set_rlink(void* hh, int link, int ic, int icr) {
+  Handle* h = (Handle*)hh;
+  return h->with([&](auto& m) {
+    if (link < 0 || link >= (int)m.rlinks.size() || ic < 0 || ic > 7 || icr < 0 || icr > 7) return (int)OR_E_ARG;
+    m.rlinks[link].ic = ic; m.rlinks[link].icr = icr;
     return (int)OR_OK;
   });
 }

@@ -40,6 +40,8 @@ def load(fast=False):
     lib.oracle_add_shell_group.argtypes = [P, C.c_int, C.c_int, ip, C.POINTER(abi.Material),
                                            C.POINTER(abi.ShellProp), dp]
     lib.oracle_set_shell_yield.argtypes = [P, C.c_int, dp]
+    lib.oracle_add_rlink.argtypes = [P, C.c_int, C.c_int, ip, C.c_int, C.c_int]
+    lib.oracle_set_rlink.argtypes = [P, C.c_int, C.c_int, C.c_int]
     lib.oracle_finalize.argtypes = [P]
     lib.oracle_step.argtypes = [P, C.c_int, C.POINTER(abi.Time), C.c_int]
     lib.oracle_get_nodes.argtypes = [P, C.c_int, dp, dp, dp, dp]
@@ -90,6 +92,9 @@ class Oracle(_DeckModel):
                    abi.ptr(thke, C.c_double))
         self._nshell += 1
         return self._nshell - 1
+
+    def _add_rlink(self, part, n, nodes, ic, icr):
+        self._call("add_rlink", part, n, abi.ptr(nodes, C.c_int), ic, icr)
 
     def step(self, ncycles):
         self._call("step", int(ncycles), self.times, self.nthreads)
