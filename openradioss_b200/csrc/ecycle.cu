@@ -260,6 +260,33 @@ int build_patches(or_ecycle* h, std::vector<GroupT>& groups, int tile, PatchSet&
   return OR_OK;
 }
 
+// Incidence lists of every patch at a fixed stride: nlmax+1 offsets, then for each
+// patch node the corners t*K+k (t: element of the patch, k: corner) that touch it,
+// in ascending order.  The kernels sum a node's corner forces in this order.
+int incidence_stride(const PatchSet& ps, int K, int tile) {
+  const int s = ps.nlmax + 1 + K * tile;
+  return s + (s & 1);
+}
+void incidence_lists(const PatchSet& ps, int K, int tile, std::vector<uint16_t>& inc) {
+  const size_t np = ps.info.size(), S = (size_t)incidence_stride(ps, K, tile), L = (size_t)ps.nlmax;
+  inc.assign(np * S, 0);
+  for (size_t p = 0; p < np; ++p) {
+    const PatchInfo& pi = ps.info[p];
+    uint16_t* ofs = &inc[p * S];
+    uint16_t* ent = ofs + L + 1;
+    std::vector<int> cnt(L + 1, 0);
+    for (int t = 0; t < pi.nel; ++t)
+      for (int k = 0; k < K; ++k) cnt[(ps.local[(size_t)(pi.elem0 + t) * K + k] & LOCAL_MASK) + 1]++;
+    for (size_t j = 0; j < L; ++j) cnt[j + 1] += cnt[j];
+    for (size_t j = 0; j <= L; ++j) ofs[j] = (uint16_t)cnt[j];
+    for (int t = 0; t < pi.nel; ++t)
+      for (int k = 0; k < K; ++k) {
+        const int l = ps.local[(size_t)(pi.elem0 + t) * K + k] & LOCAL_MASK;
+        ent[cnt[l]++] = (uint16_t)(t * K + k);
+      }
+  }
+}
+
 // Patch node and slot lists at a fixed stride of nlmax entries per patch; the
 // padding repeats the patch's first node (a valid address) with slot -1.
 void padded_lists(const PatchSet& ps, std::vector<int>& nodes, std::vector<int>& slots) {
@@ -293,6 +320,8 @@ struct Impl {
   // hexas
   PatchSet hps;
   DBuf<PatchInfo> hpatch; DBuf<HexGroupDesc> hdesc; DBuf<int> hnodes, hslots, helem; DBuf<uint4> hconn;
+  DBuf<uint16_t> hinc, sinc;
+  int hinc_stride = 0, sinc_stride = 0;
   DBuf<R> hsig, heint, hrho, hqvis, hpla, hepsd, hvol0; DBuf<double> hvol0dp;
   DBuf<double> hehour, hwpla;
   // shells
@@ -318,6 +347,7 @@ struct Impl {
     a.vol0 = hvol0.p; a.vol0dp = hvol0dp.p; a.fslot = fslot.p; a.time = time.p; a.acc = acc.p;
     a.blk_ehour = hehour.p; a.blk_wpla = hwpla.p; a.err = err.p;
     a.nelpad = hps.nelpad; a.nparts = nparts; a.npatch = (int)hps.info.size(); a.nlmax = hps.nlmax;
+    a.inc = hinc.p; a.inc_stride = hinc_stride;
     return a;
   }
   ShellArgs<R> sargs() {
@@ -329,6 +359,7 @@ struct Impl {
     a.blk_ehour = sehour.p; a.blk_wpla = swpla.p; a.err = err.p;
     a.nelpad = sps.nelpad; a.nparts = nparts; a.npatch = (int)sps.info.size(); a.maxnpt = maxnpt;
     a.nlmax = sps.nlmax;
+    a.inc = sinc.p; a.inc_stride = sinc_stride;
     return a;
   }
   NodeArgs<R> nargs(const or_ecycle* h) {
@@ -345,6 +376,7 @@ struct Impl {
   void free_all() {
     dfree(X); dfree(DX); dfree(DY); dfree(DZ); dfree(V); dfree(VR); dfree(code); dfree(adsky); dfree(tile_part);
     dfree(partd); dfree(fslot); dfree(mslot); dfree(time); dfree(acc); dfree(err); dfree(ekin); dfree(ekinr);
+    dfree(hinc); dfree(sinc);
     dfree(hpatch); dfree(hdesc); dfree(hnodes); dfree(hslots); dfree(helem); dfree(hconn); dfree(hsig); dfree(heint);
     dfree(hrho); dfree(hqvis); dfree(hpla); dfree(hepsd); dfree(hvol0); dfree(hvol0dp); dfree(hehour); dfree(hwpla);
     dfree(spatch); dfree(sdesc); dfree(snodes); dfree(sslots); dfree(selem); dfree(sdegen); dfree(sconn);
@@ -355,15 +387,21 @@ struct Impl {
   }
 };
 
+// dynamic shared memory of a patch kernel: node planes (x, y, z in FP64; velocities
+// in R), 24 planes of TILE corner forces, the incidence lists
 template <class R>
-size_t hex_smem(int nl) { return (size_t)nl * (3 * sizeof(double) + 6 * sizeof(R)); }
+size_t hex_smem(int nl, int tile, int inc_stride) {
+  return (size_t)nl * (3 * sizeof(double) + 3 * sizeof(R)) + 24 * (size_t)tile * sizeof(R) + 2 * (size_t)inc_stride;
+}
 template <class R>
-size_t shell_smem(int nl) { return (size_t)nl * (3 * sizeof(double) + 12 * sizeof(R)); }
+size_t shell_smem(int nl, int tile, int inc_stride) {
+  return (size_t)nl * (3 * sizeof(double) + 6 * sizeof(R)) + 24 * (size_t)tile * sizeof(R) + 2 * (size_t)inc_stride;
+}
 
 template <class R, int T>
 int launch_hex(or_ecycle* h, Impl<R>& m, int parity) {
   if (m.hps.info.empty()) return OR_OK;
-  size_t sm = hex_smem<R>(m.hps.nlmax);
+  size_t sm = hex_smem<R>(m.hps.nlmax, T, m.hinc_stride);
   hex_patch_kernel<R, T><<<(unsigned)m.hps.info.size(), T, sm, h->stream>>>(m.hargs(), parity);
   CK(cudaGetLastError());
   h->launches++;
@@ -372,7 +410,7 @@ int launch_hex(or_ecycle* h, Impl<R>& m, int parity) {
 template <class R, int T, int NPT>
 int launch_shell(or_ecycle* h, Impl<R>& m, int parity) {
   if (m.sps.info.empty()) return OR_OK;
-  size_t sm = shell_smem<R>(m.sps.nlmax);
+  size_t sm = shell_smem<R>(m.sps.nlmax, T, m.sinc_stride);
   shell_patch_kernel<R, T, NPT><<<(unsigned)m.sps.info.size(), T, sm, h->stream>>>(m.sargs(), parity, m.zw.p);
   CK(cudaGetLastError());
   h->launches++;
@@ -406,7 +444,8 @@ cudaError_t set_smem(F* f, int bytes) {
 
 template <class R>
 int set_smem_attrs(or_ecycle* h, Impl<R>& m) {
-  int hs = (int)hex_smem<R>(m.hps.nlmax), ss = (int)shell_smem<R>(m.sps.nlmax);
+  int hs = (int)hex_smem<R>(m.hps.nlmax, h->tile_hex, m.hinc_stride);
+  int ss = (int)shell_smem<R>(m.sps.nlmax, h->tile_shell, m.sinc_stride);
   if (hs > 200 * 1024 || ss > 200 * 1024) return fail(h, OR_E_UNSUPPORTED, "patch shared memory above 200 KB");
   CK(set_smem(hex_patch_kernel<R, 64>, hs));
   CK(set_smem(hex_patch_kernel<R, 128>, hs));
@@ -575,6 +614,10 @@ int finalize_impl(or_ecycle* h) {
     }
     std::vector<int> pn, pslot;
     padded_lists(ps, pn, pslot);
+    std::vector<uint16_t> inc;
+    incidence_lists(ps, 8, h->tile_hex, inc);
+    m.hinc_stride = incidence_stride(ps, 8, h->tile_hex);
+    if ((rc = dput(h, m.hinc, inc))) return rc;
     if ((rc = dput(h, m.hpatch, ps.info)) || (rc = dput(h, m.hdesc, desc)) || (rc = dput(h, m.hnodes, pn)) ||
         (rc = dput(h, m.hslots, pslot)) || (rc = dput(h, m.helem, elem)) || (rc = dput(h, m.hconn, conn)) ||
         (rc = dput(h, m.hrho, rho)) || (rc = dput(h, m.hvol0, vol0)) || (rc = dput(h, m.hvol0dp, vol0dp)))
@@ -627,6 +670,10 @@ int finalize_impl(or_ecycle* h) {
     }
     std::vector<int> pn, pslot;
     padded_lists(ps, pn, pslot);
+    std::vector<uint16_t> inc;
+    incidence_lists(ps, 4, h->tile_shell, inc);
+    m.sinc_stride = incidence_stride(ps, 4, h->tile_shell);
+    if ((rc = dput(h, m.sinc, inc))) return rc;
     if ((rc = dput(h, m.spatch, ps.info)) || (rc = dput(h, m.sdesc, desc)) || (rc = dput(h, m.snodes, pn)) ||
         (rc = dput(h, m.sslots, pslot)) || (rc = dput(h, m.selem, elem)) || (rc = dput(h, m.sdegen, degen)) ||
         (rc = dput(h, m.sconn, conn)) || (rc = dput(h, m.sthke, thke)) || (rc = dput(h, m.sthk, thke)) ||

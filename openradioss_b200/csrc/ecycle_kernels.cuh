@@ -99,6 +99,8 @@ struct HexArgs {
   const int* patch_nodes;     // nlmax per patch; padding repeats a node of the patch
   const int* patch_slots;     // nlmax per patch; padding -1
   const uint4* conn;          // 8 x uint16 local corners per element (colour in corner 0)
+  const unsigned short* inc;  // per patch (stride inc_stride): nlmax+1 offsets, then the
+                              // patch nodes' incident corners t*8+k in ascending order
   const int* elem_id;         // element number within its part (for NELTS)
   const double4* X;           // x, y, z, nodal mass
   const typename Vec4<R>::T* V;
@@ -113,6 +115,7 @@ struct HexArgs {
   ErrorWord* err;
   int nelpad, nparts, npatch;
   int nlmax;                  // stride of patch_nodes / patch_slots (padded per patch)
+  int inc_stride;
 };
 
 template <class R>
@@ -122,6 +125,8 @@ struct ShellArgs {
   const int* patch_nodes;     // nlmax per patch; padding repeats a node of the patch
   const int* patch_slots;     // nlmax per patch; padding -1
   const uint2* conn;          // 4 x uint16 local corners per element (colour in corner 0)
+  const unsigned short* inc;  // per patch (stride inc_stride): nlmax+1 offsets, then the
+                              // patch nodes' incident corners t*4+k in ascending order
   const int* elem_id;
   const int* degen;           // 1 if IXC(4)==IXC(5) (triangle stored as quad)
   const double4* X;
@@ -139,6 +144,7 @@ struct ShellArgs {
   ErrorWord* err;
   int nelpad, nparts, npatch, maxnpt;
   int nlmax;                  // stride of patch_nodes / patch_slots (padded per patch)
+  int inc_stride;
 };
 
 template <class R>
@@ -310,16 +316,17 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
   const int slot1 = tid + TILE < NLM ? a.patch_slots[p * NLM + tid + TILE] : -1;
   double pre_ehour = 0.0, pre_wpla = 0.0;
   if (tid == 0) { pre_ehour = a.blk_ehour[p]; pre_wpla = a.blk_wpla[p]; }
-  // shared layout, planes of NLM: x, y, z (double) | vx, vy, vz, fx, fy, fz (R)
+  // shared layout: planes of NLM x, y, z (double) | vx, vy, vz (R); 24 planes of
+  // TILE corner forces (R), plane (c*8+k) holding component c of corner k; the
+  // patch's incidence lists (uint16)
   double* sx = reinterpret_cast<double*>(smem_raw);
   double* sy = sx + NLM;
   double* sz = sy + NLM;
   R* svx = reinterpret_cast<R*>(sz + NLM);
   R* svy = svx + NLM;
   R* svz = svy + NLM;
-  R* sfx = svz + NLM;
-  R* sfy = sfx + NLM;
-  R* sfz = sfy + NLM;
+  R* sc = svz + NLM;
+  unsigned short* sinc = reinterpret_cast<unsigned short*>(sc + 24 * TILE);
   const int nelpad = a.nelpad;
   // issue every per-element load before the staging barrier so that they are in
   // flight together with the node gathers
@@ -345,7 +352,11 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
     const R4 vv = a.V[g];
     sx[j] = xx.x; sy[j] = xx.y; sz[j] = xx.z;
     svx[j] = vv.x; svy[j] = vv.y; svz[j] = vv.z;
-    sfx[j] = R(0); sfy[j] = R(0); sfz[j] = R(0);
+  }
+  {
+    const unsigned* src = reinterpret_cast<const unsigned*>(a.inc + (size_t)p * a.inc_stride);
+    unsigned* dst = reinterpret_cast<unsigned*>(sinc);
+    for (int i = tid; i < a.inc_stride / 2; i += TILE) dst[i] = src[i];
   }
   const HexGroupDesc gd = a.groups[pi.group];
   const bool active = tid < pi.nel;
@@ -644,20 +655,28 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
       }
     }
   }
-  // ---- colour-ordered shared-memory assembly ----
-  for (int c = 0; c < pi.ncolor; ++c) {
-    if (color == c) {
+  // ---- patch assembly: corner forces to shared memory, then each patch node sums
+  // its incident corners in ascending (element, corner) order ----
+  if (active) {
 #pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        const int l = lc[k];
-        sfx[l] += F[0][k]; sfy[l] += F[1][k]; sfz[l] += F[2][k];
-      }
+    for (int k = 0; k < 8; ++k) {
+      sc[(0 * 8 + k) * TILE + tid] = F[0][k];
+      sc[(1 * 8 + k) * TILE + tid] = F[1][k];
+      sc[(2 * 8 + k) * TILE + tid] = F[2][k];
     }
-    __syncthreads();
   }
+  (void)color;
+  __syncthreads();
   for (int j = tid; j < nl; j += TILE) {
+    R fx = R(0), fy = R(0), fz = R(0);
+    const int i1 = sinc[j + 1];
+    for (int i = sinc[j]; i < i1; ++i) {
+      const int q = sinc[NLM + 1 + i];
+      const int o = (q & 7) * TILE + (q >> 3);
+      fx += sc[o]; fy += sc[8 * TILE + o]; fz += sc[16 * TILE + o];
+    }
     const int s = j == tid ? slot0 : j == tid + TILE ? slot1 : a.patch_slots[p * NLM + j];
-    a.fslot[s] = mk4(sfx[j], sfy[j], sfz[j], R(0));
+    a.fslot[s] = mk4(fx, fy, fz, R(0));
   }
   // ---- dt min-reduction and energy partials ----
   block_reduce<TILE>(mykey, mybits, my_ehou, my_wpla, s_key, s_bits, s_s0, s_s1);
@@ -702,7 +721,9 @@ shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
   double* sx = reinterpret_cast<double*>(smem_raw);
   double* sy = sx + NLM;
   double* sz = sy + NLM;
-  R* sv = reinterpret_cast<R*>(sz + NLM);   // vx vy vz rx ry rz fx fy fz mx my mz: 12 planes of NLM
+  R* sv = reinterpret_cast<R*>(sz + NLM);   // vx vy vz rx ry rz: 6 planes of NLM
+  R* sc = sv + 6 * NLM;                     // 24 planes of TILE: component c of corner k at (c*4+k)
+  unsigned short* sinc = reinterpret_cast<unsigned short*>(sc + 24 * TILE);
   const int nelpad = a.nelpad;
   // per-element loads issued before the staging barrier (overlap with the gathers)
   constexpr int NP = NPT > 0 ? NPT : 1;
@@ -737,8 +758,11 @@ shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
     sx[j] = xx.x; sy[j] = xx.y; sz[j] = xx.z;
     sv[0 * NLM + j] = vv.x; sv[1 * NLM + j] = vv.y; sv[2 * NLM + j] = vv.z;
     sv[3 * NLM + j] = rr.x; sv[4 * NLM + j] = rr.y; sv[5 * NLM + j] = rr.z;
-#pragma unroll
-    for (int q = 6; q < 12; ++q) sv[q * NLM + j] = R(0);
+  }
+  {
+    const unsigned* src = reinterpret_cast<const unsigned*>(a.inc + (size_t)p * a.inc_stride);
+    unsigned* dst = reinterpret_cast<unsigned*>(sinc);
+    for (int i = tid; i < a.inc_stride / 2; i += TILE) dst[i] = src[i];
   }
   const ShellGroupDesc gd = a.groups[pi.group];
   const bool active = tid < pi.nel;
@@ -1063,23 +1087,32 @@ shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
       Mg[0][k] = -Mg[0][k]; Mg[1][k] = -Mg[1][k]; Mg[2][k] = -Mg[2][k];
     }
   }
-  // ---- colour-ordered shared-memory assembly ----
-  R* sf = sv + 6 * NLM;
-  for (int c = 0; c < pi.ncolor; ++c) {
-    if (color == c) {
+  // ---- patch assembly: corner forces and moments to shared memory, then each patch
+  // node sums its incident corners in ascending (element, corner) order ----
+  if (active) {
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const int l = lc[k];
-        sf[0 * NLM + l] += Fg[0][k]; sf[1 * NLM + l] += Fg[1][k]; sf[2 * NLM + l] += Fg[2][k];
-        sf[3 * NLM + l] += Mg[0][k]; sf[4 * NLM + l] += Mg[1][k]; sf[5 * NLM + l] += Mg[2][k];
+    for (int k = 0; k < 4; ++k) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        sc[(c * 4 + k) * TILE + tid] = Fg[c][k];
+        sc[((c + 3) * 4 + k) * TILE + tid] = Mg[c][k];
       }
     }
-    __syncthreads();
   }
+  (void)color;
+  __syncthreads();
   for (int j = tid; j < nl; j += TILE) {
+    R f0 = R(0), f1 = R(0), f2 = R(0), m0 = R(0), m1 = R(0), m2 = R(0);
+    const int i1 = sinc[j + 1];
+    for (int i = sinc[j]; i < i1; ++i) {
+      const int q = sinc[NLM + 1 + i];
+      const int o = (q & 3) * TILE + (q >> 2);
+      f0 += sc[o]; f1 += sc[4 * TILE + o]; f2 += sc[8 * TILE + o];
+      m0 += sc[12 * TILE + o]; m1 += sc[16 * TILE + o]; m2 += sc[20 * TILE + o];
+    }
     const int s = j == tid ? slot0 : j == tid + TILE ? slot1 : a.patch_slots[p * NLM + j];
-    a.fslot[s] = mk4(sf[0 * NLM + j], sf[1 * NLM + j], sf[2 * NLM + j], R(0));
-    a.mslot[s] = mk4(sf[3 * NLM + j], sf[4 * NLM + j], sf[5 * NLM + j], R(0));
+    a.fslot[s] = mk4(f0, f1, f2, R(0));
+    a.mslot[s] = mk4(m0, m1, m2, R(0));
   }
   block_reduce<TILE>(mykey, mybits, my_ehou, my_wpla, s_key, s_bits, s_s0, s_s1);
   if (tid == 0) {
