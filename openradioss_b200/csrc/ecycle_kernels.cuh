@@ -1143,27 +1143,24 @@ node_kernel(NodeArgs<R> a, int parity) {
   double* __restrict__ DZ = a.DZ;
   const unsigned char* __restrict__ codes = a.code;
   for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
+    // Node loads first, unconditionally: every part's node range is padded to whole
+    // tiles, so n < nnodpad and padding nodes hold zeros (no slots, no mass).  They
+    // are issued before the part descriptor arrives; `valid` gates the stores only.
+    const int n = tile * TILE + threadIdx.x;
+    const int k0 = adsky[n], k1 = adsky[n + 1];
+    const double4 xm = X[n];
+    R4 v = V[n];
+    const unsigned char code = codes[n];
+    const double dx = DX[n], dy = DY[n], dz = DZ[n];
+    R4 f0 = mk4(R(0), R(0), R(0), R(0)), m0 = f0, w0 = f0;
+    if (k1 > k0) f0 = fslot[k0];
+    if (VR) {                             // rotational loads issued with the others
+      w0 = VR[n];
+      if (k1 > k0 && mslot) m0 = mslot[k0];
+    }
     const int part = a.tile_part[tile];
     const PartDesc pd = a.parts[part];
-    const int n = tile * TILE + threadIdx.x;
     const bool valid = n < pd.node_end;
-    // node loads first: independent of the dt logic below
-    int k0 = 0, k1 = 0;
-    double4 xm = make_double4(0, 0, 0, 0);
-    R4 v = mk4(R(0), R(0), R(0), R(0));
-    double dx = 0, dy = 0, dz = 0;
-    unsigned char code = 0;
-    if (valid) {
-      k0 = adsky[n]; k1 = adsky[n + 1];
-      xm = X[n]; v = V[n]; code = codes[n];
-      dx = DX[n]; dy = DY[n]; dz = DZ[n];
-    }
-    R4 f0 = mk4(R(0), R(0), R(0), R(0)), m0 = f0, w0 = f0;
-    if (valid && k1 > k0) f0 = fslot[k0];
-    if (valid && pd.has_rot) {            // rotational loads issued with the others
-      w0 = VR[n];
-      if (k1 > k0) m0 = mslot[k0];
-    }
     const PartTime t0 = a.time[parity * a.nparts + part];
     PartAcc ac = a.acc[parity * a.nparts + part];
     if (a.halo_slot) {   // SPMD: time step = min over every rank's reduction (SPMD_GLOB_MIN5)
