@@ -200,6 +200,10 @@ int  or_ecycle_reset(or_ecycle* h);
 int  or_ecycle_step(or_ecycle* h, int ncycles, or_ecycle_time* t);
 
 /* --- download / upload for output and restart ---------------------------- */
+/* One part's nodes in the caller's layout (3 doubles per node; any pointer may be
+   NULL).  Synchronous; the host arrays are copied by DMA when they are pinned.
+   The copies go through a device staging buffer of 3 doubles per node of the
+   largest part, allocated by or_ecycle_finalize. */
 int  or_ecycle_get_nodes(or_ecycle* h, int part, double* x, double* d,
                          double* v, double* vr);
 int  or_ecycle_set_nodes(or_ecycle* h, int part, const double* x, const double* d,

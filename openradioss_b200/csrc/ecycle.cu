@@ -338,6 +338,8 @@ struct Impl {
   // rigid links
   DBuf<LinkDesc> linkd; DBuf<int> link_nodes, link_of; DBuf<LinkMean> link_mean;
   int nlinks = 0;
+  // staging of one nodal array of one part (3 doubles per node) for set/get_nodes
+  DBuf<double> stage;
 
   HexArgs<R> hargs() {
     HexArgs<R> a;
@@ -383,7 +385,7 @@ struct Impl {
     dfree(ssig); dfree(spla); dfree(sthk); dfree(sthke); dfree(shourg); dfree(seint); dfree(sjca);
     dfree(sehour); dfree(swpla); dfree(zw);
     dfree(halo_slot); dfree(halo_node); dfree(halo_ke);
-    dfree(linkd); dfree(link_nodes); dfree(link_of); dfree(link_mean);
+    dfree(linkd); dfree(link_nodes); dfree(link_of); dfree(link_mean); dfree(stage);
   }
 };
 
@@ -570,6 +572,11 @@ int finalize_impl(or_ecycle* h) {
     return rc;
   std::vector<double> zero(nn, 0.0);
   if ((rc = dput(h, m.DX, zero)) || (rc = dput(h, m.DY, zero)) || (rc = dput(h, m.DZ, zero))) return rc;
+  {
+    int maxn = 0;
+    for (auto& P : h->parts) maxn = std::max(maxn, P.numnod);
+    if ((rc = dalloc(h, m.stage, 3 * (size_t)maxn))) return rc;
+  }
   if ((rc = dalloc(h, m.fslot, (size_t)m.nslot))) return rc;
   CK(cudaMemset(m.fslot.p, 0, m.fslot.n * sizeof(R4)));
   if (!h->shell.empty()) {
@@ -907,71 +914,40 @@ int kernel_times_impl(or_ecycle* h, int reps, double* us) {
 
 template <class R>
 int get_nodes_impl(or_ecycle* h, int part, double* x, double* d, double* v, double* vr) {
-  typedef typename Vec4<R>::T R4;
   Impl<R>& m = *(Impl<R>*)h->impl;
   const HPart& P = h->parts[part];
   const int n = P.numnod, s = P.node_start;
+  if (n == 0) return OR_OK;
+  if (vr && !m.VR.p) std::fill(vr, vr + 3 * (size_t)n, 0.0);
+  double* dst[4] = {x, d, v, m.VR.p ? vr : nullptr};
+  for (int kind = 0; kind < 4; ++kind) {
+    if (!dst[kind]) continue;
+    node_io_kernel<R><<<(n + 255) / 256, 256, 0, h->stream>>>(kind, 0, m.stage.p, n, s, m.X.p, m.DX.p, m.DY.p, m.DZ.p,
+                                                             m.V.p, m.VR.p);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(dst[kind], m.stage.p, 3 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  }
   CK(cudaStreamSynchronize(h->stream));
-  if (x) {
-    std::vector<double4> X(n);
-    CK(cudaMemcpy(X.data(), m.X.p + s, n * sizeof(double4), cudaMemcpyDeviceToHost));
-    for (int i = 0; i < n; ++i) { x[3 * i] = X[i].x; x[3 * i + 1] = X[i].y; x[3 * i + 2] = X[i].z; }
-  }
-  if (d) {
-    std::vector<double> a(n), b(n), c(n);
-    CK(cudaMemcpy(a.data(), m.DX.p + s, n * sizeof(double), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(b.data(), m.DY.p + s, n * sizeof(double), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(c.data(), m.DZ.p + s, n * sizeof(double), cudaMemcpyDeviceToHost));
-    for (int i = 0; i < n; ++i) { d[3 * i] = a[i]; d[3 * i + 1] = b[i]; d[3 * i + 2] = c[i]; }
-  }
-  if (v) {
-    std::vector<R4> V(n);
-    CK(cudaMemcpy(V.data(), m.V.p + s, n * sizeof(R4), cudaMemcpyDeviceToHost));
-    for (int i = 0; i < n; ++i) { v[3 * i] = V[i].x; v[3 * i + 1] = V[i].y; v[3 * i + 2] = V[i].z; }
-  }
-  if (vr) {
-    if (m.VR.p) {
-      std::vector<R4> W(n);
-      CK(cudaMemcpy(W.data(), m.VR.p + s, n * sizeof(R4), cudaMemcpyDeviceToHost));
-      for (int i = 0; i < n; ++i) { vr[3 * i] = W[i].x; vr[3 * i + 1] = W[i].y; vr[3 * i + 2] = W[i].z; }
-    } else {
-      std::fill(vr, vr + 3 * (size_t)n, 0.0);
-    }
-  }
   return OR_OK;
 }
 
 template <class R>
 int set_nodes_impl(or_ecycle* h, int part, const double* x, const double* d, const double* v, const double* vr) {
-  typedef typename Vec4<R>::T R4;
   Impl<R>& m = *(Impl<R>*)h->impl;
   const HPart& P = h->parts[part];
   const int n = P.numnod, s = P.node_start;
+  if (n == 0) return OR_OK;
+  const double* src[4] = {x, d, v, m.VR.p ? vr : nullptr};
+  for (int kind = 0; kind < 4; ++kind) {
+    if (!src[kind]) continue;
+    // copy the caller's array (DMA when it is pinned), then scatter it on the device;
+    // stream order keeps the staging buffer free until the kernel has read it
+    CK(cudaMemcpyAsync(m.stage.p, src[kind], 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    node_io_kernel<R><<<(n + 255) / 256, 256, 0, h->stream>>>(kind, 1, m.stage.p, n, s, m.X.p, m.DX.p, m.DY.p, m.DZ.p,
+                                                             m.V.p, m.VR.p);
+    CK(cudaGetLastError());
+  }
   CK(cudaStreamSynchronize(h->stream));
-  if (x) {
-    std::vector<double4> X(n);
-    CK(cudaMemcpy(X.data(), m.X.p + s, n * sizeof(double4), cudaMemcpyDeviceToHost));
-    for (int i = 0; i < n; ++i) { X[i].x = x[3 * i]; X[i].y = x[3 * i + 1]; X[i].z = x[3 * i + 2]; }
-    CK(cudaMemcpy(m.X.p + s, X.data(), n * sizeof(double4), cudaMemcpyHostToDevice));
-  }
-  if (d) {
-    std::vector<double> a(n), b(n), c(n);
-    for (int i = 0; i < n; ++i) { a[i] = d[3 * i]; b[i] = d[3 * i + 1]; c[i] = d[3 * i + 2]; }
-    CK(cudaMemcpy(m.DX.p + s, a.data(), n * sizeof(double), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(m.DY.p + s, b.data(), n * sizeof(double), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(m.DZ.p + s, c.data(), n * sizeof(double), cudaMemcpyHostToDevice));
-  }
-  if (v) {
-    std::vector<R4> V(n);
-    for (int i = 0; i < n; ++i) V[i] = mk4(R(v[3 * i]), R(v[3 * i + 1]), R(v[3 * i + 2]), R(0));
-    CK(cudaMemcpy(m.V.p + s, V.data(), n * sizeof(R4), cudaMemcpyHostToDevice));
-  }
-  if (vr && m.VR.p) {
-    std::vector<R4> W(n);
-    CK(cudaMemcpy(W.data(), m.VR.p + s, n * sizeof(R4), cudaMemcpyDeviceToHost));
-    for (int i = 0; i < n; ++i) { W[i].x = R(vr[3 * i]); W[i].y = R(vr[3 * i + 1]); W[i].z = R(vr[3 * i + 2]); }
-    CK(cudaMemcpy(m.VR.p + s, W.data(), n * sizeof(R4), cudaMemcpyHostToDevice));
-  }
   return OR_OK;
 }
 

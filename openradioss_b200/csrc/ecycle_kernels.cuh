@@ -1300,6 +1300,36 @@ node_kernel(NodeArgs<R> a, int parity) {
 }
 
 // ===========================================================================
+// node input/output: one nodal array of a part between the caller's layout
+// (3 doubles per node, node-major, staged in device memory) and the device
+// layout.  kind: 0 X (keeps the mass in .w), 1 D, 2 V, 3 VR (keeps the inertia);
+// to_device: 1 stage -> device arrays, 0 device arrays -> stage.
+// ===========================================================================
+template <class R>
+__global__ void __launch_bounds__(256)
+node_io_kernel(int kind, int to_device, double* __restrict__ stage, int n, int s, double4* X, double* DX,
+               double* DY, double* DZ, typename Vec4<R>::T* V, typename Vec4<R>::T* VR) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double* q = stage + 3 * (size_t)i;
+  const int g = s + i;
+  if (to_device) {
+    const double a = q[0], b = q[1], c = q[2];
+    if (kind == 0) X[g] = make_double4(a, b, c, X[g].w);
+    else if (kind == 1) { DX[g] = a; DY[g] = b; DZ[g] = c; }
+    else if (kind == 2) V[g] = mk4(R(a), R(b), R(c), R(0));
+    else { const R w = VR[g].w; VR[g] = mk4(R(a), R(b), R(c), w); }
+  } else {
+    double a, b, c;
+    if (kind == 0) { const double4 x = X[g]; a = x.x; b = x.y; c = x.z; }
+    else if (kind == 1) { a = DX[g]; b = DY[g]; c = DZ[g]; }
+    else if (kind == 2) { const typename Vec4<R>::T v = V[g]; a = v.x; b = v.y; c = v.z; }
+    else { const typename Vec4<R>::T v = VR[g]; a = v.x; b = v.y; c = v.z; }
+    q[0] = a; q[1] = b; q[2] = c;
+  }
+}
+
+// ===========================================================================
 // rigid links (RLINK1, rlink1.F): per link (one block), MASS = sum MS and
 // AX = sum MS*A over its nodes after ACCELE and BCS10 (the node kernel's
 // ASSPAR4 order), sums in FP64 in a fixed order; mean = AX / MASS.  Same for
