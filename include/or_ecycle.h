@@ -137,7 +137,9 @@ typedef struct {
   double kinetic_rot;   /* 1/2 I |VR + DT1/2 AR|^2                          */
   double hourglass;     /* cumulative EHOUR                                 */
   double plastic_work;  /* cumulative sum sigma_y * dpla * volume           */
-  double pad;
+  double external_work; /* cumulative WFEXT of the /CLOAD and /PLOAD loads
+                           (force.F90: 1/2 (F(t-dt1)+F(t)).v * DT2 per
+                           concentrated load, F . sum v * DT1 per segment)  */
 } or_energies;
 
 /* --- lifecycle ---------------------------------------------------------- */
@@ -184,6 +186,38 @@ int  or_ecycle_add_rlink(or_ecycle* h, int part, int nnod, const int* nodes,
 /* Changes the directions of a link between steps (an engine file that no longer
    lists it: ic = icr = 0). */
 int  or_ecycle_set_rlink(or_ecycle* h, int link, int ic, int icr);
+
+/* --- loads and skewed boundary conditions (FORCE, force.F90; BCS1V) -------- */
+/* Time function of /FUNCT: npts points (x strictly ascending, npts >= 1),
+   piecewise linear with linear extrapolation beyond both ends, one point =
+   constant (FINTER, tools/curve/finter.F).  Returns its index in *func. */
+int  or_ecycle_add_function(or_ecycle* h, int npts, const double* x, const double* y, int* func);
+
+/* Concentrated loads of /CLOAD (force.F90, Parith/ON branch): on each of the nnod
+   nodes (1-based), along direction dir (1..3 force x, y, z; 4..6 moment xx, yy,
+   zz) of the global axes (skew = -1) or of skew frame `skew`, the value
+   fscale * f(TT / ascale_x) at the time TT of the cycle's start.  Each node gets
+   its own assembly slot, summed after the element contributions.  Abscissa time
+   only (Itypfun 1), no sensor.  Before finalize. */
+int  or_ecycle_add_cload(or_ecycle* h, int part, int nnod, const int* nodes, int dir, int skew,
+                         int func, double ascale_x, double fscale, int* load);
+
+/* Pressure loads of /PLOAD (force.F90, segment branch): seg holds 4 x nseg 1-based
+   node numbers (n4 = 0 for a triangle).  A quadrangle adds
+   p (x3 - x1) x (x4 - x2) / 8 to each of its four nodes, a triangle
+   p (x3 - x1) x (x3 - x2) / 6 to each of its three, p = fscale * f(TT / ascale_x),
+   with the coordinates at the cycle's start.  Before finalize. */
+int  or_ecycle_add_pload(or_ecycle* h, int part, int nseg, const int* seg, int func,
+                         double ascale_x, double fscale, int* load);
+
+/* Fixed skew frame (/SKEW/FIX after the starter's orthonormalisation): axes9 =
+   x', y', z' unit vectors, 3 doubles each (SKEW(1:9,ISK)).  Returns its index. */
+int  or_ecycle_add_skew(or_ecycle* h, const double* axes9, int* skew);
+
+/* Skew frame of each node's /BCS codes (numnod ints, -1 = global axes): the
+   fixed directions are those of the frame (BCS1V, bcs1.F), for translations and
+   rotations alike.  Before finalize. */
+int  or_ecycle_set_bcs_skew(or_ecycle* h, int part, const int* skew);
 
 /* Builds the Parith/ON assembly tables (element_pon_: ADSKY/IADS/IADC) on the
    device and allocates work buffers.  Must follow the last add_* call. */

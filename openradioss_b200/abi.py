@@ -59,7 +59,7 @@ class Time(C.Structure):
 
 class Energies(C.Structure):
     _fields_ = [("internal", C.c_double), ("kinetic", C.c_double), ("kinetic_rot", C.c_double),
-                ("hourglass", C.c_double), ("plastic_work", C.c_double), ("pad", C.c_double)]
+                ("hourglass", C.c_double), ("plastic_work", C.c_double), ("external_work", C.c_double)]
 
 
 class AdjointResponse(C.Structure):

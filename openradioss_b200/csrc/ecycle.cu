@@ -22,6 +22,7 @@
 #include <string>
 #include <thread>
 #include <vector>
+#include <array>
 
 #include "../../include/or_ecycle.h"
 #include "ecycle_kernels.cuh"
@@ -43,6 +44,7 @@ struct HPart {
   int numnod = 0;
   std::vector<double> x, v, vr, ms, in;
   std::vector<int> icodt, icodr;
+  std::vector<int> iskew;           // skew frame of the /BCS codes, -1 = global (may be empty)
   int nel_solid = 0, nel_shell = 0;
   bool has_rot = false;
   int node_start = 0, node_pad = 0, tile_start = 0;
@@ -50,6 +52,11 @@ struct HPart {
 struct HLink {
   int part = 0, ic = 0, icr = 0;
   std::vector<int> nodes;           // part-local, 0-based
+};
+struct HLoad {                      // a /CLOAD node (type 0) or a /PLOAD segment (type 1)
+  int type = 0, part = 0, func = 0, dir = 0, skew = -1;
+  int node[4] = {-1, -1, -1, -1};   // part-local, 0-based
+  double fcx = 1.0, fcy = 1.0;
 };
 struct HHex {
   int part = 0, nel = 0, gofs = 0;
@@ -91,6 +98,9 @@ struct or_ecycle {
   std::vector<HHex> hex;
   std::vector<HShell> shell;
   std::vector<HLink> links;
+  std::vector<HLoad> loads;
+  std::vector<std::vector<double>> fx, fy;   // time functions
+  std::vector<std::array<double, 9>> skews;
   bool finalized = false;
   int tile_hex = 256, tile_shell = 256, tile_node = NODE_TILE;
   // device state
@@ -340,6 +350,10 @@ struct Impl {
   int nlinks = 0;
   // staging of one nodal array of one part (3 doubles per node) for set/get_nodes
   DBuf<double> stage;
+  // loads, time functions, skew frames
+  DBuf<LoadDesc> loadd; DBuf<FuncDesc> funcd; DBuf<double> funcx, funcy, wacc, wpend;
+  DBuf<R> skw; DBuf<int> skew_of;
+  int nload = 0;
 
   HexArgs<R> hargs() {
     HexArgs<R> a;
@@ -373,6 +387,7 @@ struct Impl {
     a.split = sizeof(R) == 4;
     a.halo_slot = nullptr; a.halo_ke = nullptr; a.xbuf = nullptr; a.xbytes = 0; a.nranks = 0; a.nhalo = 0;
     a.link_of = nlinks ? link_of.p : nullptr; a.link_mean = nlinks ? link_mean.p : nullptr;
+    a.skew_of = skew_of.p; a.skews = skw.p;
     return a;
   }
   void free_all() {
@@ -386,6 +401,7 @@ struct Impl {
     dfree(sehour); dfree(swpla); dfree(zw);
     dfree(halo_slot); dfree(halo_node); dfree(halo_ke);
     dfree(linkd); dfree(link_nodes); dfree(link_of); dfree(link_mean); dfree(stage);
+    dfree(loadd); dfree(funcd); dfree(funcx); dfree(funcy); dfree(wacc); dfree(wpend); dfree(skw); dfree(skew_of);
   }
 };
 
@@ -426,7 +442,18 @@ template <class R>
 int launch_link(or_ecycle* h, Impl<R>& m) {
   if (!m.nlinks) return OR_OK;
   link_kernel<R><<<(unsigned)m.nlinks, LINK_THREADS, 0, h->stream>>>(
-      m.linkd.p, m.link_nodes.p, m.adsky.p, m.fslot.p, m.mslot.p, m.X.p, m.VR.p, m.code.p, m.link_mean.p);
+      m.linkd.p, m.link_nodes.p, m.adsky.p, m.fslot.p, m.mslot.p, m.X.p, m.VR.p, m.code.p, m.skew_of.p, m.skw.p,
+      m.link_mean.p);
+  CK(cudaGetLastError());
+  h->launches++;
+  return OR_OK;
+}
+template <class R>
+int launch_loads(or_ecycle* h, Impl<R>& m, int parity) {
+  if (!m.nload) return OR_OK;
+  load_kernel<R><<<(unsigned)((m.nload + 127) / 128), 128, 0, h->stream>>>(
+      m.loadd.p, m.nload, m.funcd.p, m.funcx.p, m.funcy.p, m.skw.p, m.time.p, parity, m.nparts, m.X.p, m.V.p, m.VR.p,
+      m.fslot.p, m.mslot.p, m.wacc.p, m.wpend.p);
   CK(cudaGetLastError());
   h->launches++;
   return OR_OK;
@@ -465,6 +492,7 @@ template <class R>
 int launch_cycle(or_ecycle* h, Impl<R>& m, int parity, cudaEvent_t* ev) {
   int rc;
   if (ev) CK(cudaEventRecord(ev[0], h->stream));
+  if ((rc = launch_loads<R>(h, m, parity))) return rc;     // FORCE (resol.F:2847), before the elements
   rc = h->tile_hex == 64 ? launch_hex<R, 64>(h, m, parity)
        : h->tile_hex == 128 ? launch_hex<R, 128>(h, m, parity) : launch_hex<R, 256>(h, m, parity);
   if (rc) return rc;
@@ -513,6 +541,16 @@ int finalize_impl(or_ecycle* h) {
   const int nhp = (int)m.hps.info.size();
   rc = build_patches<4>(h, h->shell, h->tile_shell, m.sps, node_patch, nhp);
   if (rc) return rc;
+  // load corners: their own slots, after every patch slot of their node (in load order)
+  const int lbase = nhp + (int)m.sps.info.size();
+  const int nload = (int)h->loads.size();
+  std::vector<int> load_slot(4 * (size_t)nload, -1);
+  for (int e = 0; e < nload; ++e) {
+    const HLoad& L = h->loads[e];
+    const int nc = L.type == 0 ? 1 : (L.node[3] >= 0 ? 4 : 3);
+    for (int k = 0; k < nc; ++k)
+      node_patch[h->parts[L.part].node_start + L.node[k]].push_back({lbase + 4 * e + k, 4 * e + k});
+  }
   // node-major slots: per node, its (patch) entries in ascending patch number
   std::vector<int> adsky(nn + 1, 0);
   for (int n = 0; n < nn; ++n) adsky[n + 1] = adsky[n] + (int)node_patch[n].size();
@@ -523,7 +561,8 @@ int finalize_impl(or_ecycle* h) {
     for (size_t j = 0; j < lst.size(); ++j) {
       const int pid = lst[j].first, pos = lst[j].second;
       if (pid < nhp) m.hps.slots[pos] = adsky[n] + (int)j;
-      else m.sps.slots[pos] = adsky[n] + (int)j;
+      else if (pid < lbase) m.sps.slots[pos] = adsky[n] + (int)j;
+      else load_slot[pos] = adsky[n] + (int)j;
     }
   }
   node_patch.clear();
@@ -545,6 +584,52 @@ int finalize_impl(or_ecycle* h) {
     d.node_start = P.node_start; d.node_end = P.node_start + P.numnod; d.tile_start = P.tile_start;
     d.has_rot = P.has_rot ? 1 : 0;
     pd.push_back(d);
+  }
+  // skewed /BCS: code bit 7 and the node's skew frame
+  {
+    std::vector<int> sof;
+    for (auto& P : h->parts) {
+      if (P.iskew.empty()) continue;
+      for (int i = 0; i < P.numnod; ++i) {
+        const int g = P.node_start + i;
+        if (P.iskew[i] >= 0 && (P.icodt[i] | P.icodr[i])) {
+          if (sof.empty()) sof.assign(nn, -1);
+          sof[g] = P.iskew[i];
+          code[g] |= 128;
+        }
+      }
+    }
+    std::vector<R> sk;
+    for (auto& a : h->skews) for (int k = 0; k < 9; ++k) sk.push_back(R(a[k]));
+    if ((rc = dput(h, m.skew_of, sof)) || (rc = dput(h, m.skw, sk))) return rc;
+  }
+  // loads and their time functions
+  if (nload) {
+    std::vector<LoadDesc> ld(nload);
+    for (int e = 0; e < nload; ++e) {
+      const HLoad& L = h->loads[e];
+      LoadDesc d{};
+      d.type = L.type; d.part = L.part; d.func = L.func; d.skew = L.skew; d.pad = 0;
+      d.dir = L.type == 0 ? L.dir : (L.node[3] >= 0 ? 4 : 3);
+      for (int k = 0; k < 4; ++k) {
+        d.node[k] = L.node[k] >= 0 ? h->parts[L.part].node_start + L.node[k] : 0;
+        d.slot[k] = load_slot[4 * (size_t)e + k];
+      }
+      d.fcx = L.fcx; d.fcy = L.fcy;
+      ld[e] = d;
+    }
+    std::vector<FuncDesc> fd;
+    std::vector<double> fxv, fyv;
+    for (size_t f = 0; f < h->fx.size(); ++f) {
+      fd.push_back(FuncDesc{(int)fxv.size(), (int)h->fx[f].size()});
+      fxv.insert(fxv.end(), h->fx[f].begin(), h->fx[f].end());
+      fyv.insert(fyv.end(), h->fy[f].begin(), h->fy[f].end());
+    }
+    m.nload = nload;
+    std::vector<double> zl(nload, 0.0);
+    if ((rc = dput(h, m.loadd, ld)) || (rc = dput(h, m.funcd, fd)) || (rc = dput(h, m.funcx, fxv)) ||
+        (rc = dput(h, m.funcy, fyv)) || (rc = dput(h, m.wacc, zl)) || (rc = dput(h, m.wpend, zl)))
+      return rc;
   }
   // rigid links: node lists in global padded numbering, code bit 6 on their nodes
   if (!h->links.empty()) {
@@ -727,6 +812,10 @@ int reset_impl(or_ecycle* h) {
   CK(cudaMemset(m.DX.p, 0, nn * sizeof(double)));
   CK(cudaMemset(m.DY.p, 0, nn * sizeof(double)));
   CK(cudaMemset(m.DZ.p, 0, nn * sizeof(double)));
+  if (m.nload) {
+    CK(cudaMemset(m.wacc.p, 0, m.wacc.n * sizeof(double)));
+    CK(cudaMemset(m.wpend.p, 0, m.wpend.n * sizeof(double)));
+  }
   if (!h->hex.empty()) {
     const int np = m.hps.nelpad;
     std::vector<R> rho(np, R(0));
@@ -1046,7 +1135,19 @@ int energies_impl(or_ecycle* h, int part, or_energies* e) {
   auto ekinr = d2h(m.ekinr.p, m.ekinr.n);
   const HPart& P = h->parts[part];
   for (int t = P.tile_start; t < P.tile_start + P.node_pad / NODE_TILE; ++t) { ek += ekin[t]; ekr += ekinr[t]; }
-  e->internal = ei; e->kinetic = ek; e->kinetic_rot = ekr; e->hourglass = eh; e->plastic_work = wp; e->pad = 0;
+  // external work of the part's loads: the cumulative sums, plus the last cycle's
+  // concentrated-load power times that cycle's DT2
+  double wx = 0.0;
+  if (m.nload) {
+    auto wacc = d2h(m.wacc.p, m.wacc.n);
+    auto wpend = d2h(m.wpend.p, m.wpend.n);
+    PartTime t{};
+    CK(cudaMemcpy(&t, m.time.p + h->next_parity * m.nparts + part, sizeof(PartTime), cudaMemcpyDeviceToHost));
+    for (int e = 0; e < m.nload; ++e)
+      if (h->loads[e].part == part) wx += wacc[e] + wpend[e] * t.dt2;
+  }
+  e->internal = ei; e->kinetic = ek; e->kinetic_rot = ekr; e->hourglass = eh; e->plastic_work = wp;
+  e->external_work = wx;
   CK(cudaGetLastError());
   return OR_OK;
 }
@@ -1708,6 +1809,83 @@ int or_ecycle_set_rlink(or_ecycle* h, int link, int ic, int icr) {
   return OR_OK;
 }
 
+int or_ecycle_add_function(or_ecycle* h, int npts, const double* x, const double* y, int* func) {
+  if (!h) return OR_E_ARG;
+  if (h->finalized) return fail(h, OR_E_STATE, "add_function after finalize");
+  if (npts < 1 || !x || !y) return fail(h, OR_E_ARG, "add_function: bad argument");
+  for (int i = 1; i < npts; ++i)
+    if (!(x[i] > x[i - 1])) return fail(h, OR_E_ARG, "add_function: abscissae not strictly ascending");
+  h->fx.emplace_back(x, x + npts);
+  h->fy.emplace_back(y, y + npts);
+  if (func) *func = (int)h->fx.size() - 1;
+  return OR_OK;
+}
+
+int or_ecycle_add_skew(or_ecycle* h, const double* axes9, int* skew) {
+  if (!h) return OR_E_ARG;
+  if (h->finalized) return fail(h, OR_E_STATE, "add_skew after finalize");
+  if (!axes9) return fail(h, OR_E_ARG, "add_skew: bad argument");
+  std::array<double, 9> a;
+  for (int k = 0; k < 9; ++k) a[k] = axes9[k];
+  h->skews.push_back(a);
+  if (skew) *skew = (int)h->skews.size() - 1;
+  return OR_OK;
+}
+
+int or_ecycle_add_cload(or_ecycle* h, int part, int nnod, const int* nodes, int dir, int skew, int func,
+                        double ascale_x, double fscale, int* load) {
+  if (!h) return OR_E_ARG;
+  if (h->finalized) return fail(h, OR_E_STATE, "add_cload after finalize");
+  if (part < 0 || part >= (int)h->parts.size() || nnod < 1 || !nodes || dir < 1 || dir > 6 || func < 0 ||
+      func >= (int)h->fx.size() || skew < -1 || skew >= (int)h->skews.size() || ascale_x == 0.0)
+    return fail(h, OR_E_ARG, "add_cload: bad argument");
+  HPart& P = h->parts[part];
+  if (dir > 3 && !P.has_rot) return fail(h, OR_E_ARG, "add_cload: moment on a part without rotations");
+  if (load) *load = (int)h->loads.size();
+  for (int i = 0; i < nnod; ++i) {
+    if (nodes[i] < 1 || nodes[i] > P.numnod) return fail(h, OR_E_ARG, "add_cload: node number out of range");
+    HLoad L;
+    L.type = 0; L.part = part; L.func = func; L.dir = dir; L.skew = skew; L.node[0] = nodes[i] - 1;
+    L.fcx = 1.0 / ascale_x; L.fcy = fscale;
+    h->loads.push_back(L);
+  }
+  return OR_OK;
+}
+
+int or_ecycle_add_pload(or_ecycle* h, int part, int nseg, const int* seg, int func, double ascale_x, double fscale,
+                        int* load) {
+  if (!h) return OR_E_ARG;
+  if (h->finalized) return fail(h, OR_E_STATE, "add_pload after finalize");
+  if (part < 0 || part >= (int)h->parts.size() || nseg < 1 || !seg || func < 0 || func >= (int)h->fx.size() ||
+      ascale_x == 0.0)
+    return fail(h, OR_E_ARG, "add_pload: bad argument");
+  const HPart& P = h->parts[part];
+  if (load) *load = (int)h->loads.size();
+  for (int i = 0; i < nseg; ++i) {
+    HLoad L;
+    L.type = 1; L.part = part; L.func = func; L.fcx = 1.0 / ascale_x; L.fcy = fscale;
+    for (int k = 0; k < 4; ++k) {
+      const int n = seg[4 * i + k];
+      if (k == 3 && n == 0) break;          // triangle
+      if (n < 1 || n > P.numnod) return fail(h, OR_E_ARG, "add_pload: node number out of range");
+      L.node[k] = n - 1;
+    }
+    h->loads.push_back(L);
+  }
+  return OR_OK;
+}
+
+int or_ecycle_set_bcs_skew(or_ecycle* h, int part, const int* skew) {
+  if (!h) return OR_E_ARG;
+  if (h->finalized) return fail(h, OR_E_STATE, "set_bcs_skew after finalize");
+  if (part < 0 || part >= (int)h->parts.size() || !skew) return fail(h, OR_E_ARG, "set_bcs_skew: bad argument");
+  HPart& P = h->parts[part];
+  for (int i = 0; i < P.numnod; ++i)
+    if (skew[i] < -1 || skew[i] >= (int)h->skews.size()) return fail(h, OR_E_ARG, "set_bcs_skew: skew out of range");
+  P.iskew.assign(skew, skew + P.numnod);
+  return OR_OK;
+}
+
 int or_ecycle_finalize(or_ecycle* h) {
   if (!h) return OR_E_ARG;
   if (h->finalized) return fail(h, OR_E_STATE, "finalize called twice");
@@ -1744,6 +1922,10 @@ int or_ecycle_adjoint(or_ecycle* h, int ncycles, const or_adjoint_response* r, o
   if (h->cfg.precision != OR_PREC_FP64) return fail(h, OR_E_UNSUPPORTED, "adjoint: FP64 handles only");
   if (!h->hex.empty() || h->shell.empty()) return fail(h, OR_E_UNSUPPORTED, "adjoint: shell groups only");
   if (!h->links.empty()) return fail(h, OR_E_UNSUPPORTED, "adjoint: rigid links");
+  if (!h->loads.empty()) return fail(h, OR_E_UNSUPPORTED, "adjoint: /CLOAD or /PLOAD loads");
+  for (auto& P : h->parts)
+    for (int s : P.iskew)
+      if (s >= 0) return fail(h, OR_E_UNSUPPORTED, "adjoint: skewed boundary conditions");
   for (auto& g : h->shell)
     if (g.prop.ishfram != 0) return fail(h, OR_E_UNSUPPORTED, "adjoint: ISHFRAM 0 only");
   if (r->node >= 0) {
@@ -1761,6 +1943,7 @@ int or_ecycle_set_halo(or_ecycle* h, int part, int nloc, const int* local_node, 
   if (!h->finalized) return fail(h, OR_E_STATE, "set_halo before finalize");
   if (h->parts.size() != 1 || part != 0) return fail(h, OR_E_UNSUPPORTED, "set_halo: one part per handle");
   if (!h->links.empty()) return fail(h, OR_E_UNSUPPORTED, "set_halo: rigid links across domains");
+  if (!h->loads.empty()) return fail(h, OR_E_UNSUPPORTED, "set_halo: /CLOAD or /PLOAD loads");
   if (h->spmd_k >= 0) return fail(h, OR_E_STATE, "set_halo inside spmd_begin/end");
   if (nloc < 0 || nhalo < 0 || nloc > nhalo || (nloc > 0 && (!local_node || !halo_slot)))
     return fail(h, OR_E_ARG, "set_halo: bad argument");

@@ -76,6 +76,17 @@ struct PartAcc {
   unsigned long long dtbits;  // exact dt bits (double), min
 };
 
+// one load of FORCE (force.F90): a /CLOAD node (type 0) or a /PLOAD segment (type 1)
+struct LoadDesc {
+  int type, part, func, dir;      // dir: 1..6 for a /CLOAD; 3 or 4 corners for a /PLOAD
+  int skew, pad;                  // /CLOAD skew frame, -1 = global axes
+  int node[4], slot[4];           // padded global node numbers and their assembly slots
+  double fcx, fcy;                // 1 / Ascale_x, Fscale_y
+};
+struct FuncDesc {
+  int first, count;               // points in the function tables
+};
+
 // rigid velocity link (/VEL/TRA, /VEL/ROT; rlink1.F): its nodes and directions
 struct LinkDesc {
   int first, count;     // node range in link_nodes (global padded node numbers)
@@ -179,6 +190,10 @@ struct NodeArgs {
   // acceleration in the link's directions; null without links
   const int* link_of;
   const LinkMean* link_mean;
+  // skewed /BCS: for a node with code bit 7, the fixed directions are those of
+  // skew frame skew_of[n] (9 values: x', y', z'); null without skewed BCs
+  const int* skew_of;
+  const R* skews;
 };
 
 // Exchange buffer of one rank: nhalo force sums (R4), nhalo moment sums (R4),
@@ -191,6 +206,49 @@ __host__ __device__ inline size_t halo_buffer_bytes(int nhalo) {
 // ---------------------------------------------------------------------------
 // helpers
 // ---------------------------------------------------------------------------
+// BCS1V (bcs1.F): zero the components of (x, y, z) along the fixed directions of
+// code lcod (4 = x, 2 = y, 1 = z) of skew frame sk (rows x', y', z'), projecting
+// them out in the reference's order
+template <class R>
+__device__ inline void bcs1v_skew(int lcod, const R* sk, R& x, R& y, R& z) {
+  if (!lcod) return;
+  if (lcod == 7) { x = y = z = R(0); return; }
+  auto proj = [&](int r) {
+    const R s0 = sk[3 * r], s1 = sk[3 * r + 1], s2 = sk[3 * r + 2];
+    const R aa = s0 * x + s1 * y + s2 * z;
+    x = x - s0 * aa; y = y - s1 * aa; z = z - s2 * aa;
+  };
+  switch (lcod) {
+    case 1: proj(2); break;
+    case 2: proj(1); break;
+    case 3: proj(2); proj(1); break;
+    case 4: proj(0); break;
+    case 5: proj(2); proj(0); break;
+    case 6: proj(0); proj(1); break;
+  }
+}
+
+// FINTER (tools/curve/finter.F): first segment whose right end is >= xx (the last
+// one beyond the end), linear inside and beyond both ends, evaluated from the
+// nearer end of the segment; a one-point function is constant
+template <class R>
+__device__ inline R finter(const double* fx, const double* fy, int n, R xx) {
+  if (n == 1) return R(fy[0]);
+  R dx2 = R(fx[0]) - xx;
+  for (int i = 1; i < n; ++i) {
+    const R dx1 = -dx2;
+    dx2 = R(fx[i]) - xx;
+    if (dx2 >= R(0) || i == n - 1) {
+      const R div0 = R(fx[i]) - R(fx[i - 1]);
+      R div = fabs(div0) > R(1e-16) ? fabs(div0) : R(1e-16);
+      div = div0 >= R(0) ? div : -div;
+      const R deri = (R(fy[i]) - R(fy[i - 1])) / div;
+      return dx1 <= dx2 ? R(fy[i - 1]) + dx1 * deri : R(fy[i]) - dx2 * deri;
+    }
+  }
+  return R(0);
+}
+
 __device__ inline void raise_error(ErrorWord* e, int code, int index) {
   if (atomicCAS(&e->code, 0, code) == 0) e->index = index;
 }
@@ -1207,18 +1265,28 @@ node_kernel(NodeArgs<R> a, int parity) {
       else { ax = ay = az = R(0); }
       if (!isfinite((double)ax + (double)ay + (double)az)) raise_error(a.err, 6, n);
       // BCS10 (bcs1.F:52-100)
-      if (code & 4) { v.x = R(0); ax = R(0); }
-      if (code & 2) { v.y = R(0); ay = R(0); }
-      if (code & 1) { v.z = R(0); az = R(0); }
+      const R* sk = (code & 128) ? a.skews + 9 * a.skew_of[n] : nullptr;
+      if (sk) {
+        bcs1v_skew(code & 7, sk, v.x, v.y, v.z);
+        bcs1v_skew(code & 7, sk, ax, ay, az);
+      } else {
+        if (code & 4) { v.x = R(0); ax = R(0); }
+        if (code & 2) { v.y = R(0); ay = R(0); }
+        if (code & 1) { v.z = R(0); az = R(0); }
+      }
       if (code & 64) {      // RLINK10 (resol.F:7053), then BCS10 again (resol.F:7458)
         const LinkMean* lm = &a.link_mean[a.link_of[n]];
         const int ic = lm->ic;
         if (ic & 4) ax = R(lm->a[0]);
         if (ic & 2) ay = R(lm->a[1]);
         if (ic & 1) az = R(lm->a[2]);
-        if (code & 4) ax = R(0);
-        if (code & 2) ay = R(0);
-        if (code & 1) az = R(0);
+        if (sk) {
+          bcs1v_skew(code & 7, sk, ax, ay, az);
+        } else {
+          if (code & 4) ax = R(0);
+          if (code & 2) ay = R(0);
+          if (code & 1) az = R(0);
+        }
       }
       const double dt05 = 0.5 * DT1;
       {
@@ -1251,18 +1319,27 @@ node_kernel(NodeArgs<R> a, int parity) {
         const R in = w.w;
         if (in > R(0)) { const R r = R(1) / in; rx *= r; ry *= r; rz *= r; }
         else { rx = ry = rz = R(0); }
-        if (code & 32) { w.x = R(0); rx = R(0); }
-        if (code & 16) { w.y = R(0); ry = R(0); }
-        if (code & 8)  { w.z = R(0); rz = R(0); }
+        if (sk) {
+          bcs1v_skew((code >> 3) & 7, sk, w.x, w.y, w.z);
+          bcs1v_skew((code >> 3) & 7, sk, rx, ry, rz);
+        } else {
+          if (code & 32) { w.x = R(0); rx = R(0); }
+          if (code & 16) { w.y = R(0); ry = R(0); }
+          if (code & 8)  { w.z = R(0); rz = R(0); }
+        }
         if (code & 64) {
           const LinkMean* lm = &a.link_mean[a.link_of[n]];
           const int icr = lm->icr;
           if (icr & 4) rx = R(lm->ar[0]);
           if (icr & 2) ry = R(lm->ar[1]);
           if (icr & 1) rz = R(lm->ar[2]);
-          if (code & 32) rx = R(0);
-          if (code & 16) ry = R(0);
-          if (code & 8)  rz = R(0);
+          if (sk) {
+            bcs1v_skew((code >> 3) & 7, sk, rx, ry, rz);
+          } else {
+            if (code & 32) rx = R(0);
+            if (code & 16) ry = R(0);
+            if (code & 8)  rz = R(0);
+          }
         }
         const double wx = (double)w.x + dt05 * (double)rx, wy = (double)w.y + dt05 * (double)ry,
                      wz = (double)w.z + dt05 * (double)rz;
@@ -1296,6 +1373,79 @@ node_kernel(NodeArgs<R> a, int parity) {
       }
     }
     __syncthreads();
+  }
+}
+
+// ===========================================================================
+// loads (FORCE, force.F90, Parith/ON branch): one thread per load, at the time TT
+// of the cycle's start and with the coordinates of the cycle's start; each load
+// writes its own assembly slots.  External work per load (FP64, cumulative):
+//  - /CLOAD: WFEXC = 1/2 (F(TT-DT1) + F(TT)) . v, times the cycle's DT2
+//    (resol.F:6238).  DT2 is known only after the element pass, so the power is
+//    kept in wpend and multiplied by DT2 at the next cycle's start;
+//  - /PLOAD: DT1 F . (v1 + v2 + v3 [+ v4]).
+// ===========================================================================
+template <class R>
+__global__ void __launch_bounds__(128)
+load_kernel(const LoadDesc* __restrict__ loads, int nload, const FuncDesc* __restrict__ funcs,
+            const double* __restrict__ fx, const double* __restrict__ fy, const R* __restrict__ skews,
+            const PartTime* __restrict__ time, int parity, int nparts, const double4* __restrict__ X,
+            const typename Vec4<R>::T* __restrict__ V, const typename Vec4<R>::T* __restrict__ VR,
+            typename Vec4<R>::T* __restrict__ fslot, typename Vec4<R>::T* __restrict__ mslot,
+            double* __restrict__ wacc, double* __restrict__ wpend) {
+  typedef typename Vec4<R>::T R4;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nload) return;
+  const LoadDesc L = loads[e];
+  const PartTime t0 = time[parity * nparts + L.part];
+  const FuncDesc F = funcs[L.func];
+  const R ts = R(t0.tt), dt1 = R(t0.dt2);
+  const R zero4 = R(0);
+  if (L.type == 0) {
+    const R a0 = R(L.fcy) * finter<R>(fx + F.first, fy + F.first, F.count, (ts - dt1) * R(L.fcx));
+    const R aa = R(L.fcy) * finter<R>(fx + F.first, fy + F.first, F.count, ts * R(L.fcx));
+    const bool rot = L.dir > 3;
+    const int d = rot ? L.dir - 4 : L.dir - 1;
+    const int n = L.node[0];
+    const R4 vel = rot ? VR[n] : V[n];
+    R f0 = zero4, f1 = zero4, f2 = zero4;
+    R vv;
+    if (L.skew < 0) {
+      f0 = d == 0 ? aa : zero4; f1 = d == 1 ? aa : zero4; f2 = d == 2 ? aa : zero4;
+      vv = d == 0 ? vel.x : d == 1 ? vel.y : vel.z;
+    } else {
+      const R* sk = skews + 9 * L.skew + 3 * d;
+      vv = sk[0] * vel.x + sk[1] * vel.y + sk[2] * vel.z;
+      f0 = sk[0] * aa; f1 = sk[1] * aa; f2 = sk[2] * aa;
+    }
+    const R4 fz = mk4(zero4, zero4, zero4, zero4), fv = mk4(f0, f1, f2, zero4);
+    fslot[L.slot[0]] = rot ? fz : fv;
+    if (mslot) mslot[L.slot[0]] = rot ? fv : fz;
+    wacc[e] += wpend[e] * t0.dt2;
+    wpend[e] = (double)(R(0.5) * (a0 + aa) * vv);
+  } else {
+    const R aa = R(L.fcy) * finter<R>(fx + F.first, fy + F.first, F.count, ts * R(L.fcx));
+    const bool quad = L.dir == 4;
+    // triangle: (x3 - x1) x (x3 - x2) / 6; its fourth node entry is a valid padding node
+    const double4 x1 = X[L.node[0]], x2 = X[L.node[1]], x3 = X[L.node[2]], x4 = quad ? X[L.node[3]] : x3;
+    const R ax = R(x3.x) - R(x1.x), ay = R(x3.y) - R(x1.y), az = R(x3.z) - R(x1.z);
+    const R bx = R(x4.x) - R(x2.x), by = R(x4.y) - R(x2.y), bz = R(x4.z) - R(x2.z);
+    const R NX = ay * bz - az * by, NY = az * bx - ax * bz, NZ = ax * by - ay * bx;
+    const R c = quad ? R(0.125) : R(1.0 / 6.0);
+    const R fxx = aa * NX * c, fyy = aa * NY * c, fzz = aa * NZ * c;
+    const R4 fv = mk4(fxx, fyy, fzz, zero4), fz = mk4(zero4, zero4, zero4, zero4);
+    R sv0 = zero4, sv1 = zero4, sv2 = zero4;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (k < L.dir) {
+        fslot[L.slot[k]] = fv;
+        if (mslot) mslot[L.slot[k]] = fz;
+        const R4 v = V[L.node[k]];
+        sv0 = sv0 + v.x; sv1 = sv1 + v.y; sv2 = sv2 + v.z;
+      }
+    }
+    const R sv[3] = {sv0, sv1, sv2};
+    wacc[e] += (double)(dt1 * (fxx * sv[0] + fyy * sv[1] + fzz * sv[2]));
   }
 }
 
@@ -1342,7 +1492,8 @@ __global__ void __launch_bounds__(LINK_THREADS)
 link_kernel(const LinkDesc* __restrict__ links, const int* __restrict__ link_nodes, const int* __restrict__ adsky,
             const typename Vec4<R>::T* __restrict__ fslot, const typename Vec4<R>::T* __restrict__ mslot,
             const double4* __restrict__ X, const typename Vec4<R>::T* __restrict__ VR,
-            const unsigned char* __restrict__ codes, LinkMean* __restrict__ out) {
+            const unsigned char* __restrict__ codes, const int* __restrict__ skew_of, const R* __restrict__ skews,
+            LinkMean* __restrict__ out) {
   typedef typename Vec4<R>::T R4;
   __shared__ double s_sum[8][LINK_THREADS / 32];
   const LinkDesc L = links[blockIdx.x];
@@ -1358,9 +1509,14 @@ link_kernel(const LinkDesc* __restrict__ links, const int* __restrict__ link_nod
       const R ms = R(X[n].w);
       if (ms > R(0)) { const R r = R(1) / ms; ax *= r; ay *= r; az *= r; }
       else { ax = ay = az = R(0); }
-      if (code & 4) ax = R(0);
-      if (code & 2) ay = R(0);
-      if (code & 1) az = R(0);
+      const R* sk = (code & 128) ? skews + 9 * skew_of[n] : nullptr;
+      if (sk) {
+        bcs1v_skew(code & 7, sk, ax, ay, az);
+      } else {
+        if (code & 4) ax = R(0);
+        if (code & 2) ay = R(0);
+        if (code & 1) az = R(0);
+      }
       s[0] += (double)ms; s[1] += (double)(ms * ax); s[2] += (double)(ms * ay); s[3] += (double)(ms * az);
       if (VR && mslot && L.icr) {
         R rx = R(0), ry = R(0), rz = R(0);
@@ -1369,9 +1525,13 @@ link_kernel(const LinkDesc* __restrict__ links, const int* __restrict__ link_nod
         const R in = VR[n].w;
         if (in > R(0)) { const R r = R(1) / in; rx *= r; ry *= r; rz *= r; }
         else { rx = ry = rz = R(0); }
-        if (code & 32) rx = R(0);
-        if (code & 16) ry = R(0);
-        if (code & 8)  rz = R(0);
+        if (sk) {
+          bcs1v_skew((code >> 3) & 7, sk, rx, ry, rz);
+        } else {
+          if (code & 32) rx = R(0);
+          if (code & 16) ry = R(0);
+          if (code & 8)  rz = R(0);
+        }
         s[4] += (double)in; s[5] += (double)(in * rx); s[6] += (double)(in * ry); s[7] += (double)(in * rz);
       }
     }

@@ -47,7 +47,8 @@ EXPORTS = [
     "or_ecycle_stream", "or_ecycle_device_bytes", "or_ecycle_adjoint", "or_ecycle_hex_step_noalloc",
     "or_ecycle_kernel_times", "or_ecycle_set_halo", "or_ecycle_spmd_buffer_bytes", "or_ecycle_spmd_begin",
     "or_ecycle_spmd_elements", "or_ecycle_spmd_nodes", "or_ecycle_spmd_end", "or_ecycle_add_rlink",
-    "or_ecycle_set_rlink",
+    "or_ecycle_set_rlink", "or_ecycle_add_function", "or_ecycle_add_cload", "or_ecycle_add_pload",
+    "or_ecycle_add_skew", "or_ecycle_set_bcs_skew",
 ]
 
 
@@ -67,6 +68,12 @@ def _declare(lib):
         "or_ecycle_set_shell_yield": ([P, C.c_int, dp], C.c_int),
         "or_ecycle_add_rlink": ([P, C.c_int, C.c_int, ip, C.c_int, C.c_int, ip], C.c_int),
         "or_ecycle_set_rlink": ([P, C.c_int, C.c_int, C.c_int], C.c_int),
+        "or_ecycle_add_function": ([P, C.c_int, dp, dp, ip], C.c_int),
+        "or_ecycle_add_cload": ([P, C.c_int, C.c_int, ip, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, ip],
+                                C.c_int),
+        "or_ecycle_add_pload": ([P, C.c_int, C.c_int, ip, C.c_int, C.c_double, C.c_double, ip], C.c_int),
+        "or_ecycle_add_skew": ([P, dp, ip], C.c_int),
+        "or_ecycle_set_bcs_skew": ([P, C.c_int, ip], C.c_int),
         "or_ecycle_finalize": ([P], C.c_int),
         "or_ecycle_reset": ([P], C.c_int),
         "or_ecycle_step": ([P, C.c_int, C.POINTER(abi.Time)], C.c_int),
@@ -119,6 +126,11 @@ class _DeckModel:
         self.nparts = len(deck["parts"])
         self.hex_groups = []     # (part, nel)
         self.shell_groups = []   # (part, nel, npt)
+        for f in deck.get("functions", []):
+            fx, fy = _f64(f["x"]), _f64(f["y"])
+            self._add_function(fx.size, fx, fy)
+        for ax in deck.get("skews", []):
+            self._add_skew(_f64(np.asarray(ax, np.float64).reshape(9)))
         for p in deck["parts"]:
             x, v, vr = _f64(p["x"]), _f64(p["v"]), _f64(p["vr"])
             ms, inr = _f64(p["ms"]), _f64(p["inr"])
@@ -141,6 +153,16 @@ class _DeckModel:
             for rl in p.get("rlinks", []):
                 nodes = _i32(np.asarray(rl["nodes"]) + 1)
                 self._add_rlink(part, nodes.size, nodes, int(rl.get("ic", 7)), int(rl.get("icr", 0)))
+            for cl in p.get("cloads", []):
+                nodes = _i32(np.asarray(cl["nodes"]) + 1)
+                self._add_cload(part, nodes.size, nodes, int(cl["dir"]), int(cl.get("skew", -1)), int(cl["func"]),
+                                float(cl.get("ascale_x", 1.0)), float(cl.get("fscale", 1.0)))
+            for pl in p.get("ploads", []):
+                seg = _i32(np.asarray(pl["seg"]) + 1)          # -1 (triangle) -> 0
+                self._add_pload(part, seg.shape[0], seg, int(pl["func"]), float(pl.get("ascale_x", 1.0)),
+                                float(pl.get("fscale", 1.0)))
+            if p.get("iskew") is not None:
+                self._call("set_bcs_skew", part, abi.ptr(_i32(p["iskew"]), C.c_int))
         self._call("finalize")
         self.times = (abi.Time * self.nparts)(*[abi.initial_time() for _ in range(self.nparts)])
 
@@ -179,7 +201,7 @@ class _DeckModel:
         e = abi.Energies()
         self._call("energies", part, C.byref(e))
         return dict(internal=e.internal, kinetic=e.kinetic, kinetic_rot=e.kinetic_rot,
-                    hourglass=e.hourglass, plastic_work=e.plastic_work)
+                    hourglass=e.hourglass, plastic_work=e.plastic_work, external_work=e.external_work)
 
     def time(self, part=0):
         t = self.times[part]
@@ -236,6 +258,22 @@ class ECycle(_DeckModel):
         li = C.c_int()
         self._call("add_rlink", part, n, abi.ptr(nodes, C.c_int), ic, icr, C.byref(li))
         return li.value
+
+    def _add_function(self, n, x, y):
+        k = C.c_int()
+        self._call("add_function", n, abi.ptr(x, C.c_double), abi.ptr(y, C.c_double), C.byref(k))
+
+    def _add_skew(self, axes):
+        k = C.c_int()
+        self._call("add_skew", abi.ptr(axes, C.c_double), C.byref(k))
+
+    def _add_cload(self, part, n, nodes, d, skew, func, ascale_x, fscale):
+        k = C.c_int()
+        self._call("add_cload", part, n, abi.ptr(nodes, C.c_int), d, skew, func, ascale_x, fscale, C.byref(k))
+
+    def _add_pload(self, part, n, seg, func, ascale_x, fscale):
+        k = C.c_int()
+        self._call("add_pload", part, n, abi.ptr(seg, C.c_int), func, ascale_x, fscale, C.byref(k))
 
     def step(self, ncycles):
         self._call("step", int(ncycles), self.times)

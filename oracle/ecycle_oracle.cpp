@@ -112,9 +112,16 @@ struct PartData {
   std::vector<R> fsky;        // 8*lsky
   long lsky = 0;
   int nel_solid = 0, nel_shell = 0;
-  double ehour = 0, wplast = 0;
+  double ehour = 0, wplast = 0, wext = 0;
+  std::vector<int> iskew;     // per node skew frame of the /BCS codes, -1 = global
+  long lsky_elem = 0;         // slots of the elements; load slots follow
   double ekin = 0, ekinr = 0;
 };
+
+// time function (/FUNCT) and loads (/CLOAD, /PLOAD): force.F90
+struct Func { std::vector<double> x, y; };
+struct CLoad { int part, node, dir, skew, func; double fcx, fcy; long slot; };     // one per node
+struct PLoad { int part, n[4], func; double fcx, fcy; long slot[4]; };           // one per segment
 
 // rigid velocity link (/VEL/TRA, /VEL/ROT): frelnk.F:75-101, rlink1.F
 struct RLink {
@@ -129,6 +136,10 @@ struct Model {
   std::vector<HexGroup<R>> hex;
   std::vector<ShellGroup<R>> shell;
   std::vector<RLink> rlinks;
+  std::vector<Func> funcs;
+  std::vector<std::array<double, 9>> skews;
+  std::vector<CLoad> cloads;
+  std::vector<PLoad> ploads;
   bool finalized = false;
   std::string err;
   int errcode = 0, errindex = -1;
@@ -145,6 +156,8 @@ void build_skyline(Model<R>& m) {
     std::vector<long> cnt(P.numnod + 1, 0);
     for (auto& g : m.hex) if (g.part == (int)p) for (int i = 0; i < 8 * g.nel; ++i) cnt[g.ix[i] + 1]++;
     for (auto& g : m.shell) if (g.part == (int)p) for (int i = 0; i < 4 * g.nel; ++i) cnt[g.ix[i] + 1]++;
+    for (auto& c : m.cloads) if (c.part == (int)p) cnt[c.node + 1]++;
+    for (auto& q : m.ploads) if (q.part == (int)p) for (int k = 0; k < (q.n[3] >= 0 ? 4 : 3); ++k) cnt[q.n[k] + 1]++;
     P.adsky.assign(P.numnod + 1, 0);
     for (int n = 0; n < P.numnod; ++n) P.adsky[n + 1] = P.adsky[n] + cnt[n + 1];
     P.lsky = P.adsky[P.numnod];
@@ -157,7 +170,12 @@ void build_skyline(Model<R>& m) {
       g.iadc.assign(4 * g.nel, 0);
       for (int e = 0; e < g.nel; ++e) for (int k = 0; k < 4; ++k) g.iadc[4 * e + k] = next[g.ix[4 * e + k]]++;
     }
+    // load slots: after every element slot of their node, in load order
+    for (auto& c : m.cloads) if (c.part == (int)p) c.slot = next[c.node]++;
+    for (auto& q : m.ploads) if (q.part == (int)p)
+      for (int k = 0; k < (q.n[3] >= 0 ? 4 : 3); ++k) q.slot[k] = next[q.n[k]]++;
     P.fsky.assign(8 * P.lsky, R(0));
+    if (P.iskew.empty()) P.iskew.assign(P.numnod, -1);
   }
 }
 
@@ -857,6 +875,111 @@ int shell_element(const Model<R>& m, ShellGroup<R>& g, PartData<R>& P, int i, do
 }
 
 // ----------------------------------------------------------------------------
+// FINTER (tools/curve/finter.F): first segment whose right end is >= XX (the
+// last one beyond the end), linear inside and beyond both ends, evaluated from
+// the nearer end of the segment; a one-point function is constant.
+// ----------------------------------------------------------------------------
+template <class R>
+R finter(const Func& f, R XX) {
+  const int n = (int)f.x.size();
+  if (n == 1) return R(f.y[0]);
+  R DX2 = R(f.x[0]) - XX;
+  for (int i = 1; i < n; ++i) {
+    const R DX1 = -DX2;
+    DX2 = R(f.x[i]) - XX;
+    if (DX2 >= R(0) || i == n - 1) {
+      const R DIV0 = R(f.x[i]) - R(f.x[i - 1]);
+      R DIV = std::max(std::fabs(DIV0), R(1e-16));
+      DIV = sgn(DIV, DIV0);
+      const R DERI = (R(f.y[i]) - R(f.y[i - 1])) / DIV;
+      return DX1 <= DX2 ? R(f.y[i - 1]) + DX1 * DERI : R(f.y[i]) - DX2 * DERI;
+    }
+  }
+  return R(0);
+}
+
+// BCS1V (bcs1.F): zero the components of a (or v) along the fixed directions of
+// code lcod (4 = x, 2 = y, 1 = z) of the global axes (sk == null) or of skew sk
+// (rows x', y', z'), projecting them out in the reference's order.
+template <class R>
+void bcs1v(int lcod, const double* sk, R* a) {
+  if (!lcod) return;
+  if (!sk) {
+    if (lcod & 4) a[0] = R(0);
+    if (lcod & 2) a[1] = R(0);
+    if (lcod & 1) a[2] = R(0);
+    return;
+  }
+  if (lcod == 7) { a[0] = a[1] = a[2] = R(0); return; }
+  auto proj = [&](int r) {
+    const R s0 = R(sk[3 * r]), s1 = R(sk[3 * r + 1]), s2 = R(sk[3 * r + 2]);
+    const R AA = s0 * a[0] + s1 * a[1] + s2 * a[2];
+    a[0] = a[0] - s0 * AA; a[1] = a[1] - s1 * AA; a[2] = a[2] - s2 * AA;
+  };
+  switch (lcod) {
+    case 1: proj(2); break;
+    case 2: proj(1); break;
+    case 3: proj(2); proj(1); break;
+    case 4: proj(0); break;
+    case 5: proj(2); proj(0); break;
+    case 6: proj(0); proj(1); break;
+  }
+}
+
+// FORCE (force.F90, Parith/ON): load slots at the start of the cycle, at TT and
+// the coordinates of the cycle's start.  Returns the concentrated loads' power
+// sum 1/2 (F(TT-DT1)+F(TT)).v (WFEXC) and adds the segments' DT1 F.sum v to wext.
+template <class R>
+double load_pass(Model<R>& m, int p, double tt, double dt1, double& wext) {
+  PartData<R>& P = m.parts[p];
+  double wfexc = 0;
+  for (auto& c : m.cloads) {
+    if (c.part != p) continue;
+    const Func& f = m.funcs[c.func];
+    const R ts = R(tt);
+    const R a0 = R(c.fcy) * finter<R>(f, (ts - R(dt1)) * R(c.fcx));
+    const R aa = R(c.fcy) * finter<R>(f, ts * R(c.fcx));
+    R* fs = &P.fsky[8 * c.slot];
+    for (int k = 0; k < 8; ++k) fs[k] = R(0);
+    const bool rot = c.dir > 3;
+    const int d = rot ? c.dir - 4 : c.dir - 1;
+    const R* vel = rot ? &P.vr[3 * c.node] : &P.v[3 * c.node];
+    R vv;
+    if (c.skew < 0) {
+      fs[(rot ? 3 : 0) + d] = aa;
+      vv = vel[d];
+    } else {
+      const double* sk = m.skews[c.skew].data() + 3 * d;
+      vv = R(sk[0]) * vel[0] + R(sk[1]) * vel[1] + R(sk[2]) * vel[2];
+      for (int k = 0; k < 3; ++k) fs[(rot ? 3 : 0) + k] = R(sk[k]) * aa;
+    }
+    wfexc += double(R(0.5) * (a0 + aa) * vv);
+  }
+  for (auto& q : m.ploads) {
+    if (q.part != p) continue;
+    const R aa = R(q.fcy) * finter<R>(m.funcs[q.func], R(tt) * R(q.fcx));
+    auto X = [&](int k, int c) { return R(P.x[3 * q.n[k] + c]); };
+    const bool quad = q.n[3] >= 0;
+    const int k4 = quad ? 3 : 2;          // triangle: (x3 - x1) x (x3 - x2) / 6
+    const int k2 = 1;
+    const R ax = X(2, 0) - X(0, 0), ay = X(2, 1) - X(0, 1), az = X(2, 2) - X(0, 2);
+    const R bx = X(k4, 0) - X(k2, 0), by = X(k4, 1) - X(k2, 1), bz = X(k4, 2) - X(k2, 2);
+    const R NX = ay * bz - az * by, NY = az * bx - ax * bz, NZ = ax * by - ay * bx;
+    const R c = quad ? R(0.125) : R(1.0 / 6.0);
+    const R fx = aa * NX * c, fy = aa * NY * c, fz = aa * NZ * c;
+    R sv[3] = {0, 0, 0};
+    for (int k = 0; k < (quad ? 4 : 3); ++k) {
+      R* fs = &P.fsky[8 * q.slot[k]];
+      for (int j = 0; j < 8; ++j) fs[j] = R(0);
+      fs[0] = fx; fs[1] = fy; fs[2] = fz;
+      for (int j = 0; j < 3; ++j) sv[j] = sv[j] + P.v[3 * q.n[k] + j];
+    }
+    wext += double(R(dt1) * (fx * sv[0] + fy * sv[1] + fz * sv[2]));
+  }
+  return wfexc;
+}
+
+// ----------------------------------------------------------------------------
 // One cycle of one part: element pass, ASSPAR4, dt, ACCELE, BCS10, VELOCITY, DEPLA.
 // ----------------------------------------------------------------------------
 template <class R>
@@ -870,6 +993,9 @@ int cycle(Model<R>& m, int p, or_ecycle_time& t, int nthreads, bool last) {
   int eidx = -1;
   int ityp = 0, nelt = -1;
   double ehou = 0, wpla = 0;
+  // FORCE (resol.F:2847): load slots, before the element pass
+  double wext_seg = 0;
+  const double wfexc = load_pass(m, p, t.tt, DT1, wext_seg);
   // shells first (FORINTC :4012), then solids (FORINT :4096)
   for (auto& g : m.shell) {
     if (g.part != p) continue;
@@ -914,6 +1040,9 @@ int cycle(Model<R>& m, int p, or_ecycle_time& t, int nthreads, bool last) {
   t.dt2 = DT2;
   t.dt2old = DT2;
   t.dt12 = 0.5 * (t.dt1 + t.dt2);
+  // external work: segments with DT1 in FORCE, concentrated loads WFEXC*DT2 (resol.F:6238)
+  P.wext += wext_seg;
+  P.wext += wfexc * DT2;
   const R DT12 = R(t.dt12);
   // ASSPAR4 + ACCELE (accele.F:63-123) + the acceleration part of BCS10 for node n
   auto node_acc = [&P](int n, R* a, R* ar) {
@@ -930,13 +1059,10 @@ int cycle(Model<R>& m, int p, or_ecycle_time& t, int nthreads, bool last) {
     if (inn > R(0)) { R r = R(1) / inn; ar[0] *= r; ar[1] *= r; ar[2] *= r; }
     else { ar[0] = ar[1] = ar[2] = 0; }
   };
-  auto bcs_acc = [](int ct, int cr, R* a, R* ar) {
-    if (ct & 4) a[0] = 0;
-    if (ct & 2) a[1] = 0;
-    if (ct & 1) a[2] = 0;
-    if (cr & 4) ar[0] = 0;
-    if (cr & 2) ar[1] = 0;
-    if (cr & 1) ar[2] = 0;
+  auto skew_of = [&](int n) -> const double* { return P.iskew[n] >= 0 ? m.skews[P.iskew[n]].data() : nullptr; };
+  auto bcs_acc = [&](int n, R* a, R* ar) {
+    bcs1v(P.icodt[n], skew_of(n), a);
+    bcs1v(P.icodr[n], skew_of(n), ar);
   };
   // RLINK10 / RLINK1 (resol.F:7053, rlink1.F): per link, MASS = sum MS, AX = sum MS*A
   // over its nodes after ACCELE and BCS10 (FRL6 sums in DOUBLE PRECISION), mean = AX/MASS
@@ -952,7 +1078,7 @@ int cycle(Model<R>& m, int p, or_ecycle_time& t, int nthreads, bool last) {
     for (int n : L.nodes) {
       R a[3], ar[3];
       node_acc(n, a, ar);
-      bcs_acc(P.icodt[n], P.icodr[n], a, ar);
+      bcs_acc(n, a, ar);
       const R msn = P.ms[n], inn = P.in[n];
       S[0] += double(msn); S[1] += double(msn * a[0]); S[2] += double(msn * a[1]); S[3] += double(msn * a[2]);
       S[4] += double(inn); S[5] += double(inn * ar[0]); S[6] += double(inn * ar[1]); S[7] += double(inn * ar[2]);
@@ -976,15 +1102,10 @@ int cycle(Model<R>& m, int p, or_ecycle_time& t, int nthreads, bool last) {
     if (!std::isfinite(double(a[0]) + double(a[1]) + double(a[2]))) nan_node = n;
     R* v = &P.v[3 * n];
     R* vr = &P.vr[3 * n];
-    // BCS10 / BCS1V (bcs1.F:52-100): bit 4 = x, 2 = y, 1 = z
-    int ct = P.icodt[n], cr = P.icodr[n];
-    if (ct & 4) v[0] = 0;
-    if (ct & 2) v[1] = 0;
-    if (ct & 1) v[2] = 0;
-    if (cr & 4) vr[0] = 0;
-    if (cr & 2) vr[1] = 0;
-    if (cr & 1) vr[2] = 0;
-    bcs_acc(ct, cr, a, ar);
+    // BCS10 / BCS1V (bcs1.F:52-100): bit 4 = x, 2 = y, 1 = z, global or skew axes
+    bcs1v(P.icodt[n], skew_of(n), v);
+    bcs1v(P.icodr[n], skew_of(n), vr);
+    bcs_acc(n, a, ar);
     if (!link_of.empty() && link_of[n] >= 0) {
       const int li = link_of[n];
       const auto& mu = link_mean[li];
@@ -995,7 +1116,7 @@ int cycle(Model<R>& m, int p, or_ecycle_time& t, int nthreads, bool last) {
       if (icr & 4) ar[0] = R(mu[3]);
       if (icr & 2) ar[1] = R(mu[4]);
       if (icr & 1) ar[2] = R(mu[5]);
-      bcs_acc(ct, cr, a, ar);         // resol.F:7458 reimposes the BCS
+      bcs_acc(n, a, ar);              // resol.F:7458 reimposes the BCS
     }
     if (last) {   // ECRIT (ecrit.F:262-268, 315-322): DT05 = DT1/2
       double dt05 = 0.5 * DT1;
@@ -1163,6 +1284,65 @@ int oracle_set_rlink(void* hh, int link, int ic, int icr) {
     return (int)OR_OK;
   });
 }
+int oracle_add_function(void* hh, int npts, const double* x, const double* y) {
+  Handle* h = (Handle*)hh;
+  return h->with([&](auto& m) {
+    if (npts < 1 || !x || !y) return (int)OR_E_ARG;
+    Func f;
+    f.x.assign(x, x + npts); f.y.assign(y, y + npts);
+    m.funcs.push_back(std::move(f));
+    return (int)OR_OK;
+  });
+}
+int oracle_add_cload(void* hh, int part, int nnod, const int* nodes, int dir, int skew, int func,
+                     double ascale_x, double fscale) {
+  Handle* h = (Handle*)hh;
+  return h->with([&](auto& m) {
+    if (part < 0 || part >= (int)m.parts.size() || dir < 1 || dir > 6 || func < 0 || func >= (int)m.funcs.size() ||
+        skew < -1 || skew >= (int)m.skews.size() || ascale_x == 0.0)
+      return (int)OR_E_ARG;
+    for (int i = 0; i < nnod; ++i) {
+      if (nodes[i] < 1 || nodes[i] > m.parts[part].numnod) return (int)OR_E_ARG;
+      m.cloads.push_back(CLoad{part, nodes[i] - 1, dir, skew, func, 1.0 / ascale_x, fscale, -1});
+    }
+    return (int)OR_OK;
+  });
+}
+int oracle_add_pload(void* hh, int part, int nseg, const int* seg, int func, double ascale_x, double fscale) {
+  Handle* h = (Handle*)hh;
+  return h->with([&](auto& m) {
+    if (part < 0 || part >= (int)m.parts.size() || func < 0 || func >= (int)m.funcs.size() || ascale_x == 0.0)
+      return (int)OR_E_ARG;
+    for (int i = 0; i < nseg; ++i) {
+      PLoad q{};
+      q.part = part; q.func = func; q.fcx = 1.0 / ascale_x; q.fcy = fscale;
+      for (int k = 0; k < 4; ++k) q.n[k] = seg[4 * i + k] - 1;     // n4 = 0 -> -1: triangle
+      for (int k = 0; k < 4; ++k)
+        if ((k < 3 || q.n[3] >= 0) && (q.n[k] < 0 || q.n[k] >= m.parts[part].numnod)) return (int)OR_E_ARG;
+      m.ploads.push_back(q);
+    }
+    return (int)OR_OK;
+  });
+}
+int oracle_add_skew(void* hh, const double* axes9) {
+  Handle* h = (Handle*)hh;
+  return h->with([&](auto& m) {
+    std::array<double, 9> a;
+    for (int k = 0; k < 9; ++k) a[k] = axes9[k];
+    m.skews.push_back(a);
+    return (int)OR_OK;
+  });
+}
+int oracle_set_bcs_skew(void* hh, int part, const int* skew) {
+  Handle* h = (Handle*)hh;
+  return h->with([&](auto& m) {
+    if (part < 0 || part >= (int)m.parts.size()) return (int)OR_E_ARG;
+    auto& P = m.parts[part];
+    P.iskew.assign(skew, skew + P.numnod);
+    for (int s : P.iskew) if (s < -1 || s >= (int)m.skews.size()) return (int)OR_E_ARG;
+    return (int)OR_OK;
+  });
+}
 int oracle_finalize(void* hh) {
   Handle* h = (Handle*)hh;
   return h->with([&](auto& m) { build_skyline(m); m.finalized = true; return OR_OK; });
@@ -1228,7 +1408,7 @@ int oracle_energies(void* hh, int part, or_energies* e) {
     for (auto& g : m.hex) if (g.part == part) for (int i = 0; i < g.nel; ++i) ei += double(g.eint[i]) * double(g.vol0[i]);
     for (auto& g : m.shell) if (g.part == part) for (int i = 0; i < g.nel; ++i) ei += double(g.eint[i]) + double(g.eint[g.nel + i]);
     e->internal = ei; e->kinetic = P.ekin; e->kinetic_rot = P.ekinr;
-    e->hourglass = P.ehour; e->plastic_work = P.wplast; e->pad = 0;
+    e->hourglass = P.ehour; e->plastic_work = P.wplast; e->external_work = P.wext;
     return (int)OR_OK;
   });
 }

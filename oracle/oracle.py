@@ -42,6 +42,11 @@ def load(fast=False):
     lib.oracle_set_shell_yield.argtypes = [P, C.c_int, dp]
     lib.oracle_add_rlink.argtypes = [P, C.c_int, C.c_int, ip, C.c_int, C.c_int]
     lib.oracle_set_rlink.argtypes = [P, C.c_int, C.c_int, C.c_int]
+    lib.oracle_add_function.argtypes = [P, C.c_int, dp, dp]
+    lib.oracle_add_cload.argtypes = [P, C.c_int, C.c_int, ip, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double]
+    lib.oracle_add_pload.argtypes = [P, C.c_int, C.c_int, ip, C.c_int, C.c_double, C.c_double]
+    lib.oracle_add_skew.argtypes = [P, dp]
+    lib.oracle_set_bcs_skew.argtypes = [P, C.c_int, ip]
     lib.oracle_finalize.argtypes = [P]
     lib.oracle_step.argtypes = [P, C.c_int, C.POINTER(abi.Time), C.c_int]
     lib.oracle_get_nodes.argtypes = [P, C.c_int, dp, dp, dp, dp]
@@ -95,6 +100,18 @@ class Oracle(_DeckModel):
 
     def _add_rlink(self, part, n, nodes, ic, icr):
         self._call("add_rlink", part, n, abi.ptr(nodes, C.c_int), ic, icr)
+
+    def _add_function(self, n, x, y):
+        self._call("add_function", n, abi.ptr(x, C.c_double), abi.ptr(y, C.c_double))
+
+    def _add_skew(self, axes):
+        self._call("add_skew", abi.ptr(axes, C.c_double))
+
+    def _add_cload(self, part, n, nodes, d, skew, func, ascale_x, fscale):
+        self._call("add_cload", part, n, abi.ptr(nodes, C.c_int), d, skew, func, ascale_x, fscale)
+
+    def _add_pload(self, part, n, seg, func, ascale_x, fscale):
+        self._call("add_pload", part, n, abi.ptr(seg, C.c_int), func, ascale_x, fscale)
 
     def step(self, ncycles):
         self._call("step", int(ncycles), self.times, self.nthreads)
