@@ -8,9 +8,11 @@ nodal masses and inertias:
 
 starter keywords
   /BEGIN (input version >= 2017: 20-character real fields), /NODE,
-  /SHELL/<part>, /PART, /PROP/SHELL (TYPE1), /MAT/PLAS_JOHNS (LAW2, Iflag 0),
-  /MAT/ELAST (LAW1), /DEF_SHELL, /SHFRA/V4, /BCS (no skew), /GRNOD/NODE,
-  /INIVEL/TRA (no skew), /ADMAS/0
+  /SHELL/<part>, /BRICK/<part>, /PART, /PROP/SHELL (TYPE1), /PROP/SOLID
+  (TYPE14, Isolid 1, Iframe 1, Ismstr 4), /MAT/PLAS_JOHNS (LAW2, Iflag 0),
+  /MAT/ELAST (LAW1), /DEF_SHELL, /DEF_SOLID, /SHFRA/V4, /SKEW/FIX, /BCS,
+  /GRNOD/NODE, /INIVEL/TRA (no skew), /ADMAS/0, /FUNCT, /CLOAD (time
+  abscissa, no sensor), /PLOAD (no sensor), /SURF/SEG, /SURF/PART (shell parts)
 engine keywords
   /RUN (final time), /VEL/TRA and /VEL/ROT (rigid velocity links, no skew)
 
@@ -29,7 +31,13 @@ Starter semantics restated here (the reference starter is not on the path):
   resultant law, which the element cycle does not implement;
 * shell nodal mass rho t A / 4 and inertia EMS (A / 9 + t^2 / 12), with A the
   CEVECI area 1/2 |(x3 - x1) x (x4 - x2)| (cinmas.F:369, :703; ceveci.F);
-  /ADMAS type 0 adds its mass to every node of the group;
+  hexa nodal mass rho0 V0 / 8 (smass3.F:79-94); /ADMAS type 0 adds its mass to
+  every node of the group;
+* /PROP/SOLID: Isolid, Ismstr, Iframe fall back to /DEF_SOLID, then to 1, 4, 1;
+  qa = 1.1, qb = 0.05, h = 0.1 when zero (hm_read_prop14.F:218-380);
+* /SKEW/FIX: x' = Y x Z, y' = Z x x', all three normalised (hm_read_skw.F);
+* /CLOAD and /PLOAD: Ascale_x and Fscale_y default to 1 (hm_read_cload.F,
+  hm_read_pload.F);
 * LAW2: G = E / 2(1 + nu), A11 = E / (1 - nu^2), shell sound speed
   sqrt(E / rho) (hm_read_mat02_jc.F90); SIG_max0 = 0 and EPS_p_max = 0 mean
   no limit.
@@ -127,7 +135,15 @@ class StarterDeck:
         self.inivel = []           # (vx, vy, vz, grnod id)
         self.admas = []            # (mass, grnod id)
         self.def_shell = dict(ishell=0, ismstr=0, ithick=0, iplas=0)
+        self.def_solid = dict(isolid=0, ismstr=0, iframe=0)
         self.ishfram = 0
+        self.bricks = {}           # part id -> list of (elem id, n1..n8)
+        self.funct = {}            # id -> (x list, y list)
+        self.skews = {}            # id -> 9 floats (x', y', z')
+        self.surf_seg = {}         # id -> list of (n1, n2, n3, n4), n4 = 0 for triangles
+        self.surf_part = {}        # id -> list of part ids
+        self.cload = []            # dict(func, dir, skew, grnod, ascale_x, fscale)
+        self.pload = []            # dict(surf, func, ascale_x, fscale)
         for key, lines, where in _blocks(path):
             self._block(key, lines, where)
 
@@ -149,13 +165,75 @@ class StarterDeck:
             rows = self.shells.setdefault(part, [])
             for line in L:
                 rows.append(tuple(_int(line, 10 * c) for c in range(5)))
+        elif k0 == "BRICK":
+            part = int(key[1])
+            rows = self.bricks.setdefault(part, [])
+            for line in L:
+                rows.append(tuple(_int(line, 10 * c) for c in range(9)))
+        elif k0 == "FUNCT":
+            xs, ys = [], []
+            for line in L[1:]:
+                xs.append(_real(line, 0))
+                ys.append(_real(line, 20))
+            self.funct[int(key[1])] = (xs, ys)
+        elif k0 == "SKEW":
+            if key[1].upper() != "FIX":
+                raise RadError(f"{where}: /SKEW/{key[1]} (moving frames) is not implemented")
+            Y = np.array([_real(L[2], 20 * c) for c in range(3)])
+            Z = np.array([_real(L[3], 20 * c) for c in range(3)])
+            if Y[0] == 0.0 and Y[2] == 0.0:
+                Y[1] = math.copysign(1.0, Y[1])
+            if Z[0] == 0.0 and Z[1] == 0.0:
+                Z[2] = math.copysign(1.0, Z[2])
+            X = np.cross(Y, Z)
+            Y = np.cross(Z, X)
+            ax = [v / np.linalg.norm(v) for v in (X, Y, Z)]
+            self.skews[int(key[2])] = np.concatenate(ax)
+        elif k0 == "SURF":
+            kind = key[1].upper()
+            if kind == "SEG":
+                self.surf_seg[int(key[2])] = [tuple(_int(line, 10 * c) for c in range(1, 5)) for line in L[1:]]
+            elif kind == "PART":
+                self.surf_part[int(key[2])] = _node_list(L[1:])
+            else:
+                raise RadError(f"{where}: /SURF/{key[1]} is not implemented")
+        elif k0 == "CLOAD":
+            line = L[1]
+            if _int(line, 30) != 0:
+                raise RadError(f"{where}: /CLOAD with a sensor is not implemented")
+            if _int(line, 50) not in (0, 1):
+                raise RadError(f"{where}: /CLOAD with a displacement or velocity abscissa is not implemented")
+            dirs = {"X": 1, "Y": 2, "Z": 3, "XX": 4, "YY": 5, "ZZ": 6}
+            d = line[10:20].strip().upper()
+            if d not in dirs:
+                raise RadError(f"{where}: /CLOAD direction {d!r}")
+            self.cload.append(dict(func=_int(line, 0), dir=dirs[d], skew=_int(line, 20), grnod=_int(line, 40),
+                                   ascale_x=_real(line, 60) or 1.0, fscale=_real(line, 80) or 1.0))
+        elif k0 == "PLOAD":
+            line = L[1]
+            if _int(line, 20) != 0:
+                raise RadError(f"{where}: /PLOAD with a sensor is not implemented")
+            self.pload.append(dict(surf=_int(line, 0), func=_int(line, 10), ascale_x=_real(line, 60) or 1.0,
+                                   fscale=_real(line, 80) or 1.0))
+        elif k0 == "DEF_SOLID":
+            if _int(L[0], 60) != 0:
+                raise RadError(f"{where}: /DEF_SOLID Imas (nodal mass distribution) is not implemented")
+            self.def_solid = dict(isolid=_int(L[0], 0), ismstr=_int(L[0], 10), iframe=_int(L[0], 70))
         elif k0 == "PART":
             self.parts[int(key[1])] = (_int(L[1], 0), _int(L[1], 10))
+        elif k0 == "PROP" and key[1].upper() in ("SOLID", "TYPE14"):
+            pid = int(key[2])
+            if len(L) > 3 and _real(L[3], 0) != 0.0:
+                raise RadError(f"{where}: /PROP/SOLID deltaT_min (small-strain switch) is not implemented")
+            if _int(L[1], 20) != 0:
+                raise RadError(f"{where}: /PROP/SOLID Iale is not on the element-cycle path")
+            self.props[pid] = dict(kind="solid", isolid=_int(L[1], 0), ismstr=_int(L[1], 10), iframe=_int(L[1], 70),
+                                   qa=_real(L[2], 0), qb=_real(L[2], 20), qh=_real(L[2], 40))
         elif k0 == "PROP":
             if key[1].upper() not in ("SHELL", "TYPE1"):
                 raise RadError(f"{where}: /PROP/{key[1]} is not on the element-cycle path")
             pid = int(key[2])
-            self.props[pid] = dict(
+            self.props[pid] = dict(kind="shell",
                 ishell=_int(L[1], 0), ismstr=_int(L[1], 10), ish3n=_int(L[1], 20), idrill=_int(L[1], 30),
                 hm=_real(L[2], 0), hf=_real(L[2], 20), hr=_real(L[2], 40), dm=_real(L[2], 60), dn=_real(L[2], 80),
                 n=_int(L[3], 0), istrain=_int(L[3], 10), thick=_real(L[3], 20), ashear=_real(L[3], 40),
@@ -187,10 +265,8 @@ class StarterDeck:
         elif k0 == "BCS":
             line = L[1]
             tra, rot = line[3:6], line[7:10]
-            if _int(line, 10) != 0:
-                raise RadError(f"{where}: /BCS with a skew frame is not implemented")
             code = lambda s: sum(b for ch, b in zip(s.replace(" ", "0"), (4, 2, 1)) if ch == "1")
-            self.bcs.append((code(tra), code(rot), _int(line, 20)))
+            self.bcs.append((code(tra), code(rot), _int(line, 20), _int(line, 10)))
         elif k0 == "GRNOD":
             if key[1].upper() != "NODE":
                 raise RadError(f"{where}: /GRNOD/{key[1]} is not implemented")
@@ -249,20 +325,53 @@ def _shell_flags(sd, prop):
     return ihbe, ismstr, ithk, ipla
 
 
+def _material(mat):
+    if mat["law"] == 2:
+        return decks.material(decks.LAW_JOHNSON_COOK, mat["rho"], mat["E"], mat["nu"], jc_a=mat["a"],
+                              jc_b=mat["b"], jc_n=mat["n"],
+                              epsmax=mat["epsmax"] if mat["epsmax"] > 0.0 else 1e20,
+                              sigmax=mat["sigmax"] if mat["sigmax"] > 0.0 else 1e20)
+    return decks.material(decks.LAW_ELASTIC, mat["rho"], mat["E"], mat["nu"])
+
+
 def to_deck(sd: StarterDeck, name=None):
     """The element-cycle deck of a starter deck: one part with every node (in
-    the order of /NODE), one shell group per /PART in ascending part id, and
-    ``ids`` (node ids) / ``elem_ids`` (element ids per group) for reporting."""
+    the order of /NODE); one hexa group per /PART with /BRICK elements, then one
+    shell group per /PART with /SHELL elements, each in ascending part id; the
+    time functions, skew frames, loads and skewed BCs; and ``ids`` (node ids) /
+    ``hex_ids`` / ``elem_ids`` (element ids per hexa / shell group) for
+    reporting."""
     ids = np.array(list(sd.nodes.keys()), np.int64)
     x = np.array(list(sd.nodes.values()), np.float64)
     index = {int(i): k for k, i in enumerate(ids)}
     part = decks.new_part(x)
-    elem_ids = []
+    hex_ids, elem_ids = [], []
+    for pid in sorted(sd.bricks):
+        if pid not in sd.parts:
+            raise RadError(f"/BRICK/{pid}: no /PART/{pid}")
+        prop_id, mat_id = sd.parts[pid]
+        prop, mat = sd.props[prop_id], sd.mats[mat_id]
+        if prop.get("kind") != "solid":
+            raise RadError(f"/PART/{pid}: bricks need a /PROP/SOLID")
+        ds = sd.def_solid
+        isolid = prop["isolid"] or ds["isolid"] or 1
+        ismstr = prop["ismstr"] or ds["ismstr"] or 4
+        iframe = prop["iframe"] or ds["iframe"] or 1
+        if isolid != 1 or ismstr != 4 or iframe != 1:
+            raise RadError(f"/PROP/SOLID/{prop_id}: Isolid {isolid} / Ismstr {ismstr} / Iframe {iframe}; the "
+                           "element cycle implements Isolid 1 with Ismstr 4 and Iframe 1")
+        rows = sorted(sd.bricks[pid])
+        conn = np.array([[index[n] for n in r[1:]] for r in rows], np.int64)
+        sp = decks.solid_prop(qa=prop["qa"] or 1.1, qb=prop["qb"] or 0.05, qh=prop["qh"] or 0.1)
+        decks.add_hex(part, conn, _material(mat), sp)
+        hex_ids.append(np.array([r[0] for r in rows], np.int64))
     for pid in sorted(sd.shells):
         if pid not in sd.parts:
             raise RadError(f"/SHELL/{pid}: no /PART/{pid}")
         prop_id, mat_id = sd.parts[pid]
         prop, mat = sd.props[prop_id], sd.mats[mat_id]
+        if prop.get("kind") != "shell":
+            raise RadError(f"/PART/{pid}: shells need a /PROP/SHELL")
         ihbe, ismstr, ithk, ipla = _shell_flags(sd, prop)
         if ihbe != 1 or ismstr != 2:
             raise RadError(f"/PROP/SHELL/{prop_id}: Ishell {ihbe} / Ismstr {ismstr}; the element cycle "
@@ -281,13 +390,6 @@ def to_deck(sd: StarterDeck, name=None):
             raise RadError(f"/PROP/SHELL/{prop_id}: N = {npt}")
         rows = sorted(sd.shells[pid])
         conn = np.array([[index[n] for n in r[1:]] for r in rows], np.int64)
-        if mat["law"] == 2:
-            m = decks.material(decks.LAW_JOHNSON_COOK, mat["rho"], mat["E"], mat["nu"], jc_a=mat["a"],
-                               jc_b=mat["b"], jc_n=mat["n"],
-                               epsmax=mat["epsmax"] if mat["epsmax"] > 0.0 else 1e20,
-                               sigmax=mat["sigmax"] if mat["sigmax"] > 0.0 else 1e20)
-        else:
-            m = decks.material(decks.LAW_ELASTIC, mat["rho"], mat["E"], mat["nu"])
         p = decks.shell_prop(prop["thick"], npt=npt, ithk=1 if ithk > 0 else 0,
                              hm=prop["hm"] or 0.01, hf=prop["hf"] or 0.01, hr=prop["hr"] or 0.01,
                              ishfram=sd.ishfram)
@@ -295,22 +397,70 @@ def to_deck(sd: StarterDeck, name=None):
             p["shf"] = prop["ashear"]
         if npt == 1:
             p["shf"] = 0.0
-        decks.add_shell(part, conn, m, p)
+        decks.add_shell(part, conn, _material(mat), p)
         elem_ids.append(np.array([r[0] for r in rows], np.int64))
-    for tra, rot, g in sd.bcs:
+    skew_index = {sid: k for k, sid in enumerate(sorted(sd.skews))}
+    skew_of = lambda sid, what: -1 if sid == 0 else _lookup(skew_index, sid, what)
+    iskew = -np.ones(x.shape[0], np.int32)
+    for tra, rot, g, sk in sd.bcs:
         for n in sd.grnod[g]:
             part["icodt"][index[n]] |= tra
             part["icodr"][index[n]] |= rot
+            if sk:
+                iskew[index[n]] = skew_of(sk, "/BCS skew")
+    if (iskew >= 0).any():
+        part["iskew"] = iskew
     for vx, vy, vz, g in sd.inivel:
         for n in sd.grnod[g]:
             part["v"][index[n]] = (vx, vy, vz)
     for mass, g in sd.admas:
         for n in sd.grnod[g]:
             part["ms"][index[n]] += mass
+    func_index = {fid: k for k, fid in enumerate(sorted(sd.funct))}
+    cloads, ploads = [], []
+    for c in sd.cload:
+        cloads.append(dict(nodes=np.array([index[n] for n in sd.grnod[c["grnod"]]], np.int64), dir=c["dir"],
+                           skew=skew_of(c["skew"], "/CLOAD skew"), func=_lookup(func_index, c["func"], "/CLOAD"),
+                           ascale_x=c["ascale_x"], fscale=c["fscale"]))
+    for q in sd.pload:
+        seg = _segments(sd, q["surf"], index)
+        ploads.append(dict(seg=seg, func=_lookup(func_index, q["func"], "/PLOAD"), ascale_x=q["ascale_x"],
+                           fscale=q["fscale"]))
+    if cloads:
+        part["cloads"] = cloads
+    if ploads:
+        part["ploads"] = ploads
     part["ids"] = ids
+    part["hex_ids"] = hex_ids
     part["elem_ids"] = elem_ids
     d = decks.deck([part], name=name or sd.title or "rad")
+    if sd.funct:
+        d["functions"] = [dict(x=sd.funct[f][0], y=sd.funct[f][1]) for f in sorted(sd.funct)]
+    if sd.skews:
+        d["skews"] = [sd.skews[k] for k in sorted(sd.skews)]
     return d
+
+
+def _lookup(table, key, what):
+    if key not in table:
+        raise RadError(f"{what}: id {key} is not defined")
+    return table[key]
+
+
+def _segments(sd, surf, index):
+    """0-based segments (nseg, 4) of a surface, -1 in the fourth column of a
+    three-node segment."""
+    if surf in sd.surf_seg:
+        rows = [[index[n] for n in r[:3]] + [index[r[3]] if r[3] else -1] for r in sd.surf_seg[surf]]
+    elif surf in sd.surf_part:
+        rows = []
+        for pid in sd.surf_part[surf]:
+            if pid in sd.bricks:
+                raise RadError(f"/SURF/PART/{surf}: faces of solid parts are not implemented")
+            rows += [[index[n] for n in r[1:5]] for r in sorted(sd.shells.get(pid, []))]
+    else:
+        raise RadError(f"/PLOAD: surface {surf} is not defined")
+    return np.array(rows, np.int64).reshape(-1, 4)
 
 
 def add_engine(deck, ed: EngineDeck):
@@ -324,10 +474,10 @@ def add_engine(deck, ed: EngineDeck):
 
 
 def element_id(deck, ityptst, neltst):
-    """User id of the element that set the time step (shell groups only)."""
-    if ityptst != 3 or neltst < 0:
+    """User id of the element that set the time step (ityptst 1: hexa, 3: shell)."""
+    if neltst < 0 or ityptst not in (1, 3):
         return None
-    for ids in deck["parts"][0]["elem_ids"]:
+    for ids in deck["parts"][0]["hex_ids" if ityptst == 1 else "elem_ids"]:
         if neltst < ids.size:
             return int(ids[neltst])
         neltst -= ids.size
