@@ -250,6 +250,19 @@ int  or_ecycle_get_hex_state(or_ecycle* h, int group, double* sig, double* eint,
    component-major), eint (2 x nel component-major); any pointer may be NULL */
 int  or_ecycle_get_shell_state(or_ecycle* h, int group, double* sig, double* pla,
                                double* thk, double* hourg, double* eint);
+/* Restart: element state in the layouts of the get_* calls (any pointer may be
+   NULL: left as is), and the cumulative hourglass energy, plastic work and
+   external work of a part before the restart (added to or_ecycle_energies).  With
+   the nodes (or_ecycle_set_nodes) and the time state passed to or_ecycle_step,
+   this resumes a run from the reference's restart file (RDRESB / WRRESTP).
+   or_ecycle_reset returns to the state after finalize and clears the sums. */
+int  or_ecycle_set_hex_state(or_ecycle* h, int group, const double* sig, const double* eint,
+                             const double* rho, const double* qvis, const double* pla,
+                             const double* epsd);
+int  or_ecycle_set_shell_state(or_ecycle* h, int group, const double* sig, const double* pla,
+                               const double* thk, const double* hourg, const double* eint);
+int  or_ecycle_set_energy_sums(or_ecycle* h, int part, double hourglass, double plastic_work,
+                               double external_work);
 int  or_ecycle_energies(or_ecycle* h, int part, or_energies* e);
 
 /* --- diagnostics ----------------------------------------------------------- */

@@ -45,6 +45,7 @@ struct HPart {
   std::vector<double> x, v, vr, ms, in;
   std::vector<int> icodt, icodr;
   std::vector<int> iskew;           // skew frame of the /BCS codes, -1 = global (may be empty)
+  double ehour0 = 0, wpla0 = 0, wext0 = 0;   // cumulative energies before a restart
   int nel_solid = 0, nel_shell = 0;
   bool has_rot = false;
   int node_start = 0, node_pad = 0, tile_start = 0;
@@ -1102,6 +1103,49 @@ int shell_state_impl(or_ecycle* h, int gi, double* sig, double* pla, double* thk
   return OR_OK;
 }
 
+// element state upload (restart): the group's elements at their internal indices
+template <class R>
+int put_group(or_ecycle* h, R* dev, size_t np, int ncomp, const std::vector<int>& internal, const double* src) {
+  if (!src) return OR_OK;
+  auto s = d2h(dev, (size_t)ncomp * np);
+  const size_t nel = internal.size();
+  for (int q = 0; q < ncomp; ++q)
+    for (size_t i = 0; i < nel; ++i) s[(size_t)q * np + internal[i]] = R(src[(size_t)q * nel + i]);
+  CK(cudaMemcpy(dev, s.data(), s.size() * sizeof(R), cudaMemcpyHostToDevice));
+  return OR_OK;
+}
+
+template <class R>
+int set_hex_state_impl(or_ecycle* h, int gi, const double* sig, const double* eint, const double* rho,
+                       const double* qvis, const double* pla, const double* epsd) {
+  Impl<R>& m = *(Impl<R>*)h->impl;
+  const HHex& g = h->hex[gi];
+  const size_t np = m.hps.nelpad;
+  CK(cudaStreamSynchronize(h->stream));
+  int rc;
+  if ((rc = put_group(h, m.hsig.p, np, 6, g.internal, sig)) || (rc = put_group(h, m.heint.p, np, 1, g.internal, eint)) ||
+      (rc = put_group(h, m.hrho.p, np, 1, g.internal, rho)) || (rc = put_group(h, m.hqvis.p, np, 1, g.internal, qvis)) ||
+      (rc = put_group(h, m.hpla.p, np, 1, g.internal, pla)) || (rc = put_group(h, m.hepsd.p, np, 1, g.internal, epsd)))
+    return rc;
+  return OR_OK;
+}
+
+template <class R>
+int set_shell_state_impl(or_ecycle* h, int gi, const double* sig, const double* pla, const double* thk,
+                         const double* hourg, const double* eint) {
+  Impl<R>& m = *(Impl<R>*)h->impl;
+  const HShell& g = h->shell[gi];
+  const size_t np = m.sps.nelpad;
+  const int npt = g.prop.npt;
+  CK(cudaStreamSynchronize(h->stream));
+  int rc;
+  if ((rc = put_group(h, m.ssig.p, np, 5 * npt, g.internal, sig)) || (rc = put_group(h, m.spla.p, np, npt, g.internal, pla)) ||
+      (rc = put_group(h, m.sthk.p, np, 1, g.internal, thk)) || (rc = put_group(h, m.shourg.p, np, 3, g.internal, hourg)) ||
+      (rc = put_group(h, m.seint.p, np, 2, g.internal, eint)))
+    return rc;
+  return OR_OK;
+}
+
 template <class R>
 int energies_impl(or_ecycle* h, int part, or_energies* e) {
   Impl<R>& m = *(Impl<R>*)h->impl;
@@ -1146,8 +1190,8 @@ int energies_impl(or_ecycle* h, int part, or_energies* e) {
     for (int e = 0; e < m.nload; ++e)
       if (h->loads[e].part == part) wx += wacc[e] + wpend[e] * t.dt2;
   }
-  e->internal = ei; e->kinetic = ek; e->kinetic_rot = ekr; e->hourglass = eh; e->plastic_work = wp;
-  e->external_work = wx;
+  e->internal = ei; e->kinetic = ek; e->kinetic_rot = ekr;
+  e->hourglass = P.ehour0 + eh; e->plastic_work = P.wpla0 + wp; e->external_work = P.wext0 + wx;
   CK(cudaGetLastError());
   return OR_OK;
 }
@@ -1902,6 +1946,7 @@ int or_ecycle_reset(or_ecycle* h) {
   if (!h->finalized) return fail(h, OR_E_STATE, "reset before finalize");
   cudaSetDevice(h->cfg.device);
   h->next_parity = 0;
+  for (auto& P : h->parts) P.ehour0 = P.wpla0 = P.wext0 = 0.0;
   return h->cfg.precision == OR_PREC_SPLIT ? reset_impl<float>(h) : reset_impl<double>(h);
 }
 
@@ -2005,6 +2050,28 @@ int or_ecycle_get_hex_state(or_ecycle* h, int group, double* sig, double* eint, 
   if (!h || !h->finalized || group < 0 || group >= (int)h->hex.size()) return h ? fail(h, OR_E_ARG, "get_hex_state") : OR_E_ARG;
   cudaSetDevice(h->cfg.device);
   return DISPATCH(h, hex_state_impl, group, sig, eint, rho, qvis, pla, epsd);
+}
+
+int or_ecycle_set_hex_state(or_ecycle* h, int group, const double* sig, const double* eint, const double* rho,
+                            const double* qvis, const double* pla, const double* epsd) {
+  if (!h || !h->finalized || group < 0 || group >= (int)h->hex.size()) return h ? fail(h, OR_E_ARG, "set_hex_state") : OR_E_ARG;
+  cudaSetDevice(h->cfg.device);
+  return DISPATCH(h, set_hex_state_impl, group, sig, eint, rho, qvis, pla, epsd);
+}
+
+int or_ecycle_set_shell_state(or_ecycle* h, int group, const double* sig, const double* pla, const double* thk,
+                              const double* hourg, const double* eint) {
+  if (!h || !h->finalized || group < 0 || group >= (int)h->shell.size())
+    return h ? fail(h, OR_E_ARG, "set_shell_state") : OR_E_ARG;
+  cudaSetDevice(h->cfg.device);
+  return DISPATCH(h, set_shell_state_impl, group, sig, pla, thk, hourg, eint);
+}
+
+int or_ecycle_set_energy_sums(or_ecycle* h, int part, double hourglass, double plastic_work, double external_work) {
+  if (!h || part < 0 || part >= (int)h->parts.size()) return h ? fail(h, OR_E_ARG, "set_energy_sums") : OR_E_ARG;
+  HPart& P = h->parts[part];
+  P.ehour0 = hourglass; P.wpla0 = plastic_work; P.wext0 = external_work;
+  return OR_OK;
 }
 
 int or_ecycle_get_shell_state(or_ecycle* h, int group, double* sig, double* pla, double* thk, double* hourg,

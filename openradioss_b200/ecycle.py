@@ -48,7 +48,8 @@ EXPORTS = [
     "or_ecycle_kernel_times", "or_ecycle_set_halo", "or_ecycle_spmd_buffer_bytes", "or_ecycle_spmd_begin",
     "or_ecycle_spmd_elements", "or_ecycle_spmd_nodes", "or_ecycle_spmd_end", "or_ecycle_add_rlink",
     "or_ecycle_set_rlink", "or_ecycle_add_function", "or_ecycle_add_cload", "or_ecycle_add_pload",
-    "or_ecycle_add_skew", "or_ecycle_set_bcs_skew",
+    "or_ecycle_add_skew", "or_ecycle_set_bcs_skew", "or_ecycle_set_hex_state", "or_ecycle_set_shell_state",
+    "or_ecycle_set_energy_sums",
 ]
 
 
@@ -74,6 +75,9 @@ def _declare(lib):
         "or_ecycle_add_pload": ([P, C.c_int, C.c_int, ip, C.c_int, C.c_double, C.c_double, ip], C.c_int),
         "or_ecycle_add_skew": ([P, dp, ip], C.c_int),
         "or_ecycle_set_bcs_skew": ([P, C.c_int, ip], C.c_int),
+        "or_ecycle_set_hex_state": ([P, C.c_int, dp, dp, dp, dp, dp, dp], C.c_int),
+        "or_ecycle_set_shell_state": ([P, C.c_int, dp, dp, dp, dp, dp], C.c_int),
+        "or_ecycle_set_energy_sums": ([P, C.c_int, C.c_double, C.c_double, C.c_double], C.c_int),
         "or_ecycle_finalize": ([P], C.c_int),
         "or_ecycle_reset": ([P], C.c_int),
         "or_ecycle_step": ([P, C.c_int, C.POINTER(abi.Time)], C.c_int),
@@ -277,6 +281,38 @@ class ECycle(_DeckModel):
 
     def step(self, ncycles):
         self._call("step", int(ncycles), self.times)
+
+    # --- restart -------------------------------------------------------------
+    def set_nodes(self, part, x=None, d=None, v=None, vr=None):
+        self._call("set_nodes", part, *(abi.ptr(_f64(a), C.c_double) if a is not None else None
+                                       for a in (x, d, v, vr)))
+
+    def set_hex_state(self, group, **state):
+        keys = ("sig", "eint", "rho", "qvis", "pla", "epsd")
+        arrs = [_f64(state[k]) if state.get(k) is not None else None for k in keys]
+        self._call("set_hex_state", group, *(abi.ptr(a, C.c_double) for a in arrs))
+
+    def set_shell_state(self, group, **state):
+        keys = ("sig", "pla", "thk", "hourg", "eint")
+        arrs = [_f64(state[k]) if state.get(k) is not None else None for k in keys]
+        self._call("set_shell_state", group, *(abi.ptr(a, C.c_double) for a in arrs))
+
+    def set_energy_sums(self, part, hourglass, plastic_work, external_work):
+        self._call("set_energy_sums", part, float(hourglass), float(plastic_work), float(external_work))
+
+    def restart_from(self, other):
+        """Copies another handle's state (nodes, element state, time, energy
+        sums) into this one, as a restart file would."""
+        for p in range(self.nparts):
+            n = other.get_nodes(p)
+            self.set_nodes(p, n["x"], n["d"], n["v"], n["vr"])
+            e = other.energies(p)
+            self.set_energy_sums(p, e["hourglass"], e["plastic_work"], e["external_work"])
+            self.times[p] = other.times[p]
+        for gi in range(len(self.hex_groups)):
+            self.set_hex_state(gi, **other.hex_state(gi))
+        for gi in range(len(self.shell_groups)):
+            self.set_shell_state(gi, **other.shell_state(gi))
 
     def reset(self):
         """Back to the uploaded initial state (nodes, elements, time, energies)."""
