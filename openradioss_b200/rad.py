@@ -138,6 +138,7 @@ class StarterDeck:
         self.def_solid = dict(isolid=0, ismstr=0, iframe=0)
         self.ishfram = 0
         self.bricks = {}           # part id -> list of (elem id, n1..n8)
+        self.shell_thk = {}        # part id -> {elem id: thickness} of the /SHELL cards that give one
         self.funct = {}            # id -> (x list, y list)
         self.skews = {}            # id -> 9 floats (x', y', z')
         self.surf_seg = {}         # id -> list of (n1, n2, n3, n4), n4 = 0 for triangles
@@ -163,8 +164,13 @@ class StarterDeck:
         elif k0 == "SHELL":
             part = int(key[1])
             rows = self.shells.setdefault(part, [])
+            thk = self.shell_thk.setdefault(part, {})
             for line in L:
-                rows.append(tuple(_int(line, 10 * c) for c in range(5)))
+                row = tuple(_int(line, 10 * c) for c in range(5))
+                rows.append(row)
+                t = _real(line, 80) if len(line) > 80 else 0.0
+                if t > 0.0:
+                    thk[row[0]] = t          # element thickness overriding the property's
         elif k0 == "BRICK":
             part = int(key[1])
             rows = self.bricks.setdefault(part, [])
@@ -373,6 +379,8 @@ def to_deck(sd: StarterDeck, name=None):
         if prop.get("kind") != "shell":
             raise RadError(f"/PART/{pid}: shells need a /PROP/SHELL")
         ihbe, ismstr, ithk, ipla = _shell_flags(sd, prop)
+        if ithk == 2:
+            ithk = 0                        # cgrtails.F:832-833
         if ihbe != 1 or ismstr != 2:
             raise RadError(f"/PROP/SHELL/{prop_id}: Ishell {ihbe} / Ismstr {ismstr}; the element cycle "
                            "implements Ishell 1 with Ismstr 2")
@@ -397,7 +405,9 @@ def to_deck(sd: StarterDeck, name=None):
             p["shf"] = prop["ashear"]
         if npt == 1:
             p["shf"] = 0.0
-        decks.add_shell(part, conn, _material(mat), p)
+        et = sd.shell_thk.get(pid, {})
+        thke = np.array([et.get(r[0], prop["thick"]) for r in rows], np.float64) if et else None
+        decks.add_shell(part, conn, _material(mat), p, thke=thke)
         elem_ids.append(np.array([r[0] for r in rows], np.int64))
     skew_index = {sid: k for k, sid in enumerate(sorted(sd.skews))}
     skew_of = lambda sid, what: -1 if sid == 0 else _lookup(skew_index, sid, what)
@@ -498,3 +508,216 @@ def part_masses(deck):
 
 def total_mass(deck):
     return float(np.sum(deck["parts"][0]["ms"]))
+
+
+# ---------------------------------------------------------------------------
+# writer: a deck dict as a starter deck and an engine deck (2019 block format)
+# ---------------------------------------------------------------------------
+
+def _num20(x):
+    """A real in at most 19 characters, so that a blank separates the fields: the
+    shortest exact form when it fits, else 13 significant digits (a 20-character
+    field cannot hold every double)."""
+    r = repr(float(x))
+    return r if len(r) <= 19 else f"{float(x):.13g}"
+
+
+def _f20(*v):
+    return "".join(f"{_num20(x):>20s}" for x in v)
+
+
+def _i10(*v):
+    return "".join(f"{int(x):10d}" for x in v)
+
+
+def _grnod(L, gid, title, nodes):
+    L += [f"/GRNOD/NODE/{gid}", title]
+    nodes = [int(n) for n in nodes]
+    L += [_i10(*nodes[i:i + 10]) for i in range(0, len(nodes), 10)]
+
+
+def write_starter(deck, path, part=0, title=None):
+    """Writes part ``part`` of a deck dict as a Radioss starter deck: /NODE,
+    /BRICK and /SHELL per element group (one /PART, /PROP and /MAT each),
+    /BCS, /INIVEL/TRA and /ADMAS from the nodal arrays (the added mass is the
+    nodal mass beyond the lumped element masses), /SKEW/FIX, /FUNCT, /CLOAD and
+    /PLOAD; a shell group's uniform ``pressure`` becomes a /PLOAD with a
+    constant function.  Node and element ids are 1-based indices.  Per-element
+    yield stresses have no deck form and are refused."""
+    p = deck["parts"][part]
+    x = p["x"]
+    n = x.shape[0]
+    L = ["#RADIOSS STARTER", "/BEGIN", title or deck.get("name", "deck"), _i10(2019, 0),
+         f"{'kg':>20s}{'m':>20s}{'s':>20s}", f"{'kg':>20s}{'m':>20s}{'s':>20s}",
+         "/TITLE", title or deck.get("name", "deck"), "/NODE"]
+    L += [_i10(k + 1) + _f20(*x[k]) for k in range(n)]
+    mass = np.zeros(n)
+    pid = 0
+    eid = 0
+    gid = 0
+    fid_const = None
+    funcs = list(deck.get("functions", []))
+    ploads = list(p.get("ploads", []))
+    for g in p["hex"]:
+        pid += 1
+        m = g["mat"]
+        conn = g["ixs"][:, 1:9] - 1
+        vol0 = np.asarray(g["vol0"]) if g.get("vol0") is not None else decks.hex_volumes(x, conn)
+        np.add.at(mass, conn.ravel(), np.repeat(m["rho0"] * vol0 / 8.0, 8))
+        L += _material_cards(pid, m)
+        pr = g["prop"]
+        L += [f"/PROP/SOLID/{pid}", f"solid {pid}", _i10(1, 4, 0, 0, 0, 0, 0, 1) + _f20(0.0),
+              _f20(pr["qa"], pr["qb"], pr["qh"], 0.0, 0.0), _f20(0.0, 0.0, 0.0, 0.0, 0.0),
+              f"/PART/{pid}", f"part {pid}", _i10(pid, pid, 0), f"/BRICK/{pid}"]
+        for e in range(conn.shape[0]):
+            eid += 1
+            L.append(_i10(eid, *(conn[e] + 1)))
+    for g in p["shell"]:
+        pid += 1
+        m, pr = g["mat"], g["prop"]
+        if g.get("jc_a") is not None:
+            raise ValueError("write_starter: per-element yield stresses have no .rad form")
+        conn = g["ixc"][:, 1:5] - 1
+        thk = np.asarray(g["thke"], np.float64)
+        area = decks.shell_areas(x, conn)
+        ems = m["rho0"] * thk * area / 4.0
+        np.add.at(mass, conn.ravel(), np.repeat(ems, 4))
+        L += _material_cards(pid, m)
+        L += [f"/PROP/SHELL/{pid}", f"shell {pid}", _i10(1, 2, 0, 0) + " " * 20 + _f20(0.0),
+              _f20(pr["hm"], pr["hf"], pr["hr"], 0.0, 0.0),
+              _i10(pr["npt"], 0) + _f20(pr["thk"], pr["shf"] if pr["npt"] > 1 else 0.0) +
+              _i10(1 if pr["ithk"] else 2, 0),
+              f"/PART/{pid}", f"part {pid}", _i10(pid, pid, 0), f"/SHELL/{pid}"]
+        uniform = np.allclose(thk, pr["thk"], rtol=0, atol=0)
+        for e in range(conn.shape[0]):
+            eid += 1
+            L.append(_i10(eid, *(conn[e] + 1)) + ("" if uniform else " " * 10 + _f20(0.0, thk[e])))
+        if pr.get("pressure", 0.0) != 0.0:
+            if fid_const is None:
+                funcs.append(dict(x=[0.0], y=[1.0]))
+                fid_const = len(funcs) - 1
+            ploads.append(dict(seg=conn, func=fid_const, ascale_x=1.0, fscale=-pr["pressure"]))
+    if any(g["prop"].get("ishfram", 0) == 2 for g in p["shell"]):
+        L.insert(L.index("/NODE"), "/SHFRA/V4")
+    skews = deck.get("skews", [])
+    for k, ax in enumerate(skews):
+        ax = np.asarray(ax, np.float64).reshape(3, 3)
+        L += [f"/SKEW/FIX/{k + 1}", f"skew {k + 1}", _f20(0.0, 0.0, 0.0), _f20(*ax[1]), _f20(*ax[2])]
+    iskew = p.get("iskew")
+    combos = {}
+    for i in range(n):
+        ct, cr = int(p["icodt"][i]), int(p["icodr"][i])
+        if ct or cr:
+            sk = int(iskew[i]) + 1 if iskew is not None and iskew[i] >= 0 else 0
+            combos.setdefault((ct, cr, sk), []).append(i + 1)
+    digits = lambda c: "".join("1" if c & b else "0" for b in (4, 2, 1))
+    for k, ((ct, cr, sk), nodes) in enumerate(sorted(combos.items())):
+        gid += 1
+        L += [f"/BCS/{k + 1}", f"bcs {k + 1}", f"   {digits(ct)} {digits(cr)}" + _i10(sk, gid)]
+        _grnod(L, gid, f"bcs {k + 1}", nodes)
+    vels = {}
+    for i in range(n):
+        v = tuple(float(c) for c in p["v"][i])
+        if any(v):
+            vels.setdefault(v, []).append(i + 1)
+    if np.abs(p["vr"]).max() > 0:
+        raise ValueError("write_starter: initial rotational velocities are not written")
+    for k, (v, nodes) in enumerate(sorted(vels.items())):
+        gid += 1
+        L += [f"/INIVEL/TRA/{k + 1}", f"inivel {k + 1}", _f20(*v) + _i10(gid, 0)]
+        _grnod(L, gid, f"inivel {k + 1}", nodes)
+    extra = np.asarray(p["ms"]) - mass
+    added = np.nonzero(extra > 1e-12 * max(np.abs(p["ms"]).max(), 1e-300))[0]
+    for k, i in enumerate(added):
+        gid += 1
+        L += [f"/ADMAS/0/{k + 1}", f"added mass {k + 1}", _f20(extra[i]) + _i10(gid)]
+        _grnod(L, gid, f"added mass {k + 1}", [i + 1])
+    for k, f in enumerate(funcs):
+        L += [f"/FUNCT/{k + 1}", f"function {k + 1}"] + [_f20(a, b) for a, b in zip(f["x"], f["y"])]
+    dname = {1: "X", 2: "Y", 3: "Z", 4: "XX", 5: "YY", 6: "ZZ"}
+    for k, c in enumerate(p.get("cloads", [])):
+        gid += 1
+        sk = int(c.get("skew", -1)) + 1
+        L += [f"/CLOAD/{k + 1}", f"cload {k + 1}",
+              _i10(c["func"] + 1) + f"{dname[c['dir']]:>10s}" + _i10(sk, 0, gid, 1) +
+              _f20(c.get("ascale_x", 1.0), c.get("fscale", 1.0))]
+        _grnod(L, gid, f"cload {k + 1}", np.asarray(c["nodes"]) + 1)
+    for k, q in enumerate(ploads):
+        seg = np.asarray(q["seg"])
+        L += [f"/SURF/SEG/{k + 1}", f"segments {k + 1}"]
+        L += [_i10(j + 1, *[s + 1 if s >= 0 else 0 for s in seg[j]]) for j in range(seg.shape[0])]
+        L += [f"/PLOAD/{k + 1}", f"pload {k + 1}",
+              _i10(k + 1, q["func"] + 1, 0, 0) + " " * 20 + _f20(q.get("ascale_x", 1.0), q.get("fscale", 1.0))]
+    L.append("/END")
+    with open(path, "w") as f:
+        f.write("\n".join(L) + "\n")
+
+
+def _material_cards(mid, m):
+    if m["law"] == decks.LAW_JOHNSON_COOK:
+        return [f"/MAT/PLAS_JOHNS/{mid}", f"material {mid}", _f20(m["rho0"]), _f20(m["young"], m["nu"]) + _i10(0),
+                _f20(m["jc_a"], m["jc_b"], m["jc_n"], 0.0 if m["epsmax"] >= 1e20 else m["epsmax"],
+                     0.0 if m["sigmax"] >= 1e20 else m["sigmax"]),
+                _f20(0.0, 0.0) + _i10(0, 0) + _f20(0.0, 0.0), _f20(0.0, 0.0, 0.0, 0.0)]
+    return [f"/MAT/ELAST/{mid}", f"material {mid}", _f20(m["rho0"]), _f20(m["young"], m["nu"])]
+
+
+def write_engine(path, run_name, tstop, deck=None, part=0, run=1):
+    """Writes an engine deck: /RUN to ``tstop`` and the part's rigid links as /VEL cards."""
+    L = ["#RADIOSS ENGINE", f"/RUN/{run_name}/{run}", _f20(tstop), "/PRINT/-100/55", "/PARITH/ON"]
+    if deck is not None:
+        for r in deck["parts"][part].get("rlinks", []):
+            for kind, code in (("TRA", r.get("ic", 7)), ("ROT", r.get("icr", 0))):
+                if code:
+                    dirs = "".join(c for c, b in (("X", 4), ("Y", 2), ("Z", 1)) if code & b)
+                    nodes = [int(v) + 1 for v in r["nodes"]]
+                    L.append(f"/VEL/{kind}/{dirs}")
+                    L += [_i10(*nodes[i:i + 10]) for i in range(0, len(nodes), 10)]
+    L.append("/END")
+    with open(path, "w") as f:
+        f.write("\n".join(L) + "\n")
+
+
+def _dt_estimate(deck, part=0):
+    """Initial element time step, roughly: DTFAC * length / wave speed of the
+    stiffest, smallest element (for the /RUN time of a written deck)."""
+    p = deck["parts"][part]
+    dt = np.inf
+    for g in p["hex"]:
+        m = g["mat"]
+        conn = g["ixs"][:, 1:9] - 1
+        vol = np.abs(decks.hex_volumes(p["x"], conn))
+        c = np.sqrt((m["bulk"] + 4.0 / 3.0 * m["shear"]) / m["rho0"])
+        dt = min(dt, deck.get("dtfac_solid", 0.9) * vol.min() ** (1.0 / 3.0) / c)
+    for g in p["shell"]:
+        conn = g["ixc"][:, 1:5] - 1
+        dt = min(dt, deck.get("dtfac_shell", 0.9) * np.sqrt(decks.shell_areas(p["x"], conn).min()) /
+                 g["mat"]["ssp_shell"])
+    return dt
+
+
+def main(argv=None):
+    """Writes a workload as <NAME>_0000.rad (starter) and <NAME>_0001.rad (engine):
+
+        python -m openradioss_b200.rad --workload hex_block --out DIR [--tstop T]
+    """
+    import argparse
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("--workload", required=True, choices=["hex_block", "shell_plate", "mixed_mesh", "hat_rail"])
+    ap.add_argument("--out", required=True)
+    ap.add_argument("--name", default=None)
+    ap.add_argument("--tstop", type=float, default=0.0, help="final time (default: cycles x initial dt estimate)")
+    a = ap.parse_args(argv)
+    make = {"hex_block": decks.c1_hex_block, "shell_plate": decks.c2_shell_plate, "mixed_mesh": decks.c4_mixed_mesh,
+            "hat_rail": decks.hat_rail}[a.workload]
+    d = make()
+    name = (a.name or a.workload.upper().replace("_", ""))[:8]
+    os.makedirs(a.out, exist_ok=True)
+    tstop = a.tstop or d.get("ncycles", 100) * _dt_estimate(d)
+    write_starter(d, os.path.join(a.out, f"{name}_0000.rad"))
+    write_engine(os.path.join(a.out, f"{name}_0001.rad"), name, tstop, d)
+    print(f"{a.out}/{name}_0000.rad, {name}_0001.rad (final time {tstop:.6g})")
+
+
+if __name__ == "__main__":
+    main()
