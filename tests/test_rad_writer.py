@@ -54,9 +54,9 @@ def test_shell_plate_with_pressure_and_thickness_roundtrip(tmp_path):
     assert not np.array_equal(decks_ms, p["ms"])
     got = roundtrip(d, tmp_path)
     pg = got["parts"][0]
-    # linspace thicknesses do not fit 20 characters exactly: 13 digits in the deck
-    assert np.allclose(pg["ms"], p["ms"], rtol=1e-12, atol=0)
-    assert np.allclose(pg["inr"], p["inr"], rtol=1e-12, atol=0)
+    # jittered coordinates and linspace thicknesses do not fit a field exactly: 13 digits
+    assert np.allclose(pg["ms"], p["ms"], rtol=1e-11, atol=0)
+    assert np.allclose(pg["inr"], p["inr"], rtol=1e-11, atol=0)
     assert len(pg["ploads"]) == 1 and pg["ploads"][0]["fscale"] == -2e6
     # the group pressure becomes a /PLOAD: same forces, a load slot instead of the shell's own
     from oracle.oracle import Oracle
