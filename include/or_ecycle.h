@@ -97,11 +97,15 @@ typedef struct {
   double sigmax;        /* uparam(5) SIGMX, 1e20 when unset             */
 } or_material;
 
-/* /PROP/SOLID values on the path (hm_read_prop14.F:338-361) */
+/* /PROP/SOLID values on the path (hm_read_prop14.F:338-380) */
 typedef struct {
   double qa;            /* GEO(14), default 1.1   */
   double qb;            /* GEO(15), default 0.05  */
   double qh;            /* GEO(13), default 0.1   */
+  int    jcvt;          /* IGEO(16) = Iframe - 1: 0 global frame (Jaumann stress
+                           rotation), 1 convected frame of SRCOOR3 (sforc3.F:505,
+                           :798-816, :1603-1614)                                  */
+  int    pad;
 } or_solid_prop;
 
 /* /PROP/SHELL values on the path (hm_read_prop01.F:141-317) */

@@ -42,7 +42,7 @@ class Material(C.Structure):
 
 
 class SolidProp(C.Structure):
-    _fields_ = [("qa", C.c_double), ("qb", C.c_double), ("qh", C.c_double)]
+    _fields_ = [("qa", C.c_double), ("qb", C.c_double), ("qh", C.c_double), ("jcvt", C.c_int), ("pad", C.c_int)]
 
 
 class ShellProp(C.Structure):
@@ -84,7 +84,7 @@ def make_material(m: dict) -> Material:
 
 
 def make_solid_prop(p: dict) -> SolidProp:
-    return SolidProp(p["qa"], p["qb"], p["qh"])
+    return SolidProp(p["qa"], p["qb"], p["qh"], int(p.get("jcvt", 0)), 0)
 
 
 def make_shell_prop(p: dict) -> ShellProp:

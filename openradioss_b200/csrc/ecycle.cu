@@ -322,6 +322,7 @@ struct Impl {
   typedef typename Vec4<R>::T R4;
   int nnodpad = 0, ntiles = 0, nparts = 0, nslot = 0;
   bool any_rot = false;
+  bool any_corot = false;    // a hexa group in the convected frame (JCVT /= 0)
   // nodes
   DBuf<double4> X; DBuf<double> DX, DY, DZ; DBuf<R4> V, VR; DBuf<unsigned char> code;
   DBuf<int> adsky, tile_part; DBuf<PartDesc> partd;
@@ -421,7 +422,10 @@ template <class R, int T>
 int launch_hex(or_ecycle* h, Impl<R>& m, int parity) {
   if (m.hps.info.empty()) return OR_OK;
   size_t sm = hex_smem<R>(m.hps.nlmax, T, m.hinc_stride);
-  hex_patch_kernel<R, T><<<(unsigned)m.hps.info.size(), T, sm, h->stream>>>(m.hargs(), parity);
+  if (m.any_corot)
+    hex_patch_kernel<R, T, 1><<<(unsigned)m.hps.info.size(), T, sm, h->stream>>>(m.hargs(), parity);
+  else
+    hex_patch_kernel<R, T, 0><<<(unsigned)m.hps.info.size(), T, sm, h->stream>>>(m.hargs(), parity);
   CK(cudaGetLastError());
   h->launches++;
   return OR_OK;
@@ -477,9 +481,12 @@ int set_smem_attrs(or_ecycle* h, Impl<R>& m) {
   int hs = (int)hex_smem<R>(m.hps.nlmax, h->tile_hex, m.hinc_stride);
   int ss = (int)shell_smem<R>(m.sps.nlmax, h->tile_shell, m.sinc_stride);
   if (hs > 200 * 1024 || ss > 200 * 1024) return fail(h, OR_E_UNSUPPORTED, "patch shared memory above 200 KB");
-  CK(set_smem(hex_patch_kernel<R, 64>, hs));
-  CK(set_smem(hex_patch_kernel<R, 128>, hs));
-  CK(set_smem(hex_patch_kernel<R, 256>, hs));
+  CK(set_smem(hex_patch_kernel<R, 64, 0>, hs));
+  CK(set_smem(hex_patch_kernel<R, 128, 0>, hs));
+  CK(set_smem(hex_patch_kernel<R, 256, 0>, hs));
+  CK(set_smem(hex_patch_kernel<R, 64, 1>, hs));
+  CK(set_smem(hex_patch_kernel<R, 128, 1>, hs));
+  CK(set_smem(hex_patch_kernel<R, 256, 1>, hs));
   CK(set_smem(shell_patch_kernel<R, 64, 0>, ss));
   CK(set_smem(shell_patch_kernel<R, 128, 0>, ss));
   CK(set_smem(shell_patch_kernel<R, 256, 0>, ss));
@@ -682,7 +689,8 @@ int finalize_impl(or_ecycle* h) {
     std::vector<HexGroupDesc> desc;
     for (auto& g : h->hex) {
       HexGroupDesc d{};
-      d.part = g.part; d.law = g.mat.law; d.nel = g.nel;
+      d.part = g.part; d.law = g.mat.law; d.nel = g.nel; d.jcvt = g.prop.jcvt;
+      m.any_corot = m.any_corot || g.prop.jcvt != 0;
       d.rho0 = g.mat.rho0; d.shear = g.mat.shear; d.bulk = g.mat.bulk; d.jc_a = g.mat.jc_a; d.jc_b = g.mat.jc_b;
       d.jc_n = g.mat.jc_n; d.epsmax = g.mat.epsmax; d.sigmax = g.mat.sigmax;
       d.qa = g.prop.qa; d.qb = g.prop.qb; d.qh = g.prop.qh; d.dtfac = h->cfg.dtfac_solid; d.dtmin = h->cfg.dtmin_solid;
@@ -1730,6 +1738,7 @@ int or_ecycle_add_hex_group(or_ecycle* h, int part, int nel, const int* ixs, con
   if (part < 0 || part >= (int)h->parts.size() || nel <= 0 || !ixs || !mat || !prop || !group)
     return fail(h, OR_E_ARG, "add_hex_group: bad argument");
   if (mat->law != OR_LAW_ELASTIC && mat->law != OR_LAW_JOHNSON_COOK) return fail(h, OR_E_UNSUPPORTED, "hex law");
+  if (prop->jcvt != 0 && prop->jcvt != 1) return fail(h, OR_E_UNSUPPORTED, "hex frame other than global or convected");
   HHex g;
   g.part = part; g.nel = nel; g.mat = *mat; g.prop = *prop;
   HPart& P = h->parts[part];

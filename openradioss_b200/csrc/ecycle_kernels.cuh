@@ -47,7 +47,7 @@ struct PatchInfo {
 };
 
 struct HexGroupDesc {
-  int part, law, nel, pad;
+  int part, law, nel, jcvt;       // jcvt: 1 = convected frame (Iframe 2)
   double rho0, shear, bulk, jc_a, jc_b, jc_n, epsmax, sigmax;
   double qa, qb, qh, dtfac, dtmin;
 };
@@ -353,7 +353,9 @@ __host__ __device__ constexpr int min_blocks(int ctas128, int tile) {
 // ===========================================================================
 // Per element (thread): SCOOR3, SDERI3, SDLEN3, SDEFO3, SRHO3, SROTA3, MMAIN ->
 // M1LAW / M2LAW -> MQVISCB, SHVIS3, SFINT3; corner forces into shared memory.
-template <class R, int TILE>
+// CORO = 1: groups may use the convected frame (JCVT /= 0, decided per group at
+// run time); CORO = 0 compiles that path out (the register budget of the default)
+template <class R, int TILE, int CORO>
 __global__ void __launch_bounds__(TILE, min_blocks(Occupancy<R>::hex, TILE))
 hex_patch_kernel(HexArgs<R> a, int parity) {
   typedef typename Vec4<R>::T R4;
@@ -438,6 +440,46 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
     double XD[8], YD[8], ZD[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) { XD[k] = sx[lc[k]]; YD[k] = sy[lc[k]]; ZD[k] = sz[lc[k]]; }
+    // ---- SRCOOR3 (srcoor3.F, JCVT /= 0, ISORTH = 0): convected frame R = [e1 e2 e3] of
+    // SREPISO3 (FP64 differences, r, s, t in R) and SORTHO3 (three symmetric
+    // corrections, then Gram-Schmidt); coordinates (FP64) and velocities in it ----
+    R R11 = R(1), R12 = R(0), R13 = R(0), R21 = R(0), R22 = R(1), R23 = R(0), R31 = R(0), R32 = R(0), R33 = R(1);
+    const bool corot = CORO && gd.jcvt;
+    if (corot) {
+      const R x17 = R(XD[6] - XD[0]), x28 = R(XD[7] - XD[1]), x35 = R(XD[4] - XD[2]), x46 = R(XD[5] - XD[3]);
+      const R y17 = R(YD[6] - YD[0]), y28 = R(YD[7] - YD[1]), y35 = R(YD[4] - YD[2]), y46 = R(YD[5] - YD[3]);
+      const R z17 = R(ZD[6] - ZD[0]), z28 = R(ZD[7] - ZD[1]), z35 = R(ZD[4] - ZD[2]), z46 = R(ZD[5] - ZD[3]);
+      const R a17 = x17 + x46, a28 = x28 + x35, b17 = y17 + y46, b28 = y28 + y35, c17 = z17 + z46, c28 = z28 + z35;
+      R Ux = x17 + x28 - x35 - x46, Uy = y17 + y28 - y35 - y46, Uz = z17 + z28 - z35 - z46;
+      R Vx = a17 + a28, Vy = b17 + b28, Vz = c17 + c28;
+      R Wx = a17 - a28, Wy = b17 - b28, Wz = c17 - c28;
+      auto unit = [](R& x, R& y, R& z) {
+        R aa = ssqrt(x * x + y * y + z * z);
+        if (aa != R(0)) aa = R(1) / aa;
+        x *= aa; y *= aa; z *= aa;
+      };
+      unit(Ux, Uy, Uz); unit(Vx, Vy, Vz); unit(Wx, Wy, Wz);
+#pragma unroll
+      for (int it = 0; it < 3; ++it) {
+        R e1x = Vy * Wz - Vz * Wy + Ux, e1y = Vz * Wx - Vx * Wz + Uy, e1z = Vx * Wy - Vy * Wx + Uz;
+        R e2x = Wy * Uz - Wz * Uy + Vx, e2y = Wz * Ux - Wx * Uz + Vy, e2z = Wx * Uy - Wy * Ux + Vz;
+        R e3x = Uy * Vz - Uz * Vy + Wx, e3y = Uz * Vx - Ux * Vz + Wy, e3z = Ux * Vy - Uy * Vx + Wz;
+        unit(e1x, e1y, e1z); unit(e2x, e2y, e2z); unit(e3x, e3y, e3z);
+        Ux = e1x; Uy = e1y; Uz = e1z; Vx = e2x; Vy = e2y; Vz = e2z; Wx = e3x; Wy = e3y; Wz = e3z;
+      }
+      R e3x = Uy * Vz - Uz * Vy, e3y = Uz * Vx - Ux * Vz, e3z = Ux * Vy - Uy * Vx;
+      unit(e3x, e3y, e3z);
+      R11 = Ux; R21 = Uy; R31 = Uz;
+      R12 = e3y * Uz - e3z * Uy; R22 = e3z * Ux - e3x * Uz; R32 = e3x * Uy - e3y * Ux;
+      R13 = e3x; R23 = e3y; R33 = e3z;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const double xl = (double)R11 * XD[k] + (double)R21 * YD[k] + (double)R31 * ZD[k];
+        const double yl = (double)R12 * XD[k] + (double)R22 * YD[k] + (double)R32 * ZD[k];
+        const double zl = (double)R13 * XD[k] + (double)R23 * YD[k] + (double)R33 * ZD[k];
+        XD[k] = xl; YD[k] = yl; ZD[k] = zl;
+      }
+    }
     const double X17 = XD[6] - XD[0], X28 = XD[7] - XD[1], X35 = XD[4] - XD[2], X46 = XD[5] - XD[3];
     const double Y17 = YD[6] - YD[0], Y28 = YD[7] - YD[1], Y35 = YD[4] - YD[2], Y46 = YD[5] - YD[3];
     const double Z17 = ZD[6] - ZD[0], Z28 = ZD[7] - ZD[1], Z35 = ZD[4] - ZD[2], Z46 = ZD[5] - ZD[3];
@@ -513,6 +555,15 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
     R VX[8], VY[8], VZ[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) { VX[k] = svx[lc[k]]; VY[k] = svy[lc[k]]; VZ[k] = svz[lc[k]]; }
+    if (corot) {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const R vx = R11 * VX[k] + R21 * VY[k] + R31 * VZ[k];
+        const R vy = R12 * VX[k] + R22 * VY[k] + R32 * VZ[k];
+        const R vz = R13 * VX[k] + R23 * VY[k] + R33 * VZ[k];
+        VX[k] = vx; VY[k] = vy; VZ[k] = vz;
+      }
+    }
     const R vx17 = VX[0] - VX[6], vx28 = VX[1] - VX[7], vx35 = VX[2] - VX[4], vx46 = VX[3] - VX[5];
     const R vy17 = VY[0] - VY[6], vy28 = VY[1] - VY[7], vy35 = VY[2] - VY[4], vy46 = VY[3] - VY[5];
     const R vz17 = VZ[0] - VZ[6], vz28 = VZ[1] - VZ[7], vz35 = VZ[2] - VZ[4], vz46 = VZ[3] - VZ[5];
@@ -548,7 +599,9 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
     const R S1 = st_sig[0], S2 = st_sig[1], S3 = st_sig[2];
     const R S4 = st_sig[3], S5 = st_sig[4], S6 = st_sig[5];
     R SG[6];
-    {
+    if (corot) {          // SRMALLA3 (srmall3.F): convected-frame stress, not rotated
+      SG[0] = S1; SG[1] = S2; SG[2] = S3; SG[3] = S4; SG[4] = S5; SG[5] = S6;
+    } else {
       const R q1 = R(2) * S4 * WZZ, q2 = R(2) * S6 * WYY, q3 = R(2) * S5 * WXX;
       SG[0] = S1 - q1 + q2;
       SG[1] = S2 + q1 - q3;
@@ -710,6 +763,15 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
         F[1][n1[q]] -= f; F[1][n2[q]] += f;
         f = s3 * PZ[q] + s6 * PX[q] + s5 * PY[q];
         F[2][n1[q]] -= f; F[2][n2[q]] += f;
+      }
+    }
+    if (corot) {          // SRROTA3 with R transposed (sforc3.F:1603-1614): back to global axes
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const R fx = R11 * F[0][k] + R12 * F[1][k] + R13 * F[2][k];
+        const R fy = R21 * F[0][k] + R22 * F[1][k] + R23 * F[2][k];
+        const R fz = R31 * F[0][k] + R32 * F[1][k] + R33 * F[2][k];
+        F[0][k] = fx; F[1][k] = fy; F[2][k] = fz;
       }
     }
   }

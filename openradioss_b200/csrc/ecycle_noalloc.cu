@@ -349,6 +349,7 @@ extern "C" int or_ecycle_hex_step_noalloc(int device, void* stream, int ncycles,
   if (ncycles < 0 || numnod <= 0 || nel <= 0) return OR_E_ARG;
   if ((long long)8 * nel > OR_NOALLOC_MAX_SLOTS) return OR_E_ARG;       // skyline beyond the scratch
   if (mat->law != OR_LAW_ELASTIC && mat->law != OR_LAW_JOHNSON_COOK) return OR_E_UNSUPPORTED;
+  if (prop->jcvt != 0) return OR_E_UNSUPPORTED;                          // global frame only
   if (device < 0 || device >= MAX_DEVICES) return OR_E_ARG;
   if (cudaSetDevice(device) != cudaSuccess) return OR_E_CUDA;
   if (!g_ptrs_ready[device]) {

@@ -58,8 +58,8 @@ def aluminium_jc():
     return material(LAW_JOHNSON_COOK, 2700.0, 70e9, 0.33, 350e6, 275e6, 0.36)
 
 
-def solid_prop(qa=1.1, qb=0.05, qh=0.1):
-    return dict(qa=qa, qb=qb, qh=qh)
+def solid_prop(qa=1.1, qb=0.05, qh=0.1, jcvt=0):
+    return dict(qa=qa, qb=qb, qh=qh, jcvt=jcvt)
 
 
 def shell_prop(thk, npt=5, ithk=1, hm=0.01, hf=0.01, hr=0.01, shf=5.0 / 6.0, pressure=0.0, ishfram=0):

@@ -9,7 +9,7 @@ nodal masses and inertias:
 starter keywords
   /BEGIN (input version >= 2017: 20-character real fields), /NODE,
   /SHELL/<part>, /BRICK/<part>, /PART, /PROP/SHELL (TYPE1), /PROP/SOLID
-  (TYPE14, Isolid 1, Iframe 1, Ismstr 4), /MAT/PLAS_JOHNS (LAW2, Iflag 0),
+  (TYPE14, Isolid 1, Iframe 1 or 2, Ismstr 4), /MAT/PLAS_JOHNS (LAW2, Iflag 0),
   /MAT/ELAST (LAW1), /DEF_SHELL, /DEF_SOLID, /SHFRA/V4, /SKEW/FIX, /BCS,
   /GRNOD/NODE, /INIVEL/TRA (no skew), /ADMAS/0, /FUNCT, /CLOAD (time
   abscissa, no sensor), /PLOAD (no sensor), /SURF/SEG, /SURF/PART (shell parts)
@@ -363,12 +363,13 @@ def to_deck(sd: StarterDeck, name=None):
         isolid = prop["isolid"] or ds["isolid"] or 1
         ismstr = prop["ismstr"] or ds["ismstr"] or 4
         iframe = prop["iframe"] or ds["iframe"] or 1
-        if isolid != 1 or ismstr != 4 or iframe != 1:
+        if isolid != 1 or ismstr != 4 or iframe not in (1, 2):
             raise RadError(f"/PROP/SOLID/{prop_id}: Isolid {isolid} / Ismstr {ismstr} / Iframe {iframe}; the "
-                           "element cycle implements Isolid 1 with Ismstr 4 and Iframe 1")
+                           "element cycle implements Isolid 1 with Ismstr 4 and Iframe 1 or 2")
         rows = sorted(sd.bricks[pid])
         conn = np.array([[index[n] for n in r[1:]] for r in rows], np.int64)
-        sp = decks.solid_prop(qa=prop["qa"] or 1.1, qb=prop["qb"] or 0.05, qh=prop["qh"] or 0.1)
+        sp = decks.solid_prop(qa=prop["qa"] or 1.1, qb=prop["qb"] or 0.05, qh=prop["qh"] or 0.1,
+                              jcvt=iframe - 1)              # IGEO(16) = Iframe - 1 (hm_read_prop14.F:380)
         decks.add_hex(part, conn, _material(mat), sp)
         hex_ids.append(np.array([r[0] for r in rows], np.int64))
     for pid in sorted(sd.shells):
@@ -566,7 +567,7 @@ def write_starter(deck, path, part=0, title=None):
         np.add.at(mass, conn.ravel(), np.repeat(m["rho0"] * vol0 / 8.0, 8))
         L += _material_cards(pid, m)
         pr = g["prop"]
-        L += [f"/PROP/SOLID/{pid}", f"solid {pid}", _i10(1, 4, 0, 0, 0, 0, 0, 1) + _f20(0.0),
+        L += [f"/PROP/SOLID/{pid}", f"solid {pid}", _i10(1, 4, 0, 0, 0, 0, 0, 1 + pr.get("jcvt", 0)) + _f20(0.0),
               _f20(pr["qa"], pr["qb"], pr["qh"], 0.0, 0.0), _f20(0.0, 0.0, 0.0, 0.0, 0.0),
               f"/PART/{pid}", f"part {pid}", _i10(pid, pid, 0), f"/BRICK/{pid}"]
         for e in range(conn.shape[0]):

@@ -199,6 +199,54 @@ int hex_element(const Model<R>& m, HexGroup<R>& g, PartData<R>& P, int i, double
   }
   const R OFFG = g.off[i];
   const R OFF = std::fabs(OFFG);   // ISMSTR<=4, |OFFG|<=1 branch
+  // SRCOOR3 (srcoor3.F, JCVT /= 0, ISORTH = 0, |OFFG| <= 1): the convected frame
+  // R = [e1 e2 e3] of SREPISO3 (srepiso3.F: differences in DOUBLE PRECISION, r, s, t
+  // in my_real) and SORTHO3 (sortho3.F: normalise, three symmetric corrections,
+  // then e3 = e1 x v, e2 = e3 x e1); coordinates XD (DOUBLE PRECISION) and
+  // velocities (my_real, SRROTA3) expressed in it
+  const bool corot = g.prop.jcvt != 0;
+  R R11 = 1, R12 = 0, R13 = 0, R21 = 0, R22 = 1, R23 = 0, R31 = 0, R32 = 0, R33 = 1;
+  if (corot) {
+    const R X17 = R(XD[6] - XD[0]), X28 = R(XD[7] - XD[1]), X35 = R(XD[4] - XD[2]), X46 = R(XD[5] - XD[3]);
+    const R Y17 = R(YD[6] - YD[0]), Y28 = R(YD[7] - YD[1]), Y35 = R(YD[4] - YD[2]), Y46 = R(YD[5] - YD[3]);
+    const R Z17 = R(ZD[6] - ZD[0]), Z28 = R(ZD[7] - ZD[1]), Z35 = R(ZD[4] - ZD[2]), Z46 = R(ZD[5] - ZD[3]);
+    const R A17 = X17 + X46, A28 = X28 + X35, B17 = Y17 + Y46, B28 = Y28 + Y35, C17 = Z17 + Z46, C28 = Z28 + Z35;
+    const R rx = X17 + X28 - X35 - X46, ry = Y17 + Y28 - Y35 - Y46, rz = Z17 + Z28 - Z35 - Z46;
+    const R sx = A17 + A28, sy = B17 + B28, sz = C17 + C28;
+    const R tx = A17 - A28, ty = B17 - B28, tz = C17 - C28;
+    auto unit = [](R x, R y, R z, R& ux, R& uy, R& uz) {
+      R aa = std::sqrt(x * x + y * y + z * z);
+      if (aa != R(0)) aa = R(1) / aa;
+      ux = x * aa; uy = y * aa; uz = z * aa;
+    };
+    R Ux, Uy, Uz, Vx, Vy, Vz, Wx, Wy, Wz;
+    unit(rx, ry, rz, Ux, Uy, Uz);
+    unit(sx, sy, sz, Vx, Vy, Vz);
+    unit(tx, ty, tz, Wx, Wy, Wz);
+    for (int it = 0; it < 3; ++it) {       // NITER = 3
+      const R e1x = Vy * Wz - Vz * Wy + Ux, e1y = Vz * Wx - Vx * Wz + Uy, e1z = Vx * Wy - Vy * Wx + Uz;
+      const R e2x = Wy * Uz - Wz * Uy + Vx, e2y = Wz * Ux - Wx * Uz + Vy, e2z = Wx * Uy - Wy * Ux + Vz;
+      const R e3x = Uy * Vz - Uz * Vy + Wx, e3y = Uz * Vx - Ux * Vz + Wy, e3z = Ux * Vy - Uy * Vx + Wz;
+      unit(e1x, e1y, e1z, Ux, Uy, Uz);
+      unit(e2x, e2y, e2z, Vx, Vy, Vz);
+      unit(e3x, e3y, e3z, Wx, Wy, Wz);
+    }
+    const R e1x = Ux, e1y = Uy, e1z = Uz;
+    R e3x = e1y * Vz - e1z * Vy, e3y = e1z * Vx - e1x * Vz, e3z = e1x * Vy - e1y * Vx;
+    unit(e3x, e3y, e3z, e3x, e3y, e3z);
+    const R e2x = e3y * e1z - e3z * e1y, e2y = e3z * e1x - e3x * e1z, e2z = e3x * e1y - e3y * e1x;
+    R11 = e1x; R21 = e1y; R31 = e1z; R12 = e2x; R22 = e2y; R32 = e2z; R13 = e3x; R23 = e3y; R33 = e3z;
+    for (int k = 0; k < 8; ++k) {
+      const double xl = double(R11) * XD[k] + double(R21) * YD[k] + double(R31) * ZD[k];
+      const double yl = double(R12) * XD[k] + double(R22) * YD[k] + double(R32) * ZD[k];
+      const double zl = double(R13) * XD[k] + double(R23) * YD[k] + double(R33) * ZD[k];
+      XD[k] = xl; YD[k] = yl; ZD[k] = zl;
+      const R vx = R11 * VX[k] + R21 * VY[k] + R31 * VZ[k];
+      const R vy = R12 * VX[k] + R22 * VY[k] + R32 * VZ[k];
+      const R vz = R13 * VX[k] + R23 * VY[k] + R33 * VZ[k];
+      VX[k] = vx; VY[k] = vy; VZ[k] = vz;
+    }
+  }
 
   // SDERI3 (sderi3.F:103-149 Jacobian; 264-298 inverse; 302-333 hourglass projections)
   // Geometry: FP64 form = reference dp; split form evaluates it in FP64 and casts.
@@ -314,7 +362,9 @@ int hex_element(const Model<R>& m, HexGroup<R>& g, PartData<R>& P, int i, double
   R S1 = g.sig[0 * g.nel + i], S2 = g.sig[1 * g.nel + i], S3 = g.sig[2 * g.nel + i];
   R S4 = g.sig[3 * g.nel + i], S5 = g.sig[4 * g.nel + i], S6 = g.sig[5 * g.nel + i];
   R SIG[6];
-  {
+  if (corot) {          // SRMALLA3 (srmall3.F): the convected-frame stress, not rotated
+    SIG[0] = S1; SIG[1] = S2; SIG[2] = S3; SIG[3] = S4; SIG[4] = S5; SIG[5] = S6;
+  } else {
     R Q1 = R(2) * S4 * WZZ, Q2 = R(2) * S6 * WYY, Q3 = R(2) * S5 * WXX;
     SIG[0] = S1 - Q1 + Q2;
     SIG[1] = S2 + Q1 - Q3;
@@ -502,6 +552,15 @@ int hex_element(const Model<R>& m, HexGroup<R>& g, PartData<R>& P, int i, double
       F[1][n1] -= FINT; F[1][n2] += FINT;
       FINT = sS3 * PZ[a] + sS6 * PX[a] + sS5 * PY[a];
       F[2][n1] -= FINT; F[2][n2] += FINT;
+    }
+  }
+  // SRROTA3 with R transposed (sforc3.F:1603-1614): forces back to the global frame
+  if (corot) {
+    for (int k = 0; k < 8; ++k) {
+      const R fx = R11 * F[0][k] + R12 * F[1][k] + R13 * F[2][k];
+      const R fy = R21 * F[0][k] + R22 * F[1][k] + R23 * F[2][k];
+      const R fz = R31 * F[0][k] + R32 * F[1][k] + R33 * F[2][k];
+      F[0][k] = fx; F[1][k] = fy; F[2][k] = fz;
     }
   }
   // SCUMU3P (scumu3p.F:195-260)

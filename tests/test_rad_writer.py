@@ -84,3 +84,11 @@ def test_per_element_yield_is_refused(tmp_path):
     d = decks.c5_adjoint_plate(n=4, ncycles=5)
     with pytest.raises(ValueError):
         rad.write_starter(d, str(tmp_path / "X_0000.rad"))
+
+
+def test_convected_frame_hexa_roundtrip(tmp_path):
+    d = decks.c1_hex_block(nx=3, ny=3, nz=6, ncycles=40)
+    d["parts"][0]["hex"][0]["prop"]["jcvt"] = 1         # /PROP/SOLID Iframe 2
+    got = roundtrip(d, tmp_path)
+    assert got["parts"][0]["hex"][0]["prop"]["jcvt"] == 1
+    same_run(d, got)
