@@ -343,7 +343,8 @@ typedef struct {
    exact when dt does not depend on the parameters, e.g. when DTMX is below
    every element time step.  The reverse recomputes each segment of
    r->checkpoint cycles from a stored state.  FP64 handles with shell groups
-   only (OR_E_UNSUPPORTED otherwise).  Any output pointer may be NULL.
+   only, global or skewed BCS, /CLOAD loads, no /PLOAD and no rigid links
+   (OR_E_UNSUPPORTED otherwise).  Any output pointer may be NULL.
    No counterpart in the reference, which has no adjoint. */
 int  or_ecycle_adjoint(or_ecycle* h, int ncycles, const or_adjoint_response* r, or_ecycle_time* t,
                        double* J, double* dJ_dA, double* dJ_dthk, double* dJ_dms, double* dJ_din);

@@ -47,7 +47,30 @@ struct AdjNodeArgs {
   double* dms;
   double* din;
   int nnodpad, node_tile;
+  const int* skew_of;     // skewed /BCS (code bit 7): frame of the node; may be null
+  const double* skews;
 };
+
+// reverse of the BCS1V projection: each held direction s is projected out by
+// the symmetric I - s s^T, so the transpose applies the same projections in the
+// opposite order (for the orthonormal /SKEW frames the two orders agree)
+__device__ inline void adj_bcs_skew(int lcod, const double* sk, double b[3]) {
+  if (!lcod) return;
+  if (lcod == 7) { b[0] = b[1] = b[2] = 0.0; return; }
+  auto proj = [&](int r) {
+    const double s0 = sk[3 * r], s1 = sk[3 * r + 1], s2 = sk[3 * r + 2];
+    const double aa = s0 * b[0] + s1 * b[1] + s2 * b[2];
+    b[0] -= s0 * aa; b[1] -= s1 * aa; b[2] -= s2 * aa;
+  };
+  switch (lcod) {
+    case 1: proj(2); break;
+    case 2: proj(1); break;
+    case 3: proj(1); proj(2); break;
+    case 4: proj(0); break;
+    case 5: proj(0); proj(2); break;
+    case 6: proj(1); proj(0); break;
+  }
+}
 
 __global__ void __launch_bounds__(128) adj_node_pre_kernel(AdjNodeArgs a) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
@@ -63,8 +86,15 @@ __global__ void __launch_bounds__(128) adj_node_pre_kernel(AdjNodeArgs a) {
   const double ms = a.Xn[n].w;
   // V(n+1) = V(n) + DT12 * A on free components, 0 on fixed ones; X, D += DT2 * V(n+1)
   double bar[3] = {lv.x + DT2 * (lx.x + ld.x), lv.y + DT2 * (lx.y + ld.y), lv.z + DT2 * (lx.z + ld.z)};
-  const bool fixed[3] = {(code & 4) != 0, (code & 2) != 0, (code & 1) != 0};
-  const double dv[3] = {v1.x - v0.x, v1.y - v0.y, v1.z - v0.z};
+  const double* sk = (code & 128) ? a.skews + 9 * a.skew_of[n] : nullptr;
+  const bool fixed[3] = {!sk && (code & 4) != 0, !sk && (code & 2) != 0, !sk && (code & 1) != 0};
+  double dv[3] = {v1.x - v0.x, v1.y - v0.y, v1.z - v0.z};
+  if (sk) {            // V(n+1) = P V(n) + DT12 P A: the adjoints and A = (V(n+1) - P V(n)) / DT12
+    double pv0[3] = {v0.x, v0.y, v0.z};
+    bcs1v_skew(code & 7, sk, pv0[0], pv0[1], pv0[2]);
+    dv[0] = v1.x - pv0[0]; dv[1] = v1.y - pv0[1]; dv[2] = v1.z - pv0[2];
+    adj_bcs_skew(code & 7, sk, bar);
+  }
   double lF[3] = {0, 0, 0}, dm = 0.0;
   for (int c = 0; c < 3; ++c) {
     if (fixed[c]) { bar[c] = 0.0; continue; }
@@ -81,8 +111,14 @@ __global__ void __launch_bounds__(128) adj_node_pre_kernel(AdjNodeArgs a) {
     const double4 lr = a.lamVR[n], r0 = a.VRn[n], r1 = a.VRn1[n];
     const double in = r0.w;
     double rb[3] = {lr.x, lr.y, lr.z};
-    const bool rfix[3] = {(code & 32) != 0, (code & 16) != 0, (code & 8) != 0};
-    const double dr[3] = {r1.x - r0.x, r1.y - r0.y, r1.z - r0.z};
+    const bool rfix[3] = {!sk && (code & 32) != 0, !sk && (code & 16) != 0, !sk && (code & 8) != 0};
+    double dr[3] = {r1.x - r0.x, r1.y - r0.y, r1.z - r0.z};
+    if (sk) {
+      double pr0[3] = {r0.x, r0.y, r0.z};
+      bcs1v_skew((code >> 3) & 7, sk, pr0[0], pr0[1], pr0[2]);
+      dr[0] = r1.x - pr0[0]; dr[1] = r1.y - pr0[1]; dr[2] = r1.z - pr0[2];
+      adj_bcs_skew((code >> 3) & 7, sk, rb);
+    }
     double lM[3] = {0, 0, 0}, di = 0.0;
     for (int c = 0; c < 3; ++c) {
       if (rfix[c]) { rb[c] = 0.0; continue; }

@@ -1390,6 +1390,7 @@ int adj_prepare(or_ecycle* h, Impl<double>& m, int ncycles, int K) {
       AdjGroup a{};
       orb_adj::ShellParams& P = a.P;
       P.law = g.mat.law; P.npt = g.prop.npt; P.ithk = g.prop.ithk; P.degen = 0;
+      P.ishfram = g.prop.ishfram; P.pad = 0;
       P.rho = g.mat.rho0; P.young = g.mat.young; P.nu = g.mat.nu; P.shear = g.mat.shear; P.a11 = g.mat.a11;
       P.a12 = g.mat.a12; P.jc_b = g.mat.jc_b; P.jc_n = g.mat.jc_n; P.sigmax = g.mat.sigmax;
       P.hm = g.prop.hm; P.hf = g.prop.hf; P.hr = g.prop.hr; P.shf = g.prop.shf; P.pressure = g.prop.pressure;
@@ -1591,6 +1592,7 @@ int adjoint_impl(or_ecycle* h, int N, const or_adjoint_response* r, or_ecycle_ti
       na.lamX = w.lamX.p; na.lamD = w.lamD.p; na.lamV = w.lamV.p; na.lamVR = w.lamVR.p;
       na.lamF = w.lamF.p; na.lamM = w.lamM.p; na.dms = w.dms.p; na.din = w.din.p;
       na.nnodpad = nn; na.node_tile = NODE_TILE;
+      na.skew_of = m.skew_of.p; na.skews = m.skw.p;
       adj_node_pre_kernel<<<nb_node, 128, 0, h->stream>>>(na);
       CK(cudaGetLastError());
       AdjShellArgs sa;
@@ -1976,12 +1978,9 @@ int or_ecycle_adjoint(or_ecycle* h, int ncycles, const or_adjoint_response* r, o
   if (h->cfg.precision != OR_PREC_FP64) return fail(h, OR_E_UNSUPPORTED, "adjoint: FP64 handles only");
   if (!h->hex.empty() || h->shell.empty()) return fail(h, OR_E_UNSUPPORTED, "adjoint: shell groups only");
   if (!h->links.empty()) return fail(h, OR_E_UNSUPPORTED, "adjoint: rigid links");
-  if (!h->loads.empty()) return fail(h, OR_E_UNSUPPORTED, "adjoint: /CLOAD or /PLOAD loads");
-  for (auto& P : h->parts)
-    for (int s : P.iskew)
-      if (s >= 0) return fail(h, OR_E_UNSUPPORTED, "adjoint: skewed boundary conditions");
-  for (auto& g : h->shell)
-    if (g.prop.ishfram != 0) return fail(h, OR_E_UNSUPPORTED, "adjoint: ISHFRAM 0 only");
+  for (auto& L : h->loads)     // /CLOAD forces depend on time only: no reverse terms
+    if (L.type != 0) return fail(h, OR_E_UNSUPPORTED, "adjoint: /PLOAD follower loads");
+
   if (r->node >= 0) {
     if (r->part < 0 || r->part >= (int)h->parts.size() || r->node >= h->parts[r->part].numnod || r->comp < 0 ||
         r->comp > 2)

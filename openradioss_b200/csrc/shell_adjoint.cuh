@@ -34,6 +34,7 @@ constexpr double A_EM15 = 1e-15, A_EM20 = 1e-20, A_EM30 = 1e-30;
 
 struct ShellParams {
   int law, npt, ithk, degen;
+  int ishfram, pad;       // local frame: 0, or 2 (/SHFRA/V4, cnvec3.F:82-106)
   double rho, young, nu, shear, a11, a12, jc_b, jc_n, sigmax;
   double hm, hf, hr, shf, pressure;
 };
@@ -57,6 +58,7 @@ template <int NP>
 struct ShellTape {
   double d21[3], d31[3], d41[3], d32[3], d34[3];
   double e1[3], e2[3], e3[3], n3, e3n[3], q1, q2, s, c23[3], e1p[3], n1, e1n[3], e2n[3];
+  double e2p[3], n2;      // ISHFRAM 2: e2 before its normalisation
   double X2, Y2, X3, Y3, X4, Y4, PX1, PY1, PX2, PY2, AREA, VHX, VHY;
   int area_clamped;
   double THK0, THK02, GS;
@@ -114,10 +116,29 @@ ORB_HD void shell_forward(const ShellParams& P, const float* zw, const ShellIn<N
     t.d32[c] = in.x[2][c] - in.x[1][c];
     t.d34[c] = in.x[2][c] - in.x[3][c];
   }
-  // CNVEC3, ISHFRAM = 0 (cnvec3.F:66-140)
+  // CNVEC3, ISHFRAM = 0 (cnvec3.F:66-81) or 2 (cnvec3.F:82-106)
   for (int c = 0; c < 3; ++c) { t.e1[c] = t.d21[c] + t.d34[c]; t.e2[c] = t.d32[c] + t.d41[c]; }
   v_cross(t.e1, t.e2, t.e3);
-  {
+  if (P.ishfram == 2) {
+    // e1 = |e2|^2 e1 + e2 x e3 (e3 not normalised), then e1, e3 normalised,
+    // e2 = e3 x e1 normalised
+    t.q2 = t.e2[0] * t.e2[0] + t.e2[1] * t.e2[1] + t.e2[2] * t.e2[2];
+    v_cross(t.e2, t.e3, t.c23);
+    for (int c = 0; c < 3; ++c) t.e1p[c] = t.e1[c] * t.q2 + t.c23[c];
+    double su = sqrt(t.e1p[0] * t.e1p[0] + t.e1p[1] * t.e1p[1] + t.e1p[2] * t.e1p[2]);
+    t.n1 = su;
+    su = 1.0 / (su > A_EM20 ? su : A_EM20);
+    for (int c = 0; c < 3; ++c) t.e1n[c] = t.e1p[c] * su;
+    su = sqrt(t.e3[0] * t.e3[0] + t.e3[1] * t.e3[1] + t.e3[2] * t.e3[2]);
+    t.n3 = su;
+    su = 1.0 / (su > A_EM20 ? su : A_EM20);
+    for (int c = 0; c < 3; ++c) t.e3n[c] = t.e3[c] * su;
+    v_cross(t.e3n, t.e1n, t.e2p);
+    su = sqrt(t.e2p[0] * t.e2p[0] + t.e2p[1] * t.e2p[1] + t.e2p[2] * t.e2p[2]);
+    t.n2 = su;
+    su = 1.0 / (su > A_EM20 ? su : A_EM20);
+    for (int c = 0; c < 3; ++c) t.e2n[c] = t.e2p[c] * su;
+  } else {
     double su = sqrt(t.e3[0] * t.e3[0] + t.e3[1] * t.e3[1] + t.e3[2] * t.e3[2]);
     t.n3 = su;
     su = 1.0 / (su > A_EM20 ? su : A_EM20);
@@ -670,7 +691,28 @@ ORB_HD void shell_reverse(const ShellParams& P, const float* zw, const ShellIn<N
     bd41[c] = bX4 * t.e1n[c] + bY4 * t.e2n[c];
   }
   // ---- CNVEC3 ----
-  {
+  if (P.ishfram == 2) {
+    // e2n = e2p / |e2p| ; e2p = e3n x e1n
+    double be2p[3] = {0, 0, 0};
+    v_normalize_rev(t.e2n, t.n2, be2n, be2p);
+    v_cross_rev(t.e3n, t.e1n, be2p, be3n, be1n);
+    // e3n = e3 / |e3| ; e1n = e1p / |e1p|
+    double be3[3] = {0, 0, 0}, be1p[3] = {0, 0, 0};
+    v_normalize_rev(t.e3n, t.n3, be3n, be3);
+    v_normalize_rev(t.e1n, t.n1, be1n, be1p);
+    // e1p = q2 e1 + e2 x e3 ; q2 = |e2|^2
+    double be1[3], be2[3] = {0, 0, 0};
+    for (int c = 0; c < 3; ++c) be1[c] = be1p[c] * t.q2;
+    const double bq2 = v_dot(be1p, t.e1);
+    v_cross_rev(t.e2, t.e3, be1p, be2, be3);
+    for (int c = 0; c < 3; ++c) be2[c] += 2.0 * bq2 * t.e2[c];
+    // e3 = e1 x e2
+    v_cross_rev(t.e1, t.e2, be3, be1, be2);
+    for (int c = 0; c < 3; ++c) {
+      bd21[c] += be1[c]; bd34[c] += be1[c];
+      bd32[c] += be2[c]; bd41[c] += be2[c];
+    }
+  } else {
     // e2n = e3n x e1n
     v_cross_rev(t.e3n, t.e1n, be2n, be3n, be1n);
     // e1n = e1p / |e1p|

@@ -156,6 +156,57 @@ def test_adjoint_full_size_c5_displacement():
     directional_check(200, decks.LAW_JOHNSON_COOK, 0.36, 2e6, 500, 1.0, 0.0, 1e-8, FD_REL, ("thk",))
 
 
+def with_frame_skew_cloads(d):
+    """The plate with /SHFRA/V4 element frames (ISHFRAM 2), its x = xmin edge
+    held in a skew frame tilted 25 degrees about y (x' and z' held, and the
+    rotation about y'), a ramped point load at the centre along z, and one along
+    the skew frame's y' at the middle of the skewed edge."""
+    P = d["parts"][0]
+    P["shell"][0]["prop"]["ishfram"] = 2
+    c, s = np.cos(np.radians(25.0)), np.sin(np.radians(25.0))
+    d["skews"] = [np.array([[c, 0.0, -s], [0.0, 1.0, 0.0], [s, 0.0, c]])]
+    d["functions"] = [{"x": np.array([0.0, 2e-5, 1.0]), "y": np.array([0.0, 1.0, 1.0])}]
+    x = P["x"]
+    left = np.nonzero(x[:, 0] <= x[:, 0].min() + 1e-9)[0]
+    P["icodt"][left] = 5
+    P["icodr"][left] = 2
+    P["iskew"] = -np.ones(x.shape[0], np.int32)
+    P["iskew"][left] = 0
+    mid = int(left[np.argmin(np.abs(x[left, 1] - 0.5 * (x[:, 1].min() + x[:, 1].max())))])
+    P["cloads"] = [dict(nodes=[adjoint.centre_node(d)], dir=3, func=0, fscale=5.0),
+                   dict(nodes=[mid], dir=2, skew=0, func=0, fscale=2.0)]
+    return d
+
+
+@pytest.mark.parametrize("resp", ["disp", "plastic"])
+def test_adjoint_shfra_v4_skew_bcs_and_point_loads(resp):
+    """ISHFRAM 2 element frames, a skewed /BCS edge (translations and a
+    rotation) and time-function /CLOAD point loads, linear hardening: the
+    adjoint against central differences along A, thickness and both."""
+    need_gpu()
+    n, p, N, STEP = 32, 2e6, 200, 1e-7
+    wd, wpl = (1.0, 0.0) if resp == "disp" else (0.0, 1.0)
+    A0, T0 = base_params(n)
+    mk = lambda A, T: with_frame_skew_cloads(plate(n, A, T, p, N, jc_n=1.0))
+    d0 = mk(A0, T0)
+    node = adjoint.centre_node(d0)
+    res = adjoint_run(d0, N, node, wd, wpl)
+    J0, _ = forward_J(d0, N, node, wd, wpl)
+    assert res["J"] == J0
+    assert res["J"] > 0.0 if resp == "plastic" else res["J"] != 0.0
+    gA, gT = res["dA"][0], adjoint.thickness_gradient(d0, res)[0]
+    rng = np.random.default_rng(5)
+    for name in ("A", "thk", "both"):
+        uA = rng.choice([-1.0, 1.0], A0.size) if name in ("A", "both") else 0.0 * A0
+        uT = rng.choice([-1.0, 1.0], T0.size) if name in ("thk", "both") else 0.0 * T0
+        Jp, tp = forward_J(mk(A0 * (1 + STEP * uA), T0 * (1 + STEP * uT)), N, node, wd, wpl)
+        Jm, tm = forward_J(mk(A0 * (1 - STEP * uA), T0 * (1 - STEP * uT)), N, node, wd, wpl)
+        assert tp["tt"] == tm["tt"] == res["time"]["tt"]
+        fd = (Jp - Jm) / (2 * STEP)
+        ad = float(np.dot(gA, A0 * uA) + np.dot(gT, T0 * uT))
+        assert abs(fd - ad) <= FD_REL * abs(ad), (name, fd, ad)
+
+
 def test_adjoint_nodal_mass_gradient():
     """dJ/dMS along a random direction of the nodal masses (inertias fixed)."""
     need_gpu()

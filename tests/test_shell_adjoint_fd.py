@@ -9,7 +9,8 @@ for random output weights w and a random input direction u,
 per input group (coordinates, velocities, rotational velocities, stresses,
 plastic strains, thickness, hourglass history, Johnson-Cook A), on the elastic
 and plastic branches of the radial return, LAW1 and LAW2, ITHK 0 and 1, with
-and without pressure, and for a degenerate (triangular) quad.
+and without pressure, for a degenerate (triangular) quad, and in the /SHFRA/V4
+(ISHFRAM 2) frame.
 """
 import ctypes as C
 import os
@@ -29,7 +30,7 @@ OSL = dict(f=slice(0, 12), m=slice(12, 24), sig=slice(24, 74), pla=slice(74, 84)
 
 
 class ShellParams(C.Structure):
-    _fields_ = [(n, C.c_int) for n in ("law", "npt", "ithk", "degen")] + \
+    _fields_ = [(n, C.c_int) for n in ("law", "npt", "ithk", "degen", "ishfram", "pad")] + \
                [(n, C.c_double) for n in ("rho", "young", "nu", "shear", "a11", "a12", "jc_b", "jc_n", "sigmax",
                                           "hm", "hf", "hr", "shf", "pressure")]
 
@@ -48,10 +49,11 @@ def lib(tmp_path_factory):
     return L
 
 
-def params(law=2, npt=5, ithk=1, degen=0, pressure=2e6):
+def params(law=2, npt=5, ithk=1, degen=0, pressure=2e6, ishfram=0):
     E, nu, rho = 70e9, 0.33, 2700.0
     G = E / (2 * (1 + nu))
-    return ShellParams(law=law, npt=npt, ithk=ithk, degen=degen, rho=rho, young=E, nu=nu, shear=G,
+    return ShellParams(law=law, npt=npt, ithk=ithk, degen=degen, ishfram=ishfram, pad=0, rho=rho, young=E, nu=nu,
+                       shear=G,
                        a11=E / (1 - nu * nu), a12=E * nu / (1 - nu * nu), jc_b=275e6, jc_n=0.36, sigmax=1e30,
                        hm=0.01, hf=0.01, hr=0.01, shf=5.0 / 6.0, pressure=pressure)
 
@@ -170,3 +172,16 @@ def test_degenerate_triangle(lib):
     P = params(law=2, npt=5, ithk=1, degen=1)
     a = random_input(rng, 4e8, "pos", degen=True)
     check(lib, P, a, rng)
+
+
+@pytest.mark.parametrize("seed", [20, 21])
+def test_shfra_v4_frame(lib, seed):
+    """ISHFRAM 2 (/SHFRA/V4) frame, plastic branch, with a warped quad."""
+    rng = np.random.default_rng(seed)
+    P = params(law=2, npt=5, ithk=1, ishfram=2)
+    a = random_input(rng, 4e8, "pos")
+    assert fwd(lib, P, a)[OSL["wpla"]][0] > 0.0
+    check(lib, P, a, rng)
+    # the frame matters: the same element in the default frame gives other forces
+    P0 = params(law=2, npt=5, ithk=1, ishfram=0)
+    assert not np.allclose(fwd(lib, P, a)[OSL["f"]], fwd(lib, P0, a)[OSL["f"]], rtol=1e-9, atol=0)
