@@ -21,6 +21,7 @@
 #include <numeric>
 #include <string>
 #include <thread>
+#include <utility>
 #include <vector>
 #include <array>
 
@@ -115,6 +116,7 @@ struct or_ecycle {
   int last_code = 0, last_index = -1;
   int spmd_k = -1;                    // cycle index of a running domain-decomposed step, -1 outside one
   int next_parity = 0;                // time-buffer parity of the state after the last step
+  bool pdl = true;                    // programmatic dependent launch of the cycle kernels
 };
 
 namespace {
@@ -418,30 +420,49 @@ size_t shell_smem(int nl, int tile, int inc_stride) {
   return (size_t)nl * (3 * sizeof(double) + 6 * sizeof(R)) + 24 * (size_t)tile * sizeof(R) + 2 * (size_t)inc_stride;
 }
 
+// A cycle kernel launch; with pdl, programmatic stream serialization lets its
+// blocks start before the previous kernel in the stream has finished (the
+// kernels' pdl_wait / pdl_trigger protocol keeps every read ordered).  Only the
+// element and node passes of the regular cycle use it: their alternation is what
+// the protocol relies on.
+template <class... P, class... A>
+cudaError_t launch_k(void (*k)(P...), unsigned grid, unsigned block, size_t smem, cudaStream_t s, bool pdl,
+                     A&&... args) {
+  cudaLaunchConfig_t c{};
+  c.gridDim = dim3(grid);
+  c.blockDim = dim3(block);
+  c.dynamicSmemBytes = smem;
+  c.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  c.attrs = at;
+  c.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&c, k, std::forward<A>(args)...);
+}
+
 template <class R, int T>
-int launch_hex(or_ecycle* h, Impl<R>& m, int parity) {
+int launch_hex(or_ecycle* h, Impl<R>& m, int parity, bool pdl = false) {
   if (m.hps.info.empty()) return OR_OK;
   size_t sm = hex_smem<R>(m.hps.nlmax, T, m.hinc_stride);
-  if (m.any_corot)
-    hex_patch_kernel<R, T, 1><<<(unsigned)m.hps.info.size(), T, sm, h->stream>>>(m.hargs(), parity);
-  else
-    hex_patch_kernel<R, T, 0><<<(unsigned)m.hps.info.size(), T, sm, h->stream>>>(m.hargs(), parity);
-  CK(cudaGetLastError());
+  const unsigned g = (unsigned)m.hps.info.size();
+  if (m.any_corot) CK(launch_k(hex_patch_kernel<R, T, 1>, g, T, sm, h->stream, pdl, m.hargs(), parity));
+  else CK(launch_k(hex_patch_kernel<R, T, 0>, g, T, sm, h->stream, pdl, m.hargs(), parity));
   h->launches++;
   return OR_OK;
 }
 template <class R, int T, int NPT>
-int launch_shell(or_ecycle* h, Impl<R>& m, int parity) {
+int launch_shell(or_ecycle* h, Impl<R>& m, int parity, bool pdl) {
   if (m.sps.info.empty()) return OR_OK;
   size_t sm = shell_smem<R>(m.sps.nlmax, T, m.sinc_stride);
-  shell_patch_kernel<R, T, NPT><<<(unsigned)m.sps.info.size(), T, sm, h->stream>>>(m.sargs(), parity, m.zw.p);
-  CK(cudaGetLastError());
+  CK(launch_k(shell_patch_kernel<R, T, NPT>, (unsigned)m.sps.info.size(), T, sm, h->stream, pdl, m.sargs(), parity,
+              (const float*)m.zw.p));
   h->launches++;
   return OR_OK;
 }
 template <class R, int T>
-int launch_shell_npt(or_ecycle* h, Impl<R>& m, int parity) {
-  return m.uniform_npt == 5 ? launch_shell<R, T, 5>(h, m, parity) : launch_shell<R, T, 0>(h, m, parity);
+int launch_shell_npt(or_ecycle* h, Impl<R>& m, int parity, bool pdl = false) {
+  return m.uniform_npt == 5 ? launch_shell<R, T, 5>(h, m, parity, pdl) : launch_shell<R, T, 0>(h, m, parity, pdl);
 }
 template <class R>
 int launch_link(or_ecycle* h, Impl<R>& m) {
@@ -464,9 +485,8 @@ int launch_loads(or_ecycle* h, Impl<R>& m, int parity) {
   return OR_OK;
 }
 template <class R>
-int launch_node(or_ecycle* h, Impl<R>& m, int parity) {
-  node_kernel<R, NODE_TILE><<<(unsigned)m.ntiles, NODE_TILE, 0, h->stream>>>(m.nargs(h), parity);
-  CK(cudaGetLastError());
+int launch_node(or_ecycle* h, Impl<R>& m, int parity, bool pdl = false) {
+  CK(launch_k(node_kernel<R, NODE_TILE>, (unsigned)m.ntiles, NODE_TILE, 0, h->stream, pdl, m.nargs(h), parity));
   h->launches++;
   return OR_OK;
 }
@@ -500,18 +520,21 @@ template <class R>
 int launch_cycle(or_ecycle* h, Impl<R>& m, int parity, cudaEvent_t* ev) {
   int rc;
   if (ev) CK(cudaEventRecord(ev[0], h->stream));
+  // per-phase events need the kernels serialised
+  const bool pdl = h->pdl && !ev;
   if ((rc = launch_loads<R>(h, m, parity))) return rc;     // FORCE (resol.F:2847), before the elements
-  rc = h->tile_hex == 64 ? launch_hex<R, 64>(h, m, parity)
-       : h->tile_hex == 128 ? launch_hex<R, 128>(h, m, parity) : launch_hex<R, 256>(h, m, parity);
+  rc = h->tile_hex == 64 ? launch_hex<R, 64>(h, m, parity, pdl)
+       : h->tile_hex == 128 ? launch_hex<R, 128>(h, m, parity, pdl) : launch_hex<R, 256>(h, m, parity, pdl);
   if (rc) return rc;
   if (ev) CK(cudaEventRecord(ev[1], h->stream));
-  rc = h->tile_shell == 64 ? launch_shell_npt<R, 64>(h, m, parity)
-       : h->tile_shell == 128 ? launch_shell_npt<R, 128>(h, m, parity) : launch_shell_npt<R, 256>(h, m, parity);
+  rc = h->tile_shell == 64 ? launch_shell_npt<R, 64>(h, m, parity, pdl)
+       : h->tile_shell == 128 ? launch_shell_npt<R, 128>(h, m, parity, pdl)
+                              : launch_shell_npt<R, 256>(h, m, parity, pdl);
   if (rc) return rc;
   if (ev) CK(cudaEventRecord(ev[2], h->stream));
   rc = launch_link<R>(h, m);
   if (rc) return rc;
-  rc = launch_node<R>(h, m, parity);
+  rc = launch_node<R>(h, m, parity, pdl);
   if (rc) return rc;
   if (ev) CK(cudaEventRecord(ev[3], h->stream));
   return OR_OK;
@@ -1685,6 +1708,7 @@ int or_ecycle_create(const or_ecycle_config* cfg, or_ecycle** out) {
   auto tile_ok = [](int b) { return b == 64 || b == 128 || b == 256; };
   if (tile_ok(h->cfg.block_hex)) h->tile_hex = h->cfg.block_hex;
   if (tile_ok(h->cfg.block_shell)) h->tile_shell = h->cfg.block_shell;
+  if (const char* s = std::getenv("OR_ECYCLE_PDL")) h->pdl = std::atoi(s) != 0;
   if (cudaSetDevice(cfg->device) != cudaSuccess || cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
     delete h;
     return OR_E_CUDA;

@@ -206,6 +206,19 @@ __host__ __device__ inline size_t halo_buffer_bytes(int nhalo) {
 // ---------------------------------------------------------------------------
 // helpers
 // ---------------------------------------------------------------------------
+// Programmatic dependent launch.  The cycle's kernels alternate element pass ->
+// node pass, each launched with programmatic stream serialization, so a kernel's
+// blocks can start while the previous kernel is still running.  Every kernel
+//  - issues first the loads that do not depend on the previous kernel (data written
+//    two kernels back or earlier, or static),
+//  - then pdl_wait(): returns once the previous grid has completed and its writes
+//    are visible (immediately when launched without the attribute),
+//  - then pdl_trigger(), so the next kernel may start its own prologue.
+// Because each kernel triggers only after its wait, the grid two kernels back has
+// completed whenever a kernel starts: its prologue may read that grid's output.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // BCS1V (bcs1.F): zero the components of (x, y, z) along the fixed directions of
 // code lcod (4 = x, 2 = y, 1 = z) of skew frame sk (rows x', y', z'), projecting
 // them out in the reference's order
@@ -406,17 +419,22 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
     st_pla = a.pla[e];
     st_eid = a.elem_id[e];
   }
+  {
+    const unsigned* src = reinterpret_cast<const unsigned*>(a.inc + (size_t)p * a.inc_stride);
+    unsigned* dst = reinterpret_cast<unsigned*>(sinc);
+    for (int i = tid; i < a.inc_stride / 2; i += TILE) dst[i] = src[i];
+  }
+  // X, V and the cycle's time come from the previous node pass (the node numbers
+  // are loaded after the wait: the 80-register budget of the split form has no
+  // room to hold them across it)
+  pdl_wait();
+  pdl_trigger();
   for (int j = tid; j < NLM; j += TILE) {
     const int g = a.patch_nodes[p * NLM + j];
     const double4 xx = a.X[g];
     const R4 vv = a.V[g];
     sx[j] = xx.x; sy[j] = xx.y; sz[j] = xx.z;
     svx[j] = vv.x; svy[j] = vv.y; svz[j] = vv.z;
-  }
-  {
-    const unsigned* src = reinterpret_cast<const unsigned*>(a.inc + (size_t)p * a.inc_stride);
-    unsigned* dst = reinterpret_cast<unsigned*>(sinc);
-    for (int i = tid; i < a.inc_stride / 2; i += TILE) dst[i] = src[i];
   }
   const HexGroupDesc gd = a.groups[pi.group];
   const bool active = tid < pi.nel;
@@ -426,7 +444,6 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
   const bool split = sizeof(R) == 4;
   __syncthreads();
 
-  R F[3][8];
   int lc[8];
   int color = -1;
   unsigned long long mykey = ~0ull, mybits = ~0ull;
@@ -702,38 +719,33 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
     a.rho[e] = RHON;
     a.qvis[e] = QNEW;
     // ---- SHVIS3 Flanagan-Belytschko viscous hourglass (shvis3.F:156-424, JHBE>=1) ----
+    // g-vectors of the three non-trivial modes (Gv[j][k] = sign - or + PXH), recomputed
+    // where used instead of held; the 4th mode is the pure (+-+--+-+) vector
+    const R CAQ = R(0.25) * OFF * R(gd.qh);
+    R FCL = CAQ * RHON * (AL * AL);   // VOL**TWO_THIRD
+    const R FCQ = FCL * CAQ * R(100);
+    FCL = FCL * SSP;
+    constexpr int sgn[3][8] = {{1, -1, 1, -1, 1, -1, 1, -1}, {1, 1, -1, -1, -1, -1, 1, 1}, {1, -1, -1, 1, -1, 1, 1, -1}};
+    constexpr int pq[8] = {0, 1, 2, 3, 2, 3, 0, 1};        // PXH row of corner k
+    auto gvec = [&](int j, int k) -> R {
+      return k < 4 ? R(sgn[j][k]) - PXH[pq[k]][j] : R(sgn[j][k]) + PXH[pq[k]][j];
+    };
+    R HX[4], HY[4], HZ[4];
     {
-      const R CAQ = R(0.25) * OFF * R(gd.qh);
-      R FCL = CAQ * RHON * (AL * AL);   // VOL**TWO_THIRD
-      const R FCQ = FCL * CAQ * R(100);
-      FCL = FCL * SSP;
-      // g-vectors of the three non-trivial modes; the 4th mode is the pure (+-+--+-+) vector
-      R Gv[3][8];
-      const int sgn[3][8] = {{1, -1, 1, -1, 1, -1, 1, -1}, {1, 1, -1, -1, -1, -1, 1, 1}, {1, -1, -1, 1, -1, 1, 1, -1}};
-#pragma unroll
-      for (int j = 0; j < 3; ++j) {
-        Gv[j][0] = R(sgn[j][0]) - PXH[0][j];
-        Gv[j][1] = R(sgn[j][1]) - PXH[1][j];
-        Gv[j][2] = R(sgn[j][2]) - PXH[2][j];
-        Gv[j][3] = R(sgn[j][3]) - PXH[3][j];
-        Gv[j][4] = R(sgn[j][4]) + PXH[2][j];
-        Gv[j][5] = R(sgn[j][5]) + PXH[3][j];
-        Gv[j][6] = R(sgn[j][6]) + PXH[0][j];
-        Gv[j][7] = R(sgn[j][7]) + PXH[1][j];
-      }
-      const int h4[8] = {1, -1, 1, -1, -1, 1, -1, 1};
       R HGX[4], HGY[4], HGZ[4];
 #pragma unroll
       for (int j = 0; j < 3; ++j) {
         R hx = R(0), hy = R(0), hz = R(0);
 #pragma unroll
-        for (int k = 0; k < 8; ++k) { hx += Gv[j][k] * VX[k]; hy += Gv[j][k] * VY[k]; hz += Gv[j][k] * VZ[k]; }
+        for (int k = 0; k < 8; ++k) {
+          const R g = gvec(j, k);
+          hx += g * VX[k]; hy += g * VY[k]; hz += g * VZ[k];
+        }
         HGX[j] = hx; HGY[j] = hy; HGZ[j] = hz;
       }
       HGX[3] = VX[0] - VX[1] + VX[2] - VX[3] - VX[4] + VX[5] - VX[6] + VX[7];
       HGY[3] = VY[0] - VY[1] + VY[2] - VY[3] - VY[4] + VY[5] - VY[6] + VY[7];
       HGZ[3] = VZ[0] - VZ[1] + VZ[2] - VZ[3] - VZ[4] + VZ[5] - VZ[6] + VZ[7];
-      R HX[4], HY[4], HZ[4];
       R ehou = R(0);
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
@@ -743,48 +755,38 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
         ehou += HX[j] * HGX[j] + HY[j] * HGY[j] + HZ[j] * HGZ[j];
       }
       my_ehou = (double)(DT1 * ehou);
-#pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        F[0][k] = -Gv[0][k] * HX[0] - Gv[1][k] * HX[1] - Gv[2][k] * HX[2] - R(h4[k]) * HX[3];
-        F[1][k] = -Gv[0][k] * HY[0] - Gv[1][k] * HY[1] - Gv[2][k] * HY[2] - R(h4[k]) * HY[3];
-        F[2][k] = -Gv[0][k] * HZ[0] - Gv[1][k] * HZ[1] - Gv[2][k] * HZ[2] - R(h4[k]) * HZ[3];
-      }
     }
-    // ---- SFINT3 (sfint3.F:256-321), antisymmetric pairs 1-7, 2-8, 3-5, 4-6 ----
-    {
-      const R s1 = (SG[0] - QNEW) * VOLN, s2 = (SG[1] - QNEW) * VOLN, s3 = (SG[2] - QNEW) * VOLN;
-      const R s4 = SG[3] * VOLN, s5 = SG[4] * VOLN, s6 = SG[5] * VOLN;
-      const int n1[4] = {0, 1, 2, 3}, n2[4] = {6, 7, 4, 5};
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        R f = s1 * PX[q] + s4 * PY[q] + s6 * PZ[q];
-        F[0][n1[q]] -= f; F[0][n2[q]] += f;
-        f = s2 * PY[q] + s4 * PX[q] + s5 * PZ[q];
-        F[1][n1[q]] -= f; F[1][n2[q]] += f;
-        f = s3 * PZ[q] + s6 * PX[q] + s5 * PY[q];
-        F[2][n1[q]] -= f; F[2][n2[q]] += f;
-      }
-    }
-    if (corot) {          // SRROTA3 with R transposed (sforc3.F:1603-1614): back to global axes
-#pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        const R fx = R11 * F[0][k] + R12 * F[1][k] + R13 * F[2][k];
-        const R fy = R21 * F[0][k] + R22 * F[1][k] + R23 * F[2][k];
-        const R fz = R31 * F[0][k] + R32 * F[1][k] + R33 * F[2][k];
-        F[0][k] = fx; F[1][k] = fy; F[2][k] = fz;
-      }
-    }
-  }
-  // ---- patch assembly: corner forces to shared memory, then each patch node sums
-  // its incident corners in ascending (element, corner) order ----
-  if (active) {
+    // ---- SFINT3 (sfint3.F:256-321), antisymmetric pairs 1-7, 2-8, 3-5, 4-6: corner
+    // n1[q] gets -f_q, corner n2[q] gets +f_q, added to the hourglass force ----
+    const R s1 = (SG[0] - QNEW) * VOLN, s2 = (SG[1] - QNEW) * VOLN, s3 = (SG[2] - QNEW) * VOLN;
+    const R s4 = SG[3] * VOLN, s5 = SG[4] * VOLN, s6 = SG[5] * VOLN;
+    constexpr int h4[8] = {1, -1, 1, -1, -1, 1, -1, 1};
+    // one corner at a time, straight to the corner-force planes
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-      sc[(0 * 8 + k) * TILE + tid] = F[0][k];
-      sc[(1 * 8 + k) * TILE + tid] = F[1][k];
-      sc[(2 * 8 + k) * TILE + tid] = F[2][k];
+      const R g0 = gvec(0, k), g1 = gvec(1, k), g2 = gvec(2, k);
+      R fx = -g0 * HX[0] - g1 * HX[1] - g2 * HX[2] - R(h4[k]) * HX[3];
+      R fy = -g0 * HY[0] - g1 * HY[1] - g2 * HY[2] - R(h4[k]) * HY[3];
+      R fz = -g0 * HZ[0] - g1 * HZ[1] - g2 * HZ[2] - R(h4[k]) * HZ[3];
+      const int q = pq[k];
+      const R f0 = s1 * PX[q] + s4 * PY[q] + s6 * PZ[q];
+      const R f1 = s2 * PY[q] + s4 * PX[q] + s5 * PZ[q];
+      const R f2 = s3 * PZ[q] + s6 * PX[q] + s5 * PY[q];
+      if (k < 4) { fx -= f0; fy -= f1; fz -= f2; }
+      else { fx += f0; fy += f1; fz += f2; }
+      if (corot) {        // SRROTA3 with R transposed (sforc3.F:1603-1614): back to global axes
+        const R gx = R11 * fx + R12 * fy + R13 * fz;
+        const R gy = R21 * fx + R22 * fy + R23 * fz;
+        const R gz = R31 * fx + R32 * fy + R33 * fz;
+        fx = gx; fy = gy; fz = gz;
+      }
+      sc[(0 * 8 + k) * TILE + tid] = fx;
+      sc[(1 * 8 + k) * TILE + tid] = fy;
+      sc[(2 * 8 + k) * TILE + tid] = fz;
     }
   }
+  // ---- patch assembly: each patch node sums its incident corners in ascending
+  // (element, corner) order ----
   (void)color;
   __syncthreads();
   for (int j = tid; j < nl; j += TILE) {
@@ -870,19 +872,26 @@ shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
       }
     }
   }
+  {
+    const unsigned* src = reinterpret_cast<const unsigned*>(a.inc + (size_t)p * a.inc_stride);
+    unsigned* dst = reinterpret_cast<unsigned*>(sinc);
+    for (int i = tid; i < a.inc_stride / 2; i += TILE) dst[i] = src[i];
+  }
+  // the patch's node numbers (static) go to the corner-force planes before the
+  // wait, each entry read back by the thread that wrote it; X, V, VR and the cycle's
+  // time come from the previous node pass
+  int* sidx = reinterpret_cast<int*>(sc);   // NLM <= 4 * TILE entries
+  for (int j = tid; j < NLM; j += TILE) sidx[j] = a.patch_nodes[p * NLM + j];
+  pdl_wait();
+  pdl_trigger();
   for (int j = tid; j < NLM; j += TILE) {
-    const int g = a.patch_nodes[p * NLM + j];
+    const int g = sidx[j];
     const double4 xx = a.X[g];
     const R4 vv = a.V[g];
     const R4 rr = a.VR[g];
     sx[j] = xx.x; sy[j] = xx.y; sz[j] = xx.z;
     sv[0 * NLM + j] = vv.x; sv[1 * NLM + j] = vv.y; sv[2 * NLM + j] = vv.z;
     sv[3 * NLM + j] = rr.x; sv[4 * NLM + j] = rr.y; sv[5 * NLM + j] = rr.z;
-  }
-  {
-    const unsigned* src = reinterpret_cast<const unsigned*>(a.inc + (size_t)p * a.inc_stride);
-    unsigned* dst = reinterpret_cast<unsigned*>(sinc);
-    for (int i = tid; i < a.inc_stride / 2; i += TILE) dst[i] = src[i];
   }
   const ShellGroupDesc gd = a.groups[pi.group];
   const bool active = tid < pi.nel;
@@ -1273,15 +1282,22 @@ node_kernel(NodeArgs<R> a, int parity) {
     const unsigned char code = codes[n];
     const double dx = DX[n], dy = DY[n], dz = DZ[n];
     R4 f0 = mk4(R(0), R(0), R(0), R(0)), m0 = f0, w0 = f0;
-    if (k1 > k0) f0 = fslot[k0];
-    if (VR) {                             // rotational loads issued with the others
-      w0 = VR[n];
-      if (k1 > k0 && mslot) m0 = mslot[k0];
-    }
+    if (VR) w0 = VR[n];
     const int part = a.tile_part[tile];
     const PartDesc pd = a.parts[part];
     const bool valid = n < pd.node_end;
     const PartTime t0 = a.time[parity * a.nparts + part];
+    // the slots and the time-step reduction come from the element pass; a node's
+    // first two slots are loaded together
+    pdl_wait();
+    pdl_trigger();
+    R4 f1 = mk4(R(0), R(0), R(0), R(0)), m1 = f1;
+    if (k1 > k0) f0 = fslot[k0];
+    if (k1 > k0 + 1) f1 = fslot[k0 + 1];
+    if (VR && mslot) {
+      if (k1 > k0) m0 = mslot[k0];
+      if (k1 > k0 + 1) m1 = mslot[k0 + 1];
+    }
     PartAcc ac = a.acc[parity * a.nparts + part];
     if (a.halo_slot) {   // SPMD: time step = min over every rank's reduction (SPMD_GLOB_MIN5)
       for (int r = 0; r < a.nranks; ++r) {
@@ -1309,7 +1325,8 @@ node_kernel(NodeArgs<R> a, int parity) {
     if (valid) {
       // ASSPAR4: the node's patch partials in ascending patch order
       R ax = f0.x, ay = f0.y, az = f0.z;
-      for (int k = k0 + 1; k < k1; ++k) {
+      if (k1 > k0 + 1) { ax += f1.x; ay += f1.y; az += f1.z; }
+      for (int k = k0 + 2; k < k1; ++k) {
         const R4 f = fslot[k];
         ax += f.x; ay += f.y; az += f.z;
       }
@@ -1367,7 +1384,8 @@ node_kernel(NodeArgs<R> a, int parity) {
       if (pd.has_rot) {
         R4 w = w0;
         R rx = m0.x, ry = m0.y, rz = m0.z;
-        for (int k = k0 + 1; k < k1; ++k) {
+        if (k1 > k0 + 1) { rx += m1.x; ry += m1.y; rz += m1.z; }
+        for (int k = k0 + 2; k < k1; ++k) {
           const R4 m = mslot[k];
           rx += m.x; ry += m.y; rz += m.z;
         }
