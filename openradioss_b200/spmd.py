@@ -15,7 +15,9 @@ nodal update to its nodes.  Here a rank is one process driving one handle:
   library (``or_ecycle_set_halo``) and runs cycles through the library's
   per-cycle SPMD entry points, exchanging the halo buffers with
   ``torch.distributed.all_gather_into_tensor`` on the handle's CUDA stream
-  (NCCL), or through host memory with the gloo backend.
+  (NCCL), or through host memory with the gloo backend.  With NCCL, runs of
+  ``graph_cycles`` cycles (even) are captured once into a CUDA graph, the
+  collective included, and replayed; the remainder runs eagerly.
 
 A shared node's force is the sum of every rank's partial in rank order, so all
 ranks apply the same update; the time step is the minimum over ranks.  Only
@@ -112,10 +114,16 @@ def partition(deck, world):
 class DomainRun:
     """One rank of a domain-decomposed run: one handle on this rank's GPU."""
 
-    def __init__(self, deck, rank, world, precision=abi.OR_PREC_FP64, device=0, backend="nccl", **cfg_kw):
+    def __init__(self, deck, rank, world, precision=abi.OR_PREC_FP64, device=0, backend="nccl", graph_cycles=32,
+                 **cfg_kw):
         import torch
         from .ecycle import ECycle
+        if graph_cycles and (graph_cycles < 0 or graph_cycles % 2):
+            raise ValueError("graph_cycles must be even (the time buffers alternate by cycle parity)")
         self.rank, self.world, self.backend = rank, world, backend
+        self.graph_cycles = int(graph_cycles) if backend == "nccl" else 0
+        self.graph = None
+        self._comm_ready = False
         self.dom = partition(deck, world)[rank]
         self.h = ECycle(self.dom["deck"], precision=precision, device=device, graph=0, **cfg_kw)
         hl, hs, hk = (np.ascontiguousarray(self.dom[k], np.int32) for k in ("halo_local", "halo_slot", "halo_ke"))
@@ -129,24 +137,50 @@ class DomainRun:
         self.bufs = torch.zeros(world * self.nbytes, dtype=torch.uint8, device=dev)
         self.stream = torch.cuda.ExternalStream(self.h.stream(), device=dev)
 
+    def _cycle(self):
+        """One cycle: element kernels and halo pack, the exchange, node kernel."""
+        import torch
+        import torch.distributed as dist
+        self.h._call("spmd_elements", C.c_void_p(self.buf.data_ptr()))
+        if self.backend == "nccl":
+            dist.all_gather_into_tensor(self.bufs, self.buf)
+        else:
+            host = self.buf.cpu()          # waits for this cycle's element kernels
+            parts = [torch.empty_like(host) for _ in range(self.world)]
+            dist.all_gather(parts, host)
+            self.bufs.copy_(torch.cat(parts))
+        self.h._call("spmd_nodes", C.c_void_p(self.bufs.data_ptr()), self.world)
+
     def step(self, ncycles):
-        """ncycles cycles; the same call, with the same ncycles, on every rank."""
+        """ncycles cycles; the same call, with the same ncycles, on every rank.
+
+        Every step starts at time-buffer parity 0 (``spmd_begin``), and a graph
+        holds an even number of cycles, so a replay always starts at parity 0
+        and leaves it there; the library's cycle counter advances by the
+        (even) captured count during the capture only."""
         import torch
         import torch.distributed as dist
         t = self.h.times
+        n = int(ncycles)
         self.h._call("spmd_begin", C.byref(t[0]))
-        bp, bsp = C.c_void_p(self.buf.data_ptr()), C.c_void_p(self.bufs.data_ptr())
         with torch.cuda.stream(self.stream):
-            for _ in range(int(ncycles)):
-                self.h._call("spmd_elements", bp)
-                if self.backend == "nccl":
-                    dist.all_gather_into_tensor(self.bufs, self.buf)
-                else:
-                    host = self.buf.cpu()          # waits for this cycle's element kernels
-                    parts = [torch.empty_like(host) for _ in range(self.world)]
-                    dist.all_gather(parts, host)
-                    self.bufs.copy_(torch.cat(parts))
-                self.h._call("spmd_nodes", bsp, self.world)
+            G = self.graph_cycles
+            if G and n >= G:
+                if self.graph is None:
+                    if not self._comm_ready:       # the communicator exists before a capture
+                        dist.all_gather_into_tensor(self.bufs, self.buf)
+                        torch.cuda.current_stream().synchronize()
+                        self._comm_ready = True
+                    g = torch.cuda.CUDAGraph()
+                    with torch.cuda.graph(g, stream=self.stream):
+                        for _ in range(G):
+                            self._cycle()
+                    self.graph = g
+                for _ in range(n // G):
+                    self.graph.replay()
+                n -= (n // G) * G
+            for _ in range(n):
+                self._cycle()
         self.h._call("spmd_end", C.byref(t[0]))
 
     def get_nodes(self):
@@ -156,4 +190,7 @@ class DomainRun:
         return out
 
     def close(self):
+        """Releases the graph (it holds NCCL calls: before destroy_process_group)
+        and the handle."""
+        self.graph = None
         self.h.close()

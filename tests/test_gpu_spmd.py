@@ -1,5 +1,9 @@
 """Domain-decomposed run of one mesh against the one-handle run, on one GPU.
 
+The NCCL path with the exchange captured in a CUDA graph runs as one rank
+(NCCL takes one GPU per rank): the capture, the replays and the eager
+remainder against the one-handle run, bitwise.
+
 Two ranks (processes) each run their share of the elements on the same GPU
 through the library's SPMD entry points and exchange the halo buffers over
 gloo through host memory, so their kernels never wait on each other.  The
@@ -96,3 +100,50 @@ def test_two_domains_match_one_handle(which, ncycles, precision, tol):
     for k in ("internal", "kinetic", "kinetic_rot", "hourglass"):
         tot = sum(r[4][k] for r in res)
         assert abs(tot - er[k]) <= 10 * tol * max(abs(er[k]), 1e-30), (k, tot, er[k])
+
+
+def _nccl_worker(port, which, steps, graph_cycles, precision, q):
+    import datetime
+    import torch.distributed as dist
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=120))
+    from openradioss_b200 import spmd
+    run = spmd.DomainRun(_deck(which), 0, 1, precision=precision, device=0, backend="nccl",
+                         graph_cycles=graph_cycles)
+    for n in steps:
+        run.step(n)
+    nd = run.get_nodes()
+    q.put((nd["d"], nd["v"], run.h.energies(), run.h.time(), run.graph is not None))
+    run.close()                       # releases the graph before the process group
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("which,precision", [("plate", abi.OR_PREC_FP64), ("mixed", abi.OR_PREC_SPLIT)])
+def test_nccl_exchange_in_a_cuda_graph(which, precision):
+    """Steps of 70 and 75 cycles with 32-cycle graphs: capture in the first step,
+    two replays per step, eager remainders of even and odd length."""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import multiprocessing as pymp
+    from openradioss_b200 import build
+    from openradioss_b200.ecycle import ECycle
+    build.build()
+    steps = (70, 75)
+    deck = _deck(which)
+    ref = ECycle(deck, precision=precision)
+    ref.step(sum(steps))
+    rn = ref.get_nodes()
+    ctx = pymp.get_context("spawn")
+    q = ctx.Queue()
+    p = ctx.Process(target=_nccl_worker, args=(_free_port(), which, steps, 32, precision, q))
+    p.start()
+    d, v, e, t, captured = q.get(timeout=600)
+    p.join(timeout=120)
+    assert p.exitcode == 0
+    assert captured
+    assert np.array_equal(d, rn["d"]) and np.array_equal(v, rn["v"])
+    assert t == ref.time()
+    er = ref.energies()
+    for k in ("internal", "kinetic", "kinetic_rot", "hourglass", "plastic_work"):
+        assert e[k] == er[k], (k, e[k], er[k])
