@@ -117,6 +117,7 @@ struct or_ecycle {
   int spmd_k = -1;                    // cycle index of a running domain-decomposed step, -1 outside one
   int next_parity = 0;                // time-buffer parity of the state after the last step
   bool pdl = true;                    // programmatic dependent launch of the cycle kernels
+  int nsm = 148;                      // multiprocessors of the device
 };
 
 namespace {
@@ -484,9 +485,19 @@ int launch_loads(or_ecycle* h, Impl<R>& m, int parity) {
   h->launches++;
   return OR_OK;
 }
+// node tiles beyond one wave of node_kernel_wide (1024 threads per SM): the
+// streaming form
+template <class R>
+bool node_wide(const or_ecycle* h, const Impl<R>& m) {
+  return m.ntiles > (long long)h->nsm * (1024 / NODE_TILE);
+}
 template <class R>
 int launch_node(or_ecycle* h, Impl<R>& m, int parity, bool pdl = false) {
-  CK(launch_k(node_kernel<R, NODE_TILE>, (unsigned)m.ntiles, NODE_TILE, 0, h->stream, pdl, m.nargs(h), parity));
+  const unsigned g = (unsigned)m.ntiles;
+  if (node_wide(h, m))
+    CK(launch_k(node_kernel_wide<R, NODE_TILE>, g, NODE_TILE, 0, h->stream, pdl, m.nargs(h), parity));
+  else
+    CK(launch_k(node_kernel<R, NODE_TILE>, g, NODE_TILE, 0, h->stream, pdl, m.nargs(h), parity));
   h->launches++;
   return OR_OK;
 }
@@ -1304,7 +1315,8 @@ int spmd_nodes_impl(or_ecycle* h, const void* bufs, int nranks) {
   NodeArgs<R> a = m.nargs(h);
   a.halo_slot = m.halo_slot.p; a.halo_ke = m.halo_ke.p; a.xbuf = (const unsigned char*)bufs;
   a.xbytes = halo_buffer_bytes<R>(m.nhalo); a.nranks = nranks; a.nhalo = m.nhalo;
-  node_kernel<R, NODE_TILE><<<(unsigned)m.ntiles, NODE_TILE, 0, h->stream>>>(a, parity);
+  if (node_wide(h, m)) node_kernel_wide<R, NODE_TILE><<<(unsigned)m.ntiles, NODE_TILE, 0, h->stream>>>(a, parity);
+  else node_kernel<R, NODE_TILE><<<(unsigned)m.ntiles, NODE_TILE, 0, h->stream>>>(a, parity);
   CK(cudaGetLastError());
   h->launches++;
   h->spmd_k++;
@@ -1713,6 +1725,7 @@ int or_ecycle_create(const or_ecycle_config* cfg, or_ecycle** out) {
     delete h;
     return OR_E_CUDA;
   }
+  cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, cfg->device);
   *out = h;
   return OR_OK;
 }

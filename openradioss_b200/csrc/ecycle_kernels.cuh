@@ -1257,8 +1257,7 @@ shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
 // node kernel: ASSPAR4 + dt (resol.F:5853-6226) + ACCELE + BCS10 + VELOCITY + DEPLA
 // ===========================================================================
 template <class R, int TILE>
-__global__ void __launch_bounds__(TILE)
-node_kernel(NodeArgs<R> a, int parity) {
+__device__ __forceinline__ void node_pass(NodeArgs<R> a, int parity) {
   typedef typename Vec4<R>::T R4;
   __shared__ double s_e0[TILE / 32], s_e1[TILE / 32];
   const int* __restrict__ adsky = a.adsky;
@@ -1454,6 +1453,19 @@ node_kernel(NodeArgs<R> a, int parity) {
     }
     __syncthreads();
   }
+}
+
+// Two register budgets for the same pass: node_kernel leaves the budget to the
+// compiler (a single wave is latency-bound and runs faster with more registers
+// per thread); node_kernel_wide asks for 8 blocks of 128 per SM, for meshes of
+// many node tiles, where the pass streams HBM and more loads in flight pay.
+template <class R, int TILE>
+__global__ void __launch_bounds__(TILE) node_kernel(NodeArgs<R> a, int parity) {
+  node_pass<R, TILE>(a, parity);
+}
+template <class R, int TILE>
+__global__ void __launch_bounds__(TILE, 1024 / TILE) node_kernel_wide(NodeArgs<R> a, int parity) {
+  node_pass<R, TILE>(a, parity);
 }
 
 // ===========================================================================
