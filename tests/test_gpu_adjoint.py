@@ -156,6 +156,30 @@ def test_adjoint_full_size_c5_displacement():
     directional_check(200, decks.LAW_JOHNSON_COOK, 0.36, 2e6, 500, 1.0, 0.0, 1e-8, FD_REL, ("thk",))
 
 
+@pytest.mark.parametrize("wd,wp", [(1.0, 0.0), (0.0, 1.0), (1.0, 0.5)])
+def test_adjoint_matches_fp64_reference_gradient(tmp_path, wd, wp):
+    """Every component of dJ/dA, dJ/dthk, dJ/dMS and dJ/dIN against the FP64
+    reference gradient of tests/adjoint_reference.py (oracle forward, host
+    reverse of the nodal update and the assembly, checked against central
+    differences in test_adjoint_reference.py): 6x6 adjoint plate, 60 cycles,
+    30 MPa (plastic), linear hardening, checkpoints every 16 cycles."""
+    need_gpu()
+    import adjoint_reference as ref
+    lib = ref.build_host_lib(tmp_path)
+    n, N, p = 6, 60, 3e7
+    A0, T0 = base_params(n)
+    d0 = plate(n, A0, T0, p, N, jc_n=1.0)
+    node = adjoint.centre_node(d0)
+    res = adjoint_run(d0, N, node, wd, wp, checkpoint=16)
+    rf = ref.reference_gradient(d0, N, node, 2, wd, wp, lib)
+    assert abs(res["J"] - rf["J"]) <= 1e-12 * abs(rf["J"]), (res["J"], rf["J"])
+    for k in ("dA", "dthk", "dms", "din"):
+        g, r = res[k][0], rf[k][0]
+        scale = np.abs(r).max()
+        assert scale > 0.0 or (k == "dA" and wp == 0.0 and not g.any()), k
+        assert np.abs(g - r).max() <= 1e-9 * scale, (k, np.abs(g - r).max(), scale)
+
+
 def with_frame_skew_cloads(d):
     """The plate with /SHFRA/V4 element frames (ISHFRAM 2), its x = xmin edge
     held in a skew frame tilted 25 degrees about y (x' and z' held, and the
