@@ -118,6 +118,7 @@ struct or_ecycle {
   int next_parity = 0;                // time-buffer parity of the state after the last step
   bool pdl = true;                    // programmatic dependent launch of the cycle kernels
   int nsm = 148;                      // multiprocessors of the device
+  long long graph_launches = 0;       // kernel launches in one replay of graph_exec
 };
 
 namespace {
@@ -933,12 +934,12 @@ int step_impl(or_ecycle* h, int ncycles, or_ecycle_time* t) {
       }
       CK(cudaStreamEndCapture(h->stream, &h->graph));
       CK(cudaGraphInstantiate(&h->graph_exec, h->graph, 0));
+      h->graph_launches = h->launches - l0;      // kernels in one replay (loads and links included)
       h->launches = l0;
     }
-    const long long per = (long long)GRAPH_CYCLES * ((m.hps.info.empty() ? 0 : 1) + (m.sps.info.empty() ? 0 : 1) + 1);
     for (; done + GRAPH_CYCLES <= ncycles; done += GRAPH_CYCLES) {
       CK(cudaGraphLaunch(h->graph_exec, h->stream));
-      h->launches += per;
+      h->launches += h->graph_launches;
     }
   }
   // eager cycles; without a graph each phase is bracketed by events, read back
