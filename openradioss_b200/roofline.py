@@ -60,6 +60,6 @@ def measured_peak():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
         with open(path) as f:
-            return float(json.load(f)["hbm_gbs"]), "measured"
+            return float(json.load(f)["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
     except (OSError, KeyError, ValueError):
-        return FALLBACK_HBM_GBS, "fallback"
+        return FALLBACK_HBM_GBS, "fallback (MEASURED_PEAKS.json absent: earlier copy measurement on this GPU pool)"
