@@ -178,6 +178,40 @@ def test_graph_equals_eager_bitwise(lib):
     assert a.energies() == b.energies()
 
 
+def test_programmatic_launch_on_off_bitwise(lib, monkeypatch):
+    """Graph replays with and without programmatic dependent launch of the element
+    and node passes (OR_ECYCLE_PDL, read when a handle is created) give the same
+    bits."""
+    from openradioss_b200.ecycle import ECycle
+    d = decks.c4_mixed_mesh(nx=3, ny=4, nz=6)
+    r = []
+    for flag in ("1", "0"):
+        monkeypatch.setenv("OR_ECYCLE_PDL", flag)
+        h = ECycle(d, precision=abi.OR_PREC_SPLIT)
+        h.step(70)
+        r.append((h.get_nodes(), h.energies(), h.time(), h.shell_state(0)["sig"]))
+        h.close()
+    (na, ea, ta, sa), (nb, eb, tb, sb) = r
+    assert all(np.array_equal(na[k], nb[k]) for k in ("d", "v", "vr"))
+    assert ea == eb and ta == tb and np.array_equal(sa, sb)
+
+
+@pytest.mark.parametrize("precision,tol", [(abi.OR_PREC_FP64, FP64_TOL), (abi.OR_PREC_SPLIT, 1e-5)])
+def test_wide_node_pass(lib, precision, tol):
+    """A mesh of more node tiles than one wave of the node pass's wide form (8
+    blocks of 128 per SM), so that form runs: against the oracle in the same
+    precision."""
+    import torch
+    nsm = torch.cuda.get_device_properties(0).multi_processor_count
+    d = decks.c4_mixed_mesh(nx=56, ny=56, nz=56)
+    assert (d["parts"][0]["x"].shape[0] + 127) // 128 > 8 * nsm
+    g, o = run_pair(d, 20, precision=precision, oracle_precision=precision)
+    check_nodes(g, o, tol)
+    if precision == abi.OR_PREC_FP64:
+        check_hex(g, o, tol)
+        check_energies(g, o, tol)
+
+
 def test_deterministic_repeat(lib):
     from openradioss_b200.ecycle import ECycle
     d = decks.c2_shell_plate(n=16, size=0.016, pressure=5e6)
