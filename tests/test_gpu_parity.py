@@ -212,6 +212,33 @@ def test_wide_node_pass(lib, precision, tol):
         check_energies(g, o, tol)
 
 
+def test_c2_split_error_against_the_fp64_noise_floor(lib):
+    """The C2 plate (200x200, 5 IP, LAW2, 2 MPa) as configured.  After 2000 cycles
+    the FP64 run itself moves by more than 1e-5 relative displacement when its
+    coordinates are perturbed by 1e-12 relative (plastic flow amplifies any
+    perturbation); the split form stays within three times that floor.  At 1000
+    cycles, before the floor grows, the split form is within the 1e-5 bar."""
+    from openradioss_b200.ecycle import ECycle
+    d = decks.c2_shell_plate()
+    dp = decks.c2_shell_plate()
+    x = dp["parts"][0]["x"]
+    x *= 1.0 + 1e-12 * np.random.default_rng(3).choice([-1.0, 1.0], x.shape)
+    runs = {}
+    for name, deck, prec in (("fp64", d, abi.OR_PREC_FP64), ("perturbed", dp, abi.OR_PREC_FP64),
+                             ("split", d, abi.OR_PREC_SPLIT)):
+        h = ECycle(deck, precision=prec)
+        h.step(1000)
+        mid = h.get_nodes()["d"]
+        h.step(1000)
+        runs[name] = (mid, h.get_nodes()["d"])
+        h.close()
+    assert rel(runs["split"][0], runs["fp64"][0]) < SPLIT_TOL
+    floor = rel(runs["perturbed"][1], runs["fp64"][1])
+    err = rel(runs["split"][1], runs["fp64"][1])
+    assert floor > SPLIT_TOL, floor
+    assert err < 3.0 * floor, (err, floor)
+
+
 def test_deterministic_repeat(lib):
     from openradioss_b200.ecycle import ECycle
     d = decks.c2_shell_plate(n=16, size=0.016, pressure=5e6)
