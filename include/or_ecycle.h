@@ -359,9 +359,23 @@ int  or_ecycle_adjoint(or_ecycle* h, int ncycles, const or_adjoint_response* r, 
    keeps its only scratch, the FSKY force skyline, in a static device array of
    OR_NOALLOC_MAX_SLOTS slots (8 MB, held by every GPU that loads the library).
    Larger groups are rejected with OR_E_ARG.  No cudaMalloc / cudaFree or other
-   allocating call is made.  The first call on a device looks up the scratch
-   address with that device current; make it before any stream capture.  All
-   calls share the scratch: calls that overlap on the GPU race.
+   allocating call is made.
+   The tables use the group's own slot numbering, 0-based: adsky[0] = 0,
+   ascending, adsky[numnod] = 8*nel, and iads a permutation of 0..8*nel-1 that
+   puts every corner among the slots of its own node (the engine's global
+   LSKY numbering, shared with shells and other groups, must be renumbered).
+   They are checked on the device before the first cycle; a table that fails
+   returns OR_E_ARG with nothing written and the offending element (corner
+   errors) or node (adsky errors) in t->neltst.  On a device error during the
+   cycles (OR_E_NEGVOL, OR_E_NAN) t->neltst likewise holds the element or node.
+   On success t->ityptst = 1 and t->neltst = the element that set the last DT2,
+   as the handle path reports them.
+   The first call on a device looks up the scratch address with that device
+   current (under a lock, so first calls from several host threads are safe).
+   The call is synchronous, with the bounded wait of or_ecycle_step
+   (OR_ECYCLE_TIMEOUT_S, OR_E_TIMEOUT when it expires); it cannot be called
+   inside a stream capture.  All calls share the scratch: calls that overlap on
+   the GPU race.
    Arrays: x, d, v 3 x numnod; ms, icodt numnod; conn, iads 8 x nel (0-based);
    sig 6 x nel component-major; eint, rho, qvis, pla, epsd, vol0 nel.
    stream: a cudaStream_t (NULL = legacy default stream). */

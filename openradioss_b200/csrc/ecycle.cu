@@ -905,6 +905,20 @@ int wait_stream(or_ecycle* h, cudaEvent_t ev) {
   }
 }
 
+// Bounded wait for everything queued on the handle's stream so far.  Callers
+// read results back only after it: a copy into pageable host memory blocks until
+// the stream drains, so issued first it would make the wait unbounded.  On
+// OR_E_TIMEOUT the work keeps running and the event is left to it.
+int wait_queued(or_ecycle* h) {
+  cudaEvent_t ev;
+  CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  CK(cudaEventRecord(ev, h->stream));
+  const int rc = wait_stream(h, ev);
+  if (rc == OR_E_TIMEOUT) return rc;
+  cudaEventDestroy(ev);
+  return rc;
+}
+
 template <class R>
 int step_impl(or_ecycle* h, int ncycles, or_ecycle_time* t) {
   Impl<R>& m = *(Impl<R>*)h->impl;
@@ -973,15 +987,11 @@ int step_impl(or_ecycle* h, int ncycles, or_ecycle_time* t) {
   for (auto& e : ev) cudaEventDestroy(e);
   const int fin = ncycles & 1;
   h->next_parity = fin;
+  if ((rc = wait_queued(h))) return rc;
   CK(cudaMemcpyAsync(pt.data(), m.time.p + fin * np, np * sizeof(PartTime), cudaMemcpyDeviceToHost, h->stream));
   ErrorWord ew{};
   CK(cudaMemcpyAsync(&ew, m.err.p, sizeof(ErrorWord), cudaMemcpyDeviceToHost, h->stream));
-  cudaEvent_t done_ev;
-  CK(cudaEventCreateWithFlags(&done_ev, cudaEventDisableTiming));
-  CK(cudaEventRecord(done_ev, h->stream));
-  rc = wait_stream(h, done_ev);
-  cudaEventDestroy(done_ev);
-  if (rc) return rc;
+  CK(cudaStreamSynchronize(h->stream));
   for (int p = 0; p < np; ++p) {
     t[p].tt = pt[p].tt; t[p].dt1 = pt[p].dt1; t[p].dt2 = pt[p].dt2; t[p].dt12 = pt[p].dt12;
     t[p].dt2old = pt[p].dt2old; t[p].ncycle = pt[p].ncycle; t[p].ityptst = pt[p].ityptst; t[p].neltst = pt[p].neltst;
@@ -1330,14 +1340,11 @@ int spmd_end_impl(or_ecycle* h, or_ecycle_time* t) {
   const int fin = h->spmd_k & 1;
   PartTime pt{};
   ErrorWord ew{};
+  const int rc = wait_queued(h);
+  if (rc) return rc;
   CK(cudaMemcpyAsync(&pt, m.time.p + fin, sizeof(PartTime), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaMemcpyAsync(&ew, m.err.p, sizeof(ErrorWord), cudaMemcpyDeviceToHost, h->stream));
-  cudaEvent_t ev;
-  CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-  CK(cudaEventRecord(ev, h->stream));
-  int rc = wait_stream(h, ev);
-  cudaEventDestroy(ev);
-  if (rc) return rc;
+  CK(cudaStreamSynchronize(h->stream));
   t->tt = pt.tt; t->dt1 = pt.dt1; t->dt2 = pt.dt2; t->dt12 = pt.dt12; t->dt2old = pt.dt2old;
   t->ncycle = pt.ncycle; t->ityptst = pt.ityptst; t->neltst = pt.neltst;
   h->next_parity = fin;
@@ -1506,13 +1513,10 @@ int adj_prepare(or_ecycle* h, Impl<double>& m, int ncycles, int K) {
 
 int adj_check_error(or_ecycle* h, Impl<double>& m) {
   ErrorWord ew{};
-  CK(cudaMemcpyAsync(&ew, m.err.p, sizeof(ErrorWord), cudaMemcpyDeviceToHost, h->stream));
-  cudaEvent_t ev;
-  CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-  CK(cudaEventRecord(ev, h->stream));
-  int rc = wait_stream(h, ev);
-  cudaEventDestroy(ev);
+  const int rc = wait_queued(h);
   if (rc) return rc;
+  CK(cudaMemcpyAsync(&ew, m.err.p, sizeof(ErrorWord), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
   h->last_code = ew.code;
   h->last_index = ew.index;
   if (ew.code) {

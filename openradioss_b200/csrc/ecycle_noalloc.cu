@@ -15,15 +15,28 @@
 //     hexas); larger groups are rejected with OR_E_ARG;
 //   * FP64 only, one hexa group of one part, LAW1 or LAW2;
 //   * every GPU that loads the library holds the scratch (8 MB) until exit;
+//   * the caller's tables are checked on the device before the first cycle:
+//     every connectivity entry in [0, numnod), ADSKY a CSR over 8*nel slots
+//     (ADSKY(1) = 0, ascending, ADSKY(numnod+1) = 8*nel) and IADS a permutation
+//     of [0, 8*nel) that puts each corner among its own node's slots; a table
+//     that fails is rejected with OR_E_ARG before anything is written, and the
+//     kernels also skip any slot outside the scratch;
 //   * every call shares the scratch and it keeps the last call's contents:
-//     the time-step accumulator and error word are cleared at the start of
-//     each call, the skyline slots are all rewritten every cycle; calls that
-//     overlap on the GPU (other streams, other host threads) race on it;
+//     the time-step accumulator, error word and slot counters are cleared at
+//     the start of each call, the skyline slots are all rewritten every cycle;
+//     calls that overlap on the GPU (other streams, other host threads) race
+//     on it;
 //   * the first call on a device looks the scratch's device address up once
-//     (cudaGetSymbolAddress) with that device current; make that first call
-//     before any stream capture is begun.
+//     (cudaGetSymbolAddress, under a lock) with that device current;
+//   * the call is synchronous: it waits for its own work with the bounded
+//     event poll of the handle path (OR_ECYCLE_TIMEOUT_S, default 900 s), so
+//     it cannot be recorded into a CUDA graph by stream capture.
+#include <chrono>
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
+#include <mutex>
+#include <thread>
 #include <cuda_runtime.h>
 
 #include "../../include/or_ecycle.h"
@@ -34,6 +47,7 @@ constexpr int NOALLOC_TILE = 128;
 
 struct NoallocScalars {
   unsigned long long dtbits;   // min over elements of the element dt (double bits)
+  unsigned long long dtkey;    // min of (float(dt) bits << 32 | 0x80000000 | element): NELTS
   int err_code;
   int err_index;
   double time[8];              // tt, dt1, dt2, dt12, dt2old, ncycle, ityptst, neltst
@@ -51,9 +65,33 @@ struct ScratchPtrs {
 constexpr int MAX_DEVICES = 64;
 ScratchPtrs g_ptrs[MAX_DEVICES];
 bool g_ptrs_ready[MAX_DEVICES];
+std::mutex g_ptrs_lock;          // first calls from several host threads
 
 __device__ inline void noalloc_error(NoallocScalars* sc, int code, int index) {
   if (atomicCAS(&sc->err_code, 0, code) == 0) sc->err_index = index;
+}
+
+// Table check, one thread per element corner (the scratch's first 8*nel words
+// count the corners that land on each slot): the corner's node is in
+// [0, numnod), its slot is in [0, 8*nel) and among its node's ADSKY range, and
+// no other corner took the slot.  With ADSKY checked by check_adsky_kernel this
+// makes IADS a permutation that fills every node's range exactly.
+__global__ void check_corners_kernel(int nel, int numnod, const int* __restrict__ conn, const int* __restrict__ iads,
+                                     const int* __restrict__ adsky, unsigned* count, NoallocScalars* sc) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= 8 * nel) return;
+  const int e = c >> 3, n = conn[c], s = iads[c], nslot = 8 * nel;
+  if (n < 0 || n >= numnod || s < 0 || s >= nslot) { noalloc_error(sc, OR_E_ARG, e); return; }
+  if (s < adsky[n] || s >= adsky[n + 1]) { noalloc_error(sc, OR_E_ARG, e); return; }
+  if (atomicAdd(&count[s], 1u) != 0u) noalloc_error(sc, OR_E_ARG, e);
+}
+
+// ADSKY check, one thread per node: ADSKY(1) = 0, ascending, ADSKY(numnod+1) = 8*nel
+__global__ void check_adsky_kernel(int nel, int numnod, const int* __restrict__ adsky, NoallocScalars* sc) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= numnod) return;
+  const int a0 = adsky[n], a1 = adsky[n + 1];
+  if (a1 < a0 || (n == 0 && a0 != 0) || (n == numnod - 1 && a1 != 8 * nel)) noalloc_error(sc, OR_E_ARG, n);
 }
 
 // One thread per hexa: SDERI3, SDLEN3, SDEFO3, SRHO3, SROTA3, M1LAW / M2LAW with
@@ -66,8 +104,8 @@ hex_fsky_kernel(int nel, const int* __restrict__ conn, const int* __restrict__ i
                 const double* __restrict__ vol0, or_material mt, or_solid_prop pr, double dtfac,
                 double4* fsky, NoallocScalars* sc) {
   const int e = blockIdx.x * NOALLOC_TILE + threadIdx.x;
-  __shared__ unsigned long long s_min[NOALLOC_TILE / 32];
-  unsigned long long mybits = ~0ull;
+  __shared__ unsigned long long s_min[NOALLOC_TILE / 32], s_key[NOALLOC_TILE / 32];
+  unsigned long long mybits = ~0ull, mykey = ~0ull;
   if (e < nel) {
     const double DT1 = sc->time[1];
     double XD[8], YD[8], ZD[8], VX[8], VY[8], VZ[8];
@@ -199,6 +237,7 @@ hex_fsky_kernel(int nel, const int* __restrict__ conn, const int* __restrict__ i
     const double SSP_EQ = fmax(1e-20, QX + sqrt(QX * QX + SSP * SSP));
     const double DTX = dtfac * (DELTAX / SSP_EQ);
     mybits = (unsigned long long)__double_as_longlong(DTX);
+    mykey = ((unsigned long long)__float_as_uint((float)DTX) << 32) | (0x80000000u | (unsigned)e);
     // pressure and internal energy (m1law.F:172-190, m2law.F:434-461)
     const double PNEW = mt.bulk * AMU;
     SG[0] -= PNEW; SG[1] -= PNEW; SG[2] -= PNEW;
@@ -270,22 +309,34 @@ hex_fsky_kernel(int nel, const int* __restrict__ conn, const int* __restrict__ i
         F[2][n1[q]] -= f; F[2][n2[q]] += f;
       }
     }
-    // SCUMU3P (scumu3p.F:205-260): one skyline slot per corner
+    // SCUMU3P (scumu3p.F:205-260): one skyline slot per corner; the tables were
+    // checked before the first cycle, and a slot outside the scratch is skipped
 #pragma unroll
-    for (int k = 0; k < 8; ++k) fsky[iads[8 * e + k]] = make_double4(F[0][k], F[1][k], F[2][k], 0.0);
+    for (int k = 0; k < 8; ++k) {
+      const int s = iads[8 * e + k];
+      if ((unsigned)s < (unsigned)(8 * nel)) fsky[s] = make_double4(F[0][k], F[1][k], F[2][k], 0.0);
+      else noalloc_error(sc, OR_E_ARG, e);
+    }
   }
-  // element dt min-reduction: warp shuffles, then one atomicMin per block
+  // element dt min-reduction (exact bits, and the key that names the element):
+  // warp shuffles, then one atomicMin of each per block
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     const unsigned long long b = __shfl_xor_sync(0xffffffffu, mybits, o);
+    const unsigned long long k = __shfl_xor_sync(0xffffffffu, mykey, o);
     mybits = b < mybits ? b : mybits;
+    mykey = k < mykey ? k : mykey;
   }
-  if ((threadIdx.x & 31) == 0) s_min[threadIdx.x >> 5] = mybits;
+  if ((threadIdx.x & 31) == 0) { s_min[threadIdx.x >> 5] = mybits; s_key[threadIdx.x >> 5] = mykey; }
   __syncthreads();
   if (threadIdx.x == 0) {
-    unsigned long long m = s_min[0];
-    for (int w = 1; w < NOALLOC_TILE / 32; ++w) m = s_min[w] < m ? s_min[w] : m;
+    unsigned long long m = s_min[0], q = s_key[0];
+    for (int w = 1; w < NOALLOC_TILE / 32; ++w) {
+      m = s_min[w] < m ? s_min[w] : m;
+      q = s_key[w] < q ? s_key[w] : q;
+    }
     atomicMin(&sc->dtbits, m);
+    atomicMin(&sc->dtkey, q);
   }
 }
 
@@ -295,7 +346,11 @@ __global__ void dt_kernel(NoallocScalars* sc, double growth, double dtmx) {
   double* t = sc->time;   // tt, dt1, dt2, dt12, dt2old, ncycle
   const double dt2t = __longlong_as_double((long long)sc->dtbits);
   double DT2 = 1e6;
-  if (sc->dtbits != ~0ull && dt2t < DT2) DT2 = dt2t;
+  if (sc->dtbits != ~0ull && dt2t < DT2) {   // the element that set DT2 (ITYPTS = 1, NELTS)
+    DT2 = dt2t;
+    t[6] = 1.0;
+    t[7] = (double)(int)(sc->dtkey & 0x7fffffffull);
+  }
   DT2 = fmin(fmin(DT2, growth * t[4]), dtmx);
   t[3] = 0.5 * (t[1] + DT2);
   t[2] = DT2;
@@ -303,15 +358,17 @@ __global__ void dt_kernel(NoallocScalars* sc, double growth, double dtmx) {
   t[0] += DT2;
   t[5] += 1.0;
   sc->dtbits = ~0ull;
+  sc->dtkey = ~0ull;
 }
 
-__global__ void node_fsky_kernel(int numnod, const int* __restrict__ adsky, const double4* __restrict__ fsky,
-                                 double* x, double* d, double* v, const double* __restrict__ ms,
-                                 const int* __restrict__ icodt, NoallocScalars* sc) {
+__global__ void node_fsky_kernel(int numnod, int nslot, const int* __restrict__ adsky,
+                                 const double4* __restrict__ fsky, double* x, double* d, double* v,
+                                 const double* __restrict__ ms, const int* __restrict__ icodt, NoallocScalars* sc) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= numnod) return;
   double ax = 0, ay = 0, az = 0;
-  for (int k = adsky[n]; k < adsky[n + 1]; ++k) {
+  const int k0 = max(adsky[n], 0), k1 = min(adsky[n + 1], nslot);   // within the scratch
+  for (int k = k0; k < k1; ++k) {
     const double4 f = fsky[k];
     ax += f.x; ay += f.y; az += f.z;
   }
@@ -335,6 +392,35 @@ __global__ void start_cycle_kernel(NoallocScalars* sc) {
   sc->time[1] = sc->time[2];   // DT1 = DT2 (resol.F:2639)
 }
 
+// Bounded wait for the call's own work, as the handle path's wait_stream.
+int wait_event(cudaEvent_t ev) {
+  double limit = 900.0;
+  if (const char* s = std::getenv("OR_ECYCLE_TIMEOUT_S")) limit = std::atof(s);
+  const auto t0 = std::chrono::steady_clock::now();
+  for (;;) {
+    const cudaError_t q = cudaEventQuery(ev);
+    if (q == cudaSuccess) return OR_OK;
+    if (q != cudaErrorNotReady) return OR_E_CUDA;
+    const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (el > limit) return OR_E_TIMEOUT;
+    std::this_thread::sleep_for(std::chrono::microseconds(el < 0.01 ? 5 : 200));
+  }
+}
+
+// Waits (bounded) for the work queued on s, then copies the scalars back.  The
+// wait comes first: a copy into pageable host memory blocks until the stream
+// drains, so issued before the wait it would make the wait unbounded.
+int read_scalars(cudaStream_t s, NoallocScalars* dev, NoallocScalars* out) {
+  cudaEvent_t ev;
+  if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return OR_E_CUDA;
+  const int rc = cudaEventRecord(ev, s) == cudaSuccess ? wait_event(ev) : OR_E_CUDA;
+  if (rc == OR_E_TIMEOUT) return rc;        // the work is still running: keep the event
+  cudaEventDestroy(ev);
+  if (rc) return rc;
+  if (cudaMemcpyAsync(out, dev, sizeof *out, cudaMemcpyDeviceToHost, s) != cudaSuccess) return OR_E_CUDA;
+  return cudaStreamSynchronize(s) == cudaSuccess ? OR_OK : OR_E_CUDA;
+}
+
 }  // namespace
 
 extern "C" int or_ecycle_hex_step_noalloc(int device, void* stream, int ncycles, or_ecycle_time* t,
@@ -352,23 +438,42 @@ extern "C" int or_ecycle_hex_step_noalloc(int device, void* stream, int ncycles,
   if (prop->jcvt != 0) return OR_E_UNSUPPORTED;                          // global frame only
   if (device < 0 || device >= MAX_DEVICES) return OR_E_ARG;
   if (cudaSetDevice(device) != cudaSuccess) return OR_E_CUDA;
-  if (!g_ptrs_ready[device]) {
-    ScratchPtrs p;
-    if (cudaGetSymbolAddress((void**)&p.fsky, g_fsky_scratch) != cudaSuccess) return OR_E_CUDA;
-    if (cudaGetSymbolAddress((void**)&p.sc, g_noalloc_scalars) != cudaSuccess) return OR_E_CUDA;
-    g_ptrs[device] = p;
-    g_ptrs_ready[device] = true;
+  ScratchPtrs p;
+  {
+    std::lock_guard<std::mutex> lk(g_ptrs_lock);
+    if (!g_ptrs_ready[device]) {
+      ScratchPtrs q;
+      if (cudaGetSymbolAddress((void**)&q.fsky, g_fsky_scratch) != cudaSuccess) return OR_E_CUDA;
+      if (cudaGetSymbolAddress((void**)&q.sc, g_noalloc_scalars) != cudaSuccess) return OR_E_CUDA;
+      g_ptrs[device] = q;
+      g_ptrs_ready[device] = true;
+    }
+    p = g_ptrs[device];
   }
-  const ScratchPtrs p = g_ptrs[device];
   cudaStream_t s = (cudaStream_t)stream;
+  const int nslot = 8 * nel;
   // clear what must start at zero / +inf, load the caller's time state
   NoallocScalars init;
   init.dtbits = ~0ull;
+  init.dtkey = ~0ull;
   init.err_code = 0;
   init.err_index = -1;
   init.time[0] = t->tt; init.time[1] = t->dt1; init.time[2] = t->dt2; init.time[3] = t->dt12;
-  init.time[4] = t->dt2old; init.time[5] = (double)t->ncycle; init.time[6] = 0; init.time[7] = 0;
+  init.time[4] = t->dt2old; init.time[5] = (double)t->ncycle; init.time[6] = (double)t->ityptst;
+  init.time[7] = (double)t->neltst;
   if (cudaMemcpyAsync(p.sc, &init, sizeof init, cudaMemcpyHostToDevice, s) != cudaSuccess) return OR_E_CUDA;
+  // check the caller's tables before anything is written (slot counters in the scratch)
+  NoallocScalars out;
+  {
+    unsigned* count = reinterpret_cast<unsigned*>(p.fsky);
+    if (cudaMemsetAsync(count, 0, (size_t)nslot * sizeof(unsigned), s) != cudaSuccess) return OR_E_CUDA;
+    check_adsky_kernel<<<(unsigned)((numnod + 255) / 256), 256, 0, s>>>(nel, numnod, adsky, p.sc);
+    check_corners_kernel<<<(unsigned)((nslot + 255) / 256), 256, 0, s>>>(nel, numnod, conn, iads, adsky, count, p.sc);
+    if (cudaGetLastError() != cudaSuccess) return OR_E_CUDA;
+    const int rc = read_scalars(s, p.sc, &out);
+    if (rc) return rc;
+    if (out.err_code) { t->neltst = out.err_index; return out.err_code; }
+  }
   const unsigned eb = (unsigned)((nel + NOALLOC_TILE - 1) / NOALLOC_TILE);
   const unsigned nb = (unsigned)((numnod + 255) / 256);
   for (int c = 0; c < ncycles; ++c) {
@@ -376,13 +481,14 @@ extern "C" int or_ecycle_hex_step_noalloc(int device, void* stream, int ncycles,
     hex_fsky_kernel<<<eb, NOALLOC_TILE, 0, s>>>(nel, conn, iads, x, v, sig, eint, rho, qvis, pla, epsd, vol0, *mat,
                                                  *prop, dtfac, p.fsky, p.sc);
     dt_kernel<<<1, 1, 0, s>>>(p.sc, dt_growth, dtmx);
-    node_fsky_kernel<<<nb, 256, 0, s>>>(numnod, adsky, p.fsky, x, d, v, ms, icodt, p.sc);
+    node_fsky_kernel<<<nb, 256, 0, s>>>(numnod, nslot, adsky, p.fsky, x, d, v, ms, icodt, p.sc);
   }
   if (cudaGetLastError() != cudaSuccess) return OR_E_CUDA;
-  NoallocScalars out;
-  if (cudaMemcpyAsync(&out, p.sc, sizeof out, cudaMemcpyDeviceToHost, s) != cudaSuccess) return OR_E_CUDA;
-  if (cudaStreamSynchronize(s) != cudaSuccess) return OR_E_CUDA;
+  const int rc = read_scalars(s, p.sc, &out);
+  if (rc) return rc;
   t->tt = out.time[0]; t->dt1 = out.time[1]; t->dt2 = out.time[2]; t->dt12 = out.time[3];
   t->dt2old = out.time[4]; t->ncycle = (int)out.time[5];
+  t->ityptst = (int)out.time[6]; t->neltst = (int)out.time[7];
+  if (out.err_code) t->neltst = out.err_index;
   return out.err_code;
 }

@@ -1,8 +1,8 @@
 """Extracts the golden values of the reference's miniqa RESTART/cra2 test
 into cra2_listing.json (run from the repository root, next to a reference
-checkout; OR_REFERENCE_ROOT overrides its location):
+checkout, whose location OR_REFERENCE_ROOT gives):
 
-    python tests/golden/make_cra2_listing.py
+    OR_REFERENCE_ROOT=<reference checkout> python tests/golden/make_cra2_listing.py
 
 From the reference engine's own listings (qa-tests/miniqa/RESTART/cra2/
 reference/CRA2V44_0001.out and CRA2V44_0002.out) it takes every cycle line:
@@ -16,8 +16,6 @@ import json
 import os
 import re
 
-REF = os.environ.get("OR_REFERENCE_ROOT", "/root/reference")
-CASE = os.path.join(REF, "qa-tests", "miniqa", "RESTART", "cra2")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "cra2_listing.json")
 
 LINE = re.compile(r"^\s*(\d+)\s+(\S+)\s+(\S+)\s+SHELL\s+(\d+)\s+(\S+)%\s+(\S+)\s+(\S+)\s+(\S+)\s+")
@@ -54,6 +52,10 @@ def extract(path):
 
 
 def main():
+    ref = os.environ.get("OR_REFERENCE_ROOT")
+    if not ref:
+        raise SystemExit("set OR_REFERENCE_ROOT to a reference checkout")
+    CASE = os.path.join(ref, "qa-tests", "miniqa", "RESTART", "cra2")
     r1, n1 = engine_lines(os.path.join(CASE, "reference", "CRA2V44_0001.out"))
     r2, n2 = engine_lines(os.path.join(CASE, "reference", "CRA2V44_0002.out"))
     parts, total = starter_masses(os.path.join(CASE, "reference", "CRA2V44_0000.out"))
