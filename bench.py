@@ -2,6 +2,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload shell_plate|hex_block|mixed_mesh|batched_parts]
+                    [--sub-workloads mixed_mesh] [--eager-cycles N --mesh-n M --tile T]
 
 One step = one complete run of the workload (all its cycles) from the uploaded
 initial state; the state is reset between steps outside the timed region and
@@ -11,6 +12,17 @@ share of the parts (largest-first on element count, openradioss_b200/shard.py),
 strong scaling over the fixed deck; a single-mesh deck is replicated, one copy
 per rank (weak scaling).  Neither needs a data-path collective.  Timing is the
 max over ranks of device time.  Prints one JSON line on rank 0.
+
+The line also states the split form's error against the FP64 run per output
+(nodal D, V, VR, stresses, plastic strains, internal / kinetic / hourglass
+energy, plastic work), beside the FP64 run's own sensitivity floor (the same
+FP64 run from coordinates perturbed by 1e-12) at the same cycle count, and
+both again after 1000 cycles; on one GPU it adds a record of the 2.08 M-element
+mixed mesh (split and FP64 rates, per-kernel roofline, split error).
+
+--eager-cycles N runs N cycles of a workload without a CUDA graph (one launch
+per kernel per cycle) and prints per-phase device times: the command that the
+ncu captures under profiles/ run.
 """
 from __future__ import annotations
 
@@ -49,13 +61,97 @@ def parse():
     ap.add_argument("--cycles", type=int, default=0, help="override cycles per step")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sub-workloads", default="mixed_mesh",
+                    help="comma-separated workloads recorded beside the headline on one GPU ('' = none)")
+    ap.add_argument("--sub-steps", type=int, default=3)
+    ap.add_argument("--sub-tile", type=int, default=128)
+    ap.add_argument("--eager-cycles", type=int, default=0,
+                    help="profiling mode: run this many eager cycles and print per-phase times")
+    ap.add_argument("--mesh-n", type=int, default=0, help="profiling mode: mesh size parameter (0 = workload's)")
+    ap.add_argument("--tile", type=int, default=0, help="profiling mode: elements per patch (0 = library default)")
+    ap.add_argument("--precision", default="split", choices=["split", "fp64"], help="profiling mode")
     return ap.parse_args()
 
 
-def make_deck(name):
+def make_deck(name, n=0):
+    """The workload's deck; n > 0 scales the mesh (profiling of smaller cases)."""
     from openradioss_b200 import decks
-    fn = getattr(decks, WORKLOADS[name][0])
-    return fn()
+    if not n:
+        return getattr(decks, WORKLOADS[name][0])()
+    return {"shell_plate": lambda: decks.c2_shell_plate(n=n, size=n * 1e-3),
+            "hex_block": lambda: decks.c1_hex_block(nx=n, ny=n, nz=4 * n),
+            "mixed_mesh": lambda: decks.c4_mixed_mesh(nx=n, ny=n, nz=2 * n),
+            "batched_parts": lambda: decks.c3_batched_parts()}[name]()
+
+
+def workload_config(name, deck, cycles, world, sharded):
+    """The `config` of the JSON line: the workload as both arms run it."""
+    from openradioss_b200 import decks
+    nel = decks.num_elements(deck)
+    return {"workload": name, "description": WORKLOADS[name][2], "elements_per_gpu": nel,
+            "nodes_per_gpu": decks.num_nodes(deck), "cycles_per_step": cycles,
+            "elements_per_step_all_ranks": nel if sharded else world * nel,
+            "parallelism": (f"parts sharded over {world} ranks" if sharded else f"{world} independent replica(s)"),
+            "l2": "256 MB buffer written before every timed step"}
+
+
+def outputs(h):
+    """Per-output arrays of a handle's state (the quantities the split error is stated on)."""
+    import numpy as np
+    out = {}
+    nodes = [h.get_nodes(p) for p in range(h.nparts)]
+    for k, name in (("d", "D"), ("v", "V"), ("vr", "VR")):
+        out[name] = np.concatenate([n[k].ravel() for n in nodes])
+    if h.shell_groups:
+        st = [h.shell_state(g) for g in range(len(h.shell_groups))]
+        out["sigma_shell"] = np.concatenate([s["sig"].ravel() for s in st])
+        out["pla_shell"] = np.concatenate([s["pla"].ravel() for s in st])
+    if h.hex_groups:
+        st = [h.hex_state(g) for g in range(len(h.hex_groups))]
+        out["sigma_hex"] = np.concatenate([s["sig"].ravel() for s in st])
+        out["pla_hex"] = np.concatenate([s["pla"].ravel() for s in st])
+    en = [h.energies(p) for p in range(h.nparts)]
+    for k in ("internal", "kinetic", "hourglass", "plastic_work"):
+        out["E_" + k] = np.array([sum(e[k] for e in en)])
+    return out
+
+
+def output_errors(a, b):
+    """max|a - b| / max|b| per output (0 where b is zero everywhere and a too)."""
+    import numpy as np
+    err = {}
+    for k in b:
+        den = float(np.abs(b[k]).max()) if b[k].size else 0.0
+        num = float(np.abs(a[k] - b[k]).max()) if b[k].size else 0.0
+        err[k] = num / den if den > 0 else (0.0 if num == 0 else float("inf"))
+    return err
+
+
+def perturbed_run(h, deck, cycles, eps=1e-12, seed=7):
+    """The handle's run from its uploaded state with every coordinate moved by a
+    relative eps (seeded signs): the run's own sensitivity to rounding-level input."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    h.reset()
+    for p, part in enumerate(deck["parts"]):
+        x = part["x"] * (1.0 + eps * rng.choice([-1.0, 1.0], size=part["x"].shape))
+        h.set_nodes(p, x=x)
+    h.step(cycles)
+    return outputs(h)
+
+
+def eager_profile(args):
+    """--eager-cycles: per-phase device times of eager cycles (no graph)."""
+    from openradioss_b200 import abi, build, decks
+    from openradioss_b200.ecycle import ECycle
+    build.build()
+    d = make_deck(args.workload, args.mesh_n)
+    prec = abi.OR_PREC_SPLIT if args.precision == "split" else abi.OR_PREC_FP64
+    tiles = dict(block_hex=args.tile, block_shell=args.tile) if args.tile else {}
+    h = ECycle(d, precision=prec, graph=0, **tiles)
+    h.step(args.eager_cycles)
+    print(json.dumps({"workload": args.workload, "elements": decks.num_elements(d), "cycles": args.eager_cycles,
+                      "phase_ms": h.phase_times(), "launches": h.launch_count(), "time": h.time()}))
 
 
 # ---------------------------------------------------------------------------
@@ -157,12 +253,14 @@ def reference_arm(args, rank, world):
     value = nel * per_step * args.steps / tot
     sample = (f"{per_step} cycles per step of the {args.workload} deck (of {cycles}), FP64, "
               f"C++ restatement of the reference CPU path, OpenMP {nthreads} threads")
+    sharded = world > 1 and len(deck["parts"]) > 1
     line = {"metric": "element-updates/s", "value": value, "unit": "element-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "impl": "reference",
-            "config": {"workload": args.workload, "description": WORKLOADS[args.workload][2],
-                       "elements": nel, "cycles_per_step": per_step},
+            "higher_is_better": True, "scaling": "strong" if sharded else "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded numpy decks with the workload's shapes)",
+            "impl": "reference",
+            "config": workload_config(args.workload, deck, cycles, world, sharded),
+            "sample": {"cycles_per_step": per_step, "of_cycles": cycles, "ranks_running": 1},
             "cpu_baseline": {"value": value, "unit": "element-updates/s", "cores": nthreads, "kind": "port",
                              "sample": sample},
             "e2e": {"value": value, "unit": "element-updates/s", "h2d_bytes_per_step": 0,
@@ -199,6 +297,40 @@ def adjoint_timing(device, ncycles=500, checkpoint=50, reps=3):
 
 
 # ---------------------------------------------------------------------------
+def kernel_roofline(h, deck, cycles, workload, s=4):
+    """Per-kernel device times (each phase kernel launched back to back from a graph
+    on the state a full run leaves, CUDA events on the handle's stream) and the
+    roofline of the dominant one.  Resets the handle."""
+    from openradioss_b200 import roofline
+    h.reset()
+    h.step(cycles)
+    kt = h.kernel_times(reps=64)            # microseconds per launch; resets the handle
+    eb_hex = sum(g["ixs"].shape[0] * roofline.hex_bytes(s, g["mat"]["law"]) for p in deck["parts"] for g in p["hex"])
+    eb_shell = sum(g["ixc"].shape[0] * roofline.shell_bytes(s, g["prop"]["npt"])
+                   for p in deck["parts"] for g in p["shell"])
+    eb, nb, _ = roofline.deck_bytes(deck, s)
+    peak, peak_src = roofline.measured_peak()
+    kern = {"hex": (kt["hex"] * 1e-3, eb_hex), "shell": (kt["shell"] * 1e-3, eb_shell), "node": (kt["node"] * 1e-3, nb)}
+    dom = max(kern, key=lambda k: kern[k][0])
+    dom_ms, dom_bytes = kern[dom]
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get(workload, {}).get(f"{dom}_split")
+        except (OSError, ValueError):
+            traffic = None
+    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9 if dom_ms > 0 else 0.0
+    per_kernel = {k: {"us_per_launch": v[0] * 1e3, "algorithmic_bytes": v[1],
+                      "frac": (v[1] / (v[0] * 1e-3) / 1e9 / peak) if v[0] > 0 else None}
+                  for k, v in kern.items()}
+    roof = {"bound": "hbm", "kernel": f"{dom}_patch_kernel" if dom != "node" else "node_kernel",
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic, "algorithmic_bytes_per_launch": dom_bytes,
+            "avg_launch_ms": dom_ms, "peak_source": peak_src}
+    return roof, per_kernel, eb + nb, peak
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", 0))
@@ -206,6 +338,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", 0))
     if args.impl == "reference":
         return reference_arm(args, rank, world)
+    if args.eager_cycles:
+        return eager_profile(args)
 
     import torch
     import torch.distributed as dist
@@ -214,7 +348,7 @@ def main():
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
 
-    from openradioss_b200 import abi, build, decks, roofline, shard
+    from openradioss_b200 import abi, build, decks, shard
     from openradioss_b200.ecycle import ECycle
     build.build()
     full = make_deck(args.workload)
@@ -222,7 +356,6 @@ def main():
     deck = shard.rank_deck(full, rank, world) if sharded else full
     cycles = args.cycles or WORKLOADS[args.workload][1]
     nel = decks.num_elements(deck)
-    nnod = decks.num_nodes(deck)
     # element-updates of one step over all ranks
     nel_job = decks.num_elements(full) if sharded else world * nel
 
@@ -230,9 +363,15 @@ def main():
         if world > 1:
             dist.barrier()
 
+    def max_over_ranks(*vals):
+        tt = torch.tensor(list(vals), dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        return [float(v) for v in tt]
+
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
-    def timed_runs(h, nsteps, nwarm):
+    def timed_runs(h, ncyc, nsteps, nwarm):
         s = torch.cuda.ExternalStream(h.stream())
         ms, launches = [], 0
         for k in range(nwarm + nsteps):
@@ -242,7 +381,7 @@ def main():
             barrier()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(s)
-            h.step(cycles)
+            h.step(ncyc)
             e1.record(s)
             torch.cuda.synchronize()
             if k >= nwarm:
@@ -257,54 +396,40 @@ def main():
 
     # ---- split form (the headline) ----
     hs = ECycle(deck, precision=abi.OR_PREC_SPLIT, device=local, graph=1, block_hex=bh_s, block_shell=bs_s)
-    timed_runs(hs, 0, 1)                      # graph capture + first-touch outside timing
+    timed_runs(hs, cycles, 0, 1)              # graph capture + first-touch outside timing
     sampler = ClockSampler(local)
     sampler.start()
-    ms_split, launches = timed_runs(hs, args.steps, args.warmup)
+    ms_split, launches = timed_runs(hs, cycles, args.steps, args.warmup)
     clocks = sampler.stop()
-    t_split = sum(ms_split) / len(ms_split)
-    d_split = hs.get_nodes()["d"]
+    out_split = outputs(hs)
 
     # ---- plain FP64 form ----
     hd = ECycle(deck, precision=abi.OR_PREC_FP64, device=local, graph=1, block_hex=bh_d, block_shell=bs_d)
-    timed_runs(hd, 0, 1)
-    nfp = max(2, args.steps // 2)
-    ms_fp64, _ = timed_runs(hd, nfp, 1)
-    t_fp64 = sum(ms_fp64) / len(ms_fp64)
-    d_fp64 = hd.get_nodes()["d"]
-    split_err = float(np.abs(d_split - d_fp64).max() / max(np.abs(d_fp64).max(), 1e-300))
-    del hd
+    timed_runs(hd, cycles, 0, 1)
+    ms_fp64, _ = timed_runs(hd, cycles, max(2, args.steps // 2), 1)
+    out_fp64 = outputs(hd)
 
-    # max over ranks of the mean step time
-    tt = torch.tensor([t_split, t_fp64], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-    t_split, t_fp64 = float(tt[0]), float(tt[1])
+    t_split, t_fp64 = max_over_ranks(sum(ms_split) / len(ms_split), sum(ms_fp64) / len(ms_fp64))
     value = nel_job * cycles / (t_split * 1e-3)
     value_fp64 = nel_job * cycles / (t_fp64 * 1e-3)
 
-    # ---- per-kernel device times: each phase kernel launched back to back from a
-    # graph on the state a full run leaves, CUDA events on the handle's stream ----
-    hs.reset()
-    hs.step(cycles)
-    kt = hs.kernel_times(reps=64)            # microseconds per launch; resets the handle
-    s = 4
-    eb_hex = sum(g["ixs"].shape[0] * roofline.hex_bytes(s, g["mat"]["law"]) for p in deck["parts"] for g in p["hex"])
-    eb_shell = sum(g["ixc"].shape[0] * roofline.shell_bytes(s, g["prop"]["npt"]) for p in deck["parts"] for g in p["shell"])
-    eb, nb, _ = roofline.deck_bytes(deck, s)
-    peak, peak_src = roofline.measured_peak()
-    kern = {"hex": (kt["hex"] * 1e-3, eb_hex), "shell": (kt["shell"] * 1e-3, eb_shell), "node": (kt["node"] * 1e-3, nb)}
-    dom = max(kern, key=lambda k: kern[k][0])
-    dom_ms, dom_bytes = kern[dom]
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
-        try:
-            traffic = json.load(open(tpath)).get(args.workload, {}).get(f"{dom}_split")
-        except (OSError, ValueError):
-            traffic = None
-    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9 if dom_ms > 0 else 0.0
-    cyc_bytes = eb + nb
+    # ---- split error per output, against the FP64 run's own floor (1e-12 perturbed
+    # coordinates), at the full cycle count and after 1000 cycles ----
+    accuracy = {"cycles": cycles, "split_vs_fp64": output_errors(out_split, out_fp64),
+                "fp64_floor": output_errors(perturbed_run(hd, deck, cycles), out_fp64),
+                "floor_input_perturbation": 1e-12}
+    if cycles > 1000:
+        hd.reset()
+        hd.step(1000)
+        f1000 = outputs(hd)
+        hs.reset()
+        hs.step(1000)
+        accuracy["at_1000_cycles"] = {"split_vs_fp64": output_errors(outputs(hs), f1000),
+                                      "fp64_floor": output_errors(perturbed_run(hd, deck, 1000), f1000)}
+    hd.close()
+    split_err = accuracy["split_vs_fp64"]["D"]
+
+    roof, per_kernel, cyc_bytes, peak = kernel_roofline(hs, deck, cycles, args.workload)
     cyc_achieved = cyc_bytes * cycles / (t_split * 1e-3) / 1e9
 
     # ---- end to end through the C-ABI with host buffers ----
@@ -336,16 +461,23 @@ def main():
         t1 = time.perf_counter()
         if k >= args.warmup:
             e2e_t.append(t1 - t0)
-    e2e_err = float(np.abs(host_out[0]["d"] - d_split).max() / max(np.abs(d_split).max(), 1e-300))
-    te = torch.tensor([sum(e2e_t) / len(e2e_t)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = nel_job * cycles / float(te[0])
+    d_split = out_split["D"]
+    d_e2e = np.concatenate([hb["d"].ravel() for hb in host_out])
+    e2e_same = bool(np.array_equal(d_e2e, d_split))
+    (te,) = max_over_ranks(sum(e2e_t) / len(e2e_t))
+    e2e_value = nel_job * cycles / te
+    hs.close()
 
     # ---- C5: the adjoint on the sensitivity plate (FP64), next to its forward ----
     adj = None
     if world == 1 and args.workload == "shell_plate":
         adj = adjoint_timing(local)
+
+    # ---- further workloads recorded beside the headline (one GPU) ----
+    subs = {}
+    if world == 1:
+        for name in [w for w in args.sub_workloads.split(",") if w and w != args.workload]:
+            subs[name] = sub_record(name, local, args.sub_steps, args.sub_tile, timed_runs, flush)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -357,39 +489,66 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_split, "higher_is_better": True,
             "scaling": "strong" if sharded else "weak", "vs_baseline": None, "dtype": "f32+f64",
             "data": "synthetic (seeded numpy decks with the workload's shapes)",
-            "config": {"workload": args.workload, "description": WORKLOADS[args.workload][2],
-                       "elements_per_gpu": nel, "nodes_per_gpu": nnod, "cycles_per_step": cycles,
-                       "elements_per_step_all_ranks": nel_job,
-                       "parallelism": (f"parts sharded over {world} ranks" if sharded
-                                       else f"{world} independent replica(s)"),
-                       "precision": "split: FP32 element/material math, FP64 X/D/volumes/energies",
-                       "l2": "256 MB buffer written before every timed step",
-                       "cuda_graph_cycles": 32, "tile_hex": bh_s, "tile_shell": bs_s,
+            "config": workload_config(args.workload, full, cycles, world, sharded),
+            "precision": "split: FP32 element/material math, FP64 X/D/volumes/energies",
+            "tuning": {"cuda_graph_cycles": 32, "tile_hex": bh_s, "tile_shell": bs_s,
                        "autotune_ms_per_cycle": {"split": tune_s, "fp64": tune_d}},
             "fp64": {"value": value_fp64, "ms_per_step": t_fp64, "dtype": "f64", "tile_hex": bh_d, "tile_shell": bs_d},
             "split_over_fp64": value / value_fp64,
             "split_rel_disp_error_vs_fp64": split_err,
-            "roofline": {"bound": "hbm", "kernel": f"{dom}_patch_kernel" if dom != "node" else "node_kernel",
-                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic, "algorithmic_bytes_per_launch": dom_bytes,
-                         "avg_launch_ms": dom_ms, "peak_source": peak_src},
+            "accuracy": accuracy,
+            "roofline": roof,
             "cycle_roofline": {"algorithmic_bytes_per_cycle": cyc_bytes,
                                "bytes_per_element_update": cyc_bytes / nel,
                                "achieved": cyc_achieved, "frac": cyc_achieved / peak,
-                               "kernel_ms_per_cycle": {k: v[0] for k, v in kern.items()}},
+                               "kernels": per_kernel},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "element-updates/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "same_result_as_device_run": e2e_err == 0.0},
+                    "d2h_bytes_per_step": d2h, "same_result_as_device_run": e2e_same},
             "clocks": clocks,
             "gpu_launches": launches,
         }
         if adj is not None:
             line["adjoint"] = adj
+        if subs:
+            line["workloads"] = subs
         print(json.dumps(line), flush=True)
-    del hs
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def sub_record(name, local, steps, tile, timed_runs, flush):
+    """Split and FP64 rates, per-kernel roofline and split error per output of a
+    further workload on this GPU (fixed tile, a few steps, L2 flushed between)."""
+    from openradioss_b200 import abi, decks
+    from openradioss_b200.ecycle import ECycle
+    deck = make_deck(name)
+    cycles = WORKLOADS[name][1]
+    nel = decks.num_elements(deck)
+    hs = ECycle(deck, precision=abi.OR_PREC_SPLIT, device=local, graph=1, block_hex=tile, block_shell=tile)
+    sampler = ClockSampler(local)
+    sampler.start()
+    ms_s, launches = timed_runs(hs, cycles, steps, 3)
+    clocks = sampler.stop()
+    out_s = outputs(hs)
+    hd = ECycle(deck, precision=abi.OR_PREC_FP64, device=local, graph=1, block_hex=tile, block_shell=tile)
+    ms_d, _ = timed_runs(hd, cycles, max(2, steps - 1), 1)
+    out_d = outputs(hd)
+    hd.close()
+    t_s, t_d = sum(ms_s) / len(ms_s), sum(ms_d) / len(ms_d)
+    roof, per_kernel, cyc_bytes, peak = kernel_roofline(hs, deck, cycles, name)
+    hs.close()
+    return {"config": workload_config(name, deck, cycles, 1, False), "steps": steps, "warmup": 3,
+            "value": nel * cycles / (t_s * 1e-3), "ms_per_step": t_s,
+            "fp64": {"value": nel * cycles / (t_d * 1e-3), "ms_per_step": t_d},
+            "split_over_fp64": t_d / t_s, "tile": tile,
+            "split_vs_fp64": output_errors(out_s, out_d),
+            "roofline": roof,
+            "cycle_roofline": {"algorithmic_bytes_per_cycle": cyc_bytes, "bytes_per_element_update": cyc_bytes / nel,
+                               "achieved": cyc_bytes * cycles / (t_s * 1e-3) / 1e9,
+                               "frac": cyc_bytes * cycles / (t_s * 1e-3) / 1e9 / peak, "kernels": per_kernel},
+            "clocks": clocks, "gpu_launches": launches}
 
 
 if __name__ == "__main__":

@@ -286,6 +286,15 @@ int  or_ecycle_launch_count(or_ecycle* h, long long* n);
 int  or_ecycle_stream(or_ecycle* h, void** stream);
 /* Bytes of device memory held by the handle. */
 int  or_ecycle_device_bytes(or_ecycle* h, long long* bytes);
+/* Whether or_ecycle_step runs the handle's cycles in the persistent form: one
+   cooperative launch per call in which each CTA (one per SM) keeps its patches'
+   element state in registers and their nodes in shared memory, with one grid
+   barrier per cycle.  Chosen at finalize for one part of shell groups with no
+   rigid links and no /CLOAD or /PLOAD loads, graph = 1, whose patches fit one
+   wave; OR_ECYCLE_PERSISTENT=0 in the environment turns it off.  Results are bit
+   for bit those of the per-phase kernels.  ctas, threads: its launch shape (0
+   when off; either may be NULL).  No counterpart in the reference. */
+int  or_ecycle_persistent_info(or_ecycle* h, int* on, int* ctas, int* threads);
 
 /* --- domain decomposition (one part split over ranks) ---------------------- */
 /* The reference's SPMD cycle on one mesh: each rank runs a handle with its

@@ -10,7 +10,8 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = [os.path.join(HERE, "csrc", "ecycle.cu"), os.path.join(HERE, "csrc", "ecycle_noalloc.cu")]
-DEPS = SRC + [os.path.join(HERE, "csrc", "ecycle_kernels.cuh"),
+DEPS = SRC + [os.path.join(HERE, "csrc", "ecycle_kernels.cuh"), os.path.join(HERE, "csrc", "persistent_kernel.cuh"),
+              os.path.join(HERE, "csrc", "shell_adjoint.cuh"), os.path.join(HERE, "csrc", "adjoint_kernels.cuh"),
               os.path.join(HERE, "..", "include", "or_ecycle.h")]
 OUT = os.path.join(HERE, "libor_ecycle.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

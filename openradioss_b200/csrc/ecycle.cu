@@ -27,6 +27,7 @@
 
 #include "../../include/or_ecycle.h"
 #include "ecycle_kernels.cuh"
+#include "persistent_kernel.cuh"
 #include "adjoint_kernels.cuh"
 #include "coqini_table.h"
 
@@ -360,6 +361,14 @@ struct Impl {
   DBuf<LoadDesc> loadd; DBuf<FuncDesc> funcd; DBuf<double> funcx, funcy, wacc, wpend;
   DBuf<R> skw; DBuf<int> skew_of;
   int nload = 0;
+  // persistent launch (one part of shells whose state fits on the chip)
+  struct Persist {
+    bool on = false;
+    int G = 0, P = 0, ncmax = 0;
+    size_t smem = 0;
+    DBuf<int> node_ofs, node_glob; DBuf<unsigned char> owner; DBuf<uint2> pconn;
+    DBuf<R4> fslot2, mslot2; DBuf<PartAcc> acc3; DBuf<double> ek, ekr; DBuf<unsigned> sync;
+  } per;
 
   HexArgs<R> hargs() {
     HexArgs<R> a;
@@ -408,6 +417,16 @@ struct Impl {
     dfree(halo_slot); dfree(halo_node); dfree(halo_ke);
     dfree(linkd); dfree(link_nodes); dfree(link_of); dfree(link_mean); dfree(stage);
     dfree(loadd); dfree(funcd); dfree(funcx); dfree(funcy); dfree(wacc); dfree(wpend); dfree(skw); dfree(skew_of);
+    dfree(per.node_ofs); dfree(per.node_glob); dfree(per.owner); dfree(per.pconn); dfree(per.fslot2);
+    dfree(per.mslot2); dfree(per.acc3); dfree(per.ek); dfree(per.ekr); dfree(per.sync);
+  }
+  PersistArgs pargs() {
+    PersistArgs a;
+    a.node_ofs = per.node_ofs.p; a.node_glob = per.node_glob.p; a.owner = per.owner.p; a.pconn = per.pconn.p;
+    a.fslot2 = per.fslot2.p; a.mslot2 = per.mslot2.p; a.acc3 = per.acc3.p; a.ek_node = per.ek.p;
+    a.ekr_node = per.ekr.p; a.sync = per.sync.p; a.patches_per_cta = per.P; a.ncmax = per.ncmax;
+    a.ntiles_node = ntiles;
+    return a;
   }
 };
 
@@ -525,6 +544,124 @@ int set_smem_attrs(or_ecycle* h, Impl<R>& m) {
   CK(set_smem(shell_patch_kernel<R, 64, 5>, ss));
   CK(set_smem(shell_patch_kernel<R, 128, 5>, ss));
   CK(set_smem(shell_patch_kernel<R, 256, 5>, ss));
+  return OR_OK;
+}
+
+// ----------------------------------------------------------------------------
+// persistent launch: eligibility, layout, launch
+// ----------------------------------------------------------------------------
+template <class R>
+using PersistFn = void (*)(ShellArgs<R>, NodeArgs<R>, PersistArgs, int, int, const float*);
+
+template <class R>
+PersistFn<R> persist_fn(int tile, bool npt5) {
+  if (tile == 64) return npt5 ? shell_persistent_kernel<R, 64, 5> : shell_persistent_kernel<R, 64, 0>;
+  if (tile == 128) return npt5 ? shell_persistent_kernel<R, 128, 5> : shell_persistent_kernel<R, 128, 0>;
+  return npt5 ? shell_persistent_kernel<R, 256, 5> : shell_persistent_kernel<R, 256, 0>;
+}
+
+// Sets up the persistent launch when the handle qualifies: step() through a graph
+// (cfg.graph != 0), one part, shell groups only, no rigid links and no /CLOAD or
+// /PLOAD loads (the group pressure is fine), OR_ECYCLE_PERSISTENT not 0, and the
+// patches fit one cooperative wave of at most PERSIST_THREADS threads per CTA.
+// Each CTA takes P consecutive patches (Morton order keeps them compact) and holds
+// every node they touch; nodes no element touches are spread over the CTAs.
+template <class R>
+int persist_build(or_ecycle* h, Impl<R>& m) {
+  auto& q = m.per;
+  q.on = false;
+  if (const char* s = std::getenv("OR_ECYCLE_PERSISTENT"))
+    if (std::atoi(s) == 0) return OR_OK;
+  if (!h->cfg.graph || m.nparts != 1 || !h->hex.empty() || h->shell.empty() || !h->links.empty() || m.nload)
+    return OR_OK;
+  const PatchSet& ps = m.sps;
+  const int tile = h->tile_shell;
+  const int npatch = (int)ps.info.size();
+  const int P = std::max((npatch + h->nsm - 1) / h->nsm, (128 + tile - 1) / tile);
+  if (P * tile > PERSIST_THREADS) return OR_OK;
+  const int G = (npatch + P - 1) / P;
+  std::vector<std::vector<int>> lists(G);
+  std::vector<char> held(m.nnodpad, 0);
+  for (int c = 0; c < G; ++c) {
+    for (int p = c * P; p < std::min(npatch, (c + 1) * P); ++p)
+      for (int j = 0; j < ps.info[p].nloc; ++j) lists[c].push_back(ps.nodes[ps.info[p].node_ofs + j]);
+    std::sort(lists[c].begin(), lists[c].end());
+    lists[c].erase(std::unique(lists[c].begin(), lists[c].end()), lists[c].end());
+    for (int g : lists[c]) held[g] = 1;
+  }
+  const HPart& Pt = h->parts[0];
+  for (int i = 0, k = 0; i < Pt.numnod; ++i)
+    if (!held[Pt.node_start + i]) lists[(k++) % G].push_back(Pt.node_start + i);
+  std::vector<int> ofs(G + 1, 0), glob;
+  std::vector<unsigned char> own;
+  std::vector<int> first(m.nnodpad, -1);
+  int ncmax = 0;
+  for (int c = 0; c < G; ++c) {
+    std::sort(lists[c].begin(), lists[c].end());
+    ncmax = std::max(ncmax, (int)lists[c].size());
+    for (int g : lists[c]) {
+      glob.push_back(g);
+      own.push_back(first[g] < 0 ? 1 : 0);
+      if (first[g] < 0) first[g] = c;
+    }
+    ofs[c + 1] = (int)glob.size();
+  }
+  if (ncmax > 65535) return OR_OK;
+  std::vector<uint2> pconn((size_t)ps.nelpad, make_uint2(0, 0));
+  for (int c = 0; c < G; ++c) {
+    const std::vector<int>& L = lists[c];
+    for (int p = c * P; p < std::min(npatch, (c + 1) * P); ++p) {
+      const PatchInfo& pi = ps.info[p];
+      for (int t = 0; t < pi.nel; ++t) {
+        unsigned l[4];
+        for (int k = 0; k < 4; ++k) {
+          const int g = ps.nodes[pi.node_ofs + (ps.local[(size_t)(pi.elem0 + t) * 4 + k] & LOCAL_MASK)];
+          l[k] = (unsigned)(std::lower_bound(L.begin(), L.end(), g) - L.begin());
+        }
+        pconn[(size_t)pi.elem0 + t] = make_uint2(l[0] | l[1] << 16, l[2] | l[3] << 16);
+      }
+    }
+  }
+  const size_t smem = persist_smem<R>(ncmax, tile, P, m.sinc_stride);
+  if (smem > 200 * 1024) return OR_OK;
+  const PersistFn<R> fn = persist_fn<R>(tile, m.uniform_npt == 5);
+  CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int nb = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, P * tile, smem));
+  if (nb < 1 || G > nb * h->nsm) return OR_OK;
+  int rc;
+  if ((rc = dput(h, q.node_ofs, ofs)) || (rc = dput(h, q.node_glob, glob)) || (rc = dput(h, q.owner, own)) ||
+      (rc = dput(h, q.pconn, pconn)) || (rc = dalloc(h, q.fslot2, (size_t)m.nslot)) ||
+      (rc = dalloc(h, q.mslot2, (size_t)m.nslot)) || (rc = dalloc(h, q.acc3, 3)) || (rc = dalloc(h, q.sync, 2)) ||
+      (rc = dput(h, q.ek, std::vector<double>(m.nnodpad, 0.0))) ||
+      (rc = dput(h, q.ekr, std::vector<double>(m.nnodpad, 0.0))))
+    return rc;
+  q.on = true;
+  q.G = G; q.P = P; q.ncmax = ncmax; q.smem = smem;
+  return OR_OK;
+}
+
+// ncycles cycles in one cooperative launch, from the time state of parity0
+template <class R>
+int launch_persistent(or_ecycle* h, Impl<R>& m, int ncycles, int parity0) {
+  auto& q = m.per;
+  CK(cudaMemsetAsync(q.sync.p, 0, 2 * sizeof(unsigned), h->stream));
+  CK(cudaMemsetAsync(q.acc3.p, 0xff, 3 * sizeof(PartAcc), h->stream));
+  ShellArgs<R> sa = m.sargs();
+  NodeArgs<R> na = m.nargs(h);
+  PersistArgs pa = m.pargs();
+  const float* zw = m.zw.p;
+  void* args[] = {&sa, &na, &pa, &ncycles, &parity0, &zw};
+  const PersistFn<R> fn = persist_fn<R>(h->tile_shell, m.uniform_npt == 5);
+  const cudaError_t e =
+      cudaLaunchCooperativeKernel((const void*)fn, dim3(q.G), dim3(q.P * h->tile_shell), args, q.smem, h->stream);
+  if (e == cudaErrorCooperativeLaunchTooLarge) {   // the wave no longer fits (another context holds SMs):
+    cudaGetLastError();                             // the per-phase kernels take over for good
+    q.on = false;
+    return -1;
+  }
+  CK(e);
+  h->launches++;
   return OR_OK;
 }
 
@@ -830,6 +967,7 @@ int finalize_impl(or_ecycle* h) {
   }
   rc = set_smem_attrs<R>(h, m);
   if (rc) return rc;
+  if ((rc = persist_build<R>(h, m))) return rc;
   CK(cudaDeviceSynchronize());
   return OR_OK;
 }
@@ -938,7 +1076,17 @@ int step_impl(or_ecycle* h, int ncycles, or_ecycle_time* t) {
   int rc;
   const bool use_graph = h->cfg.graph != 0;
   int done = 0;
-  if (use_graph && ncycles >= GRAPH_CYCLES) {
+  if (m.per.on) {            // every cycle in cooperative launches of an even number of cycles
+    constexpr int CHUNK = 1 << 20;
+    while (done < ncycles) {
+      const int nc = std::min(CHUNK, ncycles - done);
+      rc = launch_persistent<R>(h, m, nc, done & 1);
+      if (rc < 0) break;       // fell back: the remaining cycles run below
+      if (rc) return rc;
+      done += nc;
+    }
+  }
+  if (use_graph && ncycles - done >= GRAPH_CYCLES) {
     if (!h->graph_exec) {
       CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
       long long l0 = h->launches;
@@ -1266,6 +1414,7 @@ void destroy_impl(or_ecycle* h) {
 template <class R>
 int set_halo_impl(or_ecycle* h, int nloc, const int* local_node, const int* slot, const int* count_ke, int nhalo) {
   Impl<R>& m = *(Impl<R>*)h->impl;
+  m.per.on = false;            // a domain of a split mesh runs the phase kernels
   const HPart& P = h->parts[0];
   std::vector<int> hs(m.nnodpad, -1), hn(std::max(nhalo, 1), -1);
   std::vector<unsigned char> ke(m.nnodpad, 1);
@@ -2174,6 +2323,23 @@ int or_ecycle_stream(or_ecycle* h, void** stream) {
 int or_ecycle_device_bytes(or_ecycle* h, long long* bytes) {
   if (!h || !bytes) return OR_E_ARG;
   *bytes = h->dev_bytes;
+  return OR_OK;
+}
+
+int or_ecycle_persistent_info(or_ecycle* h, int* on, int* ctas, int* threads) {
+  if (!h || !on) return OR_E_ARG;
+  if (!h->finalized) return fail(h, OR_E_STATE, "persistent_info before finalize");
+  int g = 0, t = 0, o = 0;
+  if (h->cfg.precision == OR_PREC_SPLIT) {
+    const auto& q = ((Impl<float>*)h->impl)->per;
+    o = q.on; g = q.G; t = q.P * h->tile_shell;
+  } else {
+    const auto& q = ((Impl<double>*)h->impl)->per;
+    o = q.on; g = q.G; t = q.P * h->tile_shell;
+  }
+  *on = o;
+  if (ctas) *ctas = o ? g : 0;
+  if (threads) *threads = o ? t : 0;
   return OR_OK;
 }
 

@@ -813,6 +813,394 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
 
 
 // ===========================================================================
+// one BT shell element (CFORC3 chain), shared by the patch kernel and the
+// persistent kernel
+// ===========================================================================
+// Element state of one shell, held in registers by the thread that computes it.
+// NPT > 0: the integration-point state too (NPT points); NPT = 0: the points'
+// state stays in memory and is read and written point by point.
+template <class R, int NPT>
+struct ShellState {
+  static constexpr int NP = NPT > 0 ? NPT : 1;
+  R thk, thke, h[3], e[2], jca;
+  R sig[NP][5], pla[NP];
+  int degen, eid;
+};
+
+template <class R, int NPT>
+__device__ __forceinline__ void shell_load_state(const ShellArgs<R>& a, int e, ShellState<R, NPT>& st) {
+  const int nelpad = a.nelpad;
+  st.thk = a.thk[e];
+  st.thke = a.thke[e];
+  st.h[0] = a.hourg[0 * nelpad + e]; st.h[1] = a.hourg[1 * nelpad + e]; st.h[2] = a.hourg[2 * nelpad + e];
+  st.e[0] = a.eint[0 * nelpad + e]; st.e[1] = a.eint[1 * nelpad + e];
+  st.jca = a.jca ? a.jca[e] : R(0);
+  st.degen = a.degen[e];
+  st.eid = a.elem_id[e];
+  if (NPT > 0) {
+#pragma unroll
+    for (int ip = 0; ip < ShellState<R, NPT>::NP; ++ip) {
+#pragma unroll
+      for (int c = 0; c < 5; ++c) st.sig[ip][c] = a.sig[(ip * 5 + c) * nelpad + e];
+      st.pla[ip] = a.pla[ip * nelpad + e];
+    }
+  }
+}
+
+// Writes back the state that shell_element<KEEP = true> kept in registers.
+template <class R, int NPT>
+__device__ __forceinline__ void shell_store_state(const ShellArgs<R>& a, int e, const ShellState<R, NPT>& st) {
+  static_assert(NPT > 0, "kept state needs a fixed number of integration points");
+  const int nelpad = a.nelpad;
+  a.thk[e] = st.thk;
+  a.hourg[0 * nelpad + e] = st.h[0]; a.hourg[1 * nelpad + e] = st.h[1]; a.hourg[2 * nelpad + e] = st.h[2];
+  a.eint[0 * nelpad + e] = st.e[0]; a.eint[1 * nelpad + e] = st.e[1];
+#pragma unroll
+  for (int ip = 0; ip < NPT; ++ip) {
+#pragma unroll
+    for (int c = 0; c < 5; ++c) a.sig[(ip * 5 + c) * nelpad + e] = st.sig[ip][c];
+    a.pla[ip * nelpad + e] = st.pla[ip];
+  }
+}
+
+// CCOOR3 (from nodal planes in shared memory: x, y, z in FP64 and vx vy vz rx ry rz
+// in R, stride NLM, corner k at index lc[k]), CNVEC3, CDERI3, CCOEF3, CDLEN3,
+// CDEFO3, CCURV3, CSTRA3, MULAWC (SIGEPS01C / SIGEPS02C -> M2CPLR per
+// integration point), CHVIS3, CDT3, CFINT3, the group pressure; corner forces and
+// moments out in global axes with CUPDT3P signs.  KEEP = false writes the new
+// state to memory at index e, as each quantity is formed; KEEP = true leaves it
+// in st (for a caller that keeps the state in registers across cycles).
+template <class R, int NPT, bool KEEP>
+__device__ __forceinline__ void shell_element(const ShellArgs<R>& a, const int e, const ShellGroupDesc& gd,
+                                              const R DT1, const float* __restrict__ zw, const double* sx,
+                                              const double* sy, const double* sz, const R* sv, const int NLM,
+                                              const int (&lc)[4], ShellState<R, NPT>& st, R (&Fg)[3][4],
+                                              R (&Mg)[3][4], unsigned long long& mykey, unsigned long long& mybits,
+                                              double& my_ehou, double& my_wpla) {
+  static_assert(!KEEP || NPT > 0, "kept state needs a fixed number of integration points");
+  const int nelpad = a.nelpad;
+  const R OFF = R(1);
+  // coordinate differences in FP64, cast to R (CNVEC3 / CDERI3 inputs)
+  const double x1 = sx[lc[0]], y1 = sy[lc[0]], z1 = sz[lc[0]];
+  const R X21 = R(sx[lc[1]] - x1), Y21 = R(sy[lc[1]] - y1), Z21 = R(sz[lc[1]] - z1);
+  const R X31 = R(sx[lc[2]] - x1), Y31 = R(sy[lc[2]] - y1), Z31 = R(sz[lc[2]] - z1);
+  const R X41 = R(sx[lc[3]] - x1), Y41 = R(sy[lc[3]] - y1), Z41 = R(sz[lc[3]] - z1);
+  const R X32 = R(sx[lc[2]] - sx[lc[1]]), Y32 = R(sy[lc[2]] - sy[lc[1]]), Z32 = R(sz[lc[2]] - sz[lc[1]]);
+  const R X34 = R(sx[lc[2]] - sx[lc[3]]), Y34 = R(sy[lc[2]] - sy[lc[3]]), Z34 = R(sz[lc[2]] - sz[lc[3]]);
+  // ---- CNVEC3, ISHFRAM = 0 (cnvec3.F:66-81) or 2 (cnvec3.F:82-106) ----
+  R E1X = X21 + X34, E1Y = Y21 + Y34, E1Z = Z21 + Z34;
+  R E2X = X32 + X41, E2Y = Y32 + Y41, E2Z = Z32 + Z41;
+  R E3X = E1Y * E2Z - E1Z * E2Y, E3Y = E1Z * E2X - E1X * E2Z, E3Z = E1X * E2Y - E1Y * E2X;
+  if (gd.ishfram == 2) {
+    R su = E2X * E2X + E2Y * E2Y + E2Z * E2Z;
+    E1X = E1X * su + E2Y * E3Z - E2Z * E3Y;
+    E1Y = E1Y * su + E2Z * E3X - E2X * E3Z;
+    E1Z = E1Z * su + E2X * E3Y - E2Y * E3X;
+    su = ssqrt(E1X * E1X + E1Y * E1Y + E1Z * E1Z);
+    su = R(1) / (su > R(EM20) ? su : R(EM20));
+    E1X *= su; E1Y *= su; E1Z *= su;
+    su = ssqrt(E3X * E3X + E3Y * E3Y + E3Z * E3Z);
+    su = R(1) / (su > R(EM20) ? su : R(EM20));
+    E3X *= su; E3Y *= su; E3Z *= su;
+    E2X = E3Y * E1Z - E3Z * E1Y; E2Y = E3Z * E1X - E3X * E1Z; E2Z = E3X * E1Y - E3Y * E1X;
+    su = ssqrt(E2X * E2X + E2Y * E2Y + E2Z * E2Z);
+    su = R(1) / (su > R(EM20) ? su : R(EM20));
+    E2X *= su; E2Y *= su; E2Z *= su;
+  } else {
+    R su = E3X * E3X + E3Y * E3Y + E3Z * E3Z;
+    su = ssqrt(su);
+    su = R(1) / (su > R(EM20) ? su : R(EM20));
+    E3X *= su; E3Y *= su; E3Z *= su;
+    const R q1 = E1X * E1X + E1Y * E1Y + E1Z * E1Z;
+    const R q2 = E2X * E2X + E2Y * E2Y + E2Z * E2Z;
+    su = ssqrt(q1 / q2);
+    E1X = E1X + (E2Y * E3Z - E2Z * E3Y) * su;
+    E1Y = E1Y + (E2Z * E3X - E2X * E3Z) * su;
+    E1Z = E1Z + (E2X * E3Y - E2Y * E3X) * su;
+    su = ssqrt(E1X * E1X + E1Y * E1Y + E1Z * E1Z);
+    su = R(1) / (su > R(EM20) ? su : R(EM20));
+    E1X *= su; E1Y *= su; E1Z *= su;
+    E2X = E3Y * E1Z - E3Z * E1Y; E2Y = E3Z * E1X - E3X * E1Z; E2Z = E3X * E1Y - E3Y * E1X;
+  }
+  // ---- CDERI3 (cderi3.F:87-190) ----
+  const R X2 = E1X * X21 + E1Y * Y21 + E1Z * Z21;
+  const R Y2 = E2X * X21 + E2Y * Y21 + E2Z * Z21;
+  const R Y3 = E2X * X31 + E2Y * Y31 + E2Z * Z31;
+  const R X3 = E1X * X31 + E1Y * Y31 + E1Z * Z31;
+  const R X4 = E1X * X41 + E1Y * Y41 + E1Z * Z41;
+  const R Y4 = E2X * X41 + E2Y * Y41 + E2Z * Z41;
+  const R PX1 = R(0.5) * (Y2 - Y4), PY1 = R(0.5) * (X4 - X2), PX2 = R(0.5) * Y3, PY2 = -R(0.5) * X3;
+  R AREA = R(2) * (PY2 * PX1 - PY1 * PX2);
+  AREA = AREA > R(EM20) ? AREA : R(EM20);
+  const R VHX = (-X2 + X3 - X4) / AREA, VHY = (-Y2 + Y3 - Y4) / AREA;
+  // ---- CCOEF3 (ccoef3.F:66-160) ----
+  const R THK0 = gd.ithk > 0 ? st.thk : st.thke;
+  const R VOL0 = THK0 * AREA;
+  const R THK02 = THK0 * THK0;
+  const R RHO = R(gd.rho0), YM = R(gd.young), NU = R(gd.nu), GG = R(gd.shear);
+  const R A11 = R(gd.a11), A12 = R(gd.a12), SSP = R(gd.ssp);
+  const R H1 = R(gd.hm), H2 = R(gd.hf), H3 = R(gd.hr);
+  const int npt = NPT > 0 ? NPT : gd.npt;
+  const R SHF = npt == 1 ? R(0) : R(gd.shf);
+  const R GS = GG * SHF;
+  // ---- CDLEN3 (cdlen3.F:69-121) ----
+  R ALDT;
+  {
+    const R AL1 = X2 * X2 + Y2 * Y2;
+    const R AL2 = (X3 - X2) * (X3 - X2) + (Y3 - Y2) * (Y3 - Y2);
+    const R AL6 = X3 * X3 + Y3 * Y3;
+    const R AL3 = (X4 - X3) * (X4 - X3) + (Y4 - Y3) * (Y4 - Y3);
+    const R AL4 = X4 * X4 + Y4 * Y4;
+    const R AL5 = (X4 - X2) * (X4 - X2) + (Y4 - Y2) * (Y4 - Y2);
+    R ALMIN = fmin(fmin(AL1, AL2), AL4);
+    const R ALQ = fmin(fmin(AL3, AL5), AL6);
+    if (AL3 != R(0)) ALMIN = fmin(ALMIN, ALQ);
+    R m56 = fmax(AL5, AL6);
+    m56 = m56 > R(EM20) ? m56 : R(EM20);
+    const R DTDYN = AREA * AREA / m56;
+    ALDT = fmax(DTDYN, ALMIN);
+    const R DTHOUR = R(0.5) * (ALMIN + ALDT) / fmax(H1, H2);
+    if (DTHOUR < ALDT) ALDT = DTHOUR;
+    ALDT = ssqrt(ALDT);
+  }
+  // ---- CDEFO3, IHBE <= 1 (cdefo3.F:84-131) ----
+  R VXl[4], VYl[4], VZl[4], RXl[4], RYl[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const R vx = sv[0 * NLM + lc[k]], vy = sv[1 * NLM + lc[k]], vz = sv[2 * NLM + lc[k]];
+    VXl[k] = E1X * vx + E1Y * vy + E1Z * vz;
+    VYl[k] = E2X * vx + E2Y * vy + E2Z * vz;
+    VZl[k] = E3X * vx + E3Y * vy + E3Z * vz;
+    const R rx = sv[3 * NLM + lc[k]], ry = sv[4 * NLM + lc[k]], rz = sv[5 * NLM + lc[k]];
+    RXl[k] = E1X * rx + E1Y * ry + E1Z * rz;
+    RYl[k] = E2X * rx + E2Y * ry + E2Z * rz;
+  }
+  R EXX, EYY, EXY, EXZ, EYZ, KXX, KYY, KXY;
+  {
+    const R VZ13 = VZl[0] - VZl[2], VZ24 = VZl[1] - VZl[3];
+    EYZ = PY1 * VZ13 + PY2 * VZ24;
+    EXZ = PX1 * VZ13 + PX2 * VZ24;
+    const R DT1V4 = R(0.25) * DT1;
+    const R t2a = PY2 + PY1;
+    const R t3a = copysign(fmax(fabs(t2a), R(EM20)), t2a);
+    const R t1a = DT1V4 * (VZ13 - VZ24) * (VZ13 - VZ24) / t3a;
+    const R VX13 = VXl[0] - VXl[2] - t1a, VX24 = VXl[1] - VXl[3] + t1a;
+    EXX = PX1 * VX13 + PX2 * VX24;
+    EXY = PY1 * VX13 + PY2 * VX24;
+    const R t1b = PX2 - PX1;
+    const R t3b = copysign(fmax(fabs(t1b), R(EM20)), t1b);
+    const R t2b = DT1V4 * (VZ13 + VZ24) * (VZ13 + VZ24) / t3b;
+    const R VY13 = VYl[0] - VYl[2] + t2b, VY24 = VYl[1] - VYl[3] + t2b;
+    EXY = EXY + PX1 * VY13 + PX2 * VY24;
+    EYY = PY1 * VY13 + PY2 * VY24;
+    // ---- CCURV3 (ccurv3.F:61-86) ----
+    const R RX13 = RXl[0] - RXl[2], RXAV = RXl[0] + RXl[1] + RXl[2] + RXl[3], RX24 = RXl[1] - RXl[3];
+    KYY = -PY1 * RX13 - PY2 * RX24;
+    R kxy = PX1 * RX13 + PX2 * RX24;
+    const R RY13 = RYl[0] - RYl[2], RYAV = RYl[0] + RYl[1] + RYl[2] + RYl[3], RY24 = RYl[1] - RYl[3];
+    KXX = PX1 * RY13 + PX2 * RY24;
+    KXY = PY1 * RY13 + PY2 * RY24 - kxy;
+    EXZ = EXZ + RYAV * (R(0.25) * AREA);
+    EYZ = EYZ - RXAV * (R(0.25) * AREA);
+    // ---- CSTRA3 (cstra3.F:91-101) ----
+    const R FAC1 = DT1 / AREA;
+    EXX *= FAC1; EYY *= FAC1; EXY *= FAC1; EYZ *= FAC1; EXZ *= FAC1;
+    KXX *= FAC1; KYY *= FAC1; KXY *= FAC1;
+  }
+  // ---- MULAWC layer loop (mulawc.F90:530-560, 596-1100, 2603-2620, 2930-2990) ----
+  const float* Z0 = zw + (npt - 1) * 33;      // [Z0 | WF | WM] of the npt-point rule
+  const float* WF = Z0 + 11;
+  const float* WM = Z0 + 22;
+  R FOR[5] = {R(0), R(0), R(0), R(0), R(0)}, MOM[3] = {R(0), R(0), R(0)};
+  R FOLD[5] = {R(0), R(0), R(0), R(0), R(0)}, MOLD[3] = {R(0), R(0), R(0)};
+  R THKN = st.thk;
+  const R CA = gd.has_jca ? st.jca : R(gd.jc_a);
+  const R CB = R(gd.jc_b), CN = R(gd.jc_n), YMAX = R(gd.sigmax);
+  double wpla = 0.0;
+#pragma unroll
+  for (int ip = 0; ip < (NPT > 0 ? NPT : 10); ++ip) {
+    if (NPT == 0 && ip >= npt) break;
+    const R wf = R(NPT == 5 ? coq5(1, ip) : WF[ip]), wm = R(NPT == 5 ? coq5(2, ip) : WM[ip]);
+    R SO[5], SN[5];
+    if (NPT > 0) {
+#pragma unroll
+      for (int c = 0; c < 5; ++c) SO[c] = st.sig[NPT > 0 ? ip : 0][c];
+    } else {
+#pragma unroll
+      for (int c = 0; c < 5; ++c) SO[c] = a.sig[(ip * 5 + c) * nelpad + e];
+    }
+#pragma unroll
+    for (int c = 0; c < 5; ++c) FOLD[c] = FOLD[c] + wf * SO[c];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) MOLD[c] = MOLD[c] + wm * SO[c];
+    const R THKLYL = wf * THK0;
+    const R ZT = R(NPT == 5 ? coq5(0, ip) : Z0[ip]) * THK0;
+    const R DXX = EXX + ZT * KXX, DYY = EYY + ZT * KYY, DXY = EXY + ZT * KXY;
+    R EZZ = R(0);
+    if (gd.law == 1) {
+      // SIGEPS01C (sigeps01c.F:130-146)
+      SN[0] = SO[0] + A11 * DXX + A12 * DYY;
+      SN[1] = SO[1] + A12 * DXX + A11 * DYY;
+      SN[2] = SO[2] + GG * DXY;
+      SN[3] = SO[3] + GS * EYZ;
+      SN[4] = SO[4] + GS * EXZ;
+      EZZ = -NU * (DXX + DYY) / (R(1) - NU);
+    } else {
+      // SIGEPS02C -> M2CPLR, IPLA = 0 radial return (m2cplr.F:96-230)
+      const R A1 = YM / (R(1) - NU * NU), A2 = A1 * NU;
+      SN[0] = SO[0] + A1 * DXX + A2 * DYY;
+      SN[1] = SO[1] + A2 * DXX + A1 * DYY;
+      SN[2] = SO[2] + GG * DXY;
+      SN[3] = SO[3] + GS * EYZ;
+      SN[4] = SO[4] + GS * EXZ;
+      R PLA = NPT > 0 ? st.pla[NPT > 0 ? ip : 0] : a.pla[ip * nelpad + e];
+      R YLD = PLA == R(0) ? CA : CA + CB * exp_(CN * log_(PLA));
+      YLD = fmin(YLD, YMAX);
+      const R SVM = ssqrt(SN[0] * SN[0] + SN[1] * SN[1] - SN[0] * SN[1] + R(3) * SN[2] * SN[2]);
+      const R RR = fmin(R(1), YLD / (SVM + R(EM15)));
+      R DPLA = R(0);
+      if (RR < R(1)) {
+        SN[0] *= RR; SN[1] *= RR; SN[2] *= RR;
+        DPLA = OFF * fmax(R(0), (SVM - YLD) / YM);
+        EZZ = DPLA * (R(0.5) * (SN[0] + SN[1])) / YLD;
+        PLA = PLA + DPLA;
+        if (KEEP) st.pla[NPT > 0 ? ip : 0] = PLA;
+        else a.pla[ip * nelpad + e] = PLA;
+      }
+      EZZ = -(DXX + DYY) * NU - (R(1) - R(2) * NU) * EZZ;   // sigeps02c.F:215-224
+      EZZ = EZZ / (R(1) - NU);
+      wpla += (double)YLD * (double)DPLA * (double)AREA * (double)THKLYL;
+    }
+    THKN = THKN + EZZ * THKLYL * OFF;
+    if (KEEP) {
+#pragma unroll
+      for (int c = 0; c < 5; ++c) st.sig[NPT > 0 ? ip : 0][c] = SN[c];
+    } else {
+#pragma unroll
+      for (int c = 0; c < 5; ++c) a.sig[(ip * 5 + c) * nelpad + e] = SN[c];
+    }
+#pragma unroll
+    for (int c = 0; c < 5; ++c) FOR[c] = FOR[c] + wf * SN[c];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) MOM[c] = MOM[c] + wm * SN[c];
+  }
+  my_wpla = wpla;
+  if (KEEP) st.thk = THKN > R(EM30) ? THKN : R(EM30);
+  else a.thk[e] = THKN > R(EM30) ? THKN : R(EM30);
+  {
+    const R DEGMB = FOLD[0] * EXX + FOLD[1] * EYY + FOLD[2] * EXY + FOLD[3] * EYZ + FOLD[4] * EXZ +
+                    (FOR[0] * EXX + FOR[1] * EYY + FOR[2] * EXY + FOR[3] * EYZ + FOR[4] * EXZ);
+    const R DEGFX = MOLD[0] * KXX + MOLD[1] * KYY + MOLD[2] * KXY +
+                    (MOM[0] * KXX + MOM[1] * KYY + MOM[2] * KXY);
+    const R VOL2 = R(0.5) * VOL0;
+    if (KEEP) {
+      st.e[0] = st.e[0] + DEGMB * VOL2;
+      st.e[1] = st.e[1] + DEGFX * THK0 * VOL2;
+    } else {
+      a.eint[0 * nelpad + e] = st.e[0] + DEGMB * VOL2;
+      a.eint[1 * nelpad + e] = st.e[1] + DEGFX * THK0 * VOL2;
+    }
+  }
+  // ---- CHVIS3, ISMSTR = 2, IHBE = 1, HELAS = HVISC = 1/2, HVLIN = 0 (chvis3.F:116-300) ----
+  R H1j[3], H2j[3], H3j[3], HOUR4, HOUR5;
+  {
+    const R px1v = PX1 * VHX, px2v = PX2 * VHX, py1v = PY1 * VHY, py2v = PY2 * VHY;
+    R GAMA[4];
+    GAMA[0] = OFF * (R(1) - px1v - py1v);
+    GAMA[2] = OFF * (R(1) + px1v + py1v);
+    GAMA[1] = OFF * (-R(1) - px2v - py2v);
+    GAMA[3] = OFF * (-R(1) + px2v + py2v);
+    const R SHFPR3 = SHF / (R(3) * (R(1) + NU));
+    const R R1 = R(0.25) * RHO * R(100);
+    const R A1c = R1 * (R(0.5) * H1);
+    const R A3c = R1 * (R(0.5) * H2) * ssqrt(SHFPR3);
+    const R A5c = R(0.5) * H3 * R1 * R(0.072169);
+    const R R0e = R(0.25) * YM * R(0.5);
+    const R A7c = H1 * R0e, A8c = H2 * R0e * SHFPR3;
+    const R T2A = THK02 * AREA;
+    R H1Q = A1c * ssqrt(T2A), H2Q = A3c * THK02, H3Q = A5c * T2A;
+    const R TD = THK0 * DT1;
+    R HH1 = A7c * TD;
+    const R B1 = PX1 * PX1 + PY1 * PY1, B2 = PX2 * PX2 + PY2 * PY2;
+    R HH2 = A8c * THK02 * TD / (B1 + B2);
+    if (st.degen) { H1Q = H2Q = H3Q = HH1 = HH2 = R(0); }
+    R HG1 = VXl[0] * GAMA[0] + VXl[1] * GAMA[1] + VXl[2] * GAMA[2] + VXl[3] * GAMA[3];
+    R HG2 = VYl[0] * GAMA[0] + VYl[1] * GAMA[1] + VYl[2] * GAMA[2] + VYl[3] * GAMA[3];
+    const R hour1 = st.h[0] + HG1 * HH1;
+    const R hour2 = st.h[1] + HG2 * HH1;
+    const R HOUR1A = hour1 + HG1 * (H1Q * fabs(HG1));
+    const R HOUR2A = hour2 + HG2 * (H1Q * fabs(HG2));
+#pragma unroll
+    for (int k = 0; k < 3; ++k) { H1j[k] = HOUR1A * GAMA[k]; H2j[k] = HOUR2A * GAMA[k]; }
+    R EHOU = HOUR1A * HG1 + HOUR2A * HG2;
+    HG1 = VZl[0] * GAMA[0] + VZl[1] * GAMA[1] + VZl[2] * GAMA[2] + VZl[3] * GAMA[3];
+    const R hour3 = st.h[2] + HG1 * HH2;
+    const R HOUR3A = hour3 + HG1 * (H2Q * fabs(HG1));
+#pragma unroll
+    for (int k = 0; k < 3; ++k) H3j[k] = HOUR3A * GAMA[k];
+    EHOU = EHOU + HOUR3A * HG1;
+    HG1 = RXl[0] - RXl[1] + RXl[2] - RXl[3];
+    HG2 = RYl[0] - RYl[1] + RYl[2] - RYl[3];
+    HOUR4 = HG1 * (H3Q * fabs(HG1));
+    HOUR5 = HG2 * (H3Q * fabs(HG2));
+    EHOU = EHOU + HOUR4 * HG1 + HOUR5 * HG2;
+    my_ehou = (double)(DT1 * EHOU * OFF);
+    if (KEEP) { st.h[0] = hour1; st.h[1] = hour2; st.h[2] = hour3; }
+    else { a.hourg[0 * nelpad + e] = hour1; a.hourg[1 * nelpad + e] = hour2; a.hourg[2 * nelpad + e] = hour3; }
+  }
+  // ---- CDT3 (cdt3.F:110-115, 203-214) ----
+  {
+    const R DT = R(gd.dtfac) * ALDT / SSP;
+    if ((double)DT <= gd.dtmin) raise_error(a.err, 5, st.eid);
+    mykey = dt_key((double)DT, 3, st.eid);
+    mybits = (unsigned long long)__double_as_longlong((double)DT);
+  }
+  // ---- CFINT3, ISIGI = 0 (cfint3.F:173-260) ----
+  {
+    const R F1A = FOR[0] * THK0, F2A = FOR[1] * THK0, F3A = FOR[2] * THK0, F4A = FOR[3] * THK0, F5A = FOR[4] * THK0;
+    const R M4 = R(0.25) * (F4A * AREA), M5 = R(0.25) * (F5A * AREA);
+    const R F12 = F1A * PX2 + F3A * PY2, F22 = F2A * PY2 + F3A * PX2, F32 = F5A * PX2 + F4A * PY2;
+    const R F11 = F1A * PX1 + F3A * PY1, F21 = F2A * PY1 + F3A * PX1, F31 = F5A * PX1 + F4A * PY1;
+    const R Gc[3][3] = {{F11 + H1j[0], F12 + H1j[1], H1j[2] - F11},
+                        {F21 + H2j[0], F22 + H2j[1], H2j[2] - F21},
+                        {F31 + H3j[0], F32 + H3j[1], H3j[2] - F31}};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      Fg[0][k] = E1X * Gc[0][k] + E2X * Gc[1][k] + E3X * Gc[2][k];
+      Fg[1][k] = E1Y * Gc[0][k] + E2Y * Gc[1][k] + E3Y * Gc[2][k];
+      Fg[2][k] = E1Z * Gc[0][k] + E2Z * Gc[1][k] + E3Z * Gc[2][k];
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) Fg[c][3] = -Fg[c][0] - Fg[c][1] - Fg[c][2];
+    const R M1A = MOM[0] * THK02, M2A = MOM[1] * THK02, M3A = MOM[2] * THK02;
+    const R M11 = -M2A * PY1 - M3A * PX1, M21 = M1A * PX1 + M3A * PY1;
+    const R M12 = -M2A * PY2 - M3A * PX2, M22 = M1A * PX2 + M3A * PY2;
+    const R G1m[4] = {M11 - M4 + HOUR4 * OFF, M12 - M4 - HOUR4 * OFF, -M11 - M4 + HOUR4 * OFF, -M12 - M4 - HOUR4 * OFF};
+    const R G2m[4] = {M21 + M5 + HOUR5 * OFF, M22 + M5 - HOUR5 * OFF, -M21 + M5 + HOUR5 * OFF, -M22 + M5 - HOUR5 * OFF};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      Mg[0][k] = E1X * G1m[k] + E2X * G2m[k];
+      Mg[1][k] = E1Y * G1m[k] + E2Y * G2m[k];
+      Mg[2][k] = E1Z * G1m[k] + E2Z * G2m[k];
+    }
+  }
+  // ---- uniform pressure (load_pressure.F:201-207): F = -p N / 8, N = x13 x x24 ----
+  R PF[3] = {R(0), R(0), R(0)};
+  if (gd.pressure != 0.0) {
+    const double ax = sx[lc[2]] - x1, ay = sy[lc[2]] - y1, az = sz[lc[2]] - z1;
+    const double bx = sx[lc[3]] - sx[lc[1]], by = sy[lc[3]] - sy[lc[1]], bz = sz[lc[3]] - sz[lc[1]];
+    const R NX = R(ay * bz - az * by), NY = R(az * bx - ax * bz), NZ = R(ax * by - ay * bx);
+    const R AA = -R(gd.pressure) * R(0.125);
+    PF[0] = AA * NX; PF[1] = AA * NY; PF[2] = AA * NZ;
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    Fg[0][k] = -Fg[0][k] + PF[0]; Fg[1][k] = -Fg[1][k] + PF[1]; Fg[2][k] = -Fg[2][k] + PF[2];
+    Mg[0][k] = -Mg[0][k]; Mg[1][k] = -Mg[1][k]; Mg[2][k] = -Mg[2][k];
+  }
+}
+
+// ===========================================================================
 // shell patch kernel
 // ===========================================================================
 // Per element (thread): CCOOR3, CNVEC3, CDERI3, CCOEF3, CDLEN3, CDEFO3, CCURV3,
@@ -848,30 +1236,10 @@ shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
   unsigned short* sinc = reinterpret_cast<unsigned short*>(sc + 24 * TILE);
   const int nelpad = a.nelpad;
   // per-element loads issued before the staging barrier (overlap with the gathers)
-  constexpr int NP = NPT > 0 ? NPT : 1;
-  uint2 cw = make_uint2(0, 0);
-  R st_thk = R(1), st_thke = R(1), st_h0 = R(0), st_h1 = R(0), st_h2 = R(0), st_e0 = R(0), st_e1 = R(0);
-  R st_jca = R(0);
-  R st_sig[NP][5], st_pla[NP];
-  int st_degen = 0, st_eid = 0;
-  {   // padding elements (tid >= nel) hold valid state: load unconditionally
-    cw = a.conn[e];
-    st_thk = a.thk[e];
-    st_thke = a.thke[e];
-    st_h0 = a.hourg[0 * nelpad + e]; st_h1 = a.hourg[1 * nelpad + e]; st_h2 = a.hourg[2 * nelpad + e];
-    st_e0 = a.eint[0 * nelpad + e]; st_e1 = a.eint[1 * nelpad + e];
-    if (a.jca) st_jca = a.jca[e];
-    st_degen = a.degen[e];
-    st_eid = a.elem_id[e];
-    if (NPT > 0) {
-#pragma unroll
-      for (int ip = 0; ip < NP; ++ip) {
-#pragma unroll
-        for (int c = 0; c < 5; ++c) st_sig[ip][c] = a.sig[(ip * 5 + c) * nelpad + e];
-        st_pla[ip] = a.pla[ip * nelpad + e];
-      }
-    }
-  }
+  // padding elements (tid >= nel) hold valid state: load unconditionally
+  const uint2 cw = a.conn[e];
+  ShellState<R, NPT> st;
+  shell_load_state<R, NPT>(a, e, st);
   {
     const unsigned* src = reinterpret_cast<const unsigned*>(a.inc + (size_t)p * a.inc_stride);
     unsigned* dst = reinterpret_cast<unsigned*>(sinc);
@@ -909,312 +1277,8 @@ shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
     lc[0] = cw.x & 0xffffu; lc[1] = cw.x >> 16; lc[2] = cw.y & 0xffffu; lc[3] = cw.y >> 16;
     color = lc[0] >> COLOR_SHIFT;
     lc[0] &= LOCAL_MASK;
-    const R OFF = R(1);
-    // coordinate differences in FP64, cast to R (CNVEC3 / CDERI3 inputs)
-    const double x1 = sx[lc[0]], y1 = sy[lc[0]], z1 = sz[lc[0]];
-    const R X21 = R(sx[lc[1]] - x1), Y21 = R(sy[lc[1]] - y1), Z21 = R(sz[lc[1]] - z1);
-    const R X31 = R(sx[lc[2]] - x1), Y31 = R(sy[lc[2]] - y1), Z31 = R(sz[lc[2]] - z1);
-    const R X41 = R(sx[lc[3]] - x1), Y41 = R(sy[lc[3]] - y1), Z41 = R(sz[lc[3]] - z1);
-    const R X32 = R(sx[lc[2]] - sx[lc[1]]), Y32 = R(sy[lc[2]] - sy[lc[1]]), Z32 = R(sz[lc[2]] - sz[lc[1]]);
-    const R X34 = R(sx[lc[2]] - sx[lc[3]]), Y34 = R(sy[lc[2]] - sy[lc[3]]), Z34 = R(sz[lc[2]] - sz[lc[3]]);
-    // ---- CNVEC3, ISHFRAM = 0 (cnvec3.F:66-81) or 2 (cnvec3.F:82-106) ----
-    R E1X = X21 + X34, E1Y = Y21 + Y34, E1Z = Z21 + Z34;
-    R E2X = X32 + X41, E2Y = Y32 + Y41, E2Z = Z32 + Z41;
-    R E3X = E1Y * E2Z - E1Z * E2Y, E3Y = E1Z * E2X - E1X * E2Z, E3Z = E1X * E2Y - E1Y * E2X;
-    if (gd.ishfram == 2) {
-      R su = E2X * E2X + E2Y * E2Y + E2Z * E2Z;
-      E1X = E1X * su + E2Y * E3Z - E2Z * E3Y;
-      E1Y = E1Y * su + E2Z * E3X - E2X * E3Z;
-      E1Z = E1Z * su + E2X * E3Y - E2Y * E3X;
-      su = ssqrt(E1X * E1X + E1Y * E1Y + E1Z * E1Z);
-      su = R(1) / (su > R(EM20) ? su : R(EM20));
-      E1X *= su; E1Y *= su; E1Z *= su;
-      su = ssqrt(E3X * E3X + E3Y * E3Y + E3Z * E3Z);
-      su = R(1) / (su > R(EM20) ? su : R(EM20));
-      E3X *= su; E3Y *= su; E3Z *= su;
-      E2X = E3Y * E1Z - E3Z * E1Y; E2Y = E3Z * E1X - E3X * E1Z; E2Z = E3X * E1Y - E3Y * E1X;
-      su = ssqrt(E2X * E2X + E2Y * E2Y + E2Z * E2Z);
-      su = R(1) / (su > R(EM20) ? su : R(EM20));
-      E2X *= su; E2Y *= su; E2Z *= su;
-    } else {
-      R su = E3X * E3X + E3Y * E3Y + E3Z * E3Z;
-      su = ssqrt(su);
-      su = R(1) / (su > R(EM20) ? su : R(EM20));
-      E3X *= su; E3Y *= su; E3Z *= su;
-      const R q1 = E1X * E1X + E1Y * E1Y + E1Z * E1Z;
-      const R q2 = E2X * E2X + E2Y * E2Y + E2Z * E2Z;
-      su = ssqrt(q1 / q2);
-      E1X = E1X + (E2Y * E3Z - E2Z * E3Y) * su;
-      E1Y = E1Y + (E2Z * E3X - E2X * E3Z) * su;
-      E1Z = E1Z + (E2X * E3Y - E2Y * E3X) * su;
-      su = ssqrt(E1X * E1X + E1Y * E1Y + E1Z * E1Z);
-      su = R(1) / (su > R(EM20) ? su : R(EM20));
-      E1X *= su; E1Y *= su; E1Z *= su;
-      E2X = E3Y * E1Z - E3Z * E1Y; E2Y = E3Z * E1X - E3X * E1Z; E2Z = E3X * E1Y - E3Y * E1X;
-    }
-    // ---- CDERI3 (cderi3.F:87-190) ----
-    const R X2 = E1X * X21 + E1Y * Y21 + E1Z * Z21;
-    const R Y2 = E2X * X21 + E2Y * Y21 + E2Z * Z21;
-    const R Y3 = E2X * X31 + E2Y * Y31 + E2Z * Z31;
-    const R X3 = E1X * X31 + E1Y * Y31 + E1Z * Z31;
-    const R X4 = E1X * X41 + E1Y * Y41 + E1Z * Z41;
-    const R Y4 = E2X * X41 + E2Y * Y41 + E2Z * Z41;
-    const R PX1 = R(0.5) * (Y2 - Y4), PY1 = R(0.5) * (X4 - X2), PX2 = R(0.5) * Y3, PY2 = -R(0.5) * X3;
-    R AREA = R(2) * (PY2 * PX1 - PY1 * PX2);
-    AREA = AREA > R(EM20) ? AREA : R(EM20);
-    const R VHX = (-X2 + X3 - X4) / AREA, VHY = (-Y2 + Y3 - Y4) / AREA;
-    // ---- CCOEF3 (ccoef3.F:66-160) ----
-    const R THK0 = gd.ithk > 0 ? st_thk : st_thke;
-    const R VOL0 = THK0 * AREA;
-    const R THK02 = THK0 * THK0;
-    const R RHO = R(gd.rho0), YM = R(gd.young), NU = R(gd.nu), GG = R(gd.shear);
-    const R A11 = R(gd.a11), A12 = R(gd.a12), SSP = R(gd.ssp);
-    const R H1 = R(gd.hm), H2 = R(gd.hf), H3 = R(gd.hr);
-    const int npt = NPT > 0 ? NPT : gd.npt;
-    const R SHF = npt == 1 ? R(0) : R(gd.shf);
-    const R GS = GG * SHF;
-    // ---- CDLEN3 (cdlen3.F:69-121) ----
-    R ALDT;
-    {
-      const R AL1 = X2 * X2 + Y2 * Y2;
-      const R AL2 = (X3 - X2) * (X3 - X2) + (Y3 - Y2) * (Y3 - Y2);
-      const R AL6 = X3 * X3 + Y3 * Y3;
-      const R AL3 = (X4 - X3) * (X4 - X3) + (Y4 - Y3) * (Y4 - Y3);
-      const R AL4 = X4 * X4 + Y4 * Y4;
-      const R AL5 = (X4 - X2) * (X4 - X2) + (Y4 - Y2) * (Y4 - Y2);
-      R ALMIN = fmin(fmin(AL1, AL2), AL4);
-      const R ALQ = fmin(fmin(AL3, AL5), AL6);
-      if (AL3 != R(0)) ALMIN = fmin(ALMIN, ALQ);
-      R m56 = fmax(AL5, AL6);
-      m56 = m56 > R(EM20) ? m56 : R(EM20);
-      const R DTDYN = AREA * AREA / m56;
-      ALDT = fmax(DTDYN, ALMIN);
-      const R DTHOUR = R(0.5) * (ALMIN + ALDT) / fmax(H1, H2);
-      if (DTHOUR < ALDT) ALDT = DTHOUR;
-      ALDT = ssqrt(ALDT);
-    }
-    // ---- CDEFO3, IHBE <= 1 (cdefo3.F:84-131) ----
-    R VXl[4], VYl[4], VZl[4], RXl[4], RYl[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const R vx = sv[0 * NLM + lc[k]], vy = sv[1 * NLM + lc[k]], vz = sv[2 * NLM + lc[k]];
-      VXl[k] = E1X * vx + E1Y * vy + E1Z * vz;
-      VYl[k] = E2X * vx + E2Y * vy + E2Z * vz;
-      VZl[k] = E3X * vx + E3Y * vy + E3Z * vz;
-      const R rx = sv[3 * NLM + lc[k]], ry = sv[4 * NLM + lc[k]], rz = sv[5 * NLM + lc[k]];
-      RXl[k] = E1X * rx + E1Y * ry + E1Z * rz;
-      RYl[k] = E2X * rx + E2Y * ry + E2Z * rz;
-    }
-    R EXX, EYY, EXY, EXZ, EYZ, KXX, KYY, KXY;
-    {
-      const R VZ13 = VZl[0] - VZl[2], VZ24 = VZl[1] - VZl[3];
-      EYZ = PY1 * VZ13 + PY2 * VZ24;
-      EXZ = PX1 * VZ13 + PX2 * VZ24;
-      const R DT1V4 = R(0.25) * DT1;
-      const R t2a = PY2 + PY1;
-      const R t3a = copysign(fmax(fabs(t2a), R(EM20)), t2a);
-      const R t1a = DT1V4 * (VZ13 - VZ24) * (VZ13 - VZ24) / t3a;
-      const R VX13 = VXl[0] - VXl[2] - t1a, VX24 = VXl[1] - VXl[3] + t1a;
-      EXX = PX1 * VX13 + PX2 * VX24;
-      EXY = PY1 * VX13 + PY2 * VX24;
-      const R t1b = PX2 - PX1;
-      const R t3b = copysign(fmax(fabs(t1b), R(EM20)), t1b);
-      const R t2b = DT1V4 * (VZ13 + VZ24) * (VZ13 + VZ24) / t3b;
-      const R VY13 = VYl[0] - VYl[2] + t2b, VY24 = VYl[1] - VYl[3] + t2b;
-      EXY = EXY + PX1 * VY13 + PX2 * VY24;
-      EYY = PY1 * VY13 + PY2 * VY24;
-      // ---- CCURV3 (ccurv3.F:61-86) ----
-      const R RX13 = RXl[0] - RXl[2], RXAV = RXl[0] + RXl[1] + RXl[2] + RXl[3], RX24 = RXl[1] - RXl[3];
-      KYY = -PY1 * RX13 - PY2 * RX24;
-      R kxy = PX1 * RX13 + PX2 * RX24;
-      const R RY13 = RYl[0] - RYl[2], RYAV = RYl[0] + RYl[1] + RYl[2] + RYl[3], RY24 = RYl[1] - RYl[3];
-      KXX = PX1 * RY13 + PX2 * RY24;
-      KXY = PY1 * RY13 + PY2 * RY24 - kxy;
-      EXZ = EXZ + RYAV * (R(0.25) * AREA);
-      EYZ = EYZ - RXAV * (R(0.25) * AREA);
-      // ---- CSTRA3 (cstra3.F:91-101) ----
-      const R FAC1 = DT1 / AREA;
-      EXX *= FAC1; EYY *= FAC1; EXY *= FAC1; EYZ *= FAC1; EXZ *= FAC1;
-      KXX *= FAC1; KYY *= FAC1; KXY *= FAC1;
-    }
-    // ---- MULAWC layer loop (mulawc.F90:530-560, 596-1100, 2603-2620, 2930-2990) ----
-    const float* Z0 = zw + (npt - 1) * 33;      // [Z0 | WF | WM] of the npt-point rule
-    const float* WF = Z0 + 11;
-    const float* WM = Z0 + 22;
-    R FOR[5] = {R(0), R(0), R(0), R(0), R(0)}, MOM[3] = {R(0), R(0), R(0)};
-    R FOLD[5] = {R(0), R(0), R(0), R(0), R(0)}, MOLD[3] = {R(0), R(0), R(0)};
-    R THKN = st_thk;
-    const R CA = gd.has_jca ? st_jca : R(gd.jc_a);
-    const R CB = R(gd.jc_b), CN = R(gd.jc_n), YMAX = R(gd.sigmax);
-    double wpla = 0.0;
-#pragma unroll
-    for (int ip = 0; ip < (NPT > 0 ? NPT : 10); ++ip) {
-      if (NPT == 0 && ip >= npt) break;
-      const R wf = R(NPT == 5 ? coq5(1, ip) : WF[ip]), wm = R(NPT == 5 ? coq5(2, ip) : WM[ip]);
-      R SO[5], SN[5];
-      if (NPT > 0) {
-#pragma unroll
-        for (int c = 0; c < 5; ++c) SO[c] = st_sig[NPT > 0 ? ip : 0][c];
-      } else {
-#pragma unroll
-        for (int c = 0; c < 5; ++c) SO[c] = a.sig[(ip * 5 + c) * nelpad + e];
-      }
-#pragma unroll
-      for (int c = 0; c < 5; ++c) FOLD[c] = FOLD[c] + wf * SO[c];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) MOLD[c] = MOLD[c] + wm * SO[c];
-      const R THKLYL = wf * THK0;
-      const R ZT = R(NPT == 5 ? coq5(0, ip) : Z0[ip]) * THK0;
-      const R DXX = EXX + ZT * KXX, DYY = EYY + ZT * KYY, DXY = EXY + ZT * KXY;
-      R EZZ = R(0);
-      if (gd.law == 1) {
-        // SIGEPS01C (sigeps01c.F:130-146)
-        SN[0] = SO[0] + A11 * DXX + A12 * DYY;
-        SN[1] = SO[1] + A12 * DXX + A11 * DYY;
-        SN[2] = SO[2] + GG * DXY;
-        SN[3] = SO[3] + GS * EYZ;
-        SN[4] = SO[4] + GS * EXZ;
-        EZZ = -NU * (DXX + DYY) / (R(1) - NU);
-      } else {
-        // SIGEPS02C -> M2CPLR, IPLA = 0 radial return (m2cplr.F:96-230)
-        const R A1 = YM / (R(1) - NU * NU), A2 = A1 * NU;
-        SN[0] = SO[0] + A1 * DXX + A2 * DYY;
-        SN[1] = SO[1] + A2 * DXX + A1 * DYY;
-        SN[2] = SO[2] + GG * DXY;
-        SN[3] = SO[3] + GS * EYZ;
-        SN[4] = SO[4] + GS * EXZ;
-        R PLA = NPT > 0 ? st_pla[NPT > 0 ? ip : 0] : a.pla[ip * nelpad + e];
-        R YLD = PLA == R(0) ? CA : CA + CB * exp_(CN * log_(PLA));
-        YLD = fmin(YLD, YMAX);
-        const R SVM = ssqrt(SN[0] * SN[0] + SN[1] * SN[1] - SN[0] * SN[1] + R(3) * SN[2] * SN[2]);
-        const R RR = fmin(R(1), YLD / (SVM + R(EM15)));
-        R DPLA = R(0);
-        if (RR < R(1)) {
-          SN[0] *= RR; SN[1] *= RR; SN[2] *= RR;
-          DPLA = OFF * fmax(R(0), (SVM - YLD) / YM);
-          EZZ = DPLA * (R(0.5) * (SN[0] + SN[1])) / YLD;
-          PLA = PLA + DPLA;
-          a.pla[ip * nelpad + e] = PLA;
-        }
-        EZZ = -(DXX + DYY) * NU - (R(1) - R(2) * NU) * EZZ;   // sigeps02c.F:215-224
-        EZZ = EZZ / (R(1) - NU);
-        wpla += (double)YLD * (double)DPLA * (double)AREA * (double)THKLYL;
-      }
-      THKN = THKN + EZZ * THKLYL * OFF;
-#pragma unroll
-      for (int c = 0; c < 5; ++c) a.sig[(ip * 5 + c) * nelpad + e] = SN[c];
-#pragma unroll
-      for (int c = 0; c < 5; ++c) FOR[c] = FOR[c] + wf * SN[c];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) MOM[c] = MOM[c] + wm * SN[c];
-    }
-    my_wpla = wpla;
-    a.thk[e] = THKN > R(EM30) ? THKN : R(EM30);
-    {
-      const R DEGMB = FOLD[0] * EXX + FOLD[1] * EYY + FOLD[2] * EXY + FOLD[3] * EYZ + FOLD[4] * EXZ +
-                      (FOR[0] * EXX + FOR[1] * EYY + FOR[2] * EXY + FOR[3] * EYZ + FOR[4] * EXZ);
-      const R DEGFX = MOLD[0] * KXX + MOLD[1] * KYY + MOLD[2] * KXY +
-                      (MOM[0] * KXX + MOM[1] * KYY + MOM[2] * KXY);
-      const R VOL2 = R(0.5) * VOL0;
-      a.eint[0 * nelpad + e] = st_e0 + DEGMB * VOL2;
-      a.eint[1 * nelpad + e] = st_e1 + DEGFX * THK0 * VOL2;
-    }
-    // ---- CHVIS3, ISMSTR = 2, IHBE = 1, HELAS = HVISC = 1/2, HVLIN = 0 (chvis3.F:116-300) ----
-    R H1j[3], H2j[3], H3j[3], HOUR4, HOUR5;
-    {
-      const R px1v = PX1 * VHX, px2v = PX2 * VHX, py1v = PY1 * VHY, py2v = PY2 * VHY;
-      R GAMA[4];
-      GAMA[0] = OFF * (R(1) - px1v - py1v);
-      GAMA[2] = OFF * (R(1) + px1v + py1v);
-      GAMA[1] = OFF * (-R(1) - px2v - py2v);
-      GAMA[3] = OFF * (-R(1) + px2v + py2v);
-      const R SHFPR3 = SHF / (R(3) * (R(1) + NU));
-      const R R1 = R(0.25) * RHO * R(100);
-      const R A1c = R1 * (R(0.5) * H1);
-      const R A3c = R1 * (R(0.5) * H2) * ssqrt(SHFPR3);
-      const R A5c = R(0.5) * H3 * R1 * R(0.072169);
-      const R R0e = R(0.25) * YM * R(0.5);
-      const R A7c = H1 * R0e, A8c = H2 * R0e * SHFPR3;
-      const R T2A = THK02 * AREA;
-      R H1Q = A1c * ssqrt(T2A), H2Q = A3c * THK02, H3Q = A5c * T2A;
-      const R TD = THK0 * DT1;
-      R HH1 = A7c * TD;
-      const R B1 = PX1 * PX1 + PY1 * PY1, B2 = PX2 * PX2 + PY2 * PY2;
-      R HH2 = A8c * THK02 * TD / (B1 + B2);
-      if (st_degen) { H1Q = H2Q = H3Q = HH1 = HH2 = R(0); }
-      R HG1 = VXl[0] * GAMA[0] + VXl[1] * GAMA[1] + VXl[2] * GAMA[2] + VXl[3] * GAMA[3];
-      R HG2 = VYl[0] * GAMA[0] + VYl[1] * GAMA[1] + VYl[2] * GAMA[2] + VYl[3] * GAMA[3];
-      const R hour1 = st_h0 + HG1 * HH1;
-      const R hour2 = st_h1 + HG2 * HH1;
-      const R HOUR1A = hour1 + HG1 * (H1Q * fabs(HG1));
-      const R HOUR2A = hour2 + HG2 * (H1Q * fabs(HG2));
-#pragma unroll
-      for (int k = 0; k < 3; ++k) { H1j[k] = HOUR1A * GAMA[k]; H2j[k] = HOUR2A * GAMA[k]; }
-      R EHOU = HOUR1A * HG1 + HOUR2A * HG2;
-      HG1 = VZl[0] * GAMA[0] + VZl[1] * GAMA[1] + VZl[2] * GAMA[2] + VZl[3] * GAMA[3];
-      const R hour3 = st_h2 + HG1 * HH2;
-      const R HOUR3A = hour3 + HG1 * (H2Q * fabs(HG1));
-#pragma unroll
-      for (int k = 0; k < 3; ++k) H3j[k] = HOUR3A * GAMA[k];
-      EHOU = EHOU + HOUR3A * HG1;
-      HG1 = RXl[0] - RXl[1] + RXl[2] - RXl[3];
-      HG2 = RYl[0] - RYl[1] + RYl[2] - RYl[3];
-      HOUR4 = HG1 * (H3Q * fabs(HG1));
-      HOUR5 = HG2 * (H3Q * fabs(HG2));
-      EHOU = EHOU + HOUR4 * HG1 + HOUR5 * HG2;
-      my_ehou = (double)(DT1 * EHOU * OFF);
-      a.hourg[0 * nelpad + e] = hour1; a.hourg[1 * nelpad + e] = hour2; a.hourg[2 * nelpad + e] = hour3;
-    }
-    // ---- CDT3 (cdt3.F:110-115, 203-214) ----
-    {
-      const R DT = R(gd.dtfac) * ALDT / SSP;
-      if ((double)DT <= gd.dtmin) raise_error(a.err, 5, st_eid);
-      mykey = dt_key((double)DT, 3, st_eid);
-      mybits = (unsigned long long)__double_as_longlong((double)DT);
-    }
-    // ---- CFINT3, ISIGI = 0 (cfint3.F:173-260) ----
-    {
-      const R F1A = FOR[0] * THK0, F2A = FOR[1] * THK0, F3A = FOR[2] * THK0, F4A = FOR[3] * THK0, F5A = FOR[4] * THK0;
-      const R M4 = R(0.25) * (F4A * AREA), M5 = R(0.25) * (F5A * AREA);
-      const R F12 = F1A * PX2 + F3A * PY2, F22 = F2A * PY2 + F3A * PX2, F32 = F5A * PX2 + F4A * PY2;
-      const R F11 = F1A * PX1 + F3A * PY1, F21 = F2A * PY1 + F3A * PX1, F31 = F5A * PX1 + F4A * PY1;
-      const R Gc[3][3] = {{F11 + H1j[0], F12 + H1j[1], H1j[2] - F11},
-                          {F21 + H2j[0], F22 + H2j[1], H2j[2] - F21},
-                          {F31 + H3j[0], F32 + H3j[1], H3j[2] - F31}};
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        Fg[0][k] = E1X * Gc[0][k] + E2X * Gc[1][k] + E3X * Gc[2][k];
-        Fg[1][k] = E1Y * Gc[0][k] + E2Y * Gc[1][k] + E3Y * Gc[2][k];
-        Fg[2][k] = E1Z * Gc[0][k] + E2Z * Gc[1][k] + E3Z * Gc[2][k];
-      }
-#pragma unroll
-      for (int c = 0; c < 3; ++c) Fg[c][3] = -Fg[c][0] - Fg[c][1] - Fg[c][2];
-      const R M1A = MOM[0] * THK02, M2A = MOM[1] * THK02, M3A = MOM[2] * THK02;
-      const R M11 = -M2A * PY1 - M3A * PX1, M21 = M1A * PX1 + M3A * PY1;
-      const R M12 = -M2A * PY2 - M3A * PX2, M22 = M1A * PX2 + M3A * PY2;
-      const R G1m[4] = {M11 - M4 + HOUR4 * OFF, M12 - M4 - HOUR4 * OFF, -M11 - M4 + HOUR4 * OFF, -M12 - M4 - HOUR4 * OFF};
-      const R G2m[4] = {M21 + M5 + HOUR5 * OFF, M22 + M5 - HOUR5 * OFF, -M21 + M5 + HOUR5 * OFF, -M22 + M5 - HOUR5 * OFF};
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        Mg[0][k] = E1X * G1m[k] + E2X * G2m[k];
-        Mg[1][k] = E1Y * G1m[k] + E2Y * G2m[k];
-        Mg[2][k] = E1Z * G1m[k] + E2Z * G2m[k];
-      }
-    }
-    // ---- uniform pressure (load_pressure.F:201-207): F = -p N / 8, N = x13 x x24 ----
-    R PF[3] = {R(0), R(0), R(0)};
-    if (gd.pressure != 0.0) {
-      const double ax = sx[lc[2]] - x1, ay = sy[lc[2]] - y1, az = sz[lc[2]] - z1;
-      const double bx = sx[lc[3]] - sx[lc[1]], by = sy[lc[3]] - sy[lc[1]], bz = sz[lc[3]] - sz[lc[1]];
-      const R NX = R(ay * bz - az * by), NY = R(az * bx - ax * bz), NZ = R(ax * by - ay * bx);
-      const R AA = -R(gd.pressure) * R(0.125);
-      PF[0] = AA * NX; PF[1] = AA * NY; PF[2] = AA * NZ;
-    }
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      Fg[0][k] = -Fg[0][k] + PF[0]; Fg[1][k] = -Fg[1][k] + PF[1]; Fg[2][k] = -Fg[2][k] + PF[2];
-      Mg[0][k] = -Mg[0][k]; Mg[1][k] = -Mg[1][k]; Mg[2][k] = -Mg[2][k];
-    }
+    shell_element<R, NPT, false>(a, e, gd, DT1, zw, sx, sy, sz, sv, NLM, lc, st, Fg, Mg, mykey, mybits, my_ehou,
+                                 my_wpla);
   }
   // ---- patch assembly: corner forces and moments to shared memory, then each patch
   // node sums its incident corners in ascending (element, corner) order ----
@@ -1256,6 +1320,110 @@ shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
 // ===========================================================================
 // node kernel: ASSPAR4 + dt (resol.F:5853-6226) + ACCELE + BCS10 + VELOCITY + DEPLA
 // ===========================================================================
+// dt logic (resol.F:5853-5858, 6080, 6224-6226) of one part: DT2 from the
+// cycle's element reduction, the growth cap and DTMX, and the element that set it
+__device__ __forceinline__ void cycle_dt(const PartAcc& ac, const PartTime& t0, const double growth, const double dtmx,
+                                         const int split, double& DT2, int& ityp, int& nelt) {
+  const double dt2t = __longlong_as_double((long long)ac.dtbits);
+  DT2 = 1e6;                                         // EP06
+  ityp = t0.ityptst;
+  nelt = t0.neltst;
+  if (ac.dtbits != ~0ull && dt2t < DT2) {
+    DT2 = dt2t;
+    ityp = (ac.dtkey & 0x80000000ull) ? 1 : 3;
+    nelt = (int)(ac.dtkey & 0x7fffffffull);
+  }
+  const double cap = growth * t0.dt2old;
+  DT2 = DT2 < cap ? DT2 : cap;
+  DT2 = DT2 < dtmx ? DT2 : dtmx;
+  if (split) DT2 = (double)(float)DT2;
+}
+
+// ACCELE, BCS10 (global axes or a skew frame, bcs1.F), the rigid-link mean
+// (RLINK10, then BCS10 again), the kinetic energy at mid-step, VELOCITY and DEPLA
+// (FP64 accumulation) of one node, translations and (rot) rotations, from its
+// summed force (ax, ay, az) and moment (rx, ry, rz).  Shared by the node pass and
+// the persistent kernel, so that both produce the same bits.
+template <class R>
+__device__ __forceinline__ void node_update(const NodeArgs<R>& a, const int n, const unsigned char code, const bool rot,
+                                            R ax, R ay, R az, R rx, R ry, R rz, const R ms, const double DT1,
+                                            const double DT2, const double DT12, double& px, double& py, double& pz,
+                                            double& qx, double& qy, double& qz, typename Vec4<R>::T& v,
+                                            typename Vec4<R>::T& w, double& ek, double& ekr) {
+  // ACCELE (accele.F:63-80)
+  if (ms > R(0)) { const R r = R(1) / ms; ax *= r; ay *= r; az *= r; }
+  else { ax = ay = az = R(0); }
+  if (!isfinite((double)ax + (double)ay + (double)az)) raise_error(a.err, 6, n);
+  // BCS10 (bcs1.F:52-100)
+  const R* sk = (code & 128) ? a.skews + 9 * a.skew_of[n] : nullptr;
+  if (sk) {
+    bcs1v_skew(code & 7, sk, v.x, v.y, v.z);
+    bcs1v_skew(code & 7, sk, ax, ay, az);
+  } else {
+    if (code & 4) { v.x = R(0); ax = R(0); }
+    if (code & 2) { v.y = R(0); ay = R(0); }
+    if (code & 1) { v.z = R(0); az = R(0); }
+  }
+  if (code & 64) {      // RLINK10 (resol.F:7053), then BCS10 again (resol.F:7458)
+    const LinkMean* lm = &a.link_mean[a.link_of[n]];
+    const int ic = lm->ic;
+    if (ic & 4) ax = R(lm->a[0]);
+    if (ic & 2) ay = R(lm->a[1]);
+    if (ic & 1) az = R(lm->a[2]);
+    if (sk) {
+      bcs1v_skew(code & 7, sk, ax, ay, az);
+    } else {
+      if (code & 4) ax = R(0);
+      if (code & 2) ay = R(0);
+      if (code & 1) az = R(0);
+    }
+  }
+  const double dt05 = 0.5 * DT1;
+  {
+    const double wx = (double)v.x + dt05 * (double)ax, wy = (double)v.y + dt05 * (double)ay,
+                 wz = (double)v.z + dt05 * (double)az;
+    ek = (wx * wx + wy * wy + wz * wz) * 0.5 * (double)ms;
+  }
+  // VELOCITY (velocity.F:56-62)
+  const R dt12 = R(DT12);
+  v.x = v.x + dt12 * ax; v.y = v.y + dt12 * ay; v.z = v.z + dt12 * az;
+  // DEPLA (displacement.F:69-100), FP64 accumulation
+  const double ux = DT2 * (double)v.x, uy = DT2 * (double)v.y, uz = DT2 * (double)v.z;
+  qx = qx + ux; qy = qy + uy; qz = qz + uz;
+  px = px + ux; py = py + uy; pz = pz + uz;
+  if (rot) {
+    const R in = w.w;
+    if (in > R(0)) { const R r = R(1) / in; rx *= r; ry *= r; rz *= r; }
+    else { rx = ry = rz = R(0); }
+    if (sk) {
+      bcs1v_skew((code >> 3) & 7, sk, w.x, w.y, w.z);
+      bcs1v_skew((code >> 3) & 7, sk, rx, ry, rz);
+    } else {
+      if (code & 32) { w.x = R(0); rx = R(0); }
+      if (code & 16) { w.y = R(0); ry = R(0); }
+      if (code & 8)  { w.z = R(0); rz = R(0); }
+    }
+    if (code & 64) {
+      const LinkMean* lm = &a.link_mean[a.link_of[n]];
+      const int icr = lm->icr;
+      if (icr & 4) rx = R(lm->ar[0]);
+      if (icr & 2) ry = R(lm->ar[1]);
+      if (icr & 1) rz = R(lm->ar[2]);
+      if (sk) {
+        bcs1v_skew((code >> 3) & 7, sk, rx, ry, rz);
+      } else {
+        if (code & 32) rx = R(0);
+        if (code & 16) ry = R(0);
+        if (code & 8)  rz = R(0);
+      }
+    }
+    const double wx = (double)w.x + dt05 * (double)rx, wy = (double)w.y + dt05 * (double)ry,
+                 wz = (double)w.z + dt05 * (double)rz;
+    ekr = (wx * wx + wy * wy + wz * wz) * 0.5 * (double)in;
+    w.x = w.x + dt12 * rx; w.y = w.y + dt12 * ry; w.z = w.z + dt12 * rz;
+  }
+}
+
 template <class R, int TILE>
 __device__ __forceinline__ void node_pass(NodeArgs<R> a, int parity) {
   typedef typename Vec4<R>::T R4;
@@ -1305,19 +1473,9 @@ __device__ __forceinline__ void node_pass(NodeArgs<R> a, int parity) {
         ac.dtbits = o.dtbits < ac.dtbits ? o.dtbits : ac.dtbits;
       }
     }
-    // dt logic (resol.F:5853-5858, 6080, 6224-6226), identical in every thread
-    const double dt2t = __longlong_as_double((long long)ac.dtbits);
-    double DT2 = 1e6;                                  // EP06
-    int ityp = t0.ityptst, nelt = t0.neltst;
-    if (ac.dtbits != ~0ull && dt2t < DT2) {
-      DT2 = dt2t;
-      ityp = (ac.dtkey & 0x80000000ull) ? 1 : 3;
-      nelt = (int)(ac.dtkey & 0x7fffffffull);
-    }
-    const double cap = a.growth * t0.dt2old;
-    DT2 = DT2 < cap ? DT2 : cap;
-    DT2 = DT2 < a.dtmx ? DT2 : a.dtmx;
-    if (a.split) DT2 = (double)(float)DT2;
+    int ityp, nelt;
+    double DT2;
+    cycle_dt(ac, t0, a.growth, a.dtmx, a.split, DT2, ityp, nelt);
     const double DT1 = t0.dt2;
     const double DT12 = 0.5 * (DT1 + DT2);
     double ek = 0.0, ekr = 0.0;
@@ -1337,52 +1495,9 @@ __device__ __forceinline__ void node_pass(NodeArgs<R> a, int parity) {
           else { ax += f.x; ay += f.y; az += f.z; }
         }
       }
-      // ACCELE (accele.F:63-80)
-      const R ms = R(xm.w);
-      if (ms > R(0)) { const R r = R(1) / ms; ax *= r; ay *= r; az *= r; }
-      else { ax = ay = az = R(0); }
-      if (!isfinite((double)ax + (double)ay + (double)az)) raise_error(a.err, 6, n);
-      // BCS10 (bcs1.F:52-100)
-      const R* sk = (code & 128) ? a.skews + 9 * a.skew_of[n] : nullptr;
-      if (sk) {
-        bcs1v_skew(code & 7, sk, v.x, v.y, v.z);
-        bcs1v_skew(code & 7, sk, ax, ay, az);
-      } else {
-        if (code & 4) { v.x = R(0); ax = R(0); }
-        if (code & 2) { v.y = R(0); ay = R(0); }
-        if (code & 1) { v.z = R(0); az = R(0); }
-      }
-      if (code & 64) {      // RLINK10 (resol.F:7053), then BCS10 again (resol.F:7458)
-        const LinkMean* lm = &a.link_mean[a.link_of[n]];
-        const int ic = lm->ic;
-        if (ic & 4) ax = R(lm->a[0]);
-        if (ic & 2) ay = R(lm->a[1]);
-        if (ic & 1) az = R(lm->a[2]);
-        if (sk) {
-          bcs1v_skew(code & 7, sk, ax, ay, az);
-        } else {
-          if (code & 4) ax = R(0);
-          if (code & 2) ay = R(0);
-          if (code & 1) az = R(0);
-        }
-      }
-      const double dt05 = 0.5 * DT1;
-      {
-        const double wx = (double)v.x + dt05 * (double)ax, wy = (double)v.y + dt05 * (double)ay,
-                     wz = (double)v.z + dt05 * (double)az;
-        ek = (wx * wx + wy * wy + wz * wz) * 0.5 * (double)ms;
-      }
-      // VELOCITY (velocity.F:56-62)
-      const R dt12 = R(DT12);
-      v.x = v.x + dt12 * ax; v.y = v.y + dt12 * ay; v.z = v.z + dt12 * az;
-      V[n] = v;
-      // DEPLA (displacement.F:69-100), FP64 accumulation
-      const double ux = DT2 * (double)v.x, uy = DT2 * (double)v.y, uz = DT2 * (double)v.z;
-      DX[n] = dx + ux; DY[n] = dy + uy; DZ[n] = dz + uz;
-      X[n] = make_double4(xm.x + ux, xm.y + uy, xm.z + uz, xm.w);
+      R rx = R(0), ry = R(0), rz = R(0);
       if (pd.has_rot) {
-        R4 w = w0;
-        R rx = m0.x, ry = m0.y, rz = m0.z;
+        rx = m0.x; ry = m0.y; rz = m0.z;
         if (k1 > k0 + 1) { rx += m1.x; ry += m1.y; rz += m1.z; }
         for (int k = k0 + 2; k < k1; ++k) {
           const R4 m = mslot[k];
@@ -1395,37 +1510,15 @@ __device__ __forceinline__ void node_pass(NodeArgs<R> a, int parity) {
             else { rx += m.x; ry += m.y; rz += m.z; }
           }
         }
-        const R in = w.w;
-        if (in > R(0)) { const R r = R(1) / in; rx *= r; ry *= r; rz *= r; }
-        else { rx = ry = rz = R(0); }
-        if (sk) {
-          bcs1v_skew((code >> 3) & 7, sk, w.x, w.y, w.z);
-          bcs1v_skew((code >> 3) & 7, sk, rx, ry, rz);
-        } else {
-          if (code & 32) { w.x = R(0); rx = R(0); }
-          if (code & 16) { w.y = R(0); ry = R(0); }
-          if (code & 8)  { w.z = R(0); rz = R(0); }
-        }
-        if (code & 64) {
-          const LinkMean* lm = &a.link_mean[a.link_of[n]];
-          const int icr = lm->icr;
-          if (icr & 4) rx = R(lm->ar[0]);
-          if (icr & 2) ry = R(lm->ar[1]);
-          if (icr & 1) rz = R(lm->ar[2]);
-          if (sk) {
-            bcs1v_skew((code >> 3) & 7, sk, rx, ry, rz);
-          } else {
-            if (code & 32) rx = R(0);
-            if (code & 16) ry = R(0);
-            if (code & 8)  rz = R(0);
-          }
-        }
-        const double wx = (double)w.x + dt05 * (double)rx, wy = (double)w.y + dt05 * (double)ry,
-                     wz = (double)w.z + dt05 * (double)rz;
-        ekr = (wx * wx + wy * wy + wz * wz) * 0.5 * (double)in;
-        w.x = w.x + dt12 * rx; w.y = w.y + dt12 * ry; w.z = w.z + dt12 * rz;
-        VR[n] = w;
       }
+      double px = xm.x, py = xm.y, pz = xm.z, qx = dx, qy = dy, qz = dz;
+      R4 w = w0;
+      node_update<R>(a, n, code, pd.has_rot != 0, ax, ay, az, rx, ry, rz, R(xm.w), DT1, DT2, DT12, px, py, pz,
+                     qx, qy, qz, v, w, ek, ekr);
+      V[n] = v;
+      DX[n] = qx; DY[n] = qy; DZ[n] = qz;
+      X[n] = make_double4(px, py, pz, xm.w);
+      if (pd.has_rot) VR[n] = w;
     }
     if (valid && a.halo_slot && !a.halo_ke[n]) { ek = 0.0; ekr = 0.0; }   // counted by another rank
     // per-tile kinetic energy partials (fixed tree order -> deterministic)

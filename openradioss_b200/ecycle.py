@@ -49,7 +49,7 @@ EXPORTS = [
     "or_ecycle_spmd_elements", "or_ecycle_spmd_nodes", "or_ecycle_spmd_end", "or_ecycle_add_rlink",
     "or_ecycle_set_rlink", "or_ecycle_add_function", "or_ecycle_add_cload", "or_ecycle_add_pload",
     "or_ecycle_add_skew", "or_ecycle_set_bcs_skew", "or_ecycle_set_hex_state", "or_ecycle_set_shell_state",
-    "or_ecycle_set_energy_sums",
+    "or_ecycle_set_energy_sums", "or_ecycle_persistent_info",
 ]
 
 
@@ -98,6 +98,7 @@ def _declare(lib):
         "or_ecycle_spmd_end": ([P, C.POINTER(abi.Time)], C.c_int),
         "or_ecycle_stream": ([P, C.POINTER(C.c_void_p)], C.c_int),
         "or_ecycle_device_bytes": ([P, C.POINTER(C.c_longlong)], C.c_int),
+        "or_ecycle_persistent_info": ([P, ip, ip, ip], C.c_int),
         "or_ecycle_adjoint": ([P, C.c_int, C.POINTER(abi.AdjointResponse), C.POINTER(abi.Time), dp, dp, dp, dp, dp],
                               C.c_int),
     }
@@ -349,6 +350,12 @@ class ECycle(_DeckModel):
         s = C.c_void_p()
         self._call("stream", C.byref(s))
         return s.value
+
+    def persistent_info(self):
+        """(on, CTAs, threads per CTA) of the persistent form of step()."""
+        on, g, t = C.c_int(), C.c_int(), C.c_int()
+        self._call("persistent_info", C.byref(on), C.byref(g), C.byref(t))
+        return bool(on.value), g.value, t.value
 
     def device_bytes(self):
         n = C.c_longlong()
