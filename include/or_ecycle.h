@@ -113,7 +113,9 @@ typedef struct {
   double thk;           /* GEO(1) initial thickness (used where THKE is not given) */
   int    npt;           /* integration points through the thickness, 1..10        */
   int    ithk;          /* 1: element uses the current thickness (ITHK>0)         */
-  int    ipla;          /* 0: radial return (the only implemented IPLA)           */
+  int    ipla;          /* M2CPLR return: 0 radial (Iplas 2), 1 Newton with three
+                           iterations (Iplas 1), 2 normal projection + radial
+                           (Iplas 3); cgrtails.F:822-829 maps Iplas to IPLA        */
   int    ishfram;       /* local frame: 0 (default) or 2 (/SHFRA/V4, contrl.F:478-486;
                            cnvec3.F:82-106)                                        */
   double hm, hf, hr;    /* GEO(13..15) hourglass coefficients                     */

@@ -22,24 +22,35 @@ FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std
          "--use_fast_math"]
 
 
-def needs_build():
-    if not os.path.exists(OUT):
+# Parity variant: the same sources with floating-point contraction off (no FMA, in
+# FP64 and FP32 alike) and IEEE division and square root, the arithmetic of the
+# oracle (built with -ffp-contract=off).  Used only by the test that separates the
+# effect of FMA contraction from that of the assembly order.
+OUT_NOFMA = os.path.join(HERE, "libor_ecycle_nofma.so")
+FLAGS_NOFMA = [f for f in FLAGS if f != "--use_fast_math"] + ["-fmad=false"]
+
+
+def needs_build(out=OUT):
+    if not os.path.exists(out):
         return True
-    t = os.path.getmtime(OUT)
+    t = os.path.getmtime(out)
     return any(os.path.getmtime(f) > t for f in DEPS)
 
 
-def build(verbose=False, force=False):
-    if not force and not needs_build():
-        return OUT
-    cmd = [NVCC, *FLAGS, *(["-Xptxas", "-v"] if verbose else []), "-o", OUT, *SRC]
+def build(verbose=False, force=False, variant=None):
+    """Builds libor_ecycle.so (variant None) or the parity variant ("nofma")."""
+    out, flags = (OUT_NOFMA, FLAGS_NOFMA) if variant == "nofma" else (OUT, FLAGS)
+    if not force and not needs_build(out):
+        return out
+    cmd = [NVCC, *flags, *(["-Xptxas", "-v"] if verbose else []), "-o", out, *SRC]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
     if verbose:
         sys.stderr.write(r.stdout + r.stderr)
-    return OUT
+    return out
 
 
 if __name__ == "__main__":
-    print(build(verbose="--verbose" in sys.argv, force=True))
+    print(build(verbose="--verbose" in sys.argv, force=True,
+                variant="nofma" if "--nofma" in sys.argv else None))

@@ -914,6 +914,7 @@ int finalize_impl(or_ecycle* h) {
       ShellGroupDesc d{};
       d.part = g.part; d.law = g.mat.law; d.nel = g.nel; d.npt = g.prop.npt; d.ithk = g.prop.ithk;
       d.ishfram = g.prop.ishfram;
+      d.ipla = g.prop.ipla;
       d.has_jca = g.jca.empty() ? 0 : 1;
       any_jca = any_jca || !g.jca.empty();
       d.rho0 = g.mat.rho0; d.young = g.mat.young; d.nu = g.mat.nu; d.shear = g.mat.shear; d.a11 = g.mat.a11;
@@ -1978,7 +1979,7 @@ int or_ecycle_add_shell_group(or_ecycle* h, int part, int nel, const int* ixc, c
   if (part < 0 || part >= (int)h->parts.size() || nel <= 0 || !ixc || !mat || !prop || !group)
     return fail(h, OR_E_ARG, "add_shell_group: bad argument");
   if (prop->npt < 1 || prop->npt > 10) return fail(h, OR_E_UNSUPPORTED, "shell npt outside 1..10");
-  if (prop->ipla != 0) return fail(h, OR_E_UNSUPPORTED, "shell IPLA other than radial return");
+  if (prop->ipla < 0 || prop->ipla > 2) return fail(h, OR_E_UNSUPPORTED, "shell IPLA outside 0..2");
   if (prop->ishfram != 0 && prop->ishfram != 2) return fail(h, OR_E_UNSUPPORTED, "shell ISHFRAM other than 0 or 2");
   if (mat->law != OR_LAW_ELASTIC && mat->law != OR_LAW_JOHNSON_COOK) return fail(h, OR_E_UNSUPPORTED, "shell law");
   HShell g;
@@ -2169,6 +2170,8 @@ int or_ecycle_adjoint(or_ecycle* h, int ncycles, const or_adjoint_response* r, o
   if (h->cfg.precision != OR_PREC_FP64) return fail(h, OR_E_UNSUPPORTED, "adjoint: FP64 handles only");
   if (!h->hex.empty() || h->shell.empty()) return fail(h, OR_E_UNSUPPORTED, "adjoint: shell groups only");
   if (!h->links.empty()) return fail(h, OR_E_UNSUPPORTED, "adjoint: rigid links");
+  for (const HShell& g : h->shell)
+    if (g.prop.ipla != 0) return fail(h, OR_E_UNSUPPORTED, "adjoint: IPLA 1 and 2 (the reverse follows the radial return)");
   for (auto& L : h->loads)     // /CLOAD forces depend on time only: no reverse terms
     if (L.type != 0) return fail(h, OR_E_UNSUPPORTED, "adjoint: /PLOAD follower loads");
 

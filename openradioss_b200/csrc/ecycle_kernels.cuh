@@ -54,7 +54,7 @@ struct HexGroupDesc {
 
 struct ShellGroupDesc {
   int part, law, nel, npt;
-  int ithk, has_jca, ishfram, pad1;
+  int ithk, has_jca, ishfram, ipla;   // ipla: M2CPLR return (0 radial, 1 Newton, 2 projection)
   double rho0, young, nu, shear, a11, a12, ssp, jc_a, jc_b, jc_n, sigmax;
   double hm, hf, hr, shf, pressure, dtfac, dtmin;
 };
@@ -816,6 +816,72 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
 // one BT shell element (CFORC3 chain), shared by the patch kernel and the
 // persistent kernel
 // ===========================================================================
+// M2CPLR's iterative returns for a plane-stress point already outside the yield
+// surface test (FISOKIN = 0, no rate or thermal term): IPLA = 1, three Newton
+// iterations on DPLA with the plane-stress correction factors P, Q
+// (m2cplr.F:231-378); IPLA = 2, an approximate normal projection then a radial
+// return to the hardened yield stress (m2cplr.F:379-445).  SN: sigma xx, yy, xy
+// (updated); PLA, YLD (IPLA 2 hardens it), DPLA, EZZ (the plastic thickness
+// strain term, before SIGEPS02C's elastic part) out.  Returns whether the point
+// flowed.
+template <class R>
+__device__ __forceinline__ bool m2cplr_iterative(const int ipla, R (&SN)[5], R& PLA, R& YLD, R& DPLA, R& EZZ,
+                                                 const R CA, const R CB, const R CN, const R YMAX, const R YOUNG,
+                                                 const R NU, const R G, const R OFF) {
+  const R SMALL = R(1e-7);
+  if (ipla == 1) {
+    const R S1 = SN[0] + SN[1], S2 = SN[0] - SN[1], S3 = SN[2];
+    const R A = R(0.25) * S1 * S1;
+    const R B = R(0.75) * S2 * S2 + R(3) * S3 * S3;
+    const R SVM = ssqrt(A + B);
+    if (!(SVM > YLD && OFF == R(1))) return false;
+    const R NU1 = R(1) / (R(1) - NU), NU2 = R(1) / (R(1) + NU);
+    const R H = YLD >= YMAX ? R(0) : CN * CB * exp_((CN - R(1)) * log_(PLA + SMALL));
+    R DPLA_J = (SVM - YLD) / (R(3) * G + H);
+    const R ANU1 = A * NU1, BNU2 = R(3) * B * NU2, TWOH = R(2) * H;
+    R DPLA_I = R(0), P = R(1), Q = R(1), DR = R(0);
+#pragma unroll 1
+    for (int it = 0; it < 3; ++it) {
+      DPLA_I = DPLA_J;
+      const R PLA_I = PLA + DPLA_I;
+      DPLA = DPLA_J;
+      const R YLD_I = PLA_I == R(0) ? fmin(YMAX, CA) : fmin(YMAX, CA + CB * exp_(CN * log_(PLA_I)));
+      DR = R(0.5) * YOUNG * DPLA_I / YLD_I;
+      P = R(1) / (R(1) + DR * NU1);
+      Q = R(1) / (R(1) + R(3) * DR * NU2);
+      const R P2 = P * P, Q2 = Q * Q;
+      const R F = A * P2 + B * Q2 - YLD_I * YLD_I;
+      const R DF = -(ANU1 * P2 * P + BNU2 * Q2 * Q) * (YOUNG - DR * TWOH) / YLD_I - TWOH * YLD_I;
+      DPLA_J = DPLA_I > R(0) ? fmax(R(0), DPLA_I - F / DF) : R(0);
+    }
+    PLA = PLA + DPLA_I;
+    const R T1 = (SN[0] + SN[1]) * P, T2 = (SN[0] - SN[1]) * Q;
+    SN[0] = R(0.5) * (T1 + T2);
+    SN[1] = R(0.5) * (T1 - T2);
+    SN[2] = SN[2] * Q;
+    EZZ = DR * T1 / YOUNG;
+    return true;
+  }
+  const R SVM2 = SN[0] * SN[0] + SN[1] * SN[1] - SN[0] * SN[1] + R(3) * SN[2] * SN[2];
+  const R YLD2 = YLD * YLD;
+  if (!(SVM2 > YLD2 && OFF == R(1))) return false;
+  R SVM = ssqrt(SVM2);
+  const R H = YLD >= YMAX ? R(0) : CN * CB * exp_((CN - R(1)) * log_(PLA + SMALL));
+  const R AA = (SVM2 - YLD2) / (R(5) * SVM2 + R(3) * (-SN[0] * SN[1] + SN[2] * SN[2]));
+  const R S1 = (R(1) - R(2) * AA) * SN[0] + AA * SN[1];
+  const R S2 = AA * SN[0] + (R(1) - R(2) * AA) * SN[1];
+  const R S3 = (R(1) - R(3) * AA) * SN[2];
+  SN[0] = S1; SN[1] = S2; SN[2] = S3;
+  DPLA = OFF * (SVM - YLD) / (R(3) * G + H);
+  PLA = PLA + DPLA;
+  YLD = YLD + H * DPLA;
+  SVM = ssqrt(SN[0] * SN[0] + SN[1] * SN[1] - SN[0] * SN[1] + R(3) * SN[2] * SN[2]);
+  const R RR = fmin(R(1), YLD / fmax(R(EM20), SVM));
+  SN[0] *= RR; SN[1] *= RR; SN[2] *= RR;
+  EZZ = DPLA * R(0.5) * (SN[0] + SN[1]) / YLD;
+  return true;
+}
+
 // Element state of one shell, held in registers by the thread that computes it.
 // NPT > 0: the integration-point state too (NPT points); NPT = 0: the points'
 // state stays in memory and is read and written point by point.
@@ -1056,16 +1122,23 @@ __device__ __forceinline__ void shell_element(const ShellArgs<R>& a, const int e
       R PLA = NPT > 0 ? st.pla[NPT > 0 ? ip : 0] : a.pla[ip * nelpad + e];
       R YLD = PLA == R(0) ? CA : CA + CB * exp_(CN * log_(PLA));
       YLD = fmin(YLD, YMAX);
-      const R SVM = ssqrt(SN[0] * SN[0] + SN[1] * SN[1] - SN[0] * SN[1] + R(3) * SN[2] * SN[2]);
-      const R RR = fmin(R(1), YLD / (SVM + R(EM15)));
       R DPLA = R(0);
-      if (RR < R(1)) {
-        SN[0] *= RR; SN[1] *= RR; SN[2] *= RR;
-        DPLA = OFF * fmax(R(0), (SVM - YLD) / YM);
-        EZZ = DPLA * (R(0.5) * (SN[0] + SN[1])) / YLD;
-        PLA = PLA + DPLA;
-        if (KEEP) st.pla[NPT > 0 ? ip : 0] = PLA;
-        else a.pla[ip * nelpad + e] = PLA;
+      if (gd.ipla == 0) {
+        const R SVM = ssqrt(SN[0] * SN[0] + SN[1] * SN[1] - SN[0] * SN[1] + R(3) * SN[2] * SN[2]);
+        const R RR = fmin(R(1), YLD / (SVM + R(EM15)));
+        if (RR < R(1)) {
+          SN[0] *= RR; SN[1] *= RR; SN[2] *= RR;
+          DPLA = OFF * fmax(R(0), (SVM - YLD) / YM);
+          EZZ = DPLA * (R(0.5) * (SN[0] + SN[1])) / YLD;
+          PLA = PLA + DPLA;
+          if (KEEP) st.pla[NPT > 0 ? ip : 0] = PLA;
+          else a.pla[ip * nelpad + e] = PLA;
+        }
+      } else {
+        if (m2cplr_iterative<R>(gd.ipla, SN, PLA, YLD, DPLA, EZZ, CA, CB, CN, YMAX, YM, NU, GG, OFF)) {
+          if (KEEP) st.pla[NPT > 0 ? ip : 0] = PLA;
+          else a.pla[ip * nelpad + e] = PLA;
+        }
       }
       EZZ = -(DXX + DYY) * NU - (R(1) - R(2) * NU) * EZZ;   // sigeps02c.F:215-224
       EZZ = EZZ / (R(1) - NU);

@@ -385,8 +385,11 @@ def to_deck(sd: StarterDeck, name=None):
         if ihbe != 1 or ismstr != 2:
             raise RadError(f"/PROP/SHELL/{prop_id}: Ishell {ihbe} / Ismstr {ismstr}; the element cycle "
                            "implements Ishell 1 with Ismstr 2")
-        if ipla not in (0, 2):
-            raise RadError(f"/PROP/SHELL/{prop_id}: Iplas {ipla} (iterative return) is not implemented")
+        if ipla not in (0, 1, 2, 3):
+            raise RadError(f"/PROP/SHELL/{prop_id}: Iplas {ipla}")
+        # M2CPLR's IPLA from Iplas (cgrtails.F:822-829; the explicit default Iplas 0
+        # stays 0): 0 and 2 radial return, 1 Newton iterations, 3 normal projection
+        ipla = {0: 0, 1: 1, 2: 0, 3: 2}[ipla]
         if prop["dm"] != 0.0:
             raise RadError(f"/PROP/SHELL/{prop_id}: membrane damping dm is not implemented")
         npt = prop["n"]
@@ -402,6 +405,7 @@ def to_deck(sd: StarterDeck, name=None):
         p = decks.shell_prop(prop["thick"], npt=npt, ithk=1 if ithk > 0 else 0,
                              hm=prop["hm"] or 0.01, hf=prop["hf"] or 0.01, hr=prop["hr"] or 0.01,
                              ishfram=sd.ishfram)
+        p["ipla"] = ipla
         if prop["ashear"] != 0.0:
             p["shf"] = prop["ashear"]
         if npt == 1:
@@ -587,7 +591,7 @@ def write_starter(deck, path, part=0, title=None):
         L += [f"/PROP/SHELL/{pid}", f"shell {pid}", _i10(1, 2, 0, 0) + " " * 20 + _f20(0.0),
               _f20(pr["hm"], pr["hf"], pr["hr"], 0.0, 0.0),
               _i10(pr["npt"], 0) + _f20(pr["thk"], pr["shf"] if pr["npt"] > 1 else 0.0) +
-              _i10(1 if pr["ithk"] else 2, 0),
+              _i10(1 if pr["ithk"] else 2, {0: 2, 1: 1, 2: 3}[int(pr.get("ipla", 0))]),
               f"/PART/{pid}", f"part {pid}", _i10(pid, pid, 0), f"/SHELL/{pid}"]
         uniform = np.allclose(thk, pr["thk"], rtol=0, atol=0)
         for e in range(conn.shape[0]):

@@ -773,7 +773,7 @@ int shell_element(const Model<R>& m, ShellGroup<R>& g, PartData<R>& P, int i, do
       EZZ = -NU * (DEPSXX + DEPSYY) / (R(1) - NU);
       THKN = THKN + EZZ * THKLYL * OFF;
     } else {
-      // SIGEPS02C -> M2CPLR (m2cplr.F:96-230), IPLA=0, CC=0, FISOKIN=0, TSTAR=0
+      // SIGEPS02C -> M2CPLR (m2cplr.F:96-445), IPLA 0/1/2, CC=0, FISOKIN=0, TSTAR=0
       const R CA = g.jca.empty() ? R(mt.jc_a) : g.jca[i];
       const R CB = R(mt.jc_b), CN = R(mt.jc_n), YMAX = R(mt.sigmax);
       const R A1 = YM / (R(1) - NU * NU), A2 = A1 * NU;
@@ -785,15 +785,72 @@ int shell_element(const Model<R>& m, ShellGroup<R>& g, PartData<R>& P, int i, do
       R PLA = g.pla[ip * nel + i];
       R YLD = (PLA == R(0)) ? CA : CA + CB * std::exp(CN * std::log(PLA));
       YLD = std::min(YLD, YMAX);
-      R SVM = std::sqrt(SN[0] * SN[0] + SN[1] * SN[1] - SN[0] * SN[1] + R(3) * SN[2] * SN[2]);
-      R RR = std::min(R(1), YLD / (SVM + R(EM15)));
       R DPLA = 0;
-      if (RR < R(1)) {
-        SN[0] *= RR; SN[1] *= RR; SN[2] *= RR;
-        DPLA = OFF * std::max(R(0), (SVM - YLD) / YM);
-        R S1h = R(0.5) * (SN[0] + SN[1]);
-        EZZ = DPLA * S1h / YLD;
-        PLA = PLA + DPLA;
+      const R SMALL = R(1e-7);                       // m2cplr.F:98 SMALL = EM7
+      if (pr.ipla == 0) {
+        // IPLA = 0 radial return (m2cplr.F:199-230)
+        R SVM = std::sqrt(SN[0] * SN[0] + SN[1] * SN[1] - SN[0] * SN[1] + R(3) * SN[2] * SN[2]);
+        R RR = std::min(R(1), YLD / (SVM + R(EM15)));
+        if (RR < R(1)) {
+          SN[0] *= RR; SN[1] *= RR; SN[2] *= RR;
+          DPLA = OFF * std::max(R(0), (SVM - YLD) / YM);
+          R S1h = R(0.5) * (SN[0] + SN[1]);
+          EZZ = DPLA * S1h / YLD;
+          PLA = PLA + DPLA;
+        }
+      } else if (pr.ipla == 1) {
+        // IPLA = 1: plane-stress return with NMAX = 3 Newton iterations on DPLA
+        // (m2cplr.F:231-378, FISOKIN = 0)
+        const R S1 = SN[0] + SN[1], S2 = SN[0] - SN[1], S3 = SN[2];
+        const R A = R(0.25) * S1 * S1;
+        const R B = R(0.75) * S2 * S2 + R(3) * S3 * S3;
+        const R SVM = std::sqrt(A + B);
+        if (SVM > YLD && OFF == R(1)) {
+          const R NU1 = R(1) / (R(1) - NU), NU2 = R(1) / (R(1) + NU);
+          const R H = YLD >= YMAX ? R(0) : CN * CB * std::exp((CN - R(1)) * std::log(PLA + SMALL));
+          R DPLA_J = (SVM - YLD) / (R(3) * GG + H);
+          const R ANU1 = A * NU1, BNU2 = R(3) * B * NU2, TWOH = R(2) * H;
+          R DPLA_I = 0, P = 1, Q = 1, DR = 0;
+          for (int it = 0; it < 3; ++it) {
+            DPLA_I = DPLA_J;
+            const R PLA_I = PLA + DPLA_I;
+            DPLA = DPLA_J;
+            const R YLD_I = PLA_I == R(0) ? std::min(YMAX, CA) : std::min(YMAX, CA + CB * std::exp(CN * std::log(PLA_I)));
+            DR = R(0.5) * YM * DPLA_I / YLD_I;
+            P = R(1) / (R(1) + DR * NU1);
+            Q = R(1) / (R(1) + R(3) * DR * NU2);
+            const R P2 = P * P, Q2 = Q * Q;
+            const R F = A * P2 + B * Q2 - YLD_I * YLD_I;
+            const R DF = -(ANU1 * P2 * P + BNU2 * Q2 * Q) * (YM - DR * TWOH) / YLD_I - TWOH * YLD_I;
+            DPLA_J = DPLA_I > R(0) ? std::max(R(0), DPLA_I - F / DF) : R(0);
+          }
+          PLA = PLA + DPLA_I;
+          const R T1 = (SN[0] + SN[1]) * P, T2 = (SN[0] - SN[1]) * Q;
+          SN[0] = R(0.5) * (T1 + T2);
+          SN[1] = R(0.5) * (T1 - T2);
+          SN[2] = SN[2] * Q;
+          EZZ = DR * T1 / YM;
+        }
+      } else {
+        // IPLA = 2: approximate normal projection, then radial return (m2cplr.F:379-445)
+        const R SVM2 = SN[0] * SN[0] + SN[1] * SN[1] - SN[0] * SN[1] + R(3) * SN[2] * SN[2];
+        R SVM = std::sqrt(SVM2);
+        const R YLD2 = YLD * YLD;
+        if (SVM2 > YLD2 && OFF == R(1)) {
+          const R H = YLD >= YMAX ? R(0) : CN * CB * std::exp((CN - R(1)) * std::log(PLA + SMALL));
+          const R AA = (SVM2 - YLD2) / (R(5) * SVM2 + R(3) * (-SN[0] * SN[1] + SN[2] * SN[2]));
+          const R S1 = (R(1) - R(2) * AA) * SN[0] + AA * SN[1];
+          const R S2 = AA * SN[0] + (R(1) - R(2) * AA) * SN[1];
+          const R S3 = (R(1) - R(3) * AA) * SN[2];
+          SN[0] = S1; SN[1] = S2; SN[2] = S3;
+          DPLA = OFF * (SVM - YLD) / (R(3) * GG + H);
+          PLA = PLA + DPLA;
+          YLD = YLD + H * DPLA;
+          SVM = std::sqrt(SN[0] * SN[0] + SN[1] * SN[1] - SN[0] * SN[1] + R(3) * SN[2] * SN[2]);
+          const R RR = std::min(R(1), YLD / std::max(R(EM20), SVM));
+          SN[0] *= RR; SN[1] *= RR; SN[2] *= RR;
+          EZZ = DPLA * R(0.5) * (SN[0] + SN[1]) / YLD;
+        }
       }
       g.pla[ip * nel + i] = PLA;
       // sigeps02c.F:215-224
@@ -1268,7 +1325,7 @@ int add_hex(Model<R>& m, int part, int nel, const int* ixs, const or_material* m
 template <class R>
 int add_shell(Model<R>& m, int part, int nel, const int* ixc, const or_material* mat,
               const or_shell_prop* prop, const double* thke) {
-  if (prop->npt < 1 || prop->npt > 10 || prop->ipla != 0) return OR_E_UNSUPPORTED;
+  if (prop->npt < 1 || prop->npt > 10 || prop->ipla < 0 || prop->ipla > 2) return OR_E_UNSUPPORTED;
   if (prop->ishfram != 0 && prop->ishfram != 2) return OR_E_UNSUPPORTED;
   ShellGroup<R> g;
   g.part = part; g.nel = nel; g.mat = *mat; g.prop = *prop;

@@ -303,3 +303,17 @@ def test_kernel_times_then_reset(lib):
     b.step(40)
     assert np.array_equal(a.get_nodes()["d"], b.get_nodes()["d"])
     assert a.time() == b.time()
+
+
+@pytest.mark.parametrize("ipla", [1, 2])
+def test_shell_iterative_returns_fp64_and_split(lib, ipla):
+    """M2CPLR's IPLA 1 (Newton) and IPLA 2 (projection + radial) on a yielding
+    plate: FP64 at the bars of the radial return, split within 1e-5."""
+    d = decks.c2_shell_plate(n=20, size=0.02, pressure=8e6, ipla=ipla)
+    g, o = run_pair(d, 400)
+    assert o.shell_state(0)["pla"].max() > 0
+    check_nodes(g, o, FP64_TOL)
+    check_shell(g, o, FP64_PLASTIC_IP_TOL)
+    check_energies(g, o, FP64_TOL)
+    s, _ = run_pair(d, 400, precision=abi.OR_PREC_SPLIT)
+    assert rel(s.get_nodes()["d"], o.get_nodes()["d"]) < SPLIT_TOL

@@ -147,3 +147,49 @@ def test_hex_block_energy_balance():
     # in the first cycle); afterwards internal + kinetic + hourglass stays constant
     assert abs(totals[0] / e0 - 1.0) < 0.05
     assert np.ptp(totals) / e0 < 5e-3
+
+
+def _jc_yield(mat, pla):
+    y = np.where(pla == 0.0, mat["jc_a"], mat["jc_a"] + mat["jc_b"] * np.power(np.maximum(pla, 1e-300), mat["jc_n"]))
+    return np.minimum(y, mat["sigmax"])
+
+
+@pytest.mark.parametrize("ipla", [1, 2])
+def test_iterative_shell_returns_land_on_the_yield_surface(ipla):
+    """M2CPLR's IPLA 1 (Newton, three iterations) and IPLA 2 (projection, then a
+    radial return to YLD + H DPLA) under linear hardening (n = 1): every
+    integration point that flowed in the last cycle ends on the plane-stress von
+    Mises surface of its hardened yield stress A + B PLA, within what the
+    algorithms leave (IPLA 1 stops after three Newton steps; IPLA 2 leaves a
+    projected stress inside the surface unscaled): within 1e-5 of the yield
+    stress."""
+    d = decks.c2_shell_plate(n=10, size=0.01, pressure=20e6, ipla=ipla)
+    mat = d["parts"][0]["shell"][0]["mat"]
+    mat["jc_n"] = 1.0
+    o = Oracle(d)
+    o.step(79)
+    pla0 = o.shell_state(0)["pla"].copy()
+    o.step(1)
+    st = o.shell_state(0)
+    flowed = st["pla"] > pla0
+    assert flowed.sum() > 20
+    s = st["sig"]                                   # npt x 5 x nel
+    svm = np.sqrt(s[:, 0] ** 2 + s[:, 1] ** 2 - s[:, 0] * s[:, 1] + 3.0 * s[:, 2] ** 2)
+    yld = _jc_yield(mat, st["pla"])
+    gap = np.abs(svm - yld)[flowed] / yld[flowed]
+    assert gap.max() < 1e-5, gap.max()
+
+
+def test_iterative_shell_returns_agree_with_the_radial_return():
+    """The three plane-stress returns integrate the same plastic flow: the plate's
+    deflection after plastic yielding differs between them by a small fraction."""
+    d = {}
+    for ipla in (0, 1, 2):
+        o = Oracle(decks.c2_shell_plate(n=12, size=0.012, pressure=6e6, ipla=ipla))
+        o.step(300)
+        assert o.shell_state(0)["pla"].max() > 1e-3
+        d[ipla] = o.get_nodes()["d"][:, 2]
+    scale = np.abs(d[0]).max()
+    for ipla in (1, 2):
+        diff = np.abs(d[ipla] - d[0]).max() / scale
+        assert 1e-8 < diff < 0.05, (ipla, diff)
