@@ -155,6 +155,9 @@ class _DeckModel:
                 if g.get("jc_a") is not None:
                     self._call("set_shell_yield", gi, abi.ptr(_f64(g["jc_a"]), C.c_double))
                 self.shell_groups.append((part, ixc.shape[0], int(g["prop"]["npt"])))
+            for rb in p.get("rbodies", []):
+                sl = _i32(np.asarray(rb["slaves"]) + 1)
+                self._add_rbody(part, int(rb["master"]) + 1, sl.size, sl, _f64(rb["rby"]))
             for rl in p.get("rlinks", []):
                 nodes = _i32(np.asarray(rl["nodes"]) + 1)
                 self._add_rlink(part, nodes.size, nodes, int(rl.get("ic", 7)), int(rl.get("icr", 0)))

@@ -144,9 +144,24 @@ class StarterDeck:
         self.surf_seg = {}         # id -> list of (n1, n2, n3, n4), n4 = 0 for triangles
         self.surf_part = {}        # id -> list of part ids
         self.cload = []            # dict(func, dir, skew, grnod, ascale_x, fscale)
+        self.grnod_grnod = {}      # id -> list of /GRNOD ids (resolved into grnod after reading)
+        self.rbody = []            # dict per /RBODY card, deck order
         self.pload = []            # dict(surf, func, ascale_x, fscale)
         for key, lines, where in _blocks(path):
             self._block(key, lines, where)
+        self._resolve_group_groups()
+
+    def _resolve_group_groups(self):
+        """/GRNOD/GRNOD: the union of its member groups' nodes, in /NODE order."""
+        order = {n: k for k, n in enumerate(self.nodes)}
+        pending = dict(self.grnod_grnod)
+        while pending:
+            done = [g for g, members in pending.items() if all(m in self.grnod for m in members)]
+            if not done:
+                raise RadError(f"/GRNOD/GRNOD {sorted(pending)}: undefined or cyclic member groups")
+            for g in done:
+                nodes = {n for m in pending.pop(g) for n in self.grnod[m]}
+                self.grnod[g] = sorted(nodes, key=lambda n: order.get(n, n))
 
     def _block(self, key, L, where):
         k0 = key[0].upper()
@@ -274,9 +289,27 @@ class StarterDeck:
             code = lambda s: sum(b for ch, b in zip(s.replace(" ", "0"), (4, 2, 1)) if ch == "1")
             self.bcs.append((code(tra), code(rot), _int(line, 20), _int(line, 10)))
         elif k0 == "GRNOD":
-            if key[1].upper() != "NODE":
+            kind = key[1].upper()
+            if kind == "NODE":
+                self.grnod[int(key[2])] = _node_list(L[1:])
+            elif kind == "GRNOD":
+                self.grnod_grnod[int(key[2])] = _node_list(L[1:])
+            else:
                 raise RadError(f"{where}: /GRNOD/{key[1]} is not implemented")
-            self.grnod[int(key[2])] = _node_list(L[1:])
+        elif k0 == "RBODY":
+            line = L[1]
+            rb = dict(id=int(key[1]), master=_int(line, 0), isens=_int(line, 10), nskew=_int(line, 20),
+                      ispher=_int(line, 30), mass=_real(line, 40), grnod=_int(line, 60), icog=_int(line, 80),
+                      surf=_int(line, 90),
+                      j=[_real(L[2], 20 * c) for c in range(3)] if len(L) > 2 else [0.0] * 3,
+                      jc=[_real(L[3], 20 * c) for c in range(3)] if len(L) > 3 else [0.0] * 3,
+                      ioptoff=_int(L[4], 0) if len(L) > 4 else 0, ifail=_int(L[4], 20) if len(L) > 4 else 0)
+            if rb["isens"] or rb["nskew"] or rb["surf"] or rb["ioptoff"] or rb["ifail"]:
+                raise RadError(f"{where}: /RBODY with a sensor, skew, surface, Ioptoff or Ifail is not implemented")
+            if rb["icog"] not in (0, 1) or rb["ispher"] not in (0, 2):
+                raise RadError(f"{where}: /RBODY ICoG {rb['icog']} / Ispher {rb['ispher']}; the element "
+                               "cycle implements ICoG 1 and Ispher 2 (their defaults)")
+            self.rbody.append(rb)
         elif k0 == "INIVEL":
             if key[1].upper() != "TRA":
                 raise RadError(f"{where}: /INIVEL/{key[1]} is not implemented")
@@ -431,6 +464,16 @@ def to_deck(sd: StarterDeck, name=None):
     for mass, g in sd.admas:
         for n in sd.grnod[g]:
             part["ms"][index[n]] += mass
+    if sd.rbody:
+        part["rbodies"] = []
+        for rb in sd.rbody:
+            if rb["grnod"] not in sd.grnod:
+                raise RadError(f"/RBODY/{rb['id']}: node group {rb['grnod']} is not defined")
+            m = index[rb["master"]]
+            slaves = [index[n] for n in sd.grnod[rb["grnod"]] if index[n] != m]
+            rby, tensor = rbody_init(part, m, slaves, rb["mass"], rb["j"], rb["jc"])
+            part["rbodies"].append(dict(id=rb["id"], master=m, slaves=np.array(slaves, np.int64), rby=rby,
+                                        tensor=tensor))
     func_index = {fid: k for k, fid in enumerate(sorted(sd.funct))}
     cloads, ploads = [], []
     for c in sd.cload:
@@ -454,6 +497,93 @@ def to_deck(sd: StarterDeck, name=None):
     if sd.skews:
         d["skews"] = [sd.skews[k] for k in sorted(sd.skews)]
     return d
+
+
+def principal_inertia(I):
+    """Eigenvalues and unit eigenvectors (columns) of a symmetric 3x3 inertia
+    tensor by cyclic Jacobi rotations, the eigenvalues left in the positions of
+    the diagonal they come from (a diagonal tensor is returned as it is); the
+    principal frame of INEPRI / VALPR (inepri.F)."""
+    a = np.array(I, np.float64)
+    v = np.eye(3)
+    for _ in range(50):
+        off = abs(a[0, 1]) + abs(a[0, 2]) + abs(a[1, 2])
+        if off <= 1e-30 * (abs(a[0, 0]) + abs(a[1, 1]) + abs(a[2, 2])) or off == 0.0:
+            break
+        for p, q in ((0, 1), (0, 2), (1, 2)):
+            if a[p, q] == 0.0:
+                continue
+            theta = (a[q, q] - a[p, p]) / (2.0 * a[p, q])
+            t = math.copysign(1.0, theta) / (abs(theta) + math.sqrt(theta * theta + 1.0))
+            c = 1.0 / math.sqrt(t * t + 1.0)
+            s_ = t * c
+            rot = np.eye(3)
+            rot[p, p] = rot[q, q] = c
+            rot[p, q], rot[q, p] = s_, -s_
+            a = rot.T @ a @ rot
+            v = v @ rot
+    return np.diag(a).copy(), v
+
+
+def rbody_init(part, m, slaves, mass, j, jc):
+    """Starter initialisation of a rigid body (INIRBY, inirby.F:146-330, 340-361,
+    715-836; 3D, no skew, ICoG 1, Ispher 2): the main node takes the added mass
+    and inertia, moves to the centre of mass of itself and the secondary nodes,
+    and gets the body's mass; the inertia tensor about the new position is
+    assembled from the main node's own mass and inertia and every secondary
+    node's; its principal frame and inertias are returned as 12 values (the three
+    unit axes, then the three inertias, as RBY(1:12)) with the inertia tensor
+    itself; the main node's rotational inertia becomes the smallest principal
+    inertia.  part's ms, inr and x are updated in place."""
+    ms, inr, x = part["ms"], part["inr"], part["x"]
+    ms[m] += mass
+    if ms[m] == 0.0:
+        ms[m] = 1e-20
+    jxx, jyy, jzz = j
+    jxy, jyz, jxz = jc
+    I = np.array([[jxx, jxy, jxz], [jxy, jyy, jyz], [jxz, jyz, jzz]], np.float64)
+    for c in range(3):
+        I[c, c] += inr[m]
+    xmg = ms[m]
+    xg = x[m].copy()
+    acc = x[m] * ms[m]
+    masrb = ms[m]
+    for n in slaves:
+        acc = acc + x[n] * ms[n]
+        masrb += ms[n]
+    x[m] = acc / masrb
+    d = xg - x[m]
+    I[0, 0] += (d[1] * d[1] + d[2] * d[2]) * xmg
+    I[0, 1] -= d[0] * d[1] * xmg
+    I[0, 2] -= d[0] * d[2] * xmg
+    I[1, 0] -= d[0] * d[1] * xmg
+    I[1, 1] += (d[2] * d[2] + d[0] * d[0]) * xmg
+    I[1, 2] -= d[1] * d[2] * xmg
+    I[2, 0] -= d[0] * d[2] * xmg
+    I[2, 1] -= d[1] * d[2] * xmg
+    I[2, 2] += (d[0] * d[0] + d[1] * d[1]) * xmg
+    if len(slaves) == 1:
+        for c in range(3):
+            I[c, c] += 1e-20
+    for n in slaves:
+        r = x[n] - x[m]
+        xx, xy, xz, yy, yz, zz = r[0] * r[0], r[0] * r[1], r[0] * r[2], r[1] * r[1], r[1] * r[2], r[2] * r[2]
+        I[0, 0] += inr[n] + (yy + zz) * ms[n]
+        I[0, 1] -= xy * ms[n]
+        I[0, 2] -= xz * ms[n]
+        I[1, 0] -= xy * ms[n]
+        I[1, 1] += inr[n] + (zz + xx) * ms[n]
+        I[1, 2] -= yz * ms[n]
+        I[2, 0] -= xz * ms[n]
+        I[2, 1] -= yz * ms[n]
+        I[2, 2] += inr[n] + (xx + yy) * ms[n]
+    ip, axes = principal_inertia(I)
+    imin, imax = ip.min(), ip.max()
+    if imin <= 1e-3 * imax:                       # Ispher 2 (inirby.F:744-751)
+        ip = np.where(ip / imax < 1e-3, ip + 0.1 * imax, ip)
+    ms[m] = masrb
+    inr[m] = ip.min()
+    return np.concatenate([axes[:, 0], axes[:, 1], axes[:, 2], ip]), I
 
 
 def _lookup(table, key, what):

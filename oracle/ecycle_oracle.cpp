@@ -129,13 +129,24 @@ struct RLink {
   std::vector<int> nodes;     // 0-based, in the card's order
 };
 
+// rigid body (/RBODY after the starter's INIRBY): main node, secondary nodes, and
+// RBY(1:12) = principal axes e1, e2, e3 (RBY(1:3), (4:6), (7:9)) and inertias
+template <class R>
+struct RBody {
+  int part, master;
+  std::vector<int> slaves;    // 0-based
+  R rby[12];
+};
+
 template <class R>
 struct Model {
+  typedef R real_t;
   or_ecycle_config cfg;
   std::vector<PartData<R>> parts;
   std::vector<HexGroup<R>> hex;
   std::vector<ShellGroup<R>> shell;
   std::vector<RLink> rlinks;
+  std::vector<RBody<R>> rbodies;
   std::vector<Func> funcs;
   std::vector<std::array<double, 9>> skews;
   std::vector<CLoad> cloads;
@@ -1098,6 +1109,91 @@ double load_pass(Model<R>& m, int p, double tt, double dt1, double& wext) {
 // ----------------------------------------------------------------------------
 // One cycle of one part: element pass, ASSPAR4, dt, ACCELE, BCS10, VELOCITY, DEPLA.
 // ----------------------------------------------------------------------------
+// ROTBMR (engine/source/tools/skew/rotbmr.F): turns the principal frame RBY(1:9)
+// by the rotation vector DT*VR (VR in the principal frame), then re-orthonormalises
+template <class R>
+void rotbmr(const R* vr, R* rby, R dt) {
+  const R rx = dt * vr[0], ry = dt * vr[1], rz = dt * vr[2];
+  const R rx2 = rx * rx, ry2 = ry * ry, rz2 = rz * rz;
+  const R r2 = std::max(R(1e-10), rx2 + ry2 + rz2);
+  const R r = std::sqrt(r2);
+  R c = std::cos(r);
+  const R cm1 = R(1) - c;
+  c = c * r2;
+  const R s = std::sin(r) * r;
+  const R sz = rz * s, cz = rz * cm1;
+  const R e11 = rx2 * cm1 + c, e22 = ry2 * cm1 + c;
+  R e12 = rx * ry * cm1;
+  const R e21 = e12 - sz;
+  e12 = e12 + sz;
+  const R e13 = rx * cz - ry * s, e23 = ry * cz + rx * s;
+  R b11 = rby[0] * e11 + rby[3] * e12 + rby[6] * e13;
+  R b21 = rby[1] * e11 + rby[4] * e12 + rby[7] * e13;
+  R b31 = rby[2] * e11 + rby[5] * e12 + rby[8] * e13;
+  R b12 = rby[0] * e21 + rby[3] * e22 + rby[6] * e23;
+  R b22 = rby[1] * e21 + rby[4] * e22 + rby[7] * e23;
+  R b32 = rby[2] * e21 + rby[5] * e22 + rby[8] * e23;
+  R bn = std::sqrt(b11 * b11 + b21 * b21 + b31 * b31);
+  b11 = b11 / bn; b21 = b21 / bn; b31 = b31 / bn;
+  bn = std::sqrt(b12 * b12 + b22 * b22 + b32 * b32);
+  b12 = b12 / bn; b22 = b22 / bn; b32 = b32 / bn;
+  rby[0] = b11; rby[1] = b21; rby[2] = b31;
+  rby[3] = b12; rby[4] = b22; rby[5] = b32;
+  rby[6] = b21 * b32 - b31 * b22;
+  rby[7] = b31 * b12 - b11 * b32;
+  rby[8] = b11 * b22 - b21 * b12;
+}
+
+// RBYFOR -> RGBODFP for one rigid body (rgbodfp.F, explicit 3D, no rotational BCS on
+// the main node, Ispher 2): the secondary nodes' forces, and their moments about
+// the main node, summed in DOUBLE PRECISION (the reference's RBF6 six-part exact
+// sum; here in the secondary-node order) onto the main node (phase 1 and 2); the
+// principal frame turned by the main node's rotational velocity over DT1; the
+// moment expressed in the principal frame, the gyroscopic terms added (Euler's
+// equations), and replaced by the pseudo moment IN(M) * rotational acceleration
+// (IN(M) = the smallest principal inertia) so that ACCELE's AR = AM / IN(M) is the
+// body's rotational acceleration.  af, am: the main node's force and moment sums
+// (ASSPAR4), updated.
+template <class R, class SUM>
+void rgbodfp(RBody<R>& rb, const PartData<R>& P, R* af, R* am, R dt1, SUM raw) {
+  const int M = rb.master;
+  R* rby = rb.rby;
+  const R inm = P.in[M];
+  rby[9] = std::max(rby[9], inm);
+  rby[10] = std::max(rby[10], inm);
+  rby[11] = std::max(rby[11], inm);
+  double S[6] = {0, 0, 0, 0, 0, 0};
+  for (int n : rb.slaves) {
+    R f[3], mo[3];
+    raw(n, f, mo);
+    const R dx = R(P.x[3 * n] - P.x[3 * M]), dy = R(P.x[3 * n + 1] - P.x[3 * M + 1]),
+            dz = R(P.x[3 * n + 2] - P.x[3 * M + 2]);
+    const R f6 = mo[0] + dy * f[2] - dz * f[1];
+    const R f7 = mo[1] + dz * f[0] - dx * f[2];
+    const R f8 = mo[2] + dx * f[1] - dy * f[0];
+    S[0] += double(f[0]); S[1] += double(f[1]); S[2] += double(f[2]);
+    S[3] += double(f6); S[4] += double(f7); S[5] += double(f8);
+  }
+  for (int c = 0; c < 3; ++c) { af[c] = R(double(af[c]) + S[c]); am[c] = R(double(am[c]) + S[3 + c]); }
+  const R* vr = &P.vr[3 * M];
+  const R wa1 = am[0], wa2 = am[1], wa3 = am[2];
+  R vi[3];
+  vi[0] = rby[0] * vr[0] + rby[1] * vr[1] + rby[2] * vr[2];
+  vi[1] = rby[3] * vr[0] + rby[4] * vr[1] + rby[5] * vr[2];
+  vi[2] = rby[6] * vr[0] + rby[7] * vr[1] + rby[8] * vr[2];
+  rotbmr(vi, rby, dt1);
+  R p1 = rby[0] * wa1 + rby[1] * wa2 + rby[2] * wa3;
+  R p2 = rby[3] * wa1 + rby[4] * wa2 + rby[5] * wa3;
+  R p3 = rby[6] * wa1 + rby[7] * wa2 + rby[8] * wa3;
+  p1 = p1 + (rby[10] - rby[11]) * vi[1] * vi[2];
+  p2 = p2 + (rby[11] - rby[9]) * vi[2] * vi[0];
+  p3 = p3 + (rby[9] - rby[10]) * vi[0] * vi[1];
+  const R q1 = p1 * inm / rby[9], q2 = p2 * inm / rby[10], q3 = p3 * inm / rby[11];
+  am[0] = rby[0] * q1 + rby[3] * q2 + rby[6] * q3;
+  am[1] = rby[1] * q1 + rby[4] * q2 + rby[7] * q3;
+  am[2] = rby[2] * q1 + rby[5] * q2 + rby[8] * q3;
+}
+
 template <class R>
 int cycle(Model<R>& m, int p, or_ecycle_time& t, int nthreads, bool last) {
   PartData<R>& P = m.parts[p];
@@ -1207,11 +1303,20 @@ int cycle(Model<R>& m, int p, or_ecycle_time& t, int nthreads, bool last) {
                          icr ? S[5] / S[4] : 0.0, icr ? S[6] / S[4] : 0.0, icr ? S[7] / S[4] : 0.0});
     link_dirs.push_back({ic, icr});
   }
+  // rigid bodies: their nodes are updated after the others (RBYFOR, RBYVIT below)
+  std::vector<char> rb_node;
+  for (auto& rb : m.rbodies) {
+    if (rb.part != p) continue;
+    if (rb_node.empty()) rb_node.assign(N, 0);
+    rb_node[rb.master] = 1;
+    for (int n : rb.slaves) rb_node[n] = 2;
+  }
   // ASSPAR4 + ACCELE + BCS10 + RLINK10 + BCS10 + (energies) + VELOCITY + DEPLA, per node
   std::vector<double> ek(last ? N : 0), ekr(last ? N : 0);
   int nan_node = -1;
 #pragma omp parallel for num_threads(nthreads) schedule(static)
   for (int n = 0; n < N; ++n) {
+    if (!rb_node.empty() && rb_node[n]) continue;
     R a[3], ar[3];
     node_acc(n, a, ar);
     const R msn = P.ms[n], inn = P.in[n];
@@ -1251,11 +1356,95 @@ int cycle(Model<R>& m, int p, or_ecycle_time& t, int nthreads, bool last) {
       P.x[3 * n + c] = P.x[3 * n + c] + vdt;
     }
   }
+  // RBYFOR (resol.F:5452) before ACCELE, RBYVIT (resol.F:7515) after BCS10, then
+  // VELOCITY and DEPLA of the bodies' nodes; kinetic energy with the RBYCOR
+  // correction (rgbcor.F: the secondary nodes' energy is the body's, whose
+  // rotational part is taken in the principal frame)
+  double ek_rb = 0, ekr_rb = 0;
+  for (auto& rb : m.rbodies) {
+    if (rb.part != p) continue;
+    auto raw = [&P](int n, R* f, R* mo) {
+      f[0] = f[1] = f[2] = mo[0] = mo[1] = mo[2] = R(0);
+      for (long k = P.adsky[n]; k < P.adsky[n + 1]; ++k) {
+        const R* g = &P.fsky[8 * k];
+        f[0] = f[0] + g[0]; f[1] = f[1] + g[1]; f[2] = f[2] + g[2];
+        mo[0] = mo[0] + g[3]; mo[1] = mo[1] + g[4]; mo[2] = mo[2] + g[5];
+      }
+    };
+    const int M = rb.master;
+    R af[3], am[3];
+    raw(M, af, am);
+    rgbodfp(rb, P, af, am, R(DT1), raw);
+    // ACCELE and BCS10 of the main node
+    R a[3], ar[3];
+    const R msm = P.ms[M], inm = P.in[M];
+    for (int c = 0; c < 3; ++c) {
+      a[c] = msm > R(0) ? af[c] * (R(1) / msm) : R(0);
+      ar[c] = inm > R(0) ? am[c] * (R(1) / inm) : R(0);
+    }
+    if (!std::isfinite(double(a[0]) + double(a[1]) + double(a[2]))) nan_node = M;
+    R* vm = &P.v[3 * M];
+    R* vrm = &P.vr[3 * M];
+    bcs1v(P.icodt[M], skew_of(M), vm);
+    bcs1v(P.icodr[M], skew_of(M), vrm);
+    bcs_acc(M, a, ar);
+    // RGBODV (rgbodv.F:91-119, more than two secondary nodes)
+    const R dt2 = R(t.dt2);
+    const R vg[3] = {vrm[0] + ar[0] * DT12, vrm[1] + ar[1] * DT12, vrm[2] + ar[2] * DT12};
+    const R usdt = R(1) / DT12;
+    std::vector<R> as(3 * rb.slaves.size()), ars(3 * rb.slaves.size());
+    for (size_t i = 0; i < rb.slaves.size(); ++i) {
+      const int n = rb.slaves[i];
+      R* vn = &P.v[3 * n];
+      R* vrn = &P.vr[3 * n];
+      bcs1v(P.icodt[n], skew_of(n), vn);
+      bcs1v(P.icodr[n], skew_of(n), vrn);
+      ars[3 * i] = (vg[0] - vrn[0]) * usdt;
+      ars[3 * i + 1] = (vg[1] - vrn[1]) * usdt;
+      ars[3 * i + 2] = (vg[2] - vrn[2]) * usdt;
+      const R dx = R(P.x[3 * n] - P.x[3 * M]), dy = R(P.x[3 * n + 1] - P.x[3 * M + 1]),
+              dz = R(P.x[3 * n + 2] - P.x[3 * M + 2]);
+      const R v1x2 = vg[0] * dy, v2x1 = vg[1] * dx, v2x3 = vg[1] * dz, v3x2 = vg[2] * dy, v3x1 = vg[2] * dx,
+              v1x3 = vg[0] * dz;
+      const R vx1 = v2x3 - v3x2, vx2 = v3x1 - v1x3, vx3 = v1x2 - v2x1;
+      as[3 * i] = a[0] + (vm[0] + vx1 + R(0.5) * dt2 * (vg[1] * vx3 - vg[2] * vx2) - vn[0]) * usdt;
+      as[3 * i + 1] = a[1] + (vm[1] + vx2 + R(0.5) * dt2 * (vg[2] * vx1 - vg[0] * vx3) - vn[1]) * usdt;
+      as[3 * i + 2] = a[2] + (vm[2] + vx3 + R(0.5) * dt2 * (vg[0] * vx2 - vg[1] * vx1) - vn[2]) * usdt;
+    }
+    if (last) {   // ECRIT + RBYCOR: the body's mass on its main node, its rotation in the principal frame
+      const double dt05 = 0.5 * DT1;
+      const double vx = double(vm[0]) + dt05 * double(a[0]), vy = double(vm[1]) + dt05 * double(a[1]),
+                   vz = double(vm[2]) + dt05 * double(a[2]);
+      ek_rb += (vx * vx + vy * vy + vz * vz) * 0.5 * double(msm);
+      const R h = R(dt05);
+      const R w1 = vrm[0] + ar[0] * h, w2 = vrm[1] + ar[1] * h, w3 = vrm[2] + ar[2] * h;
+      const R* rby = rb.rby;
+      const R i1 = rby[0] * w1 + rby[1] * w2 + rby[2] * w3;
+      const R i2 = rby[3] * w1 + rby[4] * w2 + rby[5] * w3;
+      const R i3 = rby[6] * w1 + rby[7] * w2 + rby[8] * w3;
+      ekr_rb += 0.5 * (double(rby[9]) * double(i1) * double(i1) + double(rby[10]) * double(i2) * double(i2) +
+                       double(rby[11]) * double(i3) * double(i3));
+    }
+    // VELOCITY and DEPLA of the main and secondary nodes
+    auto advance = [&](int n, const R* an, const R* arn) {
+      R* v = &P.v[3 * n];
+      R* vr = &P.vr[3 * n];
+      v[0] = v[0] + DT12 * an[0]; v[1] = v[1] + DT12 * an[1]; v[2] = v[2] + DT12 * an[2];
+      vr[0] = vr[0] + DT12 * arn[0]; vr[1] = vr[1] + DT12 * arn[1]; vr[2] = vr[2] + DT12 * arn[2];
+      for (int c = 0; c < 3; ++c) {
+        double vdt = t.dt2 * double(v[c]);
+        P.d[3 * n + c] = P.d[3 * n + c] + vdt;
+        P.x[3 * n + c] = P.x[3 * n + c] + vdt;
+      }
+    };
+    for (size_t i = 0; i < rb.slaves.size(); ++i) advance(rb.slaves[i], &as[3 * i], &ars[3 * i]);
+    advance(M, a, ar);
+  }
   if (nan_node >= 0) { m.errcode = OR_E_NAN; m.errindex = nan_node; return OR_E_NAN; }
   if (last) {
     double s = 0, sr = 0;
     for (int n = 0; n < N; ++n) { s += ek[n]; sr += ekr[n]; }
-    P.ekin = s; P.ekinr = sr;
+    P.ekin = s + ek_rb; P.ekinr = sr + ekr_rb;
   }
   // TT=TT+DT2 (resol.F:8261)
   t.tt += t.dt2;
@@ -1389,6 +1578,27 @@ int oracle_add_rlink(void* hh, int part, int nnod, const int* nodes, int ic, int
       L.nodes.push_back(nodes[i] - 1);
     }
     m.rlinks.push_back(std::move(L));
+    return (int)OR_OK;
+  });
+}
+// A rigid body after the starter's initialisation: main node and nsl secondary
+// nodes (1-based), rby12 = principal axes e1, e2, e3 and principal inertias; the
+// main node's mass, inertia and position are those of add_part (the body's).
+int oracle_add_rbody(void* hh, int part, int master, int nsl, const int* slaves, const double* rby12) {
+  Handle* h = (Handle*)hh;
+  return h->with([&](auto& m) {
+    typedef typename std::remove_reference<decltype(m)>::type::real_t R;
+    if (part < 0 || part >= (int)m.parts.size() || nsl < 3 || !slaves || !rby12) return (int)OR_E_ARG;
+    const int nn = m.parts[part].numnod;
+    if (master < 1 || master > nn) return (int)OR_E_ARG;
+    RBody<R> rb;
+    rb.part = part; rb.master = master - 1;
+    for (int i = 0; i < nsl; ++i) {
+      if (slaves[i] < 1 || slaves[i] > nn || slaves[i] == master) return (int)OR_E_ARG;
+      rb.slaves.push_back(slaves[i] - 1);
+    }
+    for (int k = 0; k < 12; ++k) rb.rby[k] = R(rby12[k]);
+    m.rbodies.push_back(std::move(rb));
     return (int)OR_OK;
   });
 }

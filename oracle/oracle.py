@@ -42,6 +42,7 @@ def load(fast=False):
     lib.oracle_set_shell_yield.argtypes = [P, C.c_int, dp]
     lib.oracle_add_rlink.argtypes = [P, C.c_int, C.c_int, ip, C.c_int, C.c_int]
     lib.oracle_set_rlink.argtypes = [P, C.c_int, C.c_int, C.c_int]
+    lib.oracle_add_rbody.argtypes = [P, C.c_int, C.c_int, C.c_int, ip, dp]
     lib.oracle_add_function.argtypes = [P, C.c_int, dp, dp]
     lib.oracle_add_cload.argtypes = [P, C.c_int, C.c_int, ip, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double]
     lib.oracle_add_pload.argtypes = [P, C.c_int, C.c_int, ip, C.c_int, C.c_double, C.c_double]
@@ -100,6 +101,9 @@ class Oracle(_DeckModel):
 
     def _add_rlink(self, part, n, nodes, ic, icr):
         self._call("add_rlink", part, n, abi.ptr(nodes, C.c_int), ic, icr)
+
+    def _add_rbody(self, part, master, n, slaves, rby):
+        self._call("add_rbody", part, master, n, abi.ptr(slaves, C.c_int), abi.ptr(rby, C.c_double))
 
     def _add_function(self, n, x, y):
         self._call("add_function", n, abi.ptr(x, C.c_double), abi.ptr(y, C.c_double))
