@@ -189,6 +189,22 @@ int  or_ecycle_set_shell_yield(or_ecycle* h, int group, const double* jc_a);
    Before finalize; returns the link's index in *link. */
 int  or_ecycle_add_rlink(or_ecycle* h, int part, int nnod, const int* nodes,
                          int ic, int icr, int* link);
+/* Rigid body of /RBODY (RBYFOR rbyfor.F / RGBODFP rgbodfp.F at resol.F:5452,
+   RBYVIT rbyvit.F / RGBODV rgbodv.F at resol.F:7515, kinetic energy as RBYCOR /
+   RGBCOR rgbcor.F corrects it), after the starter's initialisation (INIRBY,
+   inirby.F): the part's arrays given to or_ecycle_add_part already hold the main
+   node at the body's centre of mass with the body's mass (MS) and its smallest
+   principal inertia (IN); rby12 = the principal axes e1, e2, e3 (3 doubles each,
+   RBY(1:9)) and the principal inertias (RBY(10:12)).  Each cycle the secondary
+   nodes' forces and moments about the main node go to the main node, the
+   principal frame turns with the body, Euler's equations give its rotational
+   acceleration, and the secondary nodes follow the body's rigid motion.
+   master: 1-based node number; slaves: nsl >= 3 distinct 1-based node numbers;
+   a node belongs to one body at most and to no rigid link; no rotational BCS on
+   the main node; no sensor, skew or surface.  Before finalize; returns the
+   body's index in *body. */
+int  or_ecycle_add_rbody(or_ecycle* h, int part, int master, int nsl, const int* slaves, const double* rby12,
+                         int* body);
 /* Changes the directions of a link between steps (an engine file that no longer
    lists it: ic = icr = 0). */
 int  or_ecycle_set_rlink(or_ecycle* h, int link, int ic, int icr);

@@ -56,6 +56,11 @@ struct HLink {
   int part = 0, ic = 0, icr = 0;
   std::vector<int> nodes;           // part-local, 0-based
 };
+struct HRBody {                     // /RBODY after the starter's initialisation
+  int part = 0, master = 0;         // part-local, 0-based
+  std::vector<int> slaves;
+  double rby[12];                   // principal axes e1, e2, e3, principal inertias
+};
 struct HLoad {                      // a /CLOAD node (type 0) or a /PLOAD segment (type 1)
   int type = 0, part = 0, func = 0, dir = 0, skew = -1;
   int node[4] = {-1, -1, -1, -1};   // part-local, 0-based
@@ -101,6 +106,7 @@ struct or_ecycle {
   std::vector<HHex> hex;
   std::vector<HShell> shell;
   std::vector<HLink> links;
+  std::vector<HRBody> rbodies;
   std::vector<HLoad> loads;
   std::vector<std::vector<double>> fx, fy;   // time functions
   std::vector<std::array<double, 9>> skews;
@@ -355,6 +361,11 @@ struct Impl {
   // rigid links
   DBuf<LinkDesc> linkd; DBuf<int> link_nodes, link_of; DBuf<LinkMean> link_mean;
   int nlinks = 0;
+  // rigid bodies: descriptors, secondary nodes, frames (12 R per body), node roles,
+  // per-body kinetic energies of the last cycle
+  DBuf<RBodyDesc> rbd; DBuf<int> rb_nodes; DBuf<R> rby; DBuf<unsigned char> rb_role; DBuf<double> rb_ek, rb_ekr;
+  std::vector<R> rby0;
+  int nrb = 0;
   // staging of one nodal array of one part (3 doubles per node) for set/get_nodes
   DBuf<double> stage;
   // loads, time functions, skew frames
@@ -403,6 +414,7 @@ struct Impl {
     a.halo_slot = nullptr; a.halo_ke = nullptr; a.xbuf = nullptr; a.xbytes = 0; a.nranks = 0; a.nhalo = 0;
     a.link_of = nlinks ? link_of.p : nullptr; a.link_mean = nlinks ? link_mean.p : nullptr;
     a.skew_of = skew_of.p; a.skews = skw.p;
+    a.rb_role = nrb ? rb_role.p : nullptr;
     return a;
   }
   void free_all() {
@@ -416,6 +428,7 @@ struct Impl {
     dfree(sehour); dfree(swpla); dfree(zw);
     dfree(halo_slot); dfree(halo_node); dfree(halo_ke);
     dfree(linkd); dfree(link_nodes); dfree(link_of); dfree(link_mean); dfree(stage);
+    dfree(rbd); dfree(rb_nodes); dfree(rby); dfree(rb_role); dfree(rb_ek); dfree(rb_ekr);
     dfree(loadd); dfree(funcd); dfree(funcx); dfree(funcy); dfree(wacc); dfree(wpend); dfree(skw); dfree(skew_of);
     dfree(per.node_ofs); dfree(per.node_glob); dfree(per.owner); dfree(per.pconn); dfree(per.fslot2);
     dfree(per.mslot2); dfree(per.acc3); dfree(per.ek); dfree(per.ekr); dfree(per.sync);
@@ -491,6 +504,15 @@ int launch_link(or_ecycle* h, Impl<R>& m) {
   link_kernel<R><<<(unsigned)m.nlinks, LINK_THREADS, 0, h->stream>>>(
       m.linkd.p, m.link_nodes.p, m.adsky.p, m.fslot.p, m.mslot.p, m.X.p, m.VR.p, m.code.p, m.skew_of.p, m.skw.p,
       m.link_mean.p);
+  CK(cudaGetLastError());
+  h->launches++;
+  return OR_OK;
+}
+template <class R>
+int launch_rbody(or_ecycle* h, Impl<R>& m, int parity) {
+  if (!m.nrb) return OR_OK;
+  rbody_kernel<R><<<(unsigned)m.nrb, RB_THREADS, 0, h->stream>>>(m.nargs(h), parity, m.rbd.p, m.rb_nodes.p, m.rby.p,
+                                                                  m.rb_ek.p, m.rb_ekr.p);
   CK(cudaGetLastError());
   h->launches++;
   return OR_OK;
@@ -572,7 +594,8 @@ int persist_build(or_ecycle* h, Impl<R>& m) {
   q.on = false;
   if (const char* s = std::getenv("OR_ECYCLE_PERSISTENT"))
     if (std::atoi(s) == 0) return OR_OK;
-  if (!h->cfg.graph || m.nparts != 1 || !h->hex.empty() || h->shell.empty() || !h->links.empty() || m.nload)
+  if (!h->cfg.graph || m.nparts != 1 || !h->hex.empty() || h->shell.empty() || !h->links.empty() || m.nload ||
+      !h->rbodies.empty())
     return OR_OK;
   const PatchSet& ps = m.sps;
   const int tile = h->tile_shell;
@@ -682,6 +705,8 @@ int launch_cycle(or_ecycle* h, Impl<R>& m, int parity, cudaEvent_t* ev) {
   if (rc) return rc;
   if (ev) CK(cudaEventRecord(ev[2], h->stream));
   rc = launch_link<R>(h, m);
+  if (rc) return rc;
+  rc = launch_rbody<R>(h, m, parity);
   if (rc) return rc;
   rc = launch_node<R>(h, m, parity, pdl);
   if (rc) return rc;
@@ -831,6 +856,31 @@ int finalize_impl(or_ecycle* h) {
         (rc = dalloc(h, m.link_mean, ld.size())))
       return rc;
     CK(cudaMemset(m.link_mean.p, 0, m.link_mean.n * sizeof(LinkMean)));
+  }
+  // rigid bodies: descriptors in add order, secondary nodes in global padded numbering
+  if (!h->rbodies.empty()) {
+    std::vector<RBodyDesc> bd;
+    std::vector<int> sl;
+    std::vector<unsigned char> role(nn, 0);
+    for (auto& B : h->rbodies) {
+      const int base = h->parts[B.part].node_start;
+      RBodyDesc d;
+      d.master = base + B.master; d.first = (int)sl.size(); d.count = (int)B.slaves.size(); d.part = B.part;
+      if (code[d.master] & 64) return fail(h, OR_E_UNSUPPORTED, "rigid body node in a rigid link");
+      role[d.master] = 1;
+      for (int n : B.slaves) {
+        if (code[base + n] & 64) return fail(h, OR_E_UNSUPPORTED, "rigid body node in a rigid link");
+        sl.push_back(base + n);
+        role[base + n] = 2;
+      }
+      bd.push_back(d);
+      for (int k = 0; k < 12; ++k) m.rby0.push_back(R(B.rby[k]));
+    }
+    m.nrb = (int)bd.size();
+    if ((rc = dput(h, m.rbd, bd)) || (rc = dput(h, m.rb_nodes, sl)) || (rc = dput(h, m.rby, m.rby0)) ||
+        (rc = dput(h, m.rb_role, role)) || (rc = dput(h, m.rb_ek, std::vector<double>(m.nrb, 0.0))) ||
+        (rc = dput(h, m.rb_ekr, std::vector<double>(m.nrb, 0.0))))
+      return rc;
   }
   if ((rc = dput(h, m.X, X)) || (rc = dput(h, m.V, V)) || (rc = dput(h, m.VR, VR)) || (rc = dput(h, m.code, code)) ||
       (rc = dput(h, m.adsky, adsky)) || (rc = dput(h, m.tile_part, tile_part)) || (rc = dput(h, m.partd, pd)))
@@ -1026,6 +1076,11 @@ int reset_impl(or_ecycle* h) {
   }
   CK(cudaMemset(m.ekin.p, 0, m.ekin.n * sizeof(double)));
   CK(cudaMemset(m.ekinr.p, 0, m.ekinr.n * sizeof(double)));
+  if (m.nrb) {
+    CK(cudaMemcpy(m.rby.p, m.rby0.data(), m.rby0.size() * sizeof(R), cudaMemcpyHostToDevice));
+    CK(cudaMemset(m.rb_ek.p, 0, m.rb_ek.n * sizeof(double)));
+    CK(cudaMemset(m.rb_ekr.p, 0, m.rb_ekr.n * sizeof(double)));
+  }
   CK(cudaDeviceSynchronize());
   return OR_OK;
 }
@@ -1381,6 +1436,12 @@ int energies_impl(or_ecycle* h, int part, or_energies* e) {
   auto ekinr = d2h(m.ekinr.p, m.ekinr.n);
   const HPart& P = h->parts[part];
   for (int t = P.tile_start; t < P.tile_start + P.node_pad / NODE_TILE; ++t) { ek += ekin[t]; ekr += ekinr[t]; }
+  if (m.nrb) {      // the bodies' energies (their nodes are left out of the tiles), in add order
+    auto bk = d2h(m.rb_ek.p, m.rb_ek.n);
+    auto bkr = d2h(m.rb_ekr.p, m.rb_ekr.n);
+    for (int b = 0; b < m.nrb; ++b)
+      if (h->rbodies[b].part == part) { ek += bk[b]; ekr += bkr[b]; }
+  }
   // external work of the part's loads: the cumulative sums, plus the last cycle's
   // concentrated-load power times that cycle's DT2
   double wx = 0.0;
@@ -2037,6 +2098,41 @@ int or_ecycle_add_rlink(or_ecycle* h, int part, int nnod, const int* nodes, int 
   return OR_OK;
 }
 
+int or_ecycle_add_rbody(or_ecycle* h, int part, int master, int nsl, const int* slaves, const double* rby12,
+                        int* body) {
+  if (!h) return OR_E_ARG;
+  if (h->finalized) return fail(h, OR_E_STATE, "add_rbody after finalize");
+  if (part < 0 || part >= (int)h->parts.size() || !slaves || !rby12 || nsl < 3)
+    return fail(h, OR_E_ARG, "add_rbody: bad argument (at least three secondary nodes)");
+  HPart& P = h->parts[part];
+  std::vector<char> seen(P.numnod, 0);
+  for (auto& o : h->rbodies)
+    if (o.part == part) {
+      seen[o.master] = 1;
+      for (int n : o.slaves) seen[n] = 1;
+    }
+  HRBody B;
+  B.part = part;
+  B.master = master - 1;
+  if (B.master < 0 || B.master >= P.numnod) return fail(h, OR_E_ARG, "add_rbody: main node out of range");
+  if (seen[B.master]) return fail(h, OR_E_UNSUPPORTED, "add_rbody: node already in a rigid body");
+  seen[B.master] = 1;
+  if (P.icodr[B.master] != 0) return fail(h, OR_E_UNSUPPORTED, "add_rbody: rotational BCS on the main node");
+  for (int i = 0; i < nsl; ++i) {
+    const int n = slaves[i] - 1;
+    if (n < 0 || n >= P.numnod) return fail(h, OR_E_ARG, "add_rbody: secondary node out of range");
+    if (seen[n]) return fail(h, OR_E_UNSUPPORTED, "add_rbody: node already in a rigid body");
+    seen[n] = 1;
+    B.slaves.push_back(n);
+  }
+  for (int k = 0; k < 12; ++k) B.rby[k] = rby12[k];
+  if (!(rby12[9] > 0 && rby12[10] > 0 && rby12[11] > 0)) return fail(h, OR_E_ARG, "add_rbody: principal inertias");
+  P.has_rot = true;                  // the main node's rotation (VR, IN)
+  h->rbodies.push_back(std::move(B));
+  if (body) *body = (int)h->rbodies.size() - 1;
+  return OR_OK;
+}
+
 int or_ecycle_set_rlink(or_ecycle* h, int link, int ic, int icr) {
   if (!h) return OR_E_ARG;
   if (link < 0 || link >= (int)h->links.size() || ic < 0 || ic > 7 || icr < 0 || icr > 7)
@@ -2170,6 +2266,7 @@ int or_ecycle_adjoint(or_ecycle* h, int ncycles, const or_adjoint_response* r, o
   if (h->cfg.precision != OR_PREC_FP64) return fail(h, OR_E_UNSUPPORTED, "adjoint: FP64 handles only");
   if (!h->hex.empty() || h->shell.empty()) return fail(h, OR_E_UNSUPPORTED, "adjoint: shell groups only");
   if (!h->links.empty()) return fail(h, OR_E_UNSUPPORTED, "adjoint: rigid links");
+  if (!h->rbodies.empty()) return fail(h, OR_E_UNSUPPORTED, "adjoint: rigid bodies");
   for (const HShell& g : h->shell)
     if (g.prop.ipla != 0) return fail(h, OR_E_UNSUPPORTED, "adjoint: IPLA 1 and 2 (the reverse follows the radial return)");
   for (auto& L : h->loads)     // /CLOAD forces depend on time only: no reverse terms
@@ -2190,6 +2287,7 @@ int or_ecycle_set_halo(or_ecycle* h, int part, int nloc, const int* local_node, 
   if (!h->finalized) return fail(h, OR_E_STATE, "set_halo before finalize");
   if (h->parts.size() != 1 || part != 0) return fail(h, OR_E_UNSUPPORTED, "set_halo: one part per handle");
   if (!h->links.empty()) return fail(h, OR_E_UNSUPPORTED, "set_halo: rigid links across domains");
+  if (!h->rbodies.empty()) return fail(h, OR_E_UNSUPPORTED, "set_halo: rigid bodies across domains");
   if (!h->loads.empty()) return fail(h, OR_E_UNSUPPORTED, "set_halo: /CLOAD or /PLOAD loads");
   if (h->spmd_k >= 0) return fail(h, OR_E_STATE, "set_halo inside spmd_begin/end");
   if (nloc < 0 || nhalo < 0 || nloc > nhalo || (nloc > 0 && (!local_node || !halo_slot)))

@@ -194,6 +194,9 @@ struct NodeArgs {
   // skew frame skew_of[n] (9 values: x', y', z'); null without skewed BCs
   const int* skew_of;
   const R* skews;
+  // rigid bodies: nodes with a nonzero role are updated by rbody_kernel and left
+  // out of this pass (their kinetic energy too); null without rigid bodies
+  const unsigned char* rb_role;
 };
 
 // Exchange buffer of one rank: nhalo force sums (R4), nhalo moment sums (R4),
@@ -1552,7 +1555,8 @@ __device__ __forceinline__ void node_pass(NodeArgs<R> a, int parity) {
     const double DT1 = t0.dt2;
     const double DT12 = 0.5 * (DT1 + DT2);
     double ek = 0.0, ekr = 0.0;
-    if (valid) {
+    const bool rb = a.rb_role && a.rb_role[n];     // updated by rbody_kernel
+    if (valid && !rb) {
       // ASSPAR4: the node's patch partials in ascending patch order
       R ax = f0.x, ay = f0.y, az = f0.z;
       if (k1 > k0 + 1) { ax += f1.x; ay += f1.y; az += f1.z; }
@@ -1817,6 +1821,250 @@ link_kernel(const LinkDesc* __restrict__ links, const int* __restrict__ link_nod
       r.ar[c] = r.icr ? t[5 + c] / t[4] : 0.0;
     }
     out[blockIdx.x] = r;
+  }
+}
+
+// ===========================================================================
+// rigid bodies (/RBODY): RBYFOR -> RGBODFP (rgbodfp.F, explicit 3D, no rotational
+// BCS on the main node), then, after ACCELE and BCS10 of the main node, RBYVIT ->
+// RGBODV (rgbodv.F, more than two secondary nodes), VELOCITY and DEPLA of every
+// node of the body, and its kinetic energy with the RBYCOR correction (rgbcor.F).
+// One block per body, between the element pass and the node pass; the node pass
+// leaves the bodies' nodes alone.
+// ===========================================================================
+struct RBodyDesc {
+  int master;           // padded global node number of the main node
+  int first, count;     // secondary nodes rb_nodes[first .. first+count-1]
+  int part;
+};
+constexpr int RB_THREADS = 128;
+
+template <class R>
+__device__ inline void rotbmr_dev(const R* vr, R* rby, R dt) {
+  const R rx = dt * vr[0], ry = dt * vr[1], rz = dt * vr[2];
+  const R rx2 = rx * rx, ry2 = ry * ry, rz2 = rz * rz;
+  const R r2 = fmax(R(1e-10), rx2 + ry2 + rz2);
+  const R r = sqrt(r2);
+  R c = cos(r);
+  const R cm1 = R(1) - c;
+  c = c * r2;
+  const R s = sin(r) * r;
+  const R sz = rz * s, cz = rz * cm1;
+  const R e11 = rx2 * cm1 + c, e22 = ry2 * cm1 + c;
+  R e12 = rx * ry * cm1;
+  const R e21 = e12 - sz;
+  e12 = e12 + sz;
+  const R e13 = rx * cz - ry * s, e23 = ry * cz + rx * s;
+  R b11 = rby[0] * e11 + rby[3] * e12 + rby[6] * e13;
+  R b21 = rby[1] * e11 + rby[4] * e12 + rby[7] * e13;
+  R b31 = rby[2] * e11 + rby[5] * e12 + rby[8] * e13;
+  R b12 = rby[0] * e21 + rby[3] * e22 + rby[6] * e23;
+  R b22 = rby[1] * e21 + rby[4] * e22 + rby[7] * e23;
+  R b32 = rby[2] * e21 + rby[5] * e22 + rby[8] * e23;
+  R bn = sqrt(b11 * b11 + b21 * b21 + b31 * b31);
+  b11 = b11 / bn; b21 = b21 / bn; b31 = b31 / bn;
+  bn = sqrt(b12 * b12 + b22 * b22 + b32 * b32);
+  b12 = b12 / bn; b22 = b22 / bn; b32 = b32 / bn;
+  rby[0] = b11; rby[1] = b21; rby[2] = b31;
+  rby[3] = b12; rby[4] = b22; rby[5] = b32;
+  rby[6] = b21 * b32 - b31 * b22;
+  rby[7] = b31 * b12 - b11 * b32;
+  rby[8] = b11 * b22 - b21 * b12;
+}
+
+template <class R>
+__global__ void __launch_bounds__(RB_THREADS)
+rbody_kernel(NodeArgs<R> a, int parity, const RBodyDesc* __restrict__ bodies, const int* __restrict__ rb_nodes,
+             R* rby_state, double* rb_ekin, double* rb_ekinr) {
+  typedef typename Vec4<R>::T R4;
+  __shared__ double s_sum[6][RB_THREADS / 32];
+  __shared__ R s_am[3], s_vg[3], s_a[3];
+  __shared__ double s_xm[3];
+  __shared__ R s_vm[3];
+  __shared__ double s_dt[3];     // DT1, DT2, DT12
+  const RBodyDesc B = bodies[blockIdx.x];
+  const int M = B.master;
+  R* rby = rby_state + 12 * (size_t)blockIdx.x;
+  const double4 xm4 = a.X[M];
+  // ASSPAR4 sum of one node's slots, in ascending slot order
+  auto raw = [&](int n, R* f, R* mo) {
+    f[0] = f[1] = f[2] = mo[0] = mo[1] = mo[2] = R(0);
+    const int k0 = a.adsky[n], k1 = a.adsky[n + 1];
+    for (int k = k0; k < k1; ++k) {
+      const R4 g = a.fslot[k];
+      f[0] = f[0] + g.x; f[1] = f[1] + g.y; f[2] = f[2] + g.z;
+      if (a.mslot) { const R4 h = a.mslot[k]; mo[0] = mo[0] + h.x; mo[1] = mo[1] + h.y; mo[2] = mo[2] + h.z; }
+    }
+  };
+  // secondary nodes' forces and moments about the main node, FP64 partial sums
+  double S[6] = {0, 0, 0, 0, 0, 0};
+  for (int i = threadIdx.x; i < B.count; i += RB_THREADS) {
+    const int n = rb_nodes[B.first + i];
+    R f[3], mo[3];
+    raw(n, f, mo);
+    const double4 xn = a.X[n];
+    const R dx = R(xn.x - xm4.x), dy = R(xn.y - xm4.y), dz = R(xn.z - xm4.z);
+    S[0] += (double)f[0]; S[1] += (double)f[1]; S[2] += (double)f[2];
+    S[3] += (double)(mo[0] + dy * f[2] - dz * f[1]);
+    S[4] += (double)(mo[1] + dz * f[0] - dx * f[2]);
+    S[5] += (double)(mo[2] + dx * f[1] - dy * f[0]);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) S[q] += __shfl_xor_sync(0xffffffffu, S[q], o);
+    if (lane == 0) s_sum[q][warp] = S[q];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double T[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      T[q] = 0.0;
+      for (int w = 0; w < RB_THREADS / 32; ++w) T[q] += s_sum[q][w];
+    }
+    const PartTime t0 = a.time[parity * a.nparts + B.part];
+    const PartAcc ac = a.acc[parity * a.nparts + B.part];
+    int ityp, nelt;
+    double DT2;
+    cycle_dt(ac, t0, a.growth, a.dtmx, a.split, DT2, ityp, nelt);
+    const double DT1 = t0.dt2;
+    const double DT12 = 0.5 * (DT1 + DT2);
+    s_dt[0] = DT1; s_dt[1] = DT2; s_dt[2] = DT12;
+    // the main node: its own slots plus the body's sums (phase 2), the frame and
+    // the pseudo moment IN(M) * rotational acceleration
+    R af[3], am[3];
+    raw(M, af, am);
+    for (int c = 0; c < 3; ++c) { af[c] = R((double)af[c] + T[c]); am[c] = R((double)am[c] + T[3 + c]); }
+    const R4 wm = a.VR[M];              // .w = IN(M), the smallest principal inertia
+    const R inm = wm.w;
+    rby[9] = fmax(rby[9], inm); rby[10] = fmax(rby[10], inm); rby[11] = fmax(rby[11], inm);
+    R vi[3];
+    vi[0] = rby[0] * wm.x + rby[1] * wm.y + rby[2] * wm.z;
+    vi[1] = rby[3] * wm.x + rby[4] * wm.y + rby[5] * wm.z;
+    vi[2] = rby[6] * wm.x + rby[7] * wm.y + rby[8] * wm.z;
+    rotbmr_dev(vi, rby, R(DT1));
+    R p1 = rby[0] * am[0] + rby[1] * am[1] + rby[2] * am[2];
+    R p2 = rby[3] * am[0] + rby[4] * am[1] + rby[5] * am[2];
+    R p3 = rby[6] * am[0] + rby[7] * am[1] + rby[8] * am[2];
+    p1 = p1 + (rby[10] - rby[11]) * vi[1] * vi[2];
+    p2 = p2 + (rby[11] - rby[9]) * vi[2] * vi[0];
+    p3 = p3 + (rby[9] - rby[10]) * vi[0] * vi[1];
+    const R q1 = p1 * inm / rby[9], q2 = p2 * inm / rby[10], q3 = p3 * inm / rby[11];
+    am[0] = rby[0] * q1 + rby[3] * q2 + rby[6] * q3;
+    am[1] = rby[1] * q1 + rby[4] * q2 + rby[7] * q3;
+    am[2] = rby[2] * q1 + rby[5] * q2 + rby[8] * q3;
+    // ACCELE and BCS10 of the main node
+    const R msm = R(xm4.w);
+    R ax[3], ar[3];
+    for (int c = 0; c < 3; ++c) {
+      ax[c] = msm > R(0) ? af[c] * (R(1) / msm) : R(0);
+      ar[c] = inm > R(0) ? am[c] * (R(1) / inm) : R(0);
+    }
+    if (!isfinite((double)ax[0] + (double)ax[1] + (double)ax[2])) raise_error(a.err, 6, M);
+    R4 v = a.V[M], w = wm;
+    const unsigned char code = a.code[M];
+    const R* sk = (code & 128) ? a.skews + 9 * a.skew_of[M] : nullptr;
+    if (sk) {
+      bcs1v_skew(code & 7, sk, v.x, v.y, v.z);
+      bcs1v_skew(code & 7, sk, ax[0], ax[1], ax[2]);
+      bcs1v_skew((code >> 3) & 7, sk, w.x, w.y, w.z);
+      bcs1v_skew((code >> 3) & 7, sk, ar[0], ar[1], ar[2]);
+    } else {
+      if (code & 4) { v.x = R(0); ax[0] = R(0); }
+      if (code & 2) { v.y = R(0); ax[1] = R(0); }
+      if (code & 1) { v.z = R(0); ax[2] = R(0); }
+      if (code & 32) { w.x = R(0); ar[0] = R(0); }
+      if (code & 16) { w.y = R(0); ar[1] = R(0); }
+      if (code & 8)  { w.z = R(0); ar[2] = R(0); }
+    }
+    const R dt12 = R(DT12);
+    s_vg[0] = w.x + ar[0] * dt12; s_vg[1] = w.y + ar[1] * dt12; s_vg[2] = w.z + ar[2] * dt12;
+    s_a[0] = ax[0]; s_a[1] = ax[1]; s_a[2] = ax[2];
+    s_vm[0] = v.x; s_vm[1] = v.y; s_vm[2] = v.z;
+    s_xm[0] = xm4.x; s_xm[1] = xm4.y; s_xm[2] = xm4.z;
+    // kinetic energy (ECRIT + RBYCOR): the body's mass on its main node, its
+    // rotation in the principal frame
+    const double dt05 = 0.5 * DT1;
+    {
+      const double vx = (double)v.x + dt05 * (double)ax[0], vy = (double)v.y + dt05 * (double)ax[1],
+                   vz = (double)v.z + dt05 * (double)ax[2];
+      rb_ekin[blockIdx.x] = (vx * vx + vy * vy + vz * vz) * 0.5 * (double)msm;
+      const R h = R(dt05);
+      const R w1 = w.x + ar[0] * h, w2 = w.y + ar[1] * h, w3 = w.z + ar[2] * h;
+      const R i1 = rby[0] * w1 + rby[1] * w2 + rby[2] * w3;
+      const R i2 = rby[3] * w1 + rby[4] * w2 + rby[5] * w3;
+      const R i3 = rby[6] * w1 + rby[7] * w2 + rby[8] * w3;
+      rb_ekinr[blockIdx.x] = 0.5 * ((double)rby[9] * (double)i1 * (double)i1 +
+                                    (double)rby[10] * (double)i2 * (double)i2 +
+                                    (double)rby[11] * (double)i3 * (double)i3);
+    }
+    s_am[0] = ar[0]; s_am[1] = ar[1]; s_am[2] = ar[2];
+  }
+  __syncthreads();
+  const double DT2 = s_dt[1];
+  const R dt12 = R(s_dt[2]), dt2 = R(DT2);
+  const R usdt = R(1) / dt12;
+  const R vg0 = s_vg[0], vg1 = s_vg[1], vg2 = s_vg[2];
+  // RGBODV: the secondary nodes move with the body; then VELOCITY and DEPLA
+  for (int i = threadIdx.x; i < B.count; i += RB_THREADS) {
+    const int n = rb_nodes[B.first + i];
+    R4 v = a.V[n], w = a.VR ? a.VR[n] : mk4(R(0), R(0), R(0), R(0));
+    const unsigned char code = a.code[n];
+    const R* sk = (code & 128) ? a.skews + 9 * a.skew_of[n] : nullptr;
+    if (sk) {
+      bcs1v_skew(code & 7, sk, v.x, v.y, v.z);
+      bcs1v_skew((code >> 3) & 7, sk, w.x, w.y, w.z);
+    } else {
+      if (code & 4) v.x = R(0);
+      if (code & 2) v.y = R(0);
+      if (code & 1) v.z = R(0);
+      if (code & 32) w.x = R(0);
+      if (code & 16) w.y = R(0);
+      if (code & 8)  w.z = R(0);
+    }
+    const R arx = (vg0 - w.x) * usdt, ary = (vg1 - w.y) * usdt, arz = (vg2 - w.z) * usdt;
+    const double4 xn = a.X[n];
+    const R dx = R(xn.x - s_xm[0]), dy = R(xn.y - s_xm[1]), dz = R(xn.z - s_xm[2]);
+    const R v1x2 = vg0 * dy, v2x1 = vg1 * dx, v2x3 = vg1 * dz, v3x2 = vg2 * dy, v3x1 = vg2 * dx, v1x3 = vg0 * dz;
+    const R vx1 = v2x3 - v3x2, vx2 = v3x1 - v1x3, vx3 = v1x2 - v2x1;
+    const R ax = s_a[0] + (s_vm[0] + vx1 + R(0.5) * dt2 * (vg1 * vx3 - vg2 * vx2) - v.x) * usdt;
+    const R ay = s_a[1] + (s_vm[1] + vx2 + R(0.5) * dt2 * (vg2 * vx1 - vg0 * vx3) - v.y) * usdt;
+    const R az = s_a[2] + (s_vm[2] + vx3 + R(0.5) * dt2 * (vg0 * vx2 - vg1 * vx1) - v.z) * usdt;
+    v.x = v.x + dt12 * ax; v.y = v.y + dt12 * ay; v.z = v.z + dt12 * az;
+    a.V[n] = v;
+    if (a.VR) {
+      w.x = w.x + dt12 * arx; w.y = w.y + dt12 * ary; w.z = w.z + dt12 * arz;
+      a.VR[n] = w;
+    }
+    const double ux = DT2 * (double)v.x, uy = DT2 * (double)v.y, uz = DT2 * (double)v.z;
+    a.DX[n] = a.DX[n] + ux; a.DY[n] = a.DY[n] + uy; a.DZ[n] = a.DZ[n] + uz;
+    a.X[n] = make_double4(xn.x + ux, xn.y + uy, xn.z + uz, xn.w);
+  }
+  __syncthreads();          // the secondary nodes read the main node's old state
+  if (threadIdx.x == 0) {
+    R4 v = a.V[M], w = a.VR[M];
+    const unsigned char code = a.code[M];
+    const R* sk = (code & 128) ? a.skews + 9 * a.skew_of[M] : nullptr;
+    if (sk) {
+      bcs1v_skew(code & 7, sk, v.x, v.y, v.z);
+      bcs1v_skew((code >> 3) & 7, sk, w.x, w.y, w.z);
+    } else {
+      if (code & 4) v.x = R(0);
+      if (code & 2) v.y = R(0);
+      if (code & 1) v.z = R(0);
+      if (code & 32) w.x = R(0);
+      if (code & 16) w.y = R(0);
+      if (code & 8)  w.z = R(0);
+    }
+    v.x = v.x + dt12 * s_a[0]; v.y = v.y + dt12 * s_a[1]; v.z = v.z + dt12 * s_a[2];
+    w.x = w.x + dt12 * s_am[0]; w.y = w.y + dt12 * s_am[1]; w.z = w.z + dt12 * s_am[2];
+    a.V[M] = v;
+    a.VR[M] = w;
+    const double ux = DT2 * (double)v.x, uy = DT2 * (double)v.y, uz = DT2 * (double)v.z;
+    a.DX[M] = a.DX[M] + ux; a.DY[M] = a.DY[M] + uy; a.DZ[M] = a.DZ[M] + uz;
+    a.X[M] = make_double4(s_xm[0] + ux, s_xm[1] + uy, s_xm[2] + uz, xm4.w);
   }
 }
 

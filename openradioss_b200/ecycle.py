@@ -49,7 +49,7 @@ EXPORTS = [
     "or_ecycle_spmd_elements", "or_ecycle_spmd_nodes", "or_ecycle_spmd_end", "or_ecycle_add_rlink",
     "or_ecycle_set_rlink", "or_ecycle_add_function", "or_ecycle_add_cload", "or_ecycle_add_pload",
     "or_ecycle_add_skew", "or_ecycle_set_bcs_skew", "or_ecycle_set_hex_state", "or_ecycle_set_shell_state",
-    "or_ecycle_set_energy_sums", "or_ecycle_persistent_info",
+    "or_ecycle_set_energy_sums", "or_ecycle_persistent_info", "or_ecycle_add_rbody",
 ]
 
 
@@ -69,6 +69,7 @@ def _declare(lib):
         "or_ecycle_set_shell_yield": ([P, C.c_int, dp], C.c_int),
         "or_ecycle_add_rlink": ([P, C.c_int, C.c_int, ip, C.c_int, C.c_int, ip], C.c_int),
         "or_ecycle_set_rlink": ([P, C.c_int, C.c_int, C.c_int], C.c_int),
+        "or_ecycle_add_rbody": ([P, C.c_int, C.c_int, C.c_int, ip, dp, ip], C.c_int),
         "or_ecycle_add_function": ([P, C.c_int, dp, dp, ip], C.c_int),
         "or_ecycle_add_cload": ([P, C.c_int, C.c_int, ip, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, ip],
                                 C.c_int),
@@ -266,6 +267,10 @@ class ECycle(_DeckModel):
         li = C.c_int()
         self._call("add_rlink", part, n, abi.ptr(nodes, C.c_int), ic, icr, C.byref(li))
         return li.value
+
+    def _add_rbody(self, part, master, n, slaves, rby):
+        body = C.c_int()
+        self._call("add_rbody", part, master, n, abi.ptr(slaves, C.c_int), abi.ptr(rby, C.c_double), C.byref(body))
 
     def _add_function(self, n, x, y):
         k = C.c_int()
