@@ -25,6 +25,8 @@
 #include <vector>
 #include <array>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/or_ecycle.h"
 #include "ecycle_kernels.cuh"
 #include "persistent_kernel.cuh"
@@ -129,6 +131,13 @@ struct or_ecycle {
 };
 
 namespace {
+
+// NVTX range over a host call (tracing: nsys and ncu show the library's calls and
+// phases on the timeline; NVTX is header-only and inert without a profiler)
+struct Trace {
+  explicit Trace(const char* name) { nvtxRangePushA(name); }
+  ~Trace() { nvtxRangePop(); }
+};
 
 int fail(or_ecycle* h, int code, const std::string& msg) {
   if (h) h->err = msg;
@@ -676,6 +685,7 @@ int launch_persistent(or_ecycle* h, Impl<R>& m, int ncycles, int parity0) {
   const float* zw = m.zw.p;
   void* args[] = {&sa, &na, &pa, &ncycles, &parity0, &zw};
   const PersistFn<R> fn = persist_fn<R>(h->tile_shell, m.uniform_npt == 5);
+  Trace tr("persistent cycles");
   const cudaError_t e =
       cudaLaunchCooperativeKernel((const void*)fn, dim3(q.G), dim3(q.P * h->tile_shell), args, q.smem, h->stream);
   if (e == cudaErrorCooperativeLaunchTooLarge) {   // the wave no longer fits (another context holds SMs):
@@ -694,6 +704,7 @@ int launch_cycle(or_ecycle* h, Impl<R>& m, int parity, cudaEvent_t* ev) {
   if (ev) CK(cudaEventRecord(ev[0], h->stream));
   // per-phase events need the kernels serialised
   const bool pdl = h->pdl && !ev;
+  Trace tr(parity ? "cycle (odd)" : "cycle (even)");
   if ((rc = launch_loads<R>(h, m, parity))) return rc;     // FORCE (resol.F:2847), before the elements
   rc = h->tile_hex == 64 ? launch_hex<R, 64>(h, m, parity, pdl)
        : h->tile_hex == 128 ? launch_hex<R, 128>(h, m, parity, pdl) : launch_hex<R, 256>(h, m, parity, pdl);
@@ -2230,6 +2241,7 @@ int or_ecycle_set_bcs_skew(or_ecycle* h, int part, const int* skew) {
 }
 
 int or_ecycle_finalize(or_ecycle* h) {
+  Trace tr("or_ecycle_finalize");
   if (!h) return OR_E_ARG;
   if (h->finalized) return fail(h, OR_E_STATE, "finalize called twice");
   if (h->parts.empty()) return fail(h, OR_E_STATE, "finalize without parts");
@@ -2241,6 +2253,7 @@ int or_ecycle_finalize(or_ecycle* h) {
 }
 
 int or_ecycle_reset(or_ecycle* h) {
+  Trace tr("or_ecycle_reset");
   if (!h) return OR_E_ARG;
   if (!h->finalized) return fail(h, OR_E_STATE, "reset before finalize");
   cudaSetDevice(h->cfg.device);
@@ -2250,6 +2263,7 @@ int or_ecycle_reset(or_ecycle* h) {
 }
 
 int or_ecycle_step(or_ecycle* h, int ncycles, or_ecycle_time* t) {
+  Trace tr("or_ecycle_step");
   if (!h) return OR_E_ARG;
   if (!h->finalized) return fail(h, OR_E_STATE, "step before finalize");
   if (ncycles < 0 || !t) return fail(h, OR_E_ARG, "step: bad argument");
@@ -2260,6 +2274,7 @@ int or_ecycle_step(or_ecycle* h, int ncycles, or_ecycle_time* t) {
 
 int or_ecycle_adjoint(or_ecycle* h, int ncycles, const or_adjoint_response* r, or_ecycle_time* t, double* J,
                       double* dJ_dA, double* dJ_dthk, double* dJ_dms, double* dJ_din) {
+  Trace tr("or_ecycle_adjoint");
   if (!h) return OR_E_ARG;
   if (!h->finalized) return fail(h, OR_E_STATE, "adjoint before finalize");
   if (ncycles <= 0 || !r || !t) return fail(h, OR_E_ARG, "adjoint: bad argument");
@@ -2402,6 +2417,7 @@ int or_ecycle_phase_times(or_ecycle* h, double* ms4) {
 }
 
 int or_ecycle_kernel_times(or_ecycle* h, int reps, double* us3) {
+  Trace tr("or_ecycle_kernel_times");
   if (!h || !us3) return OR_E_ARG;
   if (!h->finalized) return fail(h, OR_E_STATE, "kernel_times before finalize");
   if (reps <= 0 || reps > 4096) return fail(h, OR_E_ARG, "kernel_times: reps outside 1..4096");
