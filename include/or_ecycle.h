@@ -77,6 +77,8 @@ typedef struct {
   int    block_hex;     /* threads per block, hex kernel   (0 = autotuned)           */
   int    block_shell;   /* threads per block, shell kernel (0 = autotuned)           */
   int    block_node;    /* threads per block, nodal kernel (0 = autotuned)           */
+  int    persistent;    /* 0: the persistent shell cycle where eligible; -1: never
+                           (see or_ecycle_persistent_info)                          */
 } or_ecycle_config;
 
 /* PM(.,MAT) entries used on the path (hm_read_mat02_jc.F90, m1law.F, m2law.F) */
@@ -309,9 +311,13 @@ int  or_ecycle_device_bytes(or_ecycle* h, long long* bytes);
    element state in registers and their nodes in shared memory, with one grid
    barrier per cycle.  Chosen at finalize for one part of shell groups with no
    rigid links and no /CLOAD or /PLOAD loads, graph = 1, whose patches fit one
-   wave; OR_ECYCLE_PERSISTENT=0 in the environment turns it off.  Results are bit
-   for bit those of the per-phase kernels.  ctas, threads: its launch shape (0
-   when off; either may be NULL).  No counterpart in the reference. */
+   wave; cfg.persistent = -1, or OR_ECYCLE_PERSISTENT=0 in the environment, turns
+   it off.  It performs the per-phase kernels' operations in the same order, so
+   its results are theirs bit for bit when floating-point contraction is off
+   (the library built with -fmad=false); with FMA contraction the compiler may
+   fuse a multiply-add in one kernel and not in the other, and the two agree to
+   rounding.  ctas, threads: its launch shape (0 when off; either may be NULL).
+   No counterpart in the reference. */
 int  or_ecycle_persistent_info(or_ecycle* h, int* on, int* ctas, int* threads);
 
 /* --- domain decomposition (one part split over ranks) ---------------------- */
@@ -320,19 +326,32 @@ int  or_ecycle_persistent_info(or_ecycle* h, int* on, int* ctas, int* threads);
    cycle, the ranks exchange the partial force/moment sums of the nodes they
    share (SPMD_EXCH_A, resol.F after FORINT) and take the minimum of their
    element time steps (SPMD_GLOB_MIN5).  The exchange itself is the caller's
-   (NCCL all-gather over NVLink, or any transport):
+   (NCCL over NVLink, or any transport):
      or_ecycle_spmd_begin(h, t)
      per cycle: or_ecycle_spmd_elements(h, my_buf)      element kernels + pack
-                all-gather my_buf of every rank into bufs, rank order
-                or_ecycle_spmd_nodes(h, bufs, nranks)    nodal phase
+                exchange (below) into bufs
+                or_ecycle_spmd_nodes(h, bufs, nviews)    nodal phase
      or_ecycle_spmd_end(h, t)
-   A shared node's force is the sum of every rank's partial in rank order, so
-   every rank computes the same nodal update.  Buffers are device memory of
-   or_ecycle_spmd_buffer_bytes each, on the handle's device; the per-cycle
-   calls are asynchronous on the handle's stream, begin and end synchronous.
+   A buffer (or_ecycle_spmd_buffer_bytes bytes, device memory on the handle's
+   device) holds nhalo force sums of 4 reals (x, y, z, unused), nhalo moment
+   sums of 4 reals, then the 16-byte time-step reduction (two unsigned 64-bit
+   keys, minimum wins); reals are double, or float for OR_PREC_SPLIT.
+   spmd_elements packs this rank's partial sums at its halo slots.  bufs are
+   nviews such buffers, one per rank in ascending rank order, all in this
+   rank's slot numbering: this rank's own, and for other ranks their partial
+   sums at the slots of the nodes they hold (zero elsewhere).  The node pass
+   sets a halo node's force to the sum of the buffers' entries in that order,
+   and takes the time step from the minimum of the buffers' reductions: the
+   caller either passes every rank's buffer (an all-gather, nviews = ranks) or
+   only its neighbours' with the all-rank minimum already in its own reduction
+   (a neighbour exchange plus a 16-byte all-reduce, as the reference does).
+   Either way every rank holding a node computes the same nodal update.  The
+   per-cycle calls are asynchronous on the handle's stream, begin and end
+   synchronous.
    or_ecycle_set_halo: the part's nodes shared with other ranks, as nloc
-   (part-local node, global halo slot in [0, nhalo)) pairs; count_ke[i] = 0 when
-   another rank counts the node's kinetic energy (NULL: all counted).
+   (part-local node, halo slot in [0, nhalo)) pairs, the numbering of this
+   rank's buffers; count_ke[i] = 0 when another rank counts the node's kinetic
+   energy (NULL: all counted).
    One part per handle.  No counterpart in the reference's C interfaces: the
    reference does this exchange in Fortran over MPI. */
 int  or_ecycle_set_halo(or_ecycle* h, int part, int nloc, const int* local_node, const int* halo_slot,
@@ -340,7 +359,7 @@ int  or_ecycle_set_halo(or_ecycle* h, int part, int nloc, const int* local_node,
 int  or_ecycle_spmd_buffer_bytes(or_ecycle* h, long long* bytes);
 int  or_ecycle_spmd_begin(or_ecycle* h, or_ecycle_time* t);
 int  or_ecycle_spmd_elements(or_ecycle* h, void* dev_buf);
-int  or_ecycle_spmd_nodes(or_ecycle* h, const void* dev_bufs, int nranks);
+int  or_ecycle_spmd_nodes(or_ecycle* h, const void* dev_bufs, int nviews);
 int  or_ecycle_spmd_end(or_ecycle* h, or_ecycle_time* t);
 
 /* --- adjoint (design sensitivities) -------------------------------------- */
@@ -356,8 +375,10 @@ typedef struct {
   double w_plastic;
 } or_adjoint_response;
 
-/* Runs ncycles from the current state exactly like or_ecycle_step (the handle
-   ends in the same state, t is updated the same way), then the hand-written
+/* Runs ncycles from the current state exactly like or_ecycle_step with the
+   per-phase kernels (the handle ends in the same state, t is updated the same
+   way; on a handle that steps with the persistent kernel the two agree to
+   rounding, see or_ecycle_persistent_info), then the hand-written
    reverse of those cycles, and returns J and its gradient with respect to
    - dJ_dA:   the Johnson-Cook yield A of every shell element (shell groups in
               add order, elements in IXC order; 0 for LAW1 groups),

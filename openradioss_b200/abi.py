@@ -31,7 +31,7 @@ class Config(C.Structure):
                 ("dtmin_solid", C.c_double), ("dtmin_shell", C.c_double),
                 ("dtmx", C.c_double), ("dt_growth", C.c_double),
                 ("graph", C.c_int), ("block_hex", C.c_int), ("block_shell", C.c_int),
-                ("block_node", C.c_int)]
+                ("block_node", C.c_int), ("persistent", C.c_int)]
 
 
 class Material(C.Structure):
@@ -73,9 +73,9 @@ DT_GROWTH_REF = float(__import__("numpy").float32(1.1))
 
 def make_config(precision=OR_PREC_FP64, device=0, dtfac_solid=0.9, dtfac_shell=0.9,
                 dtmx=1e20, graph=1, block_hex=0, block_shell=0, block_node=0,
-                dtmin_solid=0.0, dtmin_shell=0.0):
+                dtmin_solid=0.0, dtmin_shell=0.0, persistent=0):
     return Config(precision, device, dtfac_solid, dtfac_shell, dtmin_solid, dtmin_shell, dtmx,
-                  DT_GROWTH_REF, graph, block_hex, block_shell, block_node)
+                  DT_GROWTH_REF, graph, block_hex, block_shell, block_node, persistent)
 
 
 def make_material(m: dict) -> Material:

@@ -593,7 +593,8 @@ PersistFn<R> persist_fn(int tile, bool npt5) {
 
 // Sets up the persistent launch when the handle qualifies: step() through a graph
 // (cfg.graph != 0), one part, shell groups only, no rigid links and no /CLOAD or
-// /PLOAD loads (the group pressure is fine), OR_ECYCLE_PERSISTENT not 0, and the
+// /PLOAD loads (the group pressure is fine), cfg.persistent not negative and
+// OR_ECYCLE_PERSISTENT not 0, and the
 // patches fit one cooperative wave of at most PERSIST_THREADS threads per CTA.
 // Each CTA takes P consecutive patches (Morton order keeps them compact) and holds
 // every node they touch; nodes no element touches are spread over the CTAs.
@@ -601,6 +602,7 @@ template <class R>
 int persist_build(or_ecycle* h, Impl<R>& m) {
   auto& q = m.per;
   q.on = false;
+  if (h->cfg.persistent < 0) return OR_OK;
   if (const char* s = std::getenv("OR_ECYCLE_PERSISTENT"))
     if (std::atoi(s) == 0) return OR_OK;
   if (!h->cfg.graph || m.nparts != 1 || !h->hex.empty() || h->shell.empty() || !h->links.empty() || m.nload ||

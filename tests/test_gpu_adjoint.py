@@ -63,8 +63,9 @@ def base_params(n, seed=1):
 
 
 def forward_J(deck, ncycles, node, w_disp, w_plastic):
+    """J of a regular step() on the per-phase kernels, the adjoint's forward."""
     from openradioss_b200.ecycle import ECycle
-    h = ECycle(deck, precision=abi.OR_PREC_FP64)
+    h = ECycle(deck, precision=abi.OR_PREC_FP64, persistent=-1)
     wp0 = h.energies()["plastic_work"]
     h.step(ncycles)
     J = w_disp * h.get_nodes()["d"][node, 2] + w_plastic * (h.energies()["plastic_work"] - wp0)
@@ -253,8 +254,9 @@ def test_adjoint_nodal_mass_gradient():
 
 
 def test_adjoint_leaves_the_step_state_and_is_checkpoint_independent():
-    """After or_ecycle_adjoint the handle holds what or_ecycle_step would
-    leave; the gradient does not depend on the checkpoint interval."""
+    """After or_ecycle_adjoint the handle holds what or_ecycle_step on the
+    per-phase kernels would leave; the gradient does not depend on the
+    checkpoint interval."""
     need_gpu()
     from openradioss_b200.ecycle import ECycle
     n, p, N = 32, 2e6, 120
@@ -265,7 +267,7 @@ def test_adjoint_leaves_the_step_state_and_is_checkpoint_independent():
     r7 = adjoint_run(d0, N, node, 1.0, 0.5, checkpoint=7)
     for k in ("dA", "dthk", "dms", "din"):
         assert np.array_equal(r50[k][0], r7[k][0]), k
-    h = ECycle(d0, precision=abi.OR_PREC_FP64)
+    h = ECycle(d0, precision=abi.OR_PREC_FP64, persistent=-1)
     h.step(N)
     ref = h.get_nodes()
     for k in ("x", "d", "v", "vr"):

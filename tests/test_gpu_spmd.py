@@ -4,9 +4,10 @@ The NCCL path with the exchange captured in a CUDA graph runs as one rank
 (NCCL takes one GPU per rank): the capture, the replays and the eager
 remainder against the one-handle run, bitwise.
 
-Two ranks (processes) each run their share of the elements on the same GPU
-through the library's SPMD entry points and exchange the halo buffers over
-gloo through host memory, so their kernels never wait on each other.  The
+Two and three ranks (processes) each run their share of the elements on the
+same GPU through the library's SPMD entry points and exchange the shared
+nodes' partial sums with their neighbours (spmd.HaloExchange) over gloo
+through host memory, so their kernels never wait on each other.  The
 assembled displacements, the energies and the time must match a single
 handle on the whole mesh: FP64 at 1e-10 relative (the shared nodes' force
 sums are associated by rank instead of by patch), the split form at 1e-5.
@@ -66,12 +67,14 @@ def _run(which, ncycles, precision, world=2):
     return sorted(res, key=lambda r: r[0])
 
 
-@pytest.mark.parametrize("which,ncycles,precision,tol", [
-    ("plate", 120, abi.OR_PREC_FP64, 1e-10),
-    ("mixed", 80, abi.OR_PREC_FP64, 1e-10),
-    ("plate", 120, abi.OR_PREC_SPLIT, 1e-5),
+@pytest.mark.parametrize("which,ncycles,precision,tol,world", [
+    ("plate", 120, abi.OR_PREC_FP64, 1e-10, 2),
+    ("mixed", 80, abi.OR_PREC_FP64, 1e-10, 2),
+    ("plate", 120, abi.OR_PREC_SPLIT, 1e-5, 2),
+    ("plate", 120, abi.OR_PREC_FP64, 1e-10, 3),
+    ("mixed", 80, abi.OR_PREC_SPLIT, 1e-5, 3),
 ])
-def test_two_domains_match_one_handle(which, ncycles, precision, tol):
+def test_domains_match_one_handle(which, ncycles, precision, tol, world):
     import torch
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
@@ -82,7 +85,7 @@ def test_two_domains_match_one_handle(which, ncycles, precision, tol):
     ref = ECycle(deck, precision=precision)
     ref.step(ncycles)
     rn = ref.get_nodes()
-    res = _run(which, ncycles, precision)
+    res = _run(which, ncycles, precision, world)
     n = deck["parts"][0]["x"].shape[0]
     d = np.full((n, 3), np.nan)
     for rank, ids, dd, vv, e, t in res:
@@ -131,7 +134,7 @@ def test_nccl_exchange_in_a_cuda_graph(which, precision):
     build.build()
     steps = (70, 75)
     deck = _deck(which)
-    ref = ECycle(deck, precision=precision)
+    ref = ECycle(deck, precision=precision, persistent=-1)      # the domain runs the per-phase kernels
     ref.step(sum(steps))
     rn = ref.get_nodes()
     ctx = pymp.get_context("spawn")
