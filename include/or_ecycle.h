@@ -123,6 +123,17 @@ typedef struct {
   double hm, hf, hr;    /* GEO(13..15) hourglass coefficients                     */
   double shf;           /* shear factor SHF (5/6 for ISH=0)                       */
   double pressure;      /* uniform /PLOAD-style pressure on the group, Pa (0=none)*/
+  double dn;            /* GEO(17) numerical damping Dn: the V-shape hourglass
+                           coefficient of one-point shells (mhvis3.F)             */
+  int    ishell;        /* Ishell of /PROP/SHELL as the starter leaves it
+                           (hm_read_prop01.F:141-315): 0 or 1 Q4 with CHVIS3 shape
+                           vectors (engine IHBE 1), 2 Q4 with plain hourglass
+                           vectors (IHBE 0), 3 Q4 with warping terms and CHSTI3
+                           elasto-plastic hourglass (IHBE 2), 4 Q4 with warping
+                           terms (IHBE 4).  With npt = 1, Ishell 0 and 2 become 1
+                           (hm_read_prop01.F:246-250) and the hourglass forces are
+                           MHVIS3's.  Ismstr 2 throughout.                        */
+  int    pad;
 } or_shell_prop;
 
 /* time-step state of one part, in/out of or_ecycle_step (RESOL scalars) */

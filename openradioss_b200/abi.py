@@ -48,7 +48,7 @@ class SolidProp(C.Structure):
 class ShellProp(C.Structure):
     _fields_ = [("thk", C.c_double), ("npt", C.c_int), ("ithk", C.c_int), ("ipla", C.c_int),
                 ("ishfram", C.c_int), ("hm", C.c_double), ("hf", C.c_double), ("hr", C.c_double), ("shf", C.c_double),
-                ("pressure", C.c_double)]
+                ("pressure", C.c_double), ("dn", C.c_double), ("ishell", C.c_int), ("pad", C.c_int)]
 
 
 class Time(C.Structure):
@@ -89,7 +89,8 @@ def make_solid_prop(p: dict) -> SolidProp:
 
 def make_shell_prop(p: dict) -> ShellProp:
     return ShellProp(p["thk"], int(p["npt"]), int(p["ithk"]), int(p["ipla"]), int(p.get("ishfram", 0)),
-                     p["hm"], p["hf"], p["hr"], p["shf"], p["pressure"])
+                     p["hm"], p["hf"], p["hr"], p["shf"], p["pressure"], float(p.get("dn", 0.0)),
+                     int(p.get("ishell", 1)), 0)
 
 
 def initial_time(dt2old=1e30):

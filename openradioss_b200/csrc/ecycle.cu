@@ -144,6 +144,14 @@ int fail(or_ecycle* h, int code, const std::string& msg) {
   return code;
 }
 
+// The engine's IHBE (IPARG(23)) of a shell group from the starter's Ishell:
+// 0 is the default 1 (hm_read_prop01.F:176), one integration point turns 2 into 1
+// (:246-250), and GEO(171) maps 1, 2, 3, 4 to 1, 0, 2, 4 (:305-315, cgrtails.F:553).
+int shell_ihbe(int ishell, int npt) {
+  if (ishell == 0 || (npt == 1 && ishell == 2)) ishell = 1;
+  return ishell == 1 ? 1 : ishell == 2 ? 0 : ishell == 3 ? 2 : 4;
+}
+
 #define CK(call)                                                                  \
   do {                                                                            \
     cudaError_t e_ = (call);                                                      \
@@ -345,6 +353,7 @@ struct Impl {
   bool any_corot = false;    // a hexa group in the convected frame (JCVT /= 0)
   // nodes
   DBuf<double4> X; DBuf<double> DX, DY, DZ; DBuf<R4> V, VR; DBuf<unsigned char> code;
+  DBuf<unsigned> rotmask; std::vector<unsigned> rotmask_h;   // NodeArgs::rotmask, and its host copy
   DBuf<int> adsky, tile_part; DBuf<PartDesc> partd;
   DBuf<R4> fslot, mslot;
   DBuf<PartTime> time; DBuf<PartAcc> acc; DBuf<ErrorWord> err;
@@ -424,10 +433,12 @@ struct Impl {
     a.link_of = nlinks ? link_of.p : nullptr; a.link_mean = nlinks ? link_mean.p : nullptr;
     a.skew_of = skew_of.p; a.skews = skw.p;
     a.rb_role = nrb ? rb_role.p : nullptr;
+    a.rotmask = any_rot ? rotmask.p : nullptr;
     return a;
   }
   void free_all() {
     dfree(X); dfree(DX); dfree(DY); dfree(DZ); dfree(V); dfree(VR); dfree(code); dfree(adsky); dfree(tile_part);
+    dfree(rotmask);
     dfree(partd); dfree(fslot); dfree(mslot); dfree(time); dfree(acc); dfree(err); dfree(ekin); dfree(ekinr);
     dfree(hinc); dfree(sinc);
     dfree(hpatch); dfree(hdesc); dfree(hnodes); dfree(hslots); dfree(helem); dfree(hconn); dfree(hsig); dfree(heint);
@@ -730,6 +741,20 @@ int launch_cycle(or_ecycle* h, Impl<R>& m, int parity, cudaEvent_t* ev) {
 template <class R>
 int reset_impl(or_ecycle* h);
 
+// NodeArgs::rotmask bits of part P's nodes, from its inertias and the rotational
+// velocities vr (3 per node, part order): set where the part has rotations and the
+// node's inertia or rotational velocity is nonzero, in the handle's precision.
+template <class R>
+void rot_bits(Impl<R>& m, const HPart& P, const double* vr) {
+  for (int i = 0; i < P.numnod; ++i) {
+    const int g = P.node_start + i;
+    const bool on = P.has_rot && (R(P.in[i]) > R(0) || R(vr[3 * i]) != R(0) || R(vr[3 * i + 1]) != R(0) ||
+                                  R(vr[3 * i + 2]) != R(0));
+    unsigned& w = m.rotmask_h[g >> 5];
+    w = on ? (w | (1u << (g & 31))) : (w & ~(1u << (g & 31)));
+  }
+}
+
 template <class R>
 int finalize_impl(or_ecycle* h) {
   typedef typename Vec4<R>::T R4;
@@ -895,8 +920,14 @@ int finalize_impl(or_ecycle* h) {
         (rc = dput(h, m.rb_ekr, std::vector<double>(m.nrb, 0.0))))
       return rc;
   }
+  if (m.any_rot) {
+    m.rotmask_h.assign((nn + 31) / 32, 0u);
+    for (auto& P : h->parts)
+      if (P.has_rot) rot_bits<R>(m, P, P.vr.data());
+  }
   if ((rc = dput(h, m.X, X)) || (rc = dput(h, m.V, V)) || (rc = dput(h, m.VR, VR)) || (rc = dput(h, m.code, code)) ||
-      (rc = dput(h, m.adsky, adsky)) || (rc = dput(h, m.tile_part, tile_part)) || (rc = dput(h, m.partd, pd)))
+      (rc = dput(h, m.adsky, adsky)) || (rc = dput(h, m.tile_part, tile_part)) || (rc = dput(h, m.partd, pd)) ||
+      (rc = dput(h, m.rotmask, m.rotmask_h)))
     return rc;
   std::vector<double> zero(nn, 0.0);
   if ((rc = dput(h, m.DX, zero)) || (rc = dput(h, m.DY, zero)) || (rc = dput(h, m.DZ, zero))) return rc;
@@ -978,6 +1009,8 @@ int finalize_impl(or_ecycle* h) {
       d.part = g.part; d.law = g.mat.law; d.nel = g.nel; d.npt = g.prop.npt; d.ithk = g.prop.ithk;
       d.ishfram = g.prop.ishfram;
       d.ipla = g.prop.ipla;
+      d.ihbe = shell_ihbe(g.prop.ishell, g.prop.npt);
+      d.dn = g.prop.dn;
       d.has_jca = g.jca.empty() ? 0 : 1;
       any_jca = any_jca || !g.jca.empty();
       d.rho0 = g.mat.rho0; d.young = g.mat.young; d.nu = g.mat.nu; d.shear = g.mat.shear; d.a11 = g.mat.a11;
@@ -1054,7 +1087,12 @@ int reset_impl(or_ecycle* h) {
     }
   CK(cudaMemcpy(m.X.p, X.data(), X.size() * sizeof(double4), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(m.V.p, V.data(), V.size() * sizeof(R4), cudaMemcpyHostToDevice));
-  if (m.any_rot) CK(cudaMemcpy(m.VR.p, VR.data(), VR.size() * sizeof(R4), cudaMemcpyHostToDevice));
+  if (m.any_rot) {
+    CK(cudaMemcpy(m.VR.p, VR.data(), VR.size() * sizeof(R4), cudaMemcpyHostToDevice));
+    for (auto& P : h->parts)
+      if (P.has_rot) rot_bits<R>(m, P, P.vr.data());
+    CK(cudaMemcpy(m.rotmask.p, m.rotmask_h.data(), m.rotmask_h.size() * sizeof(unsigned), cudaMemcpyHostToDevice));
+  }
   CK(cudaMemset(m.DX.p, 0, nn * sizeof(double)));
   CK(cudaMemset(m.DY.p, 0, nn * sizeof(double)));
   CK(cudaMemset(m.DZ.p, 0, nn * sizeof(double)));
@@ -1306,6 +1344,11 @@ int set_nodes_impl(or_ecycle* h, int part, const double* x, const double* d, con
     node_io_kernel<R><<<(n + 255) / 256, 256, 0, h->stream>>>(kind, 1, m.stage.p, n, s, m.X.p, m.DX.p, m.DY.p, m.DZ.p,
                                                              m.V.p, m.VR.p);
     CK(cudaGetLastError());
+  }
+  if (src[3] && P.has_rot) {     // a rotational velocity set on a node without inertia
+    rot_bits<R>(m, P, vr);
+    CK(cudaMemcpyAsync(m.rotmask.p, m.rotmask_h.data(), m.rotmask_h.size() * sizeof(unsigned), cudaMemcpyHostToDevice,
+                       h->stream));
   }
   CK(cudaStreamSynchronize(h->stream));
   return OR_OK;
@@ -2055,6 +2098,8 @@ int or_ecycle_add_shell_group(or_ecycle* h, int part, int nel, const int* ixc, c
   if (prop->npt < 1 || prop->npt > 10) return fail(h, OR_E_UNSUPPORTED, "shell npt outside 1..10");
   if (prop->ipla < 0 || prop->ipla > 2) return fail(h, OR_E_UNSUPPORTED, "shell IPLA outside 0..2");
   if (prop->ishfram != 0 && prop->ishfram != 2) return fail(h, OR_E_UNSUPPORTED, "shell ISHFRAM other than 0 or 2");
+  if (prop->ishell < 0 || prop->ishell > 4) return fail(h, OR_E_UNSUPPORTED, "shell Ishell outside 1..4");
+  if (!(prop->dn >= 0)) return fail(h, OR_E_ARG, "shell Dn negative");
   if (mat->law != OR_LAW_ELASTIC && mat->law != OR_LAW_JOHNSON_COOK) return fail(h, OR_E_UNSUPPORTED, "shell law");
   HShell g;
   g.part = part; g.nel = nel; g.mat = *mat; g.prop = *prop;
@@ -2284,8 +2329,11 @@ int or_ecycle_adjoint(or_ecycle* h, int ncycles, const or_adjoint_response* r, o
   if (!h->hex.empty() || h->shell.empty()) return fail(h, OR_E_UNSUPPORTED, "adjoint: shell groups only");
   if (!h->links.empty()) return fail(h, OR_E_UNSUPPORTED, "adjoint: rigid links");
   if (!h->rbodies.empty()) return fail(h, OR_E_UNSUPPORTED, "adjoint: rigid bodies");
-  for (const HShell& g : h->shell)
+  for (const HShell& g : h->shell) {
     if (g.prop.ipla != 0) return fail(h, OR_E_UNSUPPORTED, "adjoint: IPLA 1 and 2 (the reverse follows the radial return)");
+    if (shell_ihbe(g.prop.ishell, g.prop.npt) != 1 || g.prop.npt == 1)
+      return fail(h, OR_E_UNSUPPORTED, "adjoint: Ishell 1 with 2 to 10 points only (the reverse follows CHVIS3)");
+  }
   for (auto& L : h->loads)     // /CLOAD forces depend on time only: no reverse terms
     if (L.type != 0) return fail(h, OR_E_UNSUPPORTED, "adjoint: /PLOAD follower loads");
 

@@ -55,8 +55,10 @@ struct HexGroupDesc {
 struct ShellGroupDesc {
   int part, law, nel, npt;
   int ithk, has_jca, ishfram, ipla;   // ipla: M2CPLR return (0 radial, 1 Newton, 2 projection)
+  int ihbe, pad;                      // engine IHBE (IPARG(23)): 1, 0, 2 or 4
   double rho0, young, nu, shear, a11, a12, ssp, jc_a, jc_b, jc_n, sigmax;
   double hm, hf, hr, shf, pressure, dtfac, dtmin;
+  double dn;                          // GEO(17): one-point V-shape hourglass coefficient
 };
 
 struct PartDesc {
@@ -197,7 +199,19 @@ struct NodeArgs {
   // rigid bodies: nodes with a nonzero role are updated by rbody_kernel and left
   // out of this pass (their kinetic energy too); null without rigid bodies
   const unsigned char* rb_role;
+  // rotational nodes, one bit per node (bit n & 31 of word n >> 5): the nodes of a
+  // part with rotations whose inertia or rotational velocity is nonzero.  Only
+  // these read and write VR and their moment slots; for any other node the
+  // rotational update would leave VR as it is (zero moment over zero inertia, zero
+  // VR) and add no rotational energy.  Null when no part has rotations.
+  const unsigned* rotmask;
 };
+
+// Whether node n carries rotations in the node pass (NodeArgs::rotmask).
+template <class R>
+__device__ __forceinline__ bool rot_node(const NodeArgs<R>& a, int n) {
+  return a.rotmask && ((__ldg(a.rotmask + (n >> 5)) >> (n & 31)) & 1u);
+}
 
 // Exchange buffer of one rank: nhalo force sums (R4), nhalo moment sums (R4),
 // then the rank's PartAcc of the cycle.
@@ -998,6 +1012,7 @@ __device__ __forceinline__ void shell_element(const ShellArgs<R>& a, const int e
   const R X3 = E1X * X31 + E1Y * Y31 + E1Z * Z31;
   const R X4 = E1X * X41 + E1Y * Y41 + E1Z * Z41;
   const R Y4 = E2X * X41 + E2Y * Y41 + E2Z * Z41;
+  R Z2 = E3X * X21 + E3Y * Y21 + E3Z * Z21;      // cderi3.F:108, used by IHBE >= 2
   const R PX1 = R(0.5) * (Y2 - Y4), PY1 = R(0.5) * (X4 - X2), PX2 = R(0.5) * Y3, PY2 = -R(0.5) * X3;
   R AREA = R(2) * (PY2 * PX1 - PY1 * PX2);
   AREA = AREA > R(EM20) ? AREA : R(EM20);
@@ -1032,7 +1047,7 @@ __device__ __forceinline__ void shell_element(const ShellArgs<R>& a, const int e
     if (DTHOUR < ALDT) ALDT = DTHOUR;
     ALDT = ssqrt(ALDT);
   }
-  // ---- CDEFO3, IHBE <= 1 (cdefo3.F:84-131) ----
+  // ---- CDEFO3 (cdefo3.F:84-220): IHBE <= 1, 2 and 4 ----
   R VXl[4], VYl[4], VZl[4], RXl[4], RYl[4];
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
@@ -1044,22 +1059,64 @@ __device__ __forceinline__ void shell_element(const ShellArgs<R>& a, const int e
     RXl[k] = E1X * rx + E1Y * ry + E1Z * rz;
     RYl[k] = E2X * rx + E2Y * ry + E2Z * rz;
   }
+  const int IHBE = gd.ihbe;
   R EXX, EYY, EXY, EXZ, EYZ, KXX, KYY, KXY;
   {
     const R VZ13 = VZl[0] - VZl[2], VZ24 = VZl[1] - VZl[3];
     EYZ = PY1 * VZ13 + PY2 * VZ24;
     EXZ = PX1 * VZ13 + PX2 * VZ24;
-    const R DT1V4 = R(0.25) * DT1;
-    const R t2a = PY2 + PY1;
-    const R t3a = copysign(fmax(fabs(t2a), R(EM20)), t2a);
-    const R t1a = DT1V4 * (VZ13 - VZ24) * (VZ13 - VZ24) / t3a;
-    const R VX13 = VXl[0] - VXl[2] - t1a, VX24 = VXl[1] - VXl[3] + t1a;
+    R VX13, VX24, VY13, VY24;
+    if (IHBE <= 1) {
+      Z2 = R(0);
+      const R DT1V4 = R(0.25) * DT1;
+      const R t2a = PY2 + PY1;
+      const R t3a = copysign(fmax(fabs(t2a), R(EM20)), t2a);
+      const R t1a = DT1V4 * (VZ13 - VZ24) * (VZ13 - VZ24) / t3a;
+      VX13 = VXl[0] - VXl[2] - t1a; VX24 = VXl[1] - VXl[3] + t1a;
+      const R t1b = PX2 - PX1;
+      const R t3b = copysign(fmax(fabs(t1b), R(EM20)), t1b);
+      const R t2b = DT1V4 * (VZ13 + VZ24) * (VZ13 + VZ24) / t3b;
+      VY13 = VYl[0] - VYl[2] + t2b; VY24 = VYl[1] - VYl[3] + t2b;
+    } else if (IHBE != 4) {
+      // IHBE 2 (cdefo3.F:133-172): velocities relative to node 1, warping terms
+      const R DT1V4 = R(0.5) * DT1;
+      const R GZX = EXZ / AREA, EXZZ2 = GZX * Z2, EXZ2 = GZX * GZX * DT1V4;
+      VXl[2] = VXl[2] - EXZ2 * X3 - VXl[0];
+      VXl[1] = VXl[1] + EXZZ2 - EXZ2 * X2 - VXl[0];
+      VXl[3] = VXl[3] + EXZZ2 - EXZ2 * X4 - VXl[0];
+      VXl[0] = R(0);
+      const R GZY = EYZ / AREA, EYZZ2 = GZY * Z2, EYZ2 = GZY * GZY * DT1V4;
+      VYl[2] = VYl[2] - EYZ2 * Y3 - VYl[0];
+      VYl[1] = VYl[1] + EYZZ2 - EYZ2 * Y2 - VYl[0];
+      VYl[3] = VYl[3] + EYZZ2 - EYZ2 * Y4 - VYl[0];
+      VYl[0] = R(0);
+      const R ZZZ = (EXZ2 + EYZ2) * Z2;
+      VZl[2] = VZl[2] - GZY * Y3 - GZX * X3 - VZl[0];
+      VZl[1] = VZl[1] - GZY * Y2 - GZX * X2 - ZZZ - VZl[0];
+      VZl[3] = VZl[3] - GZY * Y4 - GZX * X4 - ZZZ - VZl[0];
+      VZl[0] = R(0);
+      VX13 = -VXl[2]; VX24 = VXl[1] - VXl[3];
+      VY13 = -VYl[2]; VY24 = VYl[1] - VYl[3];
+    } else {
+      // IHBE 4 (cdefo3.F:174-216): z1 = z3 = 0, z4 = z2
+      const R DT1V4 = R(0.5) * DT1, ZZ2 = R(0.5) * Z2;
+      const R GZX = EXZ / AREA, EXZZ2 = GZX * ZZ2, EXZ2 = GZX * GZX * DT1V4;
+      const R EXZ2PY2 = EXZ2 * PY2, EXZ2PY1 = EXZ2 * PY1;
+      VXl[0] = VXl[0] - EXZZ2 - EXZ2PY2;
+      VXl[2] = VXl[2] - EXZZ2 + EXZ2PY2;
+      VXl[1] = VXl[1] + EXZZ2 + EXZ2PY1;
+      VXl[3] = VXl[3] + EXZZ2 - EXZ2PY1;
+      const R GZY = EYZ / AREA, EYZZ2 = GZY * ZZ2, EYZ2 = GZY * GZY * DT1V4;
+      const R EYZ2PX2 = EYZ2 * PX2, EYZ2PX1 = EYZ2 * PX1;
+      VYl[0] = VYl[0] - EYZZ2 + EYZ2PX2;
+      VYl[2] = VYl[2] - EYZZ2 - EYZ2PX2;
+      VYl[1] = VYl[1] + EYZZ2 - EYZ2PX1;
+      VYl[3] = VYl[3] + EYZZ2 + EYZ2PX1;
+      VX13 = VXl[0] - VXl[2]; VX24 = VXl[1] - VXl[3];
+      VY13 = VYl[0] - VYl[2]; VY24 = VYl[1] - VYl[3];
+    }
     EXX = PX1 * VX13 + PX2 * VX24;
     EXY = PY1 * VX13 + PY2 * VX24;
-    const R t1b = PX2 - PX1;
-    const R t3b = copysign(fmax(fabs(t1b), R(EM20)), t1b);
-    const R t2b = DT1V4 * (VZ13 + VZ24) * (VZ13 + VZ24) / t3b;
-    const R VY13 = VYl[0] - VYl[2] + t2b, VY24 = VYl[1] - VYl[3] + t2b;
     EXY = EXY + PX1 * VY13 + PX2 * VY24;
     EYY = PY1 * VY13 + PY2 * VY24;
     // ---- CCURV3 (ccurv3.F:61-86) ----
@@ -1086,6 +1143,9 @@ __device__ __forceinline__ void shell_element(const ShellArgs<R>& a, const int e
   const R CA = gd.has_jca ? st.jca : R(gd.jc_a);
   const R CB = R(gd.jc_b), CN = R(gd.jc_n), YMAX = R(gd.sigmax);
   double wpla = 0.0;
+  // SIGY for CHSTI3: EP30 (ccoor3.F:126); LAW2 adds each point's yield / NPTT
+  // (mulawc.F90:565, sigeps02c.F:186-188)
+  R SIGY = gd.law == 1 ? R(1e30) : R(0);
 #pragma unroll
   for (int ip = 0; ip < (NPT > 0 ? NPT : 10); ++ip) {
     if (NPT == 0 && ip >= npt) break;
@@ -1143,6 +1203,7 @@ __device__ __forceinline__ void shell_element(const ShellArgs<R>& a, const int e
           else a.pla[ip * nelpad + e] = PLA;
         }
       }
+      SIGY = SIGY + YLD / R(npt);
       EZZ = -(DXX + DYY) * NU - (R(1) - R(2) * NU) * EZZ;   // sigeps02c.F:215-224
       EZZ = EZZ / (R(1) - NU);
       wpla += (double)YLD * (double)DPLA * (double)AREA * (double)THKLYL;
@@ -1177,50 +1238,138 @@ __device__ __forceinline__ void shell_element(const ShellArgs<R>& a, const int e
       a.eint[1 * nelpad + e] = st.e[1] + DEGFX * THK0 * VOL2;
     }
   }
-  // ---- CHVIS3, ISMSTR = 2, IHBE = 1, HELAS = HVISC = 1/2, HVLIN = 0 (chvis3.F:116-300) ----
-  R H1j[3], H2j[3], H3j[3], HOUR4, HOUR5;
+  // ---- hourglass forces (cforc3.F:593-640): MHVIS3 for one integration point,
+  // CHSTI3 for IHBE = 2, CHVIS3 otherwise; ISMSTR = 2, HELAS = HVISC = 1/2, HVLIN = 0.
+  // H1j/H2j/H3j: membrane x, y and bending forces of corners 1..3 (corner 4 from
+  // the zero sum), HOUR4/HOUR5 the hourglass moments ----
+  R H1j[3], H2j[3], H3j[3], HOUR4 = R(0), HOUR5 = R(0);
   {
-    const R px1v = PX1 * VHX, px2v = PX2 * VHX, py1v = PY1 * VHY, py2v = PY2 * VHY;
     R GAMA[4];
-    GAMA[0] = OFF * (R(1) - px1v - py1v);
-    GAMA[2] = OFF * (R(1) + px1v + py1v);
-    GAMA[1] = OFF * (-R(1) - px2v - py2v);
-    GAMA[3] = OFF * (-R(1) + px2v + py2v);
-    const R SHFPR3 = SHF / (R(3) * (R(1) + NU));
-    const R R1 = R(0.25) * RHO * R(100);
-    const R A1c = R1 * (R(0.5) * H1);
-    const R A3c = R1 * (R(0.5) * H2) * ssqrt(SHFPR3);
-    const R A5c = R(0.5) * H3 * R1 * R(0.072169);
-    const R R0e = R(0.25) * YM * R(0.5);
-    const R A7c = H1 * R0e, A8c = H2 * R0e * SHFPR3;
-    const R T2A = THK02 * AREA;
-    R H1Q = A1c * ssqrt(T2A), H2Q = A3c * THK02, H3Q = A5c * T2A;
-    const R TD = THK0 * DT1;
-    R HH1 = A7c * TD;
-    const R B1 = PX1 * PX1 + PY1 * PY1, B2 = PX2 * PX2 + PY2 * PY2;
-    R HH2 = A8c * THK02 * TD / (B1 + B2);
-    if (st.degen) { H1Q = H2Q = H3Q = HH1 = HH2 = R(0); }
-    R HG1 = VXl[0] * GAMA[0] + VXl[1] * GAMA[1] + VXl[2] * GAMA[2] + VXl[3] * GAMA[3];
-    R HG2 = VYl[0] * GAMA[0] + VYl[1] * GAMA[1] + VYl[2] * GAMA[2] + VYl[3] * GAMA[3];
-    const R hour1 = st.h[0] + HG1 * HH1;
-    const R hour2 = st.h[1] + HG2 * HH1;
-    const R HOUR1A = hour1 + HG1 * (H1Q * fabs(HG1));
-    const R HOUR2A = hour2 + HG2 * (H1Q * fabs(HG2));
+    if (IHBE >= 1) {
+      const R px1v = PX1 * VHX, px2v = PX2 * VHX, py1v = PY1 * VHY, py2v = PY2 * VHY;
+      GAMA[0] = OFF * (R(1) - px1v - py1v);
+      GAMA[2] = OFF * (R(1) + px1v + py1v);
+      GAMA[1] = OFF * (-R(1) - px2v - py2v);
+      GAMA[3] = OFF * (-R(1) + px2v + py2v);
+    } else {
+      GAMA[0] = OFF; GAMA[2] = OFF; GAMA[1] = -OFF; GAMA[3] = -OFF;
+    }
+    R hour1, hour2, hour3, EHOU;
+    if (npt == 1) {
+      // MHVIS3 (mhvis3.F:109-363): elastic terms only, V-shape bending damping Dn,
+      // no hourglass moments; IHBE >= 1 here (one point turns Ishell 2 into 1)
+      const R H4 = R(gd.dn);
+      R H4L = R(0.25) * RHO * THK0 * ssqrt(R(0.5) * H4 * AREA);
+      R H4Q = ssqrt(R(0.5) * H4) * H4L * R(100);
+      H4L = H4L * SSP;
+      const R FAC = R(0.25) * YM * THK0 * DT1 * R(0.5);
+      R H1e = H1 * FAC, H2e = H2 * FAC;
+      if (st.degen) { H4L = H4Q = H1e = H2e = R(0); }
+      const R HG1 = VXl[0] * GAMA[0] + VXl[1] * GAMA[1] + VXl[2] * GAMA[2] + VXl[3] * GAMA[3];
+      const R HG2 = VYl[0] * GAMA[0] + VYl[1] * GAMA[1] + VYl[2] * GAMA[2] + VYl[3] * GAMA[3];
+      hour1 = st.h[0] + HG1 * H1e;
+      hour2 = st.h[1] + HG2 * H1e;
+      // the viscous factors H1L, H1Q, H2L, H2Q of MHVIS3 are zero: (HOUR + 0) * GAMA
+      R Hm1[4], Hm2[4], Hb[4];
 #pragma unroll
-    for (int k = 0; k < 3; ++k) { H1j[k] = HOUR1A * GAMA[k]; H2j[k] = HOUR2A * GAMA[k]; }
-    R EHOU = HOUR1A * HG1 + HOUR2A * HG2;
-    HG1 = VZl[0] * GAMA[0] + VZl[1] * GAMA[1] + VZl[2] * GAMA[2] + VZl[3] * GAMA[3];
-    const R hour3 = st.h[2] + HG1 * HH2;
-    const R HOUR3A = hour3 + HG1 * (H2Q * fabs(HG1));
+      for (int k = 0; k < 4; ++k) { Hm1[k] = hour1 * GAMA[k]; Hm2[k] = hour2 * GAMA[k]; }
+      EHOU = VXl[0] * Hm1[0] + VXl[1] * Hm1[1] + VXl[2] * Hm1[2] + VXl[3] * Hm1[3] +
+             VYl[0] * Hm2[0] + VYl[1] * Hm2[1] + VYl[2] * Hm2[2] + VYl[3] * Hm2[3];
+      R HGb = VZl[0] * GAMA[0] + VZl[1] * GAMA[1] + VZl[2] * GAMA[2] + VZl[3] * GAMA[3];
+      hour3 = st.h[2] + HGb * H2e;
 #pragma unroll
-    for (int k = 0; k < 3; ++k) H3j[k] = HOUR3A * GAMA[k];
-    EHOU = EHOU + HOUR3A * HG1;
-    HG1 = RXl[0] - RXl[1] + RXl[2] - RXl[3];
-    HG2 = RYl[0] - RYl[1] + RYl[2] - RYl[3];
-    HOUR4 = HG1 * (H3Q * fabs(HG1));
-    HOUR5 = HG2 * (H3Q * fabs(HG2));
-    EHOU = EHOU + HOUR4 * HG1 + HOUR5 * HG2;
-    my_ehou = (double)(DT1 * EHOU * OFF);
+      for (int k = 0; k < 4; ++k) Hb[k] = hour3 * GAMA[k];
+      HGb = VZl[0] + VZl[1] - VZl[2] - VZl[3];
+      HGb = HGb * (H4L + H4Q * fabs(HGb));
+      Hb[0] = Hb[0] + HGb; Hb[1] = Hb[1] + HGb; Hb[2] = Hb[2] - HGb; Hb[3] = Hb[3] - HGb;
+      HGb = VZl[0] - VZl[1] - VZl[2] + VZl[3];
+      HGb = HGb * (H4L + H4Q * fabs(HGb));
+      Hb[0] = Hb[0] + HGb; Hb[1] = Hb[1] - HGb; Hb[2] = Hb[2] - HGb; Hb[3] = Hb[3] + HGb;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) { H1j[k] = Hm1[k]; H2j[k] = Hm2[k]; H3j[k] = Hb[k]; }
+      EHOU = EHOU + VZl[0] * Hb[0] + VZl[1] * Hb[1] + VZl[2] * Hb[2] + VZl[3] * Hb[3];
+      my_ehou = (double)(DT1 * EHOU);
+    } else if (IHBE == 2) {
+      // CHSTI3 (chsti3.F:119-320): elastic stiffness bounded by the yield stress,
+      // viscous rotational terms with SRH3 = sqrt(hr) (resol_init.F:676-682)
+      const R H3s = R(sqrt(gd.hr));
+      const R SHFPR3 = SHF / (R(3) * (R(1) + NU));
+      R H3L = H3s * R(0.072169) * (R(0.25) * RHO * THK02) * AREA;
+      R H3Q = H3s * H3L * R(100);
+      H3L = H3L * SSP;
+      const R FAC = YM * THK0 * DT1 * R(0.125);
+      R H1e = H1 * FAC;
+      const R B1 = PX1 * PX1 + PY1 * PY1, B2 = PX2 * PX2 + PY2 * PY2;
+      R H2e = H2 * FAC * THK02 * SHFPR3 / (B1 + B2);
+      if (st.degen) { H3Q = H3L = H1e = H2e = R(0); }
+      R HG1 = VXl[0] * GAMA[0] + VXl[1] * GAMA[1] + VXl[2] * GAMA[2] + VXl[3] * GAMA[3];
+      R HG2 = VYl[0] * GAMA[0] + VYl[1] * GAMA[1] + VYl[2] * GAMA[2] + VYl[3] * GAMA[3];
+      hour1 = st.h[0] + HG1 * H1e;
+      hour2 = st.h[1] + HG2 * H1e;
+      R FMAX = R(0.5) * SIGY * THK0 * ssqrt(AREA) * H1;
+      hour1 = copysign(fmin(fabs(hour1), FMAX), hour1);
+      hour2 = copysign(fmin(fabs(hour2), FMAX), hour2);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) { H1j[k] = hour1 * GAMA[k]; H2j[k] = hour2 * GAMA[k]; }
+      EHOU = hour1 * HG1 + hour2 * HG2;
+      HG1 = VZl[0] * GAMA[0] + VZl[1] * GAMA[1] + VZl[2] * GAMA[2] + VZl[3] * GAMA[3];
+      hour3 = st.h[2] + HG1 * H2e;
+      FMAX = R(0.25) * SIGY * THK0 * THK0 * H2;
+      hour3 = copysign(fmin(fabs(hour3), FMAX), hour3);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) H3j[k] = hour3 * GAMA[k];
+      EHOU = EHOU + hour3 * HG1;
+      HG1 = RXl[0] - RXl[1] + RXl[2] - RXl[3];
+      HG2 = RYl[0] - RYl[1] + RYl[2] - RYl[3];
+      HOUR4 = HG1 * (H3L + H3Q * fabs(HG1));
+      HOUR5 = HG2 * (H3L + H3Q * fabs(HG2));
+      EHOU = EHOU + HOUR4 * HG1 + HOUR5 * HG2;
+      my_ehou = (double)(DT1 * EHOU * OFF);
+    } else {
+      // CHVIS3 (chvis3.F:116-300)
+      const R SHFPR3 = SHF / (R(3) * (R(1) + NU));
+      const R R1 = R(0.25) * RHO * R(100);
+      const R A1c = R1 * (R(0.5) * H1);
+      const R A3c = R1 * (R(0.5) * H2) * ssqrt(SHFPR3);
+      const R A5c = R(0.5) * H3 * R1 * R(0.072169);
+      const R R0e = R(0.25) * YM * R(0.5);
+      const R A7c = H1 * R0e, A8c = H2 * R0e * SHFPR3;
+      const R T2A = THK02 * AREA;
+      R H1Q = A1c * ssqrt(T2A), H2Q = A3c * THK02, H3Q = A5c * T2A;
+      const R TD = THK0 * DT1;
+      R HH1 = A7c * TD;
+      const R B1 = PX1 * PX1 + PY1 * PY1, B2 = PX2 * PX2 + PY2 * PY2;
+      R HH2 = A8c * THK02 * TD / (B1 + B2);
+      if (st.degen) { H1Q = H2Q = H3Q = HH1 = HH2 = R(0); }
+      R HG1, HG2;
+      if (IHBE < 1) {
+        HG1 = (VXl[0] - VXl[1] + VXl[2] - VXl[3]) * OFF;
+        HG2 = (VYl[0] - VYl[1] + VYl[2] - VYl[3]) * OFF;
+      } else {
+        HG1 = VXl[0] * GAMA[0] + VXl[1] * GAMA[1] + VXl[2] * GAMA[2] + VXl[3] * GAMA[3];
+        HG2 = VYl[0] * GAMA[0] + VYl[1] * GAMA[1] + VYl[2] * GAMA[2] + VYl[3] * GAMA[3];
+      }
+      hour1 = st.h[0] + HG1 * HH1;
+      hour2 = st.h[1] + HG2 * HH1;
+      const R HOUR1A = hour1 + HG1 * (H1Q * fabs(HG1));
+      const R HOUR2A = hour2 + HG2 * (H1Q * fabs(HG2));
+#pragma unroll
+      for (int k = 0; k < 3; ++k) { H1j[k] = HOUR1A * GAMA[k]; H2j[k] = HOUR2A * GAMA[k]; }
+      EHOU = HOUR1A * HG1 + HOUR2A * HG2;
+      if (IHBE < 1) HG1 = (VZl[0] - VZl[1] + VZl[2] - VZl[3]) * OFF;
+      else HG1 = VZl[0] * GAMA[0] + VZl[1] * GAMA[1] + VZl[2] * GAMA[2] + VZl[3] * GAMA[3];
+      hour3 = st.h[2] + HG1 * HH2;
+      const R HOUR3A = hour3 + HG1 * (H2Q * fabs(HG1));
+#pragma unroll
+      for (int k = 0; k < 3; ++k) H3j[k] = HOUR3A * GAMA[k];
+      EHOU = EHOU + HOUR3A * HG1;
+      HG1 = RXl[0] - RXl[1] + RXl[2] - RXl[3];
+      HG2 = RYl[0] - RYl[1] + RYl[2] - RYl[3];
+      HOUR4 = HG1 * (H3Q * fabs(HG1));
+      HOUR5 = HG2 * (H3Q * fabs(HG2));
+      EHOU = EHOU + HOUR4 * HG1 + HOUR5 * HG2;
+      my_ehou = (double)(DT1 * EHOU * OFF);
+    }
     if (KEEP) { st.h[0] = hour1; st.h[1] = hour2; st.h[2] = hour3; }
     else { a.hourg[0 * nelpad + e] = hour1; a.hourg[1 * nelpad + e] = hour2; a.hourg[2 * nelpad + e] = hour3; }
   }
@@ -1234,7 +1383,12 @@ __device__ __forceinline__ void shell_element(const ShellArgs<R>& a, const int e
   // ---- CFINT3, ISIGI = 0 (cfint3.F:173-260) ----
   {
     const R F1A = FOR[0] * THK0, F2A = FOR[1] * THK0, F3A = FOR[2] * THK0, F4A = FOR[3] * THK0, F5A = FOR[4] * THK0;
-    const R M4 = R(0.25) * (F4A * AREA), M5 = R(0.25) * (F5A * AREA);
+    R M4 = F4A * AREA, M5 = F5A * AREA;
+    if (IHBE >= 2 && npt != 1) {            // cfint3.F:208-214, warping moments
+      M4 = M4 + (H2j[0] + H2j[2]) * Z2;
+      M5 = M5 + (H1j[0] + H1j[2]) * Z2;
+    }
+    M4 = M4 * R(0.25); M5 = M5 * R(0.25);
     const R F12 = F1A * PX2 + F3A * PY2, F22 = F2A * PY2 + F3A * PX2, F32 = F5A * PX2 + F4A * PY2;
     const R F11 = F1A * PX1 + F3A * PY1, F21 = F2A * PY1 + F3A * PX1, F31 = F5A * PX1 + F4A * PY1;
     const R Gc[3][3] = {{F11 + H1j[0], F12 + H1j[1], H1j[2] - F11},
@@ -1525,7 +1679,8 @@ __device__ __forceinline__ void node_pass(NodeArgs<R> a, int parity) {
     const unsigned char code = codes[n];
     const double dx = DX[n], dy = DY[n], dz = DZ[n];
     R4 f0 = mk4(R(0), R(0), R(0), R(0)), m0 = f0, w0 = f0;
-    if (VR) w0 = VR[n];
+    const bool rn = rot_node(a, n);
+    if (rn) w0 = VR[n];
     const int part = a.tile_part[tile];
     const PartDesc pd = a.parts[part];
     const bool valid = n < pd.node_end;
@@ -1537,7 +1692,7 @@ __device__ __forceinline__ void node_pass(NodeArgs<R> a, int parity) {
     R4 f1 = mk4(R(0), R(0), R(0), R(0)), m1 = f1;
     if (k1 > k0) f0 = fslot[k0];
     if (k1 > k0 + 1) f1 = fslot[k0 + 1];
-    if (VR && mslot) {
+    if (rn && mslot) {
       if (k1 > k0) m0 = mslot[k0];
       if (k1 > k0 + 1) m1 = mslot[k0 + 1];
     }
@@ -1573,7 +1728,7 @@ __device__ __forceinline__ void node_pass(NodeArgs<R> a, int parity) {
         }
       }
       R rx = R(0), ry = R(0), rz = R(0);
-      if (pd.has_rot) {
+      if (rn) {
         rx = m0.x; ry = m0.y; rz = m0.z;
         if (k1 > k0 + 1) { rx += m1.x; ry += m1.y; rz += m1.z; }
         for (int k = k0 + 2; k < k1; ++k) {
@@ -1590,12 +1745,12 @@ __device__ __forceinline__ void node_pass(NodeArgs<R> a, int parity) {
       }
       double px = xm.x, py = xm.y, pz = xm.z, qx = dx, qy = dy, qz = dz;
       R4 w = w0;
-      node_update<R>(a, n, code, pd.has_rot != 0, ax, ay, az, rx, ry, rz, R(xm.w), DT1, DT2, DT12, px, py, pz,
+      node_update<R>(a, n, code, rn, ax, ay, az, rx, ry, rz, R(xm.w), DT1, DT2, DT12, px, py, pz,
                      qx, qy, qz, v, w, ek, ekr);
       V[n] = v;
       DX[n] = qx; DY[n] = qy; DZ[n] = qz;
       X[n] = make_double4(px, py, pz, xm.w);
-      if (pd.has_rot) VR[n] = w;
+      if (rn) VR[n] = w;
     }
     if (valid && a.halo_slot && !a.halo_ke[n]) { ek = 0.0; ekr = 0.0; }   // counted by another rank
     // per-tile kinetic energy partials (fixed tree order -> deterministic)

@@ -62,10 +62,13 @@ def solid_prop(qa=1.1, qb=0.05, qh=0.1, jcvt=0):
     return dict(qa=qa, qb=qb, qh=qh, jcvt=jcvt)
 
 
-def shell_prop(thk, npt=5, ithk=1, hm=0.01, hf=0.01, hr=0.01, shf=5.0 / 6.0, pressure=0.0, ishfram=0, ipla=0):
-    """/PROP/SHELL values; ipla is M2CPLR's return (0 radial, 1 Newton, 2 projection)."""
+def shell_prop(thk, npt=5, ithk=1, hm=0.01, hf=0.01, hr=0.01, shf=5.0 / 6.0, pressure=0.0, ishfram=0, ipla=0,
+               ishell=1, dn=0.0):
+    """/PROP/SHELL values; ipla is M2CPLR's return (0 radial, 1 Newton, 2 projection),
+    ishell the formulation (1..4, as the starter leaves it), dn the one-point
+    V-shape hourglass coefficient."""
     return dict(thk=thk, npt=npt, ithk=ithk, ipla=ipla, ishfram=ishfram, hm=hm, hf=hf, hr=hr, shf=shf,
-                pressure=pressure)
+                pressure=pressure, ishell=ishell, dn=dn)
 
 
 # ---------------------------------------------------------------------------
@@ -209,14 +212,16 @@ def c1_hex_block(nx=10, ny=10, nz=40, h=1e-3, ncycles=1000, law=LAW_ELASTIC, vz=
 
 
 def c2_shell_plate(n=200, size=0.2, thk=1e-3, npt=5, pressure=2e6, ncycles=2000, seed=0,
-                   jc_a=None, thke=None, law=LAW_JOHNSON_COOK, ipla=0):
+                   jc_a=None, thke=None, law=LAW_JOHNSON_COOK, ipla=0, ishell=1, jitter=0.05):
     """Split-precision shell plate: n*n BT shells on a square plate, interior
     nodes jittered +-5 % of h, LAW2 aluminium, simply supported edges (z fixed),
-    uniform pressure step."""
-    x, conn, edge = quad_plate(n, size, jitter=0.05, seed=seed)
+    uniform pressure step; ishell picks the formulation (Ishell 1..4)."""
+    x, conn, edge = quad_plate(n, size, jitter=jitter, seed=seed)
     p = new_part(x)
     mat = aluminium_jc() if law == LAW_JOHNSON_COOK else material(LAW_ELASTIC, 2700.0, 70e9, 0.33)
-    add_shell(p, conn, mat, shell_prop(thk, npt=npt, pressure=pressure, ipla=ipla), thke=thke)
+    hm = 0.1 if ishell == 3 else 0.01             # the starter's defaults (hm_read_prop01.F:204-212)
+    add_shell(p, conn, mat, shell_prop(thk, npt=npt, pressure=pressure, ipla=ipla, ishell=ishell, hm=hm, hf=hm),
+              thke=thke)
     if jc_a is not None:
         p["shell"][0]["jc_a"] = np.asarray(jc_a, np.float64)
     p["icodt"][edge] = 1

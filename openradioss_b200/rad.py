@@ -24,8 +24,10 @@ Starter semantics restated here (the reference starter is not on the path):
 
 * /PROP/SHELL flags fall back to /DEF_SHELL, then to the built-in defaults
   Ishell 1, Ismstr 2, Ithick 0, Iplas 0 (hm_read_prop01.F:112-272,
-  defaults_mod.F90:160-165); hm = hf = hr = 0.01 when zero and shear factor
-  5/6 (hm_read_prop01.F:204-240);
+  defaults_mod.F90:160-165); Ishell 1 to 4 are read (the library maps them to
+  the engine's IHBE 1, 0, 2, 4); hm = hf = 0.1, hr = 0.01 when zero for
+  Ishell 3, hm = hf = hr = 0.01 otherwise, and shear factor 5/6
+  (hm_read_prop01.F:204-240); Dn is kept for one-point shells (MHVIS3);
 * global integration N = 0 with LAW2 becomes 3 integration points
   (cgrtails.F:795-806, warning 1912); LAW1 keeps N = 0 only with the
   resultant law, which the element cycle does not implement;
@@ -355,7 +357,8 @@ class EngineDeck:
 
 
 def _shell_flags(sd, prop):
-    """IHBE, ISMSTR, ITHK, IPLA and NPT after the starter's defaults."""
+    """Ishell, ISMSTR, ITHK and Iplas after the starter's defaults (the engine's
+    IHBE follows from Ishell in the library, hm_read_prop01.F:305-315)."""
     ds = sd.def_shell
     ihbe = prop["ishell"] or ds["ishell"] or 1
     ismstr = prop["ismstr"] or ds["ismstr"] or 2
@@ -415,9 +418,9 @@ def to_deck(sd: StarterDeck, name=None):
         ihbe, ismstr, ithk, ipla = _shell_flags(sd, prop)
         if ithk == 2:
             ithk = 0                        # cgrtails.F:832-833
-        if ihbe != 1 or ismstr != 2:
+        if ihbe not in (1, 2, 3, 4) or ismstr != 2:
             raise RadError(f"/PROP/SHELL/{prop_id}: Ishell {ihbe} / Ismstr {ismstr}; the element cycle "
-                           "implements Ishell 1 with Ismstr 2")
+                           "implements Ishell 1 to 4 with Ismstr 2")
         if ipla not in (0, 1, 2, 3):
             raise RadError(f"/PROP/SHELL/{prop_id}: Iplas {ipla}")
         # M2CPLR's IPLA from Iplas (cgrtails.F:822-829; the explicit default Iplas 0
@@ -435,9 +438,12 @@ def to_deck(sd: StarterDeck, name=None):
             raise RadError(f"/PROP/SHELL/{prop_id}: N = {npt}")
         rows = sorted(sd.shells[pid])
         conn = np.array([[index[n] for n in r[1:]] for r in rows], np.int64)
+        # hourglass defaults: 0.1 / 0.1 / 0.01 for Ishell 3, 0.01 otherwise
+        # (hm_read_prop01.F:204-212)
+        hdef = (0.1, 0.1, 0.01) if ihbe == 3 else (0.01, 0.01, 0.01)
         p = decks.shell_prop(prop["thick"], npt=npt, ithk=1 if ithk > 0 else 0,
-                             hm=prop["hm"] or 0.01, hf=prop["hf"] or 0.01, hr=prop["hr"] or 0.01,
-                             ishfram=sd.ishfram)
+                             hm=prop["hm"] or hdef[0], hf=prop["hf"] or hdef[1], hr=prop["hr"] or hdef[2],
+                             ishfram=sd.ishfram, ishell=ihbe, dn=prop["dn"])
         p["ipla"] = ipla
         if prop["ashear"] != 0.0:
             p["shf"] = prop["ashear"]
@@ -718,8 +724,8 @@ def write_starter(deck, path, part=0, title=None):
         ems = m["rho0"] * thk * area / 4.0
         np.add.at(mass, conn.ravel(), np.repeat(ems, 4))
         L += _material_cards(pid, m)
-        L += [f"/PROP/SHELL/{pid}", f"shell {pid}", _i10(1, 2, 0, 0) + " " * 20 + _f20(0.0),
-              _f20(pr["hm"], pr["hf"], pr["hr"], 0.0, 0.0),
+        L += [f"/PROP/SHELL/{pid}", f"shell {pid}", _i10(int(pr.get("ishell", 1)) or 1, 2, 0, 0) + " " * 20 + _f20(0.0),
+              _f20(pr["hm"], pr["hf"], pr["hr"], 0.0, float(pr.get("dn", 0.0))),
               _i10(pr["npt"], 0) + _f20(pr["thk"], pr["shf"] if pr["npt"] > 1 else 0.0) +
               _i10(1 if pr["ithk"] else 2, {0: 2, 1: 1, 2: 3}[int(pr.get("ipla", 0))]),
               f"/PART/{pid}", f"part {pid}", _i10(pid, pid, 0), f"/SHELL/{pid}"]

@@ -585,8 +585,18 @@ int hex_element(const Model<R>& m, HexGroup<R>& g, PartData<R>& P, int i, double
   return OR_OK;
 }
 
+// Engine IHBE (IPARG(23)) of a group from the starter's Ishell: hm_read_prop01.F:
+// 176 (0 -> the default, 1 here), 246-250 (one point: Ishell 0 and 2 -> 1),
+// 305-315 (GEO(171): 1 -> 1, 2 -> 0, 3 -> 2, 4 -> 4), cgrtails.F:553, 949.
+inline int shell_ihbe(int ishell, int npt) {
+  if (ishell == 0) ishell = 1;
+  if (npt == 1 && ishell == 2) ishell = 1;
+  return ishell == 1 ? 1 : ishell == 2 ? 0 : ishell == 3 ? 2 : 4;
+}
+
 // ----------------------------------------------------------------------------
-// CFORC3 chain for one 4-node BT shell, Ishell=1 (IHBE=1), ISMSTR=2, ISHFRAM=0 or 2.
+// CFORC3 chain for one 4-node BT shell, Ishell 1..4 (IHBE 1, 0, 2, 4), ISMSTR=2,
+// ISHFRAM=0 or 2.
 // ----------------------------------------------------------------------------
 template <class R>
 int shell_element(const Model<R>& m, ShellGroup<R>& g, PartData<R>& P, int i, double dt1d,
@@ -596,6 +606,7 @@ int shell_element(const Model<R>& m, ShellGroup<R>& g, PartData<R>& P, int i, do
   const or_material& mt = g.mat;
   const or_shell_prop& pr = g.prop;
   const int npt = pr.npt, nel = g.nel;
+  const int IHBE = shell_ihbe(pr.ishell, npt);
   int nc[4];
   for (int k = 0; k < 4; ++k) nc[k] = g.ix[4 * i + k];
   // CCOOR3 (ccoor3.F): X (my_real), V, VR
@@ -662,7 +673,7 @@ int shell_element(const Model<R>& m, ShellGroup<R>& g, PartData<R>& P, int i, do
     X3 = E1X * X31GA + E1Y * Y31GA + E1Z * Z31GA;
     X4 = E1X * X41GA + E1Y * Y41GA + E1Z * Z41GA;
     Y4 = E2X * X41GA + E2Y * Y41GA + E2Z * Z41GA;
-    Z2 = E3X * X21GA + E3Y * Y21GA + E3Z * Z21GA; (void)Z2;
+    Z2 = E3X * X21GA + E3Y * Y21GA + E3Z * Z21GA;
   }
   R PX1 = R(0.5) * (Y2 - Y4), PY1 = R(0.5) * (X4 - X2), PX2 = R(0.5) * Y3, PY2 = -R(0.5) * X3;
   R AREA = std::max(R(2) * (PY2 * PX1 - PY1 * PX2), R(EM20));
@@ -696,7 +707,9 @@ int shell_element(const Model<R>& m, ShellGroup<R>& g, PartData<R>& P, int i, do
     if (DTHOUR < ALDT) ALDT = DTHOUR;
     ALDT = std::sqrt(ALDT);
   }
-  // CDEFO3 (cdefo3.F:84-131), IHBE<=1
+  // CDEFO3 (cdefo3.F:84-220): local velocities, then per IHBE the membrane strain
+  // rates and, for IHBE 2 and 4, the warping-corrected velocities that the
+  // hourglass routines use
   R VXl[4], VYl[4], VZl[4];
   for (int k = 0; k < 4; ++k) {
     VXl[k] = E1X * VL[k][0] + E1Y * VL[k][1] + E1Z * VL[k][2];
@@ -708,19 +721,70 @@ int shell_element(const Model<R>& m, ShellGroup<R>& g, PartData<R>& P, int i, do
     R VZ13 = VZl[0] - VZl[2], VZ24 = VZl[1] - VZl[3];
     EYZ = PY1 * VZ13 + PY2 * VZ24;
     EXZ = PX1 * VZ13 + PX2 * VZ24;
-    R DT1V4 = R(0.25) * DT1;
-    R TMP2A = PY2 + PY1;
-    R TMP3A = sgn(std::max(std::fabs(TMP2A), R(EM20)), TMP2A);
-    R TMP1A = DT1V4 * (VZ13 - VZ24) * (VZ13 - VZ24) / TMP3A;
-    R VX13 = VXl[0] - VXl[2], VX24 = VXl[1] - VXl[3];
-    VX13 = VX13 - TMP1A; VX24 = VX24 + TMP1A;
+    R VX13, VX24, VY13, VY24;
+    if (IHBE <= 1) {
+      // cdefo3.F:103-131 (Z2 = 0 for the hourglass forces)
+      Z2 = R(0);
+      R DT1V4 = R(0.25) * DT1;
+      R TMP2A = PY2 + PY1;
+      R TMP3A = sgn(std::max(std::fabs(TMP2A), R(EM20)), TMP2A);
+      R TMP1A = DT1V4 * (VZ13 - VZ24) * (VZ13 - VZ24) / TMP3A;
+      VX13 = VXl[0] - VXl[2]; VX24 = VXl[1] - VXl[3];
+      VX13 = VX13 - TMP1A; VX24 = VX24 + TMP1A;
+      R TMP1B = PX2 - PX1;
+      R TMP3B = sgn(std::max(std::fabs(TMP1B), R(EM20)), TMP1B);
+      R TMP2B = DT1V4 * (VZ13 + VZ24) * (VZ13 + VZ24) / TMP3B;
+      VY13 = VYl[0] - VYl[2]; VY24 = VYl[1] - VYl[3];
+      VY13 = VY13 + TMP2B; VY24 = VY24 + TMP2B;
+    } else if (IHBE == 2 || IHBE == 3) {
+      // cdefo3.F:133-172: velocities relative to node 1, warping terms
+      R DT1V4 = R(0.5) * DT1;
+      R GZX = EXZ / AREA;
+      R EXZZ2 = GZX * Z2;
+      R EXZ2 = GZX * GZX * DT1V4;
+      VXl[2] = VXl[2] - EXZ2 * X3 - VXl[0];
+      VXl[1] = VXl[1] + EXZZ2 - EXZ2 * X2 - VXl[0];
+      VXl[3] = VXl[3] + EXZZ2 - EXZ2 * X4 - VXl[0];
+      VXl[0] = R(0);
+      R GZY = EYZ / AREA;
+      R EYZZ2 = GZY * Z2;
+      R EYZ2 = GZY * GZY * DT1V4;
+      VYl[2] = VYl[2] - EYZ2 * Y3 - VYl[0];
+      VYl[1] = VYl[1] + EYZZ2 - EYZ2 * Y2 - VYl[0];
+      VYl[3] = VYl[3] + EYZZ2 - EYZ2 * Y4 - VYl[0];
+      VYl[0] = R(0);
+      R ZZZ = (EXZ2 + EYZ2) * Z2;
+      VZl[2] = VZl[2] - GZY * Y3 - GZX * X3 - VZl[0];
+      VZl[1] = VZl[1] - GZY * Y2 - GZX * X2 - ZZZ - VZl[0];
+      VZl[3] = VZl[3] - GZY * Y4 - GZX * X4 - ZZZ - VZl[0];
+      VZl[0] = R(0);
+      VX13 = -VXl[2]; VX24 = VXl[1] - VXl[3];
+      VY13 = -VYl[2]; VY24 = VYl[1] - VYl[3];
+    } else {
+      // IHBE = 4, cdefo3.F:174-216: z1 = z3 = 0, z4 = z2
+      R DT1V4 = R(0.5) * DT1;
+      R ZZ2 = R(0.5) * Z2;
+      R GZX = EXZ / AREA;
+      R EXZZ2 = GZX * ZZ2;
+      R EXZ2 = GZX * GZX * DT1V4;
+      R EXZ2PY2 = EXZ2 * PY2, EXZ2PY1 = EXZ2 * PY1;
+      VXl[0] = VXl[0] - EXZZ2 - EXZ2PY2;
+      VXl[2] = VXl[2] - EXZZ2 + EXZ2PY2;
+      VXl[1] = VXl[1] + EXZZ2 + EXZ2PY1;
+      VXl[3] = VXl[3] + EXZZ2 - EXZ2PY1;
+      R GZY = EYZ / AREA;
+      R EYZZ2 = GZY * ZZ2;
+      R EYZ2 = GZY * GZY * DT1V4;
+      R EYZ2PX2 = EYZ2 * PX2, EYZ2PX1 = EYZ2 * PX1;
+      VYl[0] = VYl[0] - EYZZ2 + EYZ2PX2;
+      VYl[2] = VYl[2] - EYZZ2 - EYZ2PX2;
+      VYl[1] = VYl[1] + EYZZ2 - EYZ2PX1;
+      VYl[3] = VYl[3] + EYZZ2 + EYZ2PX1;
+      VX13 = VXl[0] - VXl[2]; VX24 = VXl[1] - VXl[3];
+      VY13 = VYl[0] - VYl[2]; VY24 = VYl[1] - VYl[3];
+    }
     EXX = PX1 * VX13 + PX2 * VX24;
     EXY = PY1 * VX13 + PY2 * VX24;
-    R TMP1B = PX2 - PX1;
-    R TMP3B = sgn(std::max(std::fabs(TMP1B), R(EM20)), TMP1B);
-    R TMP2B = DT1V4 * (VZ13 + VZ24) * (VZ13 + VZ24) / TMP3B;
-    R VY13 = VYl[0] - VYl[2], VY24 = VYl[1] - VYl[3];
-    VY13 = VY13 + TMP2B; VY24 = VY24 + TMP2B;
     EXY = EXY + PX1 * VY13 + PX2 * VY24;
     EYY = PY1 * VY13 + PY2 * VY24;
   }
@@ -764,6 +828,9 @@ int shell_element(const Model<R>& m, ShellGroup<R>& g, PartData<R>& P, int i, do
   R DEGFX = MOM_OLD[0] * KXX + MOM_OLD[1] * KYY + MOM_OLD[2] * KXY;
   R THKN = g.thk[i];
   double wpla = 0;
+  // SIGY: EP30 from CCOOR3 (ccoor3.F:126); LAW2 restarts it at 0 and adds each
+  // point's yield stress / NPTT (mulawc.F90:565, sigeps02c.F:186-188)
+  R SIGY = mt.law == OR_LAW_JOHNSON_COOK ? R(0) : R(1e30);
   for (int ip = 0; ip < npt; ++ip) {
     R THKLY = R(WF1[npt - 1][ip]);
     R THKLYL = THKLY * THK0;
@@ -864,6 +931,7 @@ int shell_element(const Model<R>& m, ShellGroup<R>& g, PartData<R>& P, int i, do
         }
       }
       g.pla[ip * nel + i] = PLA;
+      SIGY = SIGY + YLD / R(npt);
       // sigeps02c.F:215-224
       EZZ = -(DEPSXX + DEPSYY) * NU - (R(1) - R(2) * NU) * EZZ;
       EZZ = EZZ / (R(1) - NU);
@@ -885,62 +953,174 @@ int shell_element(const Model<R>& m, ShellGroup<R>& g, PartData<R>& P, int i, do
     g.eint[0 * nel + i] = g.eint[0 * nel + i] + DEGMB * VOL2;
     g.eint[1 * nel + i] = g.eint[1 * nel + i] + DEGFX * THK0 * VOL2;
   }
-  // CHVIS3 (chvis3.F:116-300), ISMSTR=2, IHBE=1, NODADT=0, HELAS=HVISC=1/2, HVLIN=0
+  // Hourglass forces (cforc3.F:593-640): MHVIS3 for one integration point,
+  // CHSTI3 for IHBE = 2, CHVIS3 otherwise; ISMSTR=2, NODADT=0, HELAS=HVISC=1/2,
+  // HVLIN=0.  H1j/H2j/H3j: membrane x, y and bending hourglass forces of corners
+  // 1..3 (corner 4 follows from their sum being zero), B1j/B2j the moments.
   R H1j[3], H2j[3], H3j[3], B1j[4], B2j[4];
   {
-    const R HELAS = R(0.5), HVISC = R(0.5), HVLIN = R(0);
-    R PX1V = PX1 * VHX, PX2V = PX2 * VHX, PY1V = PY1 * VHY, PY2V = PY2 * VHY;
+    const R HELAS = R(0.5), HVISC = R(0.5);
     R GAMA[4];
-    GAMA[0] = OFF * (R(1) - PX1V - PY1V);
-    GAMA[2] = OFF * (R(1) + PX1V + PY1V);
-    GAMA[1] = OFF * (-R(1) - PX2V - PY2V);
-    GAMA[3] = OFF * (-R(1) + PX2V + PY2V);
-    R SHFPR3 = SHF / (R(3) * (R(1) + NU));
-    R HVISH1 = HVISC * H1, HVISH2 = HVISC * H2;
-    R R0 = R(0.25) * RHO;
-    R R1 = R0 * R(100);
-    R0 = R0 * HVLIN;
-    R A1c = R1 * HVISH1;
-    R SRSHFPR3 = std::sqrt(SHFPR3);
-    R A3c = R1 * HVISH2 * SRSHFPR3;
-    R A5c = HELAS * H3 * R1 * R(0.072169);
-    R R0e = R(0.25) * YM * HELAS;
-    R A7c = H1 * R0e;
-    R A8c = H2 * R0e * SHFPR3;
-    R T2A = THK02 * AREA;
-    R TSA = std::sqrt(T2A);
-    R H1Q = A1c * TSA, H1L = R(0);
-    R H2Q = A3c * THK02, H2L = R(0);
-    R H3Q = A5c * T2A, H3L = R(0);
-    (void)R0;
-    R TD = THK0 * DT1;
-    R HH1 = A7c * TD;
-    R B1 = PX1 * PX1 + PY1 * PY1, B2 = PX2 * PX2 + PY2 * PY2;
-    R HH2 = A8c * THK02 * TD / (B1 + B2);
-    if (nc[2] == nc[3]) { H1Q = H1L = H2Q = H2L = H3Q = H3L = HH1 = HH2 = R(0); }
-    R HG1 = VXl[0] * GAMA[0] + VXl[1] * GAMA[1] + VXl[2] * GAMA[2] + VXl[3] * GAMA[3];
-    R HG2 = VYl[0] * GAMA[0] + VYl[1] * GAMA[1] + VYl[2] * GAMA[2] + VYl[3] * GAMA[3];
+    if (IHBE >= 1) {
+      R PX1V = PX1 * VHX, PX2V = PX2 * VHX, PY1V = PY1 * VHY, PY2V = PY2 * VHY;
+      GAMA[0] = OFF * (R(1) - PX1V - PY1V);
+      GAMA[2] = OFF * (R(1) + PX1V + PY1V);
+      GAMA[1] = OFF * (-R(1) - PX2V - PY2V);
+      GAMA[3] = OFF * (-R(1) + PX2V + PY2V);
+    } else {
+      GAMA[0] = OFF; GAMA[2] = OFF; GAMA[1] = -OFF; GAMA[3] = -OFF;
+    }
+    const bool degen = nc[2] == nc[3];
     R* HOUR = &g.hourg[0];
-    R hour1 = HOUR[0 * nel + i] + HG1 * HH1;
-    R hour2 = HOUR[1 * nel + i] + HG2 * HH1;
-    R HOUR1A = hour1 + HG1 * (H1L + H1Q * std::fabs(HG1));
-    R HOUR2A = hour2 + HG2 * (H1L + H1Q * std::fabs(HG2));
-    for (int k = 0; k < 3; ++k) { H1j[k] = HOUR1A * GAMA[k]; H2j[k] = HOUR2A * GAMA[k]; }
-    R EHOU = HOUR1A * HG1 + HOUR2A * HG2;
-    HG1 = VZl[0] * GAMA[0] + VZl[1] * GAMA[1] + VZl[2] * GAMA[2] + VZl[3] * GAMA[3];
-    R hour3 = HOUR[2 * nel + i] + HG1 * HH2;
-    R HOUR3A = hour3 + HG1 * (H2L + H2Q * std::fabs(HG1));
-    for (int k = 0; k < 3; ++k) H3j[k] = HOUR3A * GAMA[k];
-    EHOU = EHOU + HOUR3A * HG1;
-    HG1 = RX[0] - RX[1] + RX[2] - RX[3];
-    HG2 = RY[0] - RY[1] + RY[2] - RY[3];
-    R HOUR4 = HG1 * (H3L + H3Q * std::fabs(HG1));
-    R HOUR5 = HG2 * (H3L + H3Q * std::fabs(HG2));
-    EHOU = EHOU + HOUR4 * HG1 + HOUR5 * HG2;
-    EHOU = DT1 * EHOU * OFF;
-    B1j[0] = HOUR4 * OFF; B1j[1] = -HOUR4 * OFF; B1j[2] = HOUR4 * OFF; B1j[3] = -HOUR4 * OFF;
-    B2j[0] = HOUR5 * OFF; B2j[1] = -HOUR5 * OFF; B2j[2] = HOUR5 * OFF; B2j[3] = -HOUR5 * OFF;
-    HOUR[0 * nel + i] = hour1; HOUR[1 * nel + i] = hour2; HOUR[2 * nel + i] = hour3;
+    R EHOU;
+    if (npt == 1) {
+      // MHVIS3 (mhvis3.F:109-363): elastic membrane and bending terms, V-shape
+      // bending damping Dn, no hourglass moments
+      const R H4 = R(pr.dn);
+      R FAC = R(0.25) * RHO * THK0;
+      R H1L = R(0), H1Q = R(0), H2L = R(0), H2Q = R(0);
+      R H4L = FAC * std::sqrt(HVISC * H4 * AREA);
+      R H4Q = std::sqrt(HVISC * H4) * H4L * R(100);
+      H4L = H4L * SSP;
+      FAC = R(0.25) * YM * THK0 * DT1 * HELAS;
+      R H1e = H1 * FAC, H2e = H2 * FAC;
+      if (degen) { H1Q = H1L = H2Q = H2L = H4L = H4Q = H1e = H2e = R(0); }
+      R Hm1[4], Hm2[4], Hb[4];
+      R HG1, HG2;
+      if (IHBE < 1) {
+        HG1 = VXl[0] - VXl[1] + VXl[2] - VXl[3];
+        HG2 = VYl[0] - VYl[1] + VYl[2] - VYl[3];
+      } else {
+        HG1 = VXl[0] * GAMA[0] + VXl[1] * GAMA[1] + VXl[2] * GAMA[2] + VXl[3] * GAMA[3];
+        HG2 = VYl[0] * GAMA[0] + VYl[1] * GAMA[1] + VYl[2] * GAMA[2] + VYl[3] * GAMA[3];
+      }
+      R hour1 = HOUR[0 * nel + i] + HG1 * H1e;
+      R hour2 = HOUR[1 * nel + i] + HG2 * H1e;
+      HG1 = HG1 * (H1L + H1Q * std::fabs(HG1));
+      HG2 = HG2 * (H1L + H1Q * std::fabs(HG2));
+      if (IHBE < 1) {
+        Hm1[0] = hour1 + HG1; Hm1[1] = -hour1 - HG1; Hm1[2] = hour1 + HG1; Hm1[3] = -hour1 - HG1;
+        Hm2[0] = hour2 + HG2; Hm2[1] = -hour2 - HG2; Hm2[2] = hour2 + HG2; Hm2[3] = -hour2 - HG2;
+      } else {
+        for (int k = 0; k < 4; ++k) { Hm1[k] = (hour1 + HG1) * GAMA[k]; Hm2[k] = (hour2 + HG2) * GAMA[k]; }
+      }
+      EHOU = VXl[0] * Hm1[0] + VXl[1] * Hm1[1] + VXl[2] * Hm1[2] + VXl[3] * Hm1[3] +
+             VYl[0] * Hm2[0] + VYl[1] * Hm2[1] + VYl[2] * Hm2[2] + VYl[3] * Hm2[3];
+      if (IHBE < 1) HG1 = VZl[0] - VZl[1] + VZl[2] - VZl[3];
+      else HG1 = VZl[0] * GAMA[0] + VZl[1] * GAMA[1] + VZl[2] * GAMA[2] + VZl[3] * GAMA[3];
+      R hour3 = HOUR[2 * nel + i] + HG1 * H2e;
+      HG1 = HG1 * (H2L + H2Q * std::fabs(HG1));
+      if (IHBE < 1) {
+        Hb[0] = hour3 + HG1; Hb[1] = -hour3 - HG1; Hb[2] = hour3 + HG1; Hb[3] = -hour3 - HG1;
+      } else {
+        for (int k = 0; k < 4; ++k) Hb[k] = (hour3 + HG1) * GAMA[k];
+      }
+      HG1 = VZl[0] + VZl[1] - VZl[2] - VZl[3];
+      HG1 = HG1 * (H4L + H4Q * std::fabs(HG1));
+      Hb[0] = Hb[0] + HG1; Hb[1] = Hb[1] + HG1; Hb[2] = Hb[2] - HG1; Hb[3] = Hb[3] - HG1;
+      HG1 = VZl[0] - VZl[1] - VZl[2] + VZl[3];
+      HG1 = HG1 * (H4L + H4Q * std::fabs(HG1));
+      Hb[0] = Hb[0] + HG1; Hb[1] = Hb[1] - HG1; Hb[2] = Hb[2] - HG1; Hb[3] = Hb[3] + HG1;
+      for (int k = 0; k < 3; ++k) { H1j[k] = Hm1[k]; H2j[k] = Hm2[k]; H3j[k] = Hb[k]; }
+      for (int k = 0; k < 4; ++k) { B1j[k] = R(0); B2j[k] = R(0); }
+      EHOU = EHOU + VZl[0] * Hb[0] + VZl[1] * Hb[1] + VZl[2] * Hb[2] + VZl[3] * Hb[3];
+      EHOU = DT1 * EHOU;
+      HOUR[0 * nel + i] = hour1; HOUR[1 * nel + i] = hour2; HOUR[2 * nel + i] = hour3;
+    } else if (IHBE == 2) {
+      // CHSTI3 (chsti3.F:119-320): elastic hourglass stiffness bounded by the
+      // yield stress SIGY, viscous rotational terms with SRH3 = sqrt(hr)
+      // (resol_init.F:676-682)
+      const R HP1 = H1, HP2 = H2, H3s = R(std::sqrt(pr.hr));
+      const R SHFPR3 = SHF / (R(3) * (R(1) + NU));
+      R FAC = R(0.25) * RHO * THK02;
+      R H3L = H3s * R(0.072169) * FAC * AREA;
+      R H3Q = H3s * H3L * R(100);
+      H3L = H3L * SSP;
+      FAC = YM * THK0 * DT1 * R(0.125);
+      R H1e = HP1 * FAC;
+      const R B1 = PX1 * PX1 + PY1 * PY1, B2 = PX2 * PX2 + PY2 * PY2;
+      R H2e = HP2 * FAC * THK02 * SHFPR3 / (B1 + B2);
+      if (degen) { H3Q = H3L = H1e = H2e = R(0); }
+      R HG1 = VXl[0] * GAMA[0] + VXl[1] * GAMA[1] + VXl[2] * GAMA[2] + VXl[3] * GAMA[3];
+      R HG2 = VYl[0] * GAMA[0] + VYl[1] * GAMA[1] + VYl[2] * GAMA[2] + VYl[3] * GAMA[3];
+      R hour1 = HOUR[0 * nel + i] + HG1 * H1e;
+      R hour2 = HOUR[1 * nel + i] + HG2 * H1e;
+      R FMAX = R(0.5) * SIGY * THK0 * std::sqrt(AREA) * HP1;
+      hour1 = sgn(std::min(std::fabs(hour1), FMAX), hour1);
+      hour2 = sgn(std::min(std::fabs(hour2), FMAX), hour2);
+      for (int k = 0; k < 3; ++k) { H1j[k] = hour1 * GAMA[k]; H2j[k] = hour2 * GAMA[k]; }
+      EHOU = hour1 * HG1 + hour2 * HG2;
+      HG1 = VZl[0] * GAMA[0] + VZl[1] * GAMA[1] + VZl[2] * GAMA[2] + VZl[3] * GAMA[3];
+      R hour3 = HOUR[2 * nel + i] + HG1 * H2e;
+      FMAX = R(0.25) * SIGY * THK0 * THK0 * HP2;
+      hour3 = sgn(std::min(std::fabs(hour3), FMAX), hour3);
+      for (int k = 0; k < 3; ++k) H3j[k] = hour3 * GAMA[k];
+      EHOU = EHOU + hour3 * HG1;
+      HG1 = RX[0] - RX[1] + RX[2] - RX[3];
+      HG2 = RY[0] - RY[1] + RY[2] - RY[3];
+      R HOUR4 = HG1 * (H3L + H3Q * std::fabs(HG1));
+      R HOUR5 = HG2 * (H3L + H3Q * std::fabs(HG2));
+      EHOU = EHOU + HOUR4 * HG1 + HOUR5 * HG2;
+      EHOU = DT1 * EHOU * OFF;
+      B1j[0] = HOUR4 * OFF; B1j[1] = -HOUR4 * OFF; B1j[2] = HOUR4 * OFF; B1j[3] = -HOUR4 * OFF;
+      B2j[0] = HOUR5 * OFF; B2j[1] = -HOUR5 * OFF; B2j[2] = HOUR5 * OFF; B2j[3] = -HOUR5 * OFF;
+      HOUR[0 * nel + i] = hour1; HOUR[1 * nel + i] = hour2; HOUR[2 * nel + i] = hour3;
+    } else {
+      // CHVIS3 (chvis3.F:116-300)
+      const R HVLIN = R(0);
+      R SHFPR3 = SHF / (R(3) * (R(1) + NU));
+      R HVISH1 = HVISC * H1, HVISH2 = HVISC * H2;
+      R R0 = R(0.25) * RHO;
+      R R1 = R0 * R(100);
+      R0 = R0 * HVLIN;
+      R A1c = R1 * HVISH1;
+      R SRSHFPR3 = std::sqrt(SHFPR3);
+      R A3c = R1 * HVISH2 * SRSHFPR3;
+      R A5c = HELAS * H3 * R1 * R(0.072169);
+      R R0e = R(0.25) * YM * HELAS;
+      R A7c = H1 * R0e;
+      R A8c = H2 * R0e * SHFPR3;
+      R T2A = THK02 * AREA;
+      R TSA = std::sqrt(T2A);
+      R H1Q = A1c * TSA, H1L = R(0);
+      R H2Q = A3c * THK02, H2L = R(0);
+      R H3Q = A5c * T2A, H3L = R(0);
+      (void)R0;
+      R TD = THK0 * DT1;
+      R HH1 = A7c * TD;
+      R B1 = PX1 * PX1 + PY1 * PY1, B2 = PX2 * PX2 + PY2 * PY2;
+      R HH2 = A8c * THK02 * TD / (B1 + B2);
+      if (degen) { H1Q = H1L = H2Q = H2L = H3Q = H3L = HH1 = HH2 = R(0); }
+      R HG1, HG2;
+      if (IHBE < 1) {
+        HG1 = (VXl[0] - VXl[1] + VXl[2] - VXl[3]) * OFF;
+        HG2 = (VYl[0] - VYl[1] + VYl[2] - VYl[3]) * OFF;
+      } else {
+        HG1 = VXl[0] * GAMA[0] + VXl[1] * GAMA[1] + VXl[2] * GAMA[2] + VXl[3] * GAMA[3];
+        HG2 = VYl[0] * GAMA[0] + VYl[1] * GAMA[1] + VYl[2] * GAMA[2] + VYl[3] * GAMA[3];
+      }
+      R hour1 = HOUR[0 * nel + i] + HG1 * HH1;
+      R hour2 = HOUR[1 * nel + i] + HG2 * HH1;
+      R HOUR1A = hour1 + HG1 * (H1L + H1Q * std::fabs(HG1));
+      R HOUR2A = hour2 + HG2 * (H1L + H1Q * std::fabs(HG2));
+      for (int k = 0; k < 3; ++k) { H1j[k] = HOUR1A * GAMA[k]; H2j[k] = HOUR2A * GAMA[k]; }
+      EHOU = HOUR1A * HG1 + HOUR2A * HG2;
+      if (IHBE < 1) HG1 = (VZl[0] - VZl[1] + VZl[2] - VZl[3]) * OFF;
+      else HG1 = VZl[0] * GAMA[0] + VZl[1] * GAMA[1] + VZl[2] * GAMA[2] + VZl[3] * GAMA[3];
+      R hour3 = HOUR[2 * nel + i] + HG1 * HH2;
+      R HOUR3A = hour3 + HG1 * (H2L + H2Q * std::fabs(HG1));
+      for (int k = 0; k < 3; ++k) H3j[k] = HOUR3A * GAMA[k];
+      EHOU = EHOU + HOUR3A * HG1;
+      HG1 = RX[0] - RX[1] + RX[2] - RX[3];
+      HG2 = RY[0] - RY[1] + RY[2] - RY[3];
+      R HOUR4 = HG1 * (H3L + H3Q * std::fabs(HG1));
+      R HOUR5 = HG2 * (H3L + H3Q * std::fabs(HG2));
+      EHOU = EHOU + HOUR4 * HG1 + HOUR5 * HG2;
+      EHOU = DT1 * EHOU * OFF;
+      B1j[0] = HOUR4 * OFF; B1j[1] = -HOUR4 * OFF; B1j[2] = HOUR4 * OFF; B1j[3] = -HOUR4 * OFF;
+      B2j[0] = HOUR5 * OFF; B2j[1] = -HOUR5 * OFF; B2j[2] = HOUR5 * OFF; B2j[3] = -HOUR5 * OFF;
+      HOUR[0 * nel + i] = hour1; HOUR[1 * nel + i] = hour2; HOUR[2 * nel + i] = hour3;
+    }
     ehou_out += double(EHOU);
   }
   // CDT3 (cdt3.F:110-115, 203-214), NODADT=0, IDTMIN(3)=2
@@ -966,6 +1146,10 @@ int shell_element(const Model<R>& m, ShellGroup<R>& g, PartData<R>& P, int i, do
       Fg[2][k] = E1Z * Gc[0][k] + E2Z * Gc[1][k] + E3Z * Gc[2][k];
     }
     for (int c = 0; c < 3; ++c) Fg[c][3] = -Fg[c][0] - Fg[c][1] - Fg[c][2];
+    if (IHBE >= 2 && npt != 1) {          // cfint3.F:208-214, warping moments
+      M4 = M4 + (H2j[0] + H2j[2]) * Z2;
+      M5 = M5 + (H1j[0] + H1j[2]) * Z2;
+    }
     R M1A = MOM[0] * THK02, M2A = MOM[1] * THK02, M3A = MOM[2] * THK02;
     M4 = M4 * R(0.25); M5 = M5 * R(0.25);
     R M11 = -M2A * PY1 - M3A * PX1, M21 = M1A * PX1 + M3A * PY1;
@@ -1515,6 +1699,7 @@ template <class R>
 int add_shell(Model<R>& m, int part, int nel, const int* ixc, const or_material* mat,
               const or_shell_prop* prop, const double* thke) {
   if (prop->npt < 1 || prop->npt > 10 || prop->ipla < 0 || prop->ipla > 2) return OR_E_UNSUPPORTED;
+  if (prop->ishell < 0 || prop->ishell > 4 || !(prop->dn >= 0)) return OR_E_UNSUPPORTED;
   if (prop->ishfram != 0 && prop->ishfram != 2) return OR_E_UNSUPPORTED;
   ShellGroup<R> g;
   g.part = part; g.nel = nel; g.mat = *mat; g.prop = *prop;
