@@ -123,3 +123,26 @@ def test_reader_refuses_what_it_does_not_implement(tmp_path):
     open(path, "w").write(text)
     with pytest.raises(rad.RadError, match="INTER"):
         rad.StarterDeck(str(path))
+
+
+@pytest.mark.parametrize("ishell,npt,hm,hr", [(2, 5, 0.01, 0.01), (3, 5, 0.1, 0.01), (4, 1, 0.01, 0.01)])
+def test_reader_shell_formulations_and_their_defaults(tmp_path, ishell, npt, hm, hr):
+    """Ishell 2 to 4 pass through with the starter's hourglass defaults (0.1, 0.1,
+    0.01 for Ishell 3; hm_read_prop01.F:204-212) and Dn; other Ishell values are
+    refused."""
+    path = tmp_path / "FORM_0000.rad"
+    write_deck(path)
+    text = open(path).read()
+    old = "/PROP/SHELL/2\nshell\n" + i10(0, 0, 0, 0) + " " * 20 + f20(0.0) + "\n" + f20(0.0, 0.0, 0.0, 0.0, 0.0) + \
+        "\n" + i10(5, 0)
+    assert old in text
+    new = "/PROP/SHELL/2\nshell\n" + i10(ishell, 0, 0, 0) + " " * 20 + f20(0.0) + "\n" + \
+        f20(0.0, 0.0, 0.0, 0.0, 0.02) + "\n" + i10(npt, 0)
+    open(path, "w").write(text.replace(old, new))
+    pr = rad.to_deck(rad.StarterDeck(str(path)))["parts"][0]["shell"][0]["prop"]
+    assert pr["ishell"] == ishell and pr["npt"] == npt
+    assert (pr["hm"], pr["hf"], pr["hr"]) == (hm, hm, hr)
+    assert pr["dn"] == 0.02
+    open(path, "w").write(text.replace(old, new.replace(i10(ishell, 0, 0, 0), i10(12, 0, 0, 0))))
+    with pytest.raises(rad.RadError, match="Ishell 12"):
+        rad.to_deck(rad.StarterDeck(str(path)))
