@@ -1,10 +1,12 @@
-"""Tile-shape autotuner for the patch kernels.
+"""Autotuner for the cycle's launch form.
 
-For a deck and precision, builds one handle per candidate tile (elements per
-patch = threads per CTA of the hexa and shell kernels), times a few hundred
-graph-replayed cycles with CUDA events on the handle's stream, and returns the
-fastest.  Results are cached per (deck name, element count, precision, GPU) in
-``autotune_cache.json`` beside this file.
+For a deck and precision, builds one handle per candidate: each tile (elements
+per patch = threads per CTA of the hexa and shell kernels), and for a deck
+that can run the persistent shell cycle, each tile both with it and with the
+per-phase kernels.  It times a few hundred graph-replayed cycles of each with
+CUDA events on the handle's stream and returns the fastest.  Results are cached
+per (deck name, element count, precision, GPU) in ``autotune_cache.json``
+beside this file.
 
     python -m openradioss_b200.autotune --workload shell_plate
 """
@@ -38,7 +40,9 @@ def _time_cycles(h, ncycles):
 
 
 def tune(deck, precision=abi.OR_PREC_SPLIT, ncycles=256, use_cache=True, device=0, verbose=False):
-    """Returns (block_hex, block_shell, {candidate: ms per cycle})."""
+    """Returns (block_hex, block_shell, persistent, {candidate: ms per cycle});
+    persistent is the cfg.persistent value of the fastest form (0: the persistent
+    cycle where eligible, -1: the per-phase kernels)."""
     import torch
     from .ecycle import ECycle
     gpu = torch.cuda.get_device_name(device)
@@ -49,27 +53,36 @@ def tune(deck, precision=abi.OR_PREC_SPLIT, ncycles=256, use_cache=True, device=
             cache = json.load(open(CACHE))
         except (OSError, ValueError):
             cache = {}
-    if use_cache and key in cache:
+    if use_cache and key in cache and "persistent" in cache[key]:
         c = cache[key]
-        return c["block_hex"], c["block_shell"], c["ms_per_cycle"]
+        return c["block_hex"], c["block_shell"], c["persistent"], c["ms_per_cycle"]
     has_hex = any(p["hex"] for p in deck["parts"])
     has_shell = any(p["shell"] for p in deck["parts"])
     timings = {}
     for t in CANDIDATES:
-        h = ECycle(deck, precision=precision, device=device, graph=1, block_hex=t, block_shell=t)
-        timings[t] = _time_cycles(h, ncycles)
-        h.close()
-        if verbose:
-            print(f"tile {t}: {timings[t] * 1e3:.2f} us/cycle", flush=True)
+        for pers in (0, -1):
+            h = ECycle(deck, precision=precision, device=device, graph=1, block_hex=t, block_shell=t,
+                       persistent=pers)
+            on = h.persistent_info()[0]
+            k = (t, 0 if on else -1)
+            timings[k] = _time_cycles(h, ncycles)
+            h.close()
+            if verbose:
+                print(f"tile {t} {'persistent' if on else 'phase kernels'}: {timings[k] * 1e3:.2f} us/cycle",
+                      flush=True)
+            if not on:
+                break                     # no persistent form at this tile: the phase kernels are timed
     best = min(timings, key=timings.get)
-    bh = best if has_hex else 256
-    bs = best if has_shell else 256
-    cache[key] = {"block_hex": bh, "block_shell": bs, "ms_per_cycle": {str(k): v for k, v in timings.items()}}
+    bh = best[0] if has_hex else 256
+    bs = best[0] if has_shell else 256
+    name = lambda k: f"{k[0]}{'p' if k[1] == 0 else ''}"
+    cache[key] = {"block_hex": bh, "block_shell": bs, "persistent": best[1],
+                  "ms_per_cycle": {name(k): v for k, v in timings.items()}}
     try:
         json.dump(cache, open(CACHE, "w"), indent=1, sort_keys=True)
     except OSError:
         pass
-    return bh, bs, cache[key]["ms_per_cycle"]
+    return bh, bs, best[1], cache[key]["ms_per_cycle"]
 
 
 def main():
