@@ -667,7 +667,7 @@ int persist_build(or_ecycle* h, Impl<R>& m) {
       }
     }
   }
-  const size_t smem = persist_smem<R>(ncmax, tile, P, m.sinc_stride);
+  const size_t smem = persist_smem<R>(ncmax, tile, P, m.sinc_stride, ps.nlmax);
   if (smem > 200 * 1024) return OR_OK;
   const PersistFn<R> fn = persist_fn<R>(tile, m.uniform_npt == 5);
   CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

@@ -133,16 +133,19 @@ __device__ inline void group_reduce(unsigned long long& key, unsigned long long&
 constexpr int PERSIST_THREADS = 384;
 
 template <class R>
-__host__ __device__ inline size_t persist_smem(int ncmax, int tile, int P, int inc_stride) {
+__host__ __device__ inline size_t persist_smem(int ncmax, int tile, int P, int inc_stride, int nlmax) {
   // node planes: x y z dx dy dz (FP64), vx vy vz rx ry rz ms in (R), global index
   // (int), owner and code (bytes); per patch: 24 corner planes of TILE (R), the
-  // incidence lists (uint16), reduction scratch
+  // incidence lists (uint16), reduction scratch, the slot of each patch node (int);
+  // per held node its slot range (int2)
   const size_t nodes = (size_t)ncmax * (6 * sizeof(double) + 8 * sizeof(R) + sizeof(int) + 2);
   const size_t nodes_al = (nodes + 15) / 16 * 16;
   const size_t corners = (size_t)P * 24 * tile * sizeof(R);
   const size_t inc = ((size_t)P * inc_stride * 2 + 15) / 16 * 16;
   const size_t red = (size_t)P * (tile / 32) * 32;
-  return nodes_al + corners + inc + red;
+  const size_t slots = ((size_t)P * nlmax * sizeof(int) + 15) / 16 * 16;
+  const size_t ranges = (size_t)ncmax * sizeof(int2);
+  return nodes_al + corners + inc + red + slots + ranges;
 }
 
 template <class R, int TILE, int NPT>
@@ -183,6 +186,12 @@ shell_persistent_kernel(ShellArgs<R> a, NodeArgs<R> na, PersistArgs pa, int ncyc
   double* s_s1 = s_s0 + NW;
   R* sc = sc_all + (size_t)sub * 24 * TILE;
   unsigned short* sinc = sinc_all + (size_t)sub * a.inc_stride;
+  // slot numbers of the patch nodes and slot ranges of the held nodes, read once
+  // here instead of from global memory in every cycle
+  int* sslot_all = reinterpret_cast<int*>(red_base + (size_t)P * NW * 32);
+  int* sslot = sslot_all + (size_t)sub * a.nlmax;
+  int2* srange = reinterpret_cast<int2*>(reinterpret_cast<unsigned char*>(sslot_all) +
+                                         ((size_t)P * a.nlmax * sizeof(int) + 15) / 16 * 16);
 
   // ---- this CTA's patch and element ----
   const int p = cta * P + sub;
@@ -208,11 +217,13 @@ shell_persistent_kernel(ShellArgs<R> a, NodeArgs<R> na, PersistArgs pa, int ncyc
     sglob[i] = g;
     sown[i] = pa.owner[n0 + i];
     scode[i] = na.code[g];
+    srange[i] = make_int2(na.adsky[g], na.adsky[g + 1]);
   }
   if (has_patch) {
     const unsigned* src = reinterpret_cast<const unsigned*>(a.inc + (size_t)p * a.inc_stride);
     unsigned* dst = reinterpret_cast<unsigned*>(sinc);
     for (int i = lt; i < a.inc_stride / 2; i += TILE) dst[i] = src[i];
+    for (int j = lt; j < a.patch[p].nloc; j += TILE) sslot[j] = a.patch_slots[p * a.nlmax + j];
   }
   ShellState<R, NPT> st;
   if (KEEP) shell_load_state<R, NPT>(a, e, st);
@@ -261,7 +272,7 @@ shell_persistent_kernel(ShellArgs<R> a, NodeArgs<R> na, PersistArgs pa, int ncyc
         f0 += sc[o]; f1 += sc[4 * TILE + o]; f2 += sc[8 * TILE + o];
         m0 += sc[12 * TILE + o]; m1 += sc[16 * TILE + o]; m2 += sc[20 * TILE + o];
       }
-      const int s = a.patch_slots[p * NLM + j];
+      const int s = sslot[j];
       st_cg(&fslot[s], mk4(f0, f1, f2, R(0)));
       st_cg(&mslot[s], mk4(m0, m1, m2, R(0)));
     }
@@ -284,17 +295,35 @@ shell_persistent_kernel(ShellArgs<R> a, NodeArgs<R> na, PersistArgs pa, int ncyc
     const double DTc1 = t.dt2;
     const double DT12 = 0.5 * (DTc1 + DT2);
     const bool last = c == ncycles - 1;
-    for (int i = tid; i < nn; i += blockDim.x) {
+    // a thread's nodes are i0 = tid + 2 j blockDim.x and i0 + blockDim.x: the first two
+    // slots of both are loaded before either is summed, so four L2 reads are in flight
+    for (int i0 = tid; i0 < nn; i0 += 2 * blockDim.x) {
+    R4 F0[2], F1[2], M0[2], M1[2];
+    int2 rg[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int i = i0 + u * blockDim.x;
+      rg[u] = i < nn ? srange[i] : make_int2(0, 0);
+      F0[u] = F1[u] = M0[u] = M1[u] = mk4(R(0), R(0), R(0), R(0));
+      if (rg[u].y > rg[u].x) { F0[u] = ld_cg(&fslot[rg[u].x]); M0[u] = ld_cg(&mslot[rg[u].x]); }
+      if (rg[u].y > rg[u].x + 1) { F1[u] = ld_cg(&fslot[rg[u].x + 1]); M1[u] = ld_cg(&mslot[rg[u].x + 1]); }
+    }
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int i = i0 + u * blockDim.x;
+      if (i >= nn) break;
       const int g = sglob[i];
-      const int k0 = na.adsky[g], k1 = na.adsky[g + 1];
+      const int k0 = rg[u].x, k1 = rg[u].y;
       R ax = R(0), ay = R(0), az = R(0), rx = R(0), ry = R(0), rz = R(0);
       if (k1 > k0) {
-        const R4 f = ld_cg(&fslot[k0]);
-        ax = f.x; ay = f.y; az = f.z;
-        const R4 m = ld_cg(&mslot[k0]);
-        rx = m.x; ry = m.y; rz = m.z;
+        ax = F0[u].x; ay = F0[u].y; az = F0[u].z;
+        rx = M0[u].x; ry = M0[u].y; rz = M0[u].z;
       }
-      for (int k = k0 + 1; k < k1; ++k) {
+      if (k1 > k0 + 1) {
+        ax += F1[u].x; ay += F1[u].y; az += F1[u].z;
+        rx += M1[u].x; ry += M1[u].y; rz += M1[u].z;
+      }
+      for (int k = k0 + 2; k < k1; ++k) {
         const R4 f = ld_cg(&fslot[k]);
         ax += f.x; ay += f.y; az += f.z;
         const R4 m = ld_cg(&mslot[k]);
@@ -310,6 +339,7 @@ shell_persistent_kernel(ShellArgs<R> a, NodeArgs<R> na, PersistArgs pa, int ncyc
       sv[0 * NC + i] = v.x; sv[1 * NC + i] = v.y; sv[2 * NC + i] = v.z;
       sv[3 * NC + i] = w.x; sv[4 * NC + i] = w.y; sv[5 * NC + i] = w.z;
       if (last && sown[i]) { pa.ek_node[g] = ek; pa.ekr_node[g] = ekr; }
+    }
     }
     if (cta == 0 && tid == 0) {            // reuse in two cycles: everyone has read it
       PartAcc r; r.dtkey = ~0ull; r.dtbits = ~0ull;
