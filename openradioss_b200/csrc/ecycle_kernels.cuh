@@ -201,9 +201,9 @@ struct NodeArgs {
   const unsigned char* rb_role;
   // rotational nodes, one bit per node (bit n & 31 of word n >> 5): the nodes of a
   // part with rotations whose inertia or rotational velocity is nonzero.  Only
-  // these read and write VR and their moment slots; for any other node the
-  // rotational update would leave VR as it is (zero moment over zero inertia, zero
-  // VR) and add no rotational energy.  Null when no part has rotations.
+  // these read their moment slots and write VR; for any other node the rotational
+  // update would leave VR as it is (zero moment over zero inertia, zero VR) and add
+  // no rotational energy.  Null when no part has rotations.
   const unsigned* rotmask;
 };
 
@@ -1059,7 +1059,9 @@ __device__ __forceinline__ void shell_element(const ShellArgs<R>& a, const int e
     RXl[k] = E1X * rx + E1Y * ry + E1Z * rz;
     RYl[k] = E2X * rx + E2Y * ry + E2Z * rz;
   }
-  const int IHBE = gd.ihbe;
+  // NPT = 5 kernels are launched only when every group is Ishell 1 (IHBE 1): the
+  // other branches compile out of them
+  const int IHBE = NPT == 5 ? 1 : gd.ihbe;
   R EXX, EYY, EXY, EXZ, EYZ, KXX, KYY, KXY;
   {
     const R VZ13 = VZl[0] - VZl[2], VZ24 = VZl[1] - VZl[3];
@@ -1679,8 +1681,10 @@ __device__ __forceinline__ void node_pass(NodeArgs<R> a, int parity) {
     const unsigned char code = codes[n];
     const double dx = DX[n], dy = DY[n], dz = DZ[n];
     R4 f0 = mk4(R(0), R(0), R(0), R(0)), m0 = f0, w0 = f0;
+    // VR is loaded before the rotational-node bit arrives (a dependent load would
+    // lengthen the pass's latency chain); only rotational nodes use and write it
     const bool rn = rot_node(a, n);
-    if (rn) w0 = VR[n];
+    if (VR) w0 = VR[n];
     const int part = a.tile_part[tile];
     const PartDesc pd = a.parts[part];
     const bool valid = n < pd.node_end;

@@ -66,15 +66,20 @@ __device__ __forceinline__ void st_cg(double4* p, double4 v) {
 
 // one grid-wide barrier: arrive, then poll the counter until every CTA arrived at
 // this barrier; true when the launch must end (a CTA gave up waiting)
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
 __device__ __forceinline__ bool grid_barrier(unsigned* sync, unsigned target, ErrorWord* err, int* s_abort) {
   __syncthreads();
   if (threadIdx.x == 0) {
-    __threadfence();
+    __threadfence();                          // release: this CTA's slot writes and reductions
     atomicAdd(&sync[0], 1u);
     const long long t0 = clock64();
     int ab = 0;
     for (;;) {
-      const unsigned v = __ldcg(&sync[0]);
+      const unsigned v = ld_acquire(&sync[0]);  // acquire: every CTA's writes before its arrival
       if (v >= target) break;
       if (__ldcg(&sync[1])) { ab = 1; break; }
       if (clock64() - t0 > (1ll << 31)) {           // about a second at the SM clock
@@ -85,7 +90,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned* sync, unsigned target, Er
       }
       __nanosleep(32);
     }
-    __threadfence();
+    if (ab) __threadfence();
     *s_abort = ab;
   }
   __syncthreads();
@@ -266,6 +271,7 @@ shell_persistent_kernel(ShellArgs<R> a, NodeArgs<R> na, PersistArgs pa, int ncyc
     for (int j = lt; j < nl; j += TILE) {
       R f0 = R(0), f1 = R(0), f2 = R(0), m0 = R(0), m1 = R(0), m2 = R(0);
       const int i1 = sinc[j + 1];
+#pragma unroll 4
       for (int i = sinc[j]; i < i1; ++i) {
         const int q = sinc[NLM + 1 + i];
         const int o = (q & 3) * TILE + (q >> 2);
@@ -286,6 +292,23 @@ shell_persistent_kernel(ShellArgs<R> a, NodeArgs<R> na, PersistArgs pa, int ncyc
     }
     if (grid_barrier(pa.sync, (unsigned)(c + 1) * (unsigned)G, a.err, &s_abort)) return;
     // ---------------- node phase ----------------
+    // A thread's nodes are i0 = tid + 2 j blockDim.x and i0 + blockDim.x.  The first
+    // two slots of both are loaded before either is summed, and for the first pair
+    // before the cycle's dt reduction is read, so that all these L2 reads are in
+    // flight together.
+    R4 F0[2], F1[2], M0[2], M1[2];
+    int2 rg[2];
+    auto prefetch = [&](int i0) {
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int i = i0 + u * blockDim.x;
+        rg[u] = i < nn ? srange[i] : make_int2(0, 0);
+        F0[u] = F1[u] = M0[u] = M1[u] = mk4(R(0), R(0), R(0), R(0));
+        if (rg[u].y > rg[u].x) { F0[u] = ld_cg(&fslot[rg[u].x]); M0[u] = ld_cg(&mslot[rg[u].x]); }
+        if (rg[u].y > rg[u].x + 1) { F1[u] = ld_cg(&fslot[rg[u].x + 1]); M1[u] = ld_cg(&mslot[rg[u].x + 1]); }
+      }
+    };
+    prefetch(tid);
     PartAcc ac;
     ac.dtkey = __ldcg(&pa.acc3[c % 3].dtkey);
     ac.dtbits = __ldcg(&pa.acc3[c % 3].dtbits);
@@ -295,19 +318,8 @@ shell_persistent_kernel(ShellArgs<R> a, NodeArgs<R> na, PersistArgs pa, int ncyc
     const double DTc1 = t.dt2;
     const double DT12 = 0.5 * (DTc1 + DT2);
     const bool last = c == ncycles - 1;
-    // a thread's nodes are i0 = tid + 2 j blockDim.x and i0 + blockDim.x: the first two
-    // slots of both are loaded before either is summed, so four L2 reads are in flight
     for (int i0 = tid; i0 < nn; i0 += 2 * blockDim.x) {
-    R4 F0[2], F1[2], M0[2], M1[2];
-    int2 rg[2];
-#pragma unroll
-    for (int u = 0; u < 2; ++u) {
-      const int i = i0 + u * blockDim.x;
-      rg[u] = i < nn ? srange[i] : make_int2(0, 0);
-      F0[u] = F1[u] = M0[u] = M1[u] = mk4(R(0), R(0), R(0), R(0));
-      if (rg[u].y > rg[u].x) { F0[u] = ld_cg(&fslot[rg[u].x]); M0[u] = ld_cg(&mslot[rg[u].x]); }
-      if (rg[u].y > rg[u].x + 1) { F1[u] = ld_cg(&fslot[rg[u].x + 1]); M1[u] = ld_cg(&mslot[rg[u].x + 1]); }
-    }
+    if (i0 != tid) prefetch(i0);
 #pragma unroll
     for (int u = 0; u < 2; ++u) {
       const int i = i0 + u * blockDim.x;
