@@ -5,8 +5,8 @@ workload runs at its configured size (mesh, material, loads, codes) for as
 many cycles as the oracle finishes in seconds:
 * C1 hexa block 10x10x40, LAW1, all 1000 cycles, FP64;
 * C2 shell plate 200x200, 5 IP, LAW2, 200 cycles, FP64 and split;
-* C3 64 uneven parts, each on its own time step, 20 cycles, FP64;
-* C4 2.0 M hexas + 80,000 shells, 20 cycles, FP64.
+* C3 64 uneven parts, each on its own time step, 20 cycles, FP64 and split;
+* C4 2.0 M hexas + 80,000 shells, 20 cycles, FP64 and split.
 
 Bars: FP64 1e-10 relative (normwise), split 1e-5 relative nodal displacement
 against the split oracle and the FP64 oracle.  Some quantities of these runs
@@ -127,3 +127,20 @@ def test_c4_mixed_mesh_full_size_fp64(lib):
     check_hex(g, o, FP64_TOL)
     check_shell(g, o, FP64_TOL)
     check_energies(g, o, FP64_TOL)
+
+
+@pytest.mark.parametrize("workload", ["c3", "c4"])
+def test_split_full_size_against_split_oracle(lib, workload):
+    """C3 (64 parts) and C4 (2.08 M elements) in the split form at full size, 20
+    cycles: nodal displacements within 1e-5 of the split oracle and of the FP64
+    oracle, per part."""
+    from oracle.oracle import Oracle
+    d = decks.c3_batched_parts() if workload == "c3" else decks.c4_mixed_mesh()
+    g, o = run_pair(d, 20, precision=abi.OR_PREC_SPLIT, oracle_precision=abi.OR_PREC_SPLIT)
+    o64 = Oracle(d, precision=abi.OR_PREC_FP64, nthreads=8)
+    o64.step(20)
+    for p in range(g.nparts):
+        a = g.get_nodes(p)["d"]
+        assert rel(a, o.get_nodes(p)["d"]) < SPLIT_TOL, (p, rel(a, o.get_nodes(p)["d"]))
+        assert rel(a, o64.get_nodes(p)["d"]) < SPLIT_TOL, (p, rel(a, o64.get_nodes(p)["d"]))
+        assert g.time(p)["ncycle"] == o.time(p)["ncycle"]
