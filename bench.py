@@ -67,6 +67,9 @@ def parse():
     ap.add_argument("--sub-tile", type=int, default=128)
     ap.add_argument("--eager-cycles", type=int, default=0,
                     help="profiling mode: run this many eager cycles and print per-phase times")
+    ap.add_argument("--persistent-cycles", type=int, default=0,
+                    help="profiling mode: three step() calls of this many cycles through the persistent shell "
+                         "cycle, timed with events")
     ap.add_argument("--mesh-n", type=int, default=0, help="profiling mode: mesh size parameter (0 = workload's)")
     ap.add_argument("--tile", type=int, default=0, help="profiling mode: elements per patch (0 = library default)")
     ap.add_argument("--precision", default="split", choices=["split", "fp64"], help="profiling mode")
@@ -138,6 +141,34 @@ def perturbed_run(h, deck, cycles, eps=1e-12, seed=7):
         h.set_nodes(p, x=x)
     h.step(cycles)
     return outputs(h)
+
+
+def persistent_profile(args):
+    """--persistent-cycles: the persistent shell cycle alone (one launch per step() call)."""
+    import torch
+    from openradioss_b200 import abi, build, decks
+    from openradioss_b200.ecycle import ECycle
+    build.build()
+    d = make_deck(args.workload, args.mesh_n)
+    prec = abi.OR_PREC_SPLIT if args.precision == "split" else abi.OR_PREC_FP64
+    tiles = dict(block_shell=args.tile) if args.tile else {}
+    h = ECycle(d, precision=prec, graph=1, **tiles)
+    on, ctas, threads = h.persistent_info()
+    if not on:
+        raise SystemExit("this deck does not run the persistent shell cycle")
+    s = torch.cuda.ExternalStream(h.stream())
+    ms = []
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(s)
+        h.step(args.persistent_cycles)
+        e1.record(s)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    print(json.dumps({"workload": args.workload, "elements": decks.num_elements(d), "ctas": ctas, "threads": threads,
+                      "cycles_per_launch": args.persistent_cycles,
+                      "us_per_cycle": [m * 1e3 / args.persistent_cycles for m in ms]}))
 
 
 def eager_profile(args):
@@ -359,6 +390,8 @@ def main():
         return reference_arm(args, rank, world)
     if args.eager_cycles:
         return eager_profile(args)
+    if args.persistent_cycles:
+        return persistent_profile(args)
 
     import torch
     import torch.distributed as dist

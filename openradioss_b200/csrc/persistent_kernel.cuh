@@ -97,6 +97,14 @@ __device__ __forceinline__ bool grid_barrier(unsigned* sync, unsigned target, Er
   return *s_abort != 0;
 }
 
+// minimum of a 64-bit unsigned value over the warp, from two 32-bit hardware
+// reductions (high words, then the low words of the lanes holding the high minimum)
+__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v) {
+  const unsigned hi = __reduce_min_sync(0xffffffffu, (unsigned)(v >> 32));
+  const unsigned lo = __reduce_min_sync(0xffffffffu, (unsigned)(v >> 32) == hi ? (unsigned)v : 0xffffffffu);
+  return ((unsigned long long)hi << 32) | lo;
+}
+
 // the dt-key / dt-bits min and the two energy sums of a group of TILE threads
 // (threads g*TILE .. g*TILE+TILE-1), with the operation order of block_reduce
 template <int TILE>
@@ -162,6 +170,7 @@ shell_persistent_kernel(ShellArgs<R> a, NodeArgs<R> na, PersistArgs pa, int ncyc
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int s_abort;
   __shared__ double s_e0[PERSIST_THREADS / 32], s_e1[PERSIST_THREADS / 32];
+  __shared__ unsigned long long s_dt[2];        // the CTA's dt key and dt bits minimum of a cycle
   const int tid = threadIdx.x;
   const int cta = blockIdx.x, G = gridDim.x;
   const int P = pa.patches_per_cta, NC = pa.ncmax;
@@ -239,8 +248,11 @@ shell_persistent_kernel(ShellArgs<R> a, NodeArgs<R> na, PersistArgs pa, int ncyc
   }
   const ShellGroupDesc gd = a.groups[has_patch ? pi.group : 0];
   const int nl = has_patch ? pi.nloc : 0;
-  double cum_ehour = 0.0, cum_wpla = 0.0;       // the patch's cumulative energies (its leader thread)
-  if (has_patch && lt == 0) { cum_ehour = a.blk_ehour[p]; cum_wpla = a.blk_wpla[p]; }
+  // Energies: each thread adds its element's hourglass energy and plastic work over
+  // the launch's cycles; the patch sums them once at the end onto its cumulative
+  // partials (the phase kernels sum per cycle, so the two agree to FP64 rounding).
+  double cum_ehou_t = 0.0, cum_wpla_t = 0.0;
+  if (tid == 0) { s_dt[0] = ~0ull; s_dt[1] = ~0ull; }
   PartTime t = na.time[parity0];
   R4* fs[2] = {a.fslot, reinterpret_cast<R4*>(pa.fslot2)};
   R4* ms_[2] = {a.mslot, reinterpret_cast<R4*>(pa.mslot2)};
@@ -266,8 +278,20 @@ shell_persistent_kernel(ShellArgs<R> a, NodeArgs<R> na, PersistArgs pa, int ncyc
           sc[((q + 3) * 4 + k) * TILE + lt] = Mg[q][k];
         }
       }
+      cum_ehou_t += my_ehou;
+      cum_wpla_t += my_wpla;
+    }
+    {   // the CTA's dt minimum: per warp in registers, then one shared atomic per warp
+      const unsigned long long wk = warp_min_u64(mykey), wb = warp_min_u64(mybits);
+      if ((tid & 31) == 0) { atomicMin(&s_dt[0], wk); atomicMin(&s_dt[1], wb); }
     }
     __syncthreads();
+    if (tid == 0) {      // to the grid's reduction at once, ahead of the patch sums
+      PartAcc* acc = &pa.acc3[c % 3];
+      atomicMin(&acc->dtkey, s_dt[0]);
+      atomicMin(&acc->dtbits, s_dt[1]);
+      s_dt[0] = ~0ull; s_dt[1] = ~0ull;        // no warp touches them again before the grid barrier
+    }
     for (int j = lt; j < nl; j += TILE) {
       R f0 = R(0), f1 = R(0), f2 = R(0), m0 = R(0), m1 = R(0), m2 = R(0);
       const int i1 = sinc[j + 1];
@@ -281,14 +305,6 @@ shell_persistent_kernel(ShellArgs<R> a, NodeArgs<R> na, PersistArgs pa, int ncyc
       const int s = sslot[j];
       st_cg(&fslot[s], mk4(f0, f1, f2, R(0)));
       st_cg(&mslot[s], mk4(m0, m1, m2, R(0)));
-    }
-    group_reduce<TILE>(mykey, mybits, my_ehou, my_wpla, s_key, s_bits, s_s0, s_s1);
-    if (has_patch && lt == 0) {
-      PartAcc* acc = &pa.acc3[c % 3];
-      atomicMin(&acc->dtkey, mykey);
-      atomicMin(&acc->dtbits, mybits);
-      cum_ehour = cum_ehour + my_ehou;
-      cum_wpla = cum_wpla + my_wpla;
     }
     if (grid_barrier(pa.sync, (unsigned)(c + 1) * (unsigned)G, a.err, &s_abort)) return;
     // ---------------- node phase ----------------
@@ -374,7 +390,14 @@ shell_persistent_kernel(ShellArgs<R> a, NodeArgs<R> na, PersistArgs pa, int ncyc
   if constexpr (KEEP) {
     if (has_patch) shell_store_state<R, NPT>(a, e, st);
   }
-  if (has_patch && lt == 0) { a.blk_ehour[p] = cum_ehour; a.blk_wpla[p] = cum_wpla; }
+  {
+    unsigned long long k0 = ~0ull, k1 = ~0ull;
+    group_reduce<TILE>(k0, k1, cum_ehou_t, cum_wpla_t, s_key, s_bits, s_s0, s_s1);
+    if (has_patch && lt == 0) {
+      a.blk_ehour[p] = a.blk_ehour[p] + cum_ehou_t;
+      a.blk_wpla[p] = a.blk_wpla[p] + cum_wpla_t;
+    }
+  }
   if (cta == 0 && tid == 0) {
     const int fin = (parity0 + ncycles) & 1;
     na.time[fin] = t;

@@ -4,8 +4,10 @@ A handle of one shell part without rigid links or loads runs all the cycles of
 a step() call in one cooperative launch (openradioss_b200/csrc/
 persistent_kernel.cuh).  It performs the same operations in the same order as
 the patch and node kernels, so with floating-point contraction off (the
-library built with -fmad=false) every output is bitwise equal to a handle built
-with cfg.persistent = -1: nodes, element state, energies, time state.  With
+library built with -fmad=false) the nodes, the element state and the time state
+are bitwise equal to a handle built with cfg.persistent = -1; the energies,
+which the persistent form sums over its cycles per element before summing over
+the patch, agree to FP64 rounding (1e-13 relative).  With
 FMA contraction (the product build) the compiler may fuse a multiply-add in
 one kernel and not in the other; there the two forms are held to the parity
 bars against each other and against the oracle.
@@ -55,7 +57,9 @@ def assert_same(a, b):
         sa, sb = a.shell_state(g), b.shell_state(g)
         for k in sa:
             assert np.array_equal(sa[k], sb[k]), (g, k)
-    assert a.energies() == b.energies()
+    ea, eb = a.energies(), b.energies()
+    for k in eb:
+        assert abs(ea[k] - eb[k]) <= 1e-13 * abs(eb[k]), (k, ea[k], eb[k])
     assert a.time() == b.time()
 
 
