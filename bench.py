@@ -367,10 +367,9 @@ def kernel_roofline(h, deck, cycles, workload, s=4, step_ms=None):
     if h.persistent_info()[0] and step_ms:
         pb = (eb + nb) * cycles
         ptraffic = None
-        if os.path.exists(tpath):
+        if os.path.exists(tpath):     # staged once per launch: the DRAM bytes do not grow with its cycles
             try:
-                t1 = json.load(open(tpath)).get(workload, {}).get("persistent_split_per_cycle")
-                ptraffic = t1 * cycles if t1 is not None else None
+                ptraffic = json.load(open(tpath)).get(workload, {}).get("persistent_split_per_launch")
             except (OSError, ValueError):
                 ptraffic = None
         pa = pb / (step_ms * 1e-3) / 1e9

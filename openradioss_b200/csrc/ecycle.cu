@@ -354,6 +354,7 @@ struct Impl {
   // nodes
   DBuf<double4> X; DBuf<double> DX, DY, DZ; DBuf<R4> V, VR; DBuf<unsigned char> code;
   DBuf<unsigned> rotmask; std::vector<unsigned> rotmask_h;   // NodeArgs::rotmask, and its host copy
+  int rot_sparse = 0;                                         // NodeArgs::rot_sparse
   DBuf<int> adsky, tile_part; DBuf<PartDesc> partd;
   DBuf<R4> fslot, mslot;
   DBuf<PartTime> time; DBuf<PartAcc> acc; DBuf<ErrorWord> err;
@@ -435,6 +436,7 @@ struct Impl {
     a.skew_of = skew_of.p; a.skews = skw.p;
     a.rb_role = nrb ? rb_role.p : nullptr;
     a.rotmask = any_rot ? rotmask.p : nullptr;
+    a.rot_sparse = rot_sparse;
     return a;
   }
   void free_all() {
@@ -925,6 +927,9 @@ int finalize_impl(or_ecycle* h) {
     m.rotmask_h.assign((nn + 31) / 32, 0u);
     for (auto& P : h->parts)
       if (P.has_rot) rot_bits<R>(m, P, P.vr.data());
+    long long nrot = 0;
+    for (unsigned w : m.rotmask_h) nrot += __builtin_popcount(w);
+    m.rot_sparse = 2 * nrot < (long long)nn ? 1 : 0;
   }
   if ((rc = dput(h, m.X, X)) || (rc = dput(h, m.V, V)) || (rc = dput(h, m.VR, VR)) || (rc = dput(h, m.code, code)) ||
       (rc = dput(h, m.adsky, adsky)) || (rc = dput(h, m.tile_part, tile_part)) || (rc = dput(h, m.partd, pd)) ||

@@ -205,6 +205,11 @@ struct NodeArgs {
   // update would leave VR as it is (zero moment over zero inertia, zero VR) and add
   // no rotational energy.  Null when no part has rotations.
   const unsigned* rotmask;
+  // 1 when fewer than half of the nodes are rotational (a solid mesh with a shell
+  // skin): VR is then read only for rotational nodes, after their bit.  0: VR is
+  // read for every node ahead of the bit, which keeps the latency chain of a
+  // one-wave pass short.
+  int rot_sparse;
 };
 
 // Whether node n carries rotations in the node pass (NodeArgs::rotmask).
@@ -1684,7 +1689,7 @@ __device__ __forceinline__ void node_pass(NodeArgs<R> a, int parity) {
     // VR is loaded before the rotational-node bit arrives (a dependent load would
     // lengthen the pass's latency chain); only rotational nodes use and write it
     const bool rn = rot_node(a, n);
-    if (VR) w0 = VR[n];
+    if (VR && (!a.rot_sparse || rn)) w0 = VR[n];
     const int part = a.tile_part[tile];
     const PartDesc pd = a.parts[part];
     const bool valid = n < pd.node_end;
