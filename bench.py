@@ -2,7 +2,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload shell_plate|hex_block|mixed_mesh|batched_parts]
-                    [--sub-workloads mixed_mesh] [--eager-cycles N --mesh-n M --tile T]
+                    [--sub-workloads mixed_mesh,batched_parts] [--eager-cycles N --mesh-n M --tile T]
 
 One step = one complete run of the workload (all its cycles) from the uploaded
 initial state; the state is reset between steps outside the timed region and
@@ -61,7 +61,7 @@ def parse():
     ap.add_argument("--cycles", type=int, default=0, help="override cycles per step")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--sub-workloads", default="mixed_mesh",
+    ap.add_argument("--sub-workloads", default="mixed_mesh,batched_parts",
                     help="comma-separated workloads recorded beside the headline on one GPU ('' = none)")
     ap.add_argument("--sub-steps", type=int, default=3)
     ap.add_argument("--sub-tile", type=int, default=128)
@@ -487,39 +487,8 @@ def main():
     cyc_achieved = cyc_bytes * cycles / (t_split * 1e-3) / 1e9
 
     # ---- end to end through the C-ABI with host buffers ----
-    # per step: upload the initial X, D, V, VR from pinned host buffers, run all
-    # cycles, download X, D, V, VR into separate pinned host buffers
-    import ctypes as C
-    dptr = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
-    pinned = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float64)).pin_memory().numpy()
-    host_in, host_out = [], []
-    for p in deck["parts"]:
-        n = p["x"].shape[0]
-        host_in.append({"x": pinned(p["x"]), "d": pinned(np.zeros((n, 3))), "v": pinned(p["v"]),
-                        "vr": pinned(p["vr"])})
-        host_out.append({k: pinned(np.zeros((n, 3))) for k in ("x", "d", "v", "vr")})
-    h2d = sum(sum(a.nbytes for a in hb.values()) for hb in host_in)
-    d2h = sum(sum(a.nbytes for a in hb.values()) for hb in host_out)
-    e2e_t = []
-    for k in range(args.warmup + max(2, args.steps // 2)):
-        hs.reset()
-        flush.fill_(float(k))
-        torch.cuda.synchronize()
-        barrier()
-        t0 = time.perf_counter()
-        for pi, hb in enumerate(host_in):
-            hs._call("set_nodes", pi, *(dptr(hb[q]) for q in ("x", "d", "v", "vr")))
-        hs.step(cycles)
-        for pi, hb in enumerate(host_out):
-            hs._call("get_nodes", pi, *(dptr(hb[q]) for q in ("x", "d", "v", "vr")))
-        t1 = time.perf_counter()
-        if k >= args.warmup:
-            e2e_t.append(t1 - t0)
-    d_split = out_split["D"]
-    d_e2e = np.concatenate([hb["d"].ravel() for hb in host_out])
-    e2e_same = bool(np.array_equal(d_e2e, d_split))
-    (te,) = max_over_ranks(sum(e2e_t) / len(e2e_t))
-    e2e_value = nel_job * cycles / te
+    e2e_value, h2d, d2h, e2e_same = e2e_rate(hs, deck, cycles, args.warmup, max(2, args.steps // 2), flush, barrier,
+                                             max_over_ranks, out_split["D"], nel_job)
     hs.close()
 
     # ---- C5: the adjoint on the sensitivity plate (FP64), next to its forward ----
@@ -531,7 +500,8 @@ def main():
     subs = {}
     if world == 1:
         for name in [w for w in args.sub_workloads.split(",") if w and w != args.workload]:
-            subs[name] = sub_record(name, local, args.sub_steps, args.sub_tile, timed_runs, flush)
+            subs[name] = sub_record(name, local, args.sub_steps, args.sub_tile, timed_runs, flush, barrier,
+                                    max_over_ranks)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -575,7 +545,45 @@ def main():
         dist.destroy_process_group()
 
 
-def sub_record(name, local, steps, tile, timed_runs, flush):
+def e2e_rate(hs, deck, cycles, nwarm, nsteps, flush, barrier, max_over_ranks, d_ref, nel_job):
+    """The metric end to end through the C-ABI with host buffers: per step, upload
+    the initial X, D, V, VR from pinned host buffers, run all cycles, download X, D,
+    V, VR into separate pinned host buffers.  Returns (rate, h2d bytes, d2h bytes,
+    whether the downloaded D equals the device run's)."""
+    import ctypes as C
+    import torch
+    dptr = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    pinned = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float64)).pin_memory().numpy()
+    host_in, host_out = [], []
+    for p in deck["parts"]:
+        n = p["x"].shape[0]
+        host_in.append({"x": pinned(p["x"]), "d": pinned(np.zeros((n, 3))), "v": pinned(p["v"]),
+                        "vr": pinned(p["vr"])})
+        host_out.append({k: pinned(np.zeros((n, 3))) for k in ("x", "d", "v", "vr")})
+    h2d = sum(sum(a.nbytes for a in hb.values()) for hb in host_in)
+    d2h = sum(sum(a.nbytes for a in hb.values()) for hb in host_out)
+    e2e_t = []
+    for k in range(nwarm + nsteps):
+        hs.reset()
+        flush.fill_(float(k))
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        for pi, hb in enumerate(host_in):
+            hs._call("set_nodes", pi, *(dptr(hb[q]) for q in ("x", "d", "v", "vr")))
+        hs.step(cycles)
+        for pi, hb in enumerate(host_out):
+            hs._call("get_nodes", pi, *(dptr(hb[q]) for q in ("x", "d", "v", "vr")))
+        t1 = time.perf_counter()
+        if k >= nwarm:
+            e2e_t.append(t1 - t0)
+    d_e2e = np.concatenate([hb["d"].ravel() for hb in host_out])
+    same = bool(np.array_equal(d_e2e, d_ref))
+    (te,) = max_over_ranks(sum(e2e_t) / len(e2e_t))
+    return nel_job * cycles / te, h2d, d2h, same
+
+
+def sub_record(name, local, steps, tile, timed_runs, flush, barrier, max_over_ranks):
     """Split and FP64 rates, per-kernel roofline and split error per output of a
     further workload on this GPU (fixed tile, a few steps, L2 flushed between)."""
     from openradioss_b200 import abi, decks
@@ -594,6 +602,7 @@ def sub_record(name, local, steps, tile, timed_runs, flush):
     out_d = outputs(hd)
     hd.close()
     t_s, t_d = sum(ms_s) / len(ms_s), sum(ms_d) / len(ms_d)
+    e2e_value, h2d, d2h, same = e2e_rate(hs, deck, cycles, 1, 2, flush, barrier, max_over_ranks, out_s["D"], nel)
     roof, per_kernel, cyc_bytes, peak = kernel_roofline(hs, deck, cycles, name)
     hs.close()
     return {"config": workload_config(name, deck, cycles, 1, False), "steps": steps, "warmup": 3,
@@ -605,6 +614,8 @@ def sub_record(name, local, steps, tile, timed_runs, flush):
             "cycle_roofline": {"algorithmic_bytes_per_cycle": cyc_bytes, "bytes_per_element_update": cyc_bytes / nel,
                                "achieved": cyc_bytes * cycles / (t_s * 1e-3) / 1e9,
                                "frac": cyc_bytes * cycles / (t_s * 1e-3) / 1e9 / peak, "kernels": per_kernel},
+            "e2e": {"value": e2e_value, "unit": "element-updates/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "same_result_as_device_run": same},
             "clocks": clocks, "gpu_launches": launches}
 
 

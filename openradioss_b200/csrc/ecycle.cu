@@ -373,8 +373,8 @@ struct Impl {
   DBuf<double> sehour, swpla;
   DBuf<float> zw;
   int maxnpt = 1;
-  int uniform_npt = 0;       // 5 when every shell group has 5 points and IHBE 1 (the kernels specialised
-                             // for that form), else 0 (the general kernels)
+  int uniform_npt = 0;       // 5 when every shell group has 5 points, IHBE 1 and IPLA 0 (the kernels
+                             // specialised for that form), else 0 (the general kernels)
   // domain decomposition: halo nodes of this rank's part
   DBuf<int> halo_slot, halo_node; DBuf<unsigned char> halo_ke;
   int nhalo = -1;            // -1: no halo set
@@ -1028,7 +1028,7 @@ int finalize_impl(or_ecycle* h) {
     }
     m.uniform_npt = h->shell[0].prop.npt == 5 ? 5 : 0;
     for (auto& g : h->shell)
-      if (g.prop.npt != 5 || shell_ihbe(g.prop.ishell, g.prop.npt) != 1) m.uniform_npt = 0;
+      if (g.prop.npt != 5 || shell_ihbe(g.prop.ishell, g.prop.npt) != 1 || g.prop.ipla != 0) m.uniform_npt = 0;
     std::vector<uint2> conn(np, make_uint2(0, 0));
     std::vector<int> elem(np, 0), degen(np, 0);
     std::vector<R> thke(np, R(1)), jca(any_jca ? np : 0, R(0));

@@ -1064,9 +1064,10 @@ __device__ __forceinline__ void shell_element(const ShellArgs<R>& a, const int e
     RXl[k] = E1X * rx + E1Y * ry + E1Z * rz;
     RYl[k] = E2X * rx + E2Y * ry + E2Z * rz;
   }
-  // NPT = 5 kernels are launched only when every group is Ishell 1 (IHBE 1): the
-  // other branches compile out of them
+  // NPT = 5 kernels are launched only when every group is Ishell 1 (IHBE 1) with
+  // M2CPLR's radial return (IPLA 0): the other branches compile out of them
   const int IHBE = NPT == 5 ? 1 : gd.ihbe;
+  const int IPLA = NPT == 5 ? 0 : gd.ipla;
   R EXX, EYY, EXY, EXZ, EYZ, KXX, KYY, KXY;
   {
     const R VZ13 = VZl[0] - VZl[2], VZ24 = VZl[1] - VZl[3];
@@ -1193,7 +1194,7 @@ __device__ __forceinline__ void shell_element(const ShellArgs<R>& a, const int e
       R YLD = PLA == R(0) ? CA : CA + CB * exp_(CN * log_(PLA));
       YLD = fmin(YLD, YMAX);
       R DPLA = R(0);
-      if (gd.ipla == 0) {
+      if (IPLA == 0) {
         const R SVM = ssqrt(SN[0] * SN[0] + SN[1] * SN[1] - SN[0] * SN[1] + R(3) * SN[2] * SN[2]);
         const R RR = fmin(R(1), YLD / (SVM + R(EM15)));
         if (RR < R(1)) {
@@ -1205,7 +1206,7 @@ __device__ __forceinline__ void shell_element(const ShellArgs<R>& a, const int e
           else a.pla[ip * nelpad + e] = PLA;
         }
       } else {
-        if (m2cplr_iterative<R>(gd.ipla, SN, PLA, YLD, DPLA, EZZ, CA, CB, CN, YMAX, YM, NU, GG, OFF)) {
+        if (m2cplr_iterative<R>(IPLA, SN, PLA, YLD, DPLA, EZZ, CA, CB, CN, YMAX, YM, NU, GG, OFF)) {
           if (KEEP) st.pla[NPT > 0 ? ip : 0] = PLA;
           else a.pla[ip * nelpad + e] = PLA;
         }
