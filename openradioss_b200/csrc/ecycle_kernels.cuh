@@ -783,17 +783,23 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
     const R s1 = (SG[0] - QNEW) * VOLN, s2 = (SG[1] - QNEW) * VOLN, s3 = (SG[2] - QNEW) * VOLN;
     const R s4 = SG[3] * VOLN, s5 = SG[4] * VOLN, s6 = SG[5] * VOLN;
     constexpr int h4[8] = {1, -1, 1, -1, -1, 1, -1, 1};
-    // one corner at a time, straight to the corner-force planes
+    // corners in the pairs of SFINT3 that share a stress term (1-7, 2-8, 3-5, 4-6),
+    // straight to the corner-force planes
+    constexpr int korder[8] = {0, 6, 1, 7, 2, 4, 3, 5};
+    R f0 = R(0), f1 = R(0), f2 = R(0);
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
+    for (int kk = 0; kk < 8; ++kk) {
+      const int k = korder[kk];
       const R g0 = gvec(0, k), g1 = gvec(1, k), g2 = gvec(2, k);
       R fx = -g0 * HX[0] - g1 * HX[1] - g2 * HX[2] - R(h4[k]) * HX[3];
       R fy = -g0 * HY[0] - g1 * HY[1] - g2 * HY[2] - R(h4[k]) * HY[3];
       R fz = -g0 * HZ[0] - g1 * HZ[1] - g2 * HZ[2] - R(h4[k]) * HZ[3];
-      const int q = pq[k];
-      const R f0 = s1 * PX[q] + s4 * PY[q] + s6 * PZ[q];
-      const R f1 = s2 * PY[q] + s4 * PX[q] + s5 * PZ[q];
-      const R f2 = s3 * PZ[q] + s6 * PX[q] + s5 * PY[q];
+      if ((kk & 1) == 0) {                  // the pair's first corner: its stress term
+        const int q = pq[k];
+        f0 = s1 * PX[q] + s4 * PY[q] + s6 * PZ[q];
+        f1 = s2 * PY[q] + s4 * PX[q] + s5 * PZ[q];
+        f2 = s3 * PZ[q] + s6 * PX[q] + s5 * PY[q];
+      }
       if (k < 4) { fx -= f0; fy -= f1; fz -= f2; }
       else { fx += f0; fy += f1; fz += f2; }
       if (corot) {        // SRROTA3 with R transposed (sforc3.F:1603-1614): back to global axes
