@@ -1587,13 +1587,14 @@ __device__ __forceinline__ void cycle_dt(const PartAcc& ac, const PartTime& t0, 
 // (RLINK10, then BCS10 again), the kinetic energy at mid-step, VELOCITY and DEPLA
 // (FP64 accumulation) of one node, translations and (rot) rotations, from its
 // summed force (ax, ay, az) and moment (rx, ry, rz).  Shared by the node pass and
-// the persistent kernel, so that both produce the same bits.
+// the persistent kernel, so that both produce the same bits.  want_ek = false
+// skips the kinetic energies (a cycle whose energies nobody reads).
 template <class R>
 __device__ __forceinline__ void node_update(const NodeArgs<R>& a, const int n, const unsigned char code, const bool rot,
                                             R ax, R ay, R az, R rx, R ry, R rz, const R ms, const double DT1,
                                             const double DT2, const double DT12, double& px, double& py, double& pz,
                                             double& qx, double& qy, double& qz, typename Vec4<R>::T& v,
-                                            typename Vec4<R>::T& w, double& ek, double& ekr) {
+                                            typename Vec4<R>::T& w, double& ek, double& ekr, const bool want_ek = true) {
   // ACCELE (accele.F:63-80)
   if (ms > R(0)) { const R r = R(1) / ms; ax *= r; ay *= r; az *= r; }
   else { ax = ay = az = R(0); }
@@ -1623,7 +1624,7 @@ __device__ __forceinline__ void node_update(const NodeArgs<R>& a, const int n, c
     }
   }
   const double dt05 = 0.5 * DT1;
-  {
+  if (want_ek) {
     const double wx = (double)v.x + dt05 * (double)ax, wy = (double)v.y + dt05 * (double)ay,
                  wz = (double)v.z + dt05 * (double)az;
     ek = (wx * wx + wy * wy + wz * wz) * 0.5 * (double)ms;
@@ -1661,9 +1662,11 @@ __device__ __forceinline__ void node_update(const NodeArgs<R>& a, const int n, c
         if (code & 8)  rz = R(0);
       }
     }
-    const double wx = (double)w.x + dt05 * (double)rx, wy = (double)w.y + dt05 * (double)ry,
-                 wz = (double)w.z + dt05 * (double)rz;
-    ekr = (wx * wx + wy * wy + wz * wz) * 0.5 * (double)in;
+    if (want_ek) {
+      const double wx = (double)w.x + dt05 * (double)rx, wy = (double)w.y + dt05 * (double)ry,
+                   wz = (double)w.z + dt05 * (double)rz;
+      ekr = (wx * wx + wy * wy + wz * wz) * 0.5 * (double)in;
+    }
     w.x = w.x + dt12 * rx; w.y = w.y + dt12 * ry; w.z = w.z + dt12 * rz;
   }
 }

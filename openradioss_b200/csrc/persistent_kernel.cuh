@@ -362,7 +362,7 @@ shell_persistent_kernel(ShellArgs<R> a, NodeArgs<R> na, PersistArgs pa, int ncyc
       R4 w = mk4(sv[3 * NC + i], sv[4 * NC + i], sv[5 * NC + i], sin_[i]);
       double ek = 0.0, ekr = 0.0;
       node_update<R>(na, g, scode[i], true, ax, ay, az, rx, ry, rz, sms[i], DTc1, DT2, DT12, px, py, pz, qx, qy, qz,
-                     v, w, ek, ekr);
+                     v, w, ek, ekr, last);        // only the launch's last cycle reports kinetic energy
       sx[i] = px; sy[i] = py; sz[i] = pz; sdx[i] = qx; sdy[i] = qy; sdz[i] = qz;
       sv[0 * NC + i] = v.x; sv[1 * NC + i] = v.y; sv[2 * NC + i] = v.z;
       sv[3 * NC + i] = w.x; sv[4 * NC + i] = w.y; sv[5 * NC + i] = w.z;
