@@ -1220,7 +1220,7 @@ __device__ __forceinline__ void shell_element(const ShellArgs<R>& a, const int e
       SIGY = SIGY + YLD / R(npt);
       EZZ = -(DXX + DYY) * NU - (R(1) - R(2) * NU) * EZZ;   // sigeps02c.F:215-224
       EZZ = EZZ / (R(1) - NU);
-      wpla += (double)YLD * (double)DPLA * (double)AREA * (double)THKLYL;
+      if (DPLA != R(0)) wpla += (double)YLD * (double)DPLA * (double)AREA * (double)THKLYL;
     }
     THKN = THKN + EZZ * THKLYL * OFF;
     if (KEEP) {
@@ -1428,12 +1428,13 @@ __device__ __forceinline__ void shell_element(const ShellArgs<R>& a, const int e
       Mg[2][k] = E1Z * G1m[k] + E2Z * G2m[k];
     }
   }
-  // ---- uniform pressure (load_pressure.F:201-207): F = -p N / 8, N = x13 x x24 ----
+  // ---- uniform pressure (load_pressure.F:201-207): F = -p N / 8, N = x13 x x24,
+  // the diagonals taken in FP64 and the cross product in R ----
   R PF[3] = {R(0), R(0), R(0)};
   if (gd.pressure != 0.0) {
-    const double ax = sx[lc[2]] - x1, ay = sy[lc[2]] - y1, az = sz[lc[2]] - z1;
-    const double bx = sx[lc[3]] - sx[lc[1]], by = sy[lc[3]] - sy[lc[1]], bz = sz[lc[3]] - sz[lc[1]];
-    const R NX = R(ay * bz - az * by), NY = R(az * bx - ax * bz), NZ = R(ax * by - ay * bx);
+    const R ax = R(sx[lc[2]] - x1), ay = R(sy[lc[2]] - y1), az = R(sz[lc[2]] - z1);
+    const R bx = R(sx[lc[3]] - sx[lc[1]]), by = R(sy[lc[3]] - sy[lc[1]]), bz = R(sz[lc[3]] - sz[lc[1]]);
+    const R NX = ay * bz - az * by, NY = az * bx - ax * bz, NZ = ax * by - ay * bx;
     const R AA = -R(gd.pressure) * R(0.125);
     PF[0] = AA * NX; PF[1] = AA * NY; PF[2] = AA * NZ;
   }

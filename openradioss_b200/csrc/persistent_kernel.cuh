@@ -97,6 +97,13 @@ __device__ __forceinline__ bool grid_barrier(unsigned* sync, unsigned target, Er
   return *s_abort != 0;
 }
 
+// pairs of reals for the corner-force planes of the persistent kernel
+template <class R> struct Vec2;
+template <> struct Vec2<float> { typedef float2 T; };
+template <> struct Vec2<double> { typedef double2 T; };
+__device__ __forceinline__ float2 mk2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ double2 mk2(double a, double b) { return make_double2(a, b); }
+
 // minimum of a 64-bit unsigned value over the warp, from two 32-bit hardware
 // reductions (high words, then the low words of the lanes holding the high minimum)
 __device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v) {
@@ -270,13 +277,14 @@ shell_persistent_kernel(ShellArgs<R> a, NodeArgs<R> na, PersistArgs pa, int ncyc
       if (!KEEP) shell_load_state<R, NPT>(a, e, st);
       shell_element<R, NPT, KEEP>(a, e, gd, DT1, zw, sx, sy, sz, sv, NC, lc, st, Fg, Mg, mykey, mybits, my_ehou,
                                   my_wpla);
+      // corner forces and moments as three planes of pairs (fx fy | fz mx | my mz),
+      // corner k of element lt at k * TILE + lt
+      typename Vec2<R>::T* sc2 = reinterpret_cast<typename Vec2<R>::T*>(sc);
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {
-          sc[(q * 4 + k) * TILE + lt] = Fg[q][k];
-          sc[((q + 3) * 4 + k) * TILE + lt] = Mg[q][k];
-        }
+        sc2[(0 * 4 + k) * TILE + lt] = mk2(Fg[0][k], Fg[1][k]);
+        sc2[(1 * 4 + k) * TILE + lt] = mk2(Fg[2][k], Mg[0][k]);
+        sc2[(2 * 4 + k) * TILE + lt] = mk2(Mg[1][k], Mg[2][k]);
       }
       cum_ehou_t += my_ehou;
       cum_wpla_t += my_wpla;
@@ -295,12 +303,14 @@ shell_persistent_kernel(ShellArgs<R> a, NodeArgs<R> na, PersistArgs pa, int ncyc
     for (int j = lt; j < nl; j += TILE) {
       R f0 = R(0), f1 = R(0), f2 = R(0), m0 = R(0), m1 = R(0), m2 = R(0);
       const int i1 = sinc[j + 1];
+      const typename Vec2<R>::T* sc2 = reinterpret_cast<const typename Vec2<R>::T*>(sc);
 #pragma unroll 4
       for (int i = sinc[j]; i < i1; ++i) {
         const int q = sinc[NLM + 1 + i];
         const int o = (q & 3) * TILE + (q >> 2);
-        f0 += sc[o]; f1 += sc[4 * TILE + o]; f2 += sc[8 * TILE + o];
-        m0 += sc[12 * TILE + o]; m1 += sc[16 * TILE + o]; m2 += sc[20 * TILE + o];
+        const typename Vec2<R>::T p0 = sc2[o], p1 = sc2[4 * TILE + o], p2 = sc2[8 * TILE + o];
+        f0 += p0.x; f1 += p0.y; f2 += p1.x;
+        m0 += p1.y; m1 += p2.x; m2 += p2.y;
       }
       const int s = sslot[j];
       st_cg(&fslot[s], mk4(f0, f1, f2, R(0)));

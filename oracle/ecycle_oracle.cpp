@@ -1163,14 +1163,17 @@ int shell_element(const Model<R>& m, ShellGroup<R>& g, PartData<R>& P, int i, do
     }
   }
   // /PLOAD-style uniform pressure (load_pressure.F:201-207): F = -p N/8 per node,
-  // N = (x3-x1) x (x4-x2) from the current coordinates, added to the corner slot.
+  // N = (x3-x1) x (x4-x2) from the current coordinates, added to the corner slot;
+  // the diagonals in FP64 (my_real X differences in the FP64 form), the cross
+  // product in my_real.
   R PF[3] = {0, 0, 0};
   if (pr.pressure != 0.0) {
     double ax = XG[2] - XG[0], ay = YG[2] - YG[0], az = ZG[2] - ZG[0];
     double bx = XG[3] - XG[1], by = YG[3] - YG[1], bz = ZG[3] - ZG[1];
     if (!split) { ax = P.x[3*nc[2]] - P.x[3*nc[0]]; ay = P.x[3*nc[2]+1] - P.x[3*nc[0]+1]; az = P.x[3*nc[2]+2] - P.x[3*nc[0]+2];
                   bx = P.x[3*nc[3]] - P.x[3*nc[1]]; by = P.x[3*nc[3]+1] - P.x[3*nc[1]+1]; bz = P.x[3*nc[3]+2] - P.x[3*nc[1]+2]; }
-    R NX = R(ay * bz - az * by), NY = R(az * bx - ax * bz), NZ = R(ax * by - ay * bx);
+    const R Ax = R(ax), Ay = R(ay), Az = R(az), Bx = R(bx), By = R(by), Bz = R(bz);
+    R NX = Ay * Bz - Az * By, NY = Az * Bx - Ax * Bz, NZ = Ax * By - Ay * Bx;
     R AA = -R(pr.pressure) * R(0.125);
     PF[0] = AA * NX; PF[1] = AA * NY; PF[2] = AA * NZ;
   }
