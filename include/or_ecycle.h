@@ -49,7 +49,8 @@ extern "C" {
 #define OR_E_NEGVOL         4   /* zero/negative volume (SCHKJABT3, MSGID 166)    */
 #define OR_E_DTMIN          5   /* element time step <= DTMIN (MQVISCB/CDT3)     */
 #define OR_E_NAN            6   /* NaN/Inf in nodal acceleration                 */
-#define OR_E_TIMEOUT        7   /* bounded host wait expired                     */
+#define OR_E_TIMEOUT        7   /* a bounded wait expired: the host's wait for a
+                                   step, or a grid barrier of the persistent cycle */
 #define OR_E_UNSUPPORTED    8   /* option outside the implemented path           */
 #define OR_E_NOMEM          9   /* device allocation failed                      */
 

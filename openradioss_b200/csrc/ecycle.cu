@@ -396,6 +396,7 @@ struct Impl {
   struct Persist {
     bool on = false;
     int G = 0, P = 0, ncmax = 0;
+    int stall_cta = -1;        // test hook, OR_ECYCLE_TEST_STALL_CTA
     size_t smem = 0;
     DBuf<int> node_ofs, node_glob; DBuf<unsigned char> owner; DBuf<uint2> pconn;
     DBuf<R4> fslot2, mslot2; DBuf<PartAcc> acc3; DBuf<double> ek, ekr; DBuf<unsigned> sync;
@@ -462,6 +463,7 @@ struct Impl {
     a.fslot2 = per.fslot2.p; a.mslot2 = per.mslot2.p; a.acc3 = per.acc3.p; a.ek_node = per.ek.p;
     a.ekr_node = per.ekr.p; a.sync = per.sync.p; a.patches_per_cta = per.P; a.ncmax = per.ncmax;
     a.ntiles_node = ntiles;
+    a.stall_cta = per.stall_cta;
     return a;
   }
 };
@@ -684,6 +686,8 @@ int persist_build(or_ecycle* h, Impl<R>& m) {
       (rc = dput(h, q.ek, std::vector<double>(m.nnodpad, 0.0))) ||
       (rc = dput(h, q.ekr, std::vector<double>(m.nnodpad, 0.0))))
     return rc;
+  q.stall_cta = -1;
+  if (const char* st = std::getenv("OR_ECYCLE_TEST_STALL_CTA")) q.stall_cta = std::atoi(st);
   q.on = true;
   q.G = G; q.P = P; q.ncmax = ncmax; q.smem = smem;
   return OR_OK;

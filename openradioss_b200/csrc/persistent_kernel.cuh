@@ -48,6 +48,8 @@ struct PersistArgs {
   int patches_per_cta;        // P
   int ncmax;                  // node capacity of a CTA (stride of the shared planes)
   int ntiles_node;            // node tiles of NODE tile size 128 (kinetic energy partials)
+  int stall_cta;              // test hook (OR_ECYCLE_TEST_STALL_CTA): this CTA does not arrive at the
+                              // first cycle's barrier, so the others' bounded waits run out; -1 off
 };
 
 // L2-coherent loads and stores (bypassing L1) of the data other SMs write during
@@ -71,11 +73,12 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
-__device__ __forceinline__ bool grid_barrier(unsigned* sync, unsigned target, ErrorWord* err, int* s_abort) {
+__device__ __forceinline__ bool grid_barrier(unsigned* sync, unsigned target, ErrorWord* err, int* s_abort,
+                                             bool arrive = true) {
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();                          // release: this CTA's slot writes and reductions
-    atomicAdd(&sync[0], 1u);
+    if (arrive) atomicAdd(&sync[0], 1u);
     const long long t0 = clock64();
     int ab = 0;
     for (;;) {
@@ -316,7 +319,8 @@ shell_persistent_kernel(ShellArgs<R> a, NodeArgs<R> na, PersistArgs pa, int ncyc
       st_cg(&fslot[s], mk4(f0, f1, f2, R(0)));
       st_cg(&mslot[s], mk4(m0, m1, m2, R(0)));
     }
-    if (grid_barrier(pa.sync, (unsigned)(c + 1) * (unsigned)G, a.err, &s_abort)) return;
+    if (grid_barrier(pa.sync, (unsigned)(c + 1) * (unsigned)G, a.err, &s_abort, !(c == 0 && cta == pa.stall_cta)))
+      return;
     // ---------------- node phase ----------------
     // A thread's nodes are i0 = tid + 2 j blockDim.x and i0 + blockDim.x.  The first
     // two slots of both are loaded before either is summed, and for the first pair

@@ -7,6 +7,10 @@ checks itself, never by a GPU fault.
   non-finite acceleration it produces and names the node;
 * OR_E_TIMEOUT: the host's bounded wait given a limit far below the run's
   length; the cycles finish on the GPU, the handle is then destroyed cleanly;
+  and the persistent cycle's grid barrier, with one CTA held back from the first
+  barrier by the OR_ECYCLE_TEST_STALL_CTA hook: the others give up after about a
+  second, set the abort flag and return, the step reports OR_E_TIMEOUT, and the
+  handle runs again after a reset;
 * upload rejections: node numbers outside the part in IXS / IXC, non-positive
   shell thickness, non-finite coordinates or velocities.
 """
@@ -102,6 +106,30 @@ def test_bounded_wait_expires_then_handle_closes(lib):
     h = ECycle(d, precision=abi.OR_PREC_SPLIT)
     h.step(64)
     assert np.isfinite(h.get_nodes()["d"]).all()
+
+
+def test_persistent_barrier_wait_expires(lib, monkeypatch):
+    import torch
+    from openradioss_b200.ecycle import ECycle, ECycleError
+    d = decks.c2_shell_plate(n=40, size=0.04)
+    monkeypatch.setenv("OR_ECYCLE_TEST_STALL_CTA", "3")
+    g = ECycle(d, precision=abi.OR_PREC_SPLIT)
+    monkeypatch.delenv("OR_ECYCLE_TEST_STALL_CTA")
+    on, ctas, _ = g.persistent_info()
+    assert on and ctas > 3
+    with pytest.raises(ECycleError) as ei:
+        g.step(8)
+    assert ei.value.code == abi.OR_E_TIMEOUT
+    code, idx = g.error_info()
+    assert code == abi.OR_E_TIMEOUT and 0 <= idx < ctas
+    torch.cuda.synchronize()                    # the kernel returned; the context is usable
+    g.close()
+    h = ECycle(d, precision=abi.OR_PREC_SPLIT)
+    r = ECycle(d, precision=abi.OR_PREC_SPLIT, persistent=-1)
+    h.step(8)
+    r.step(8)
+    assert h.persistent_info()[0]
+    assert np.abs(h.get_nodes()["d"] - r.get_nodes()["d"]).max() <= 1e-5 * np.abs(r.get_nodes()["d"]).max()
 
 
 def _expect_arg_error(deck):
