@@ -70,6 +70,8 @@ def parse():
     ap.add_argument("--persistent-cycles", type=int, default=0,
                     help="profiling mode: three step() calls of this many cycles through the persistent shell "
                          "cycle, timed with events")
+    ap.add_argument("--adjoint-cycles", type=int, default=0,
+                    help="profiling mode: one or_ecycle_adjoint over this many cycles of the C5 plate (FP64)")
     ap.add_argument("--mesh-n", type=int, default=0, help="profiling mode: mesh size parameter (0 = workload's)")
     ap.add_argument("--tile", type=int, default=0, help="profiling mode: elements per patch (0 = library default)")
     ap.add_argument("--precision", default="split", choices=["split", "fp64"], help="profiling mode")
@@ -391,6 +393,13 @@ def main():
         return eager_profile(args)
     if args.persistent_cycles:
         return persistent_profile(args)
+    if args.adjoint_cycles:
+        import torch
+        from openradioss_b200 import build
+        build.build()
+        torch.cuda.set_device(0)
+        print(json.dumps(adjoint_timing(0, ncycles=args.adjoint_cycles, reps=1)))
+        return None
 
     import torch
     import torch.distributed as dist
