@@ -350,56 +350,37 @@ shell_persistent_kernel(ShellArgs<R> a, NodeArgs<R> na, PersistArgs pa, int ncyc
     const bool last = c == ncycles - 1;
     for (int i0 = tid; i0 < nn; i0 += 2 * blockDim.x) {
     if (i0 != tid) prefetch(i0);
-    // both nodes' inputs first, then both updates (independent register work the
-    // compiler can interleave), then both write-backs
-    double px[2], py[2], pz[2], qx[2], qy[2], qz[2], ek[2] = {0.0, 0.0}, ekr[2] = {0.0, 0.0};
-    R4 v[2], w[2];
-    R ax[2], ay[2], az[2], rx[2], ry[2], rz[2], msn[2];
-    unsigned char cd[2];
-    int gn[2];
-    bool ok[2];
 #pragma unroll
     for (int u = 0; u < 2; ++u) {
       const int i = i0 + u * blockDim.x;
-      ok[u] = i < nn;
-      const int ii = ok[u] ? i : i0;
-      gn[u] = sglob[ii];
+      if (i >= nn) break;
+      const int g = sglob[i];
       const int k0 = rg[u].x, k1 = rg[u].y;
-      ax[u] = ay[u] = az[u] = rx[u] = ry[u] = rz[u] = R(0);
+      R ax = R(0), ay = R(0), az = R(0), rx = R(0), ry = R(0), rz = R(0);
       if (k1 > k0) {
-        ax[u] = F0[u].x; ay[u] = F0[u].y; az[u] = F0[u].z;
-        rx[u] = M0[u].x; ry[u] = M0[u].y; rz[u] = M0[u].z;
+        ax = F0[u].x; ay = F0[u].y; az = F0[u].z;
+        rx = M0[u].x; ry = M0[u].y; rz = M0[u].z;
       }
       if (k1 > k0 + 1) {
-        ax[u] += F1[u].x; ay[u] += F1[u].y; az[u] += F1[u].z;
-        rx[u] += M1[u].x; ry[u] += M1[u].y; rz[u] += M1[u].z;
+        ax += F1[u].x; ay += F1[u].y; az += F1[u].z;
+        rx += M1[u].x; ry += M1[u].y; rz += M1[u].z;
       }
       for (int k = k0 + 2; k < k1; ++k) {
         const R4 f = ld_cg(&fslot[k]);
-        ax[u] += f.x; ay[u] += f.y; az[u] += f.z;
+        ax += f.x; ay += f.y; az += f.z;
         const R4 m = ld_cg(&mslot[k]);
-        rx[u] += m.x; ry[u] += m.y; rz[u] += m.z;
+        rx += m.x; ry += m.y; rz += m.z;
       }
-      px[u] = sx[ii]; py[u] = sy[ii]; pz[u] = sz[ii]; qx[u] = sdx[ii]; qy[u] = sdy[ii]; qz[u] = sdz[ii];
-      v[u] = mk4(sv[0 * NC + ii], sv[1 * NC + ii], sv[2 * NC + ii], R(0));
-      w[u] = mk4(sv[3 * NC + ii], sv[4 * NC + ii], sv[5 * NC + ii], sin_[ii]);
-      cd[u] = scode[ii];
-      msn[u] = sms[ii];
-    }
-#pragma unroll
-    for (int u = 0; u < 2; ++u) {
-      if (ok[u])        // only the launch's last cycle reports kinetic energy
-        node_update<R>(na, gn[u], cd[u], true, ax[u], ay[u], az[u], rx[u], ry[u], rz[u], msn[u], DTc1, DT2, DT12,
-                       px[u], py[u], pz[u], qx[u], qy[u], qz[u], v[u], w[u], ek[u], ekr[u], last);
-    }
-#pragma unroll
-    for (int u = 0; u < 2; ++u) {
-      if (!ok[u]) continue;
-      const int i = i0 + u * blockDim.x;
-      sx[i] = px[u]; sy[i] = py[u]; sz[i] = pz[u]; sdx[i] = qx[u]; sdy[i] = qy[u]; sdz[i] = qz[u];
-      sv[0 * NC + i] = v[u].x; sv[1 * NC + i] = v[u].y; sv[2 * NC + i] = v[u].z;
-      sv[3 * NC + i] = w[u].x; sv[4 * NC + i] = w[u].y; sv[5 * NC + i] = w[u].z;
-      if (last && sown[i]) { pa.ek_node[gn[u]] = ek[u]; pa.ekr_node[gn[u]] = ekr[u]; }
+      double px = sx[i], py = sy[i], pz = sz[i], qx = sdx[i], qy = sdy[i], qz = sdz[i];
+      R4 v = mk4(sv[0 * NC + i], sv[1 * NC + i], sv[2 * NC + i], R(0));
+      R4 w = mk4(sv[3 * NC + i], sv[4 * NC + i], sv[5 * NC + i], sin_[i]);
+      double ek = 0.0, ekr = 0.0;
+      node_update<R>(na, g, scode[i], true, ax, ay, az, rx, ry, rz, sms[i], DTc1, DT2, DT12, px, py, pz, qx, qy, qz,
+                     v, w, ek, ekr, last);        // only the launch's last cycle reports kinetic energy
+      sx[i] = px; sy[i] = py; sz[i] = pz; sdx[i] = qx; sdy[i] = qy; sdz[i] = qz;
+      sv[0 * NC + i] = v.x; sv[1 * NC + i] = v.y; sv[2 * NC + i] = v.z;
+      sv[3 * NC + i] = w.x; sv[4 * NC + i] = w.y; sv[5 * NC + i] = w.z;
+      if (last && sown[i]) { pa.ek_node[g] = ek; pa.ekr_node[g] = ekr; }
     }
     }
     if (cta == 0 && tid == 0) {            // reuse in two cycles: everyone has read it
