@@ -304,7 +304,7 @@ int build_patches(or_ecycle* h, std::vector<GroupT>& groups, int tile, PatchSet&
 // in ascending order.  The kernels sum a node's corner forces in this order.
 int incidence_stride(const PatchSet& ps, int K, int tile) {
   const int s = ps.nlmax + 1 + K * tile;
-  return s + (s & 1);
+  return (s + 7) & ~7;   // 16-byte rows: the hexa kernel stages them by bulk copy
 }
 void incidence_lists(const PatchSet& ps, int K, int tile, std::vector<uint16_t>& inc) {
   const size_t np = ps.info.size(), S = (size_t)incidence_stride(ps, K, tile), L = (size_t)ps.nlmax;
@@ -468,11 +468,12 @@ struct Impl {
   }
 };
 
-// dynamic shared memory of a patch kernel: node planes (x, y, z in FP64; velocities
-// in R), 24 planes of TILE corner forces, the incidence lists
+// dynamic shared memory of a patch kernel.  Hexa: the layout of hex_smem_bytes.
+// Shell: node planes (x, y, z in FP64; velocities and rotational velocities in R),
+// 24 planes of TILE corner forces, the incidence lists.
 template <class R>
 size_t hex_smem(int nl, int tile, int inc_stride) {
-  return (size_t)nl * (3 * sizeof(double) + 3 * sizeof(R)) + 24 * (size_t)tile * sizeof(R) + 2 * (size_t)inc_stride;
+  return hex_smem_bytes<R>(nl, tile, inc_stride);
 }
 template <class R>
 size_t shell_smem(int nl, int tile, int inc_stride) {

@@ -347,12 +347,12 @@ __device__ inline void block_reduce(unsigned long long& key, unsigned long long&
 // ===========================================================================
 // Resident 128-thread CTAs per SM each patch kernel is compiled for (the
 // minimum-blocks argument of __launch_bounds__, scaled to the tile).  The
-// kernels are issue/latency-bound with ~170-255 live registers unbounded, so
-// more resident warps pay for the spilled registers (which stay in L1); the
-// defaults are the fastest caps of a sweep on B200: hexa FP32 6 CTAs (80
-// registers), shell FP32 3 (168), hexa FP64 4 (128), shell FP64 3 (168).
+// kernels are issue/latency-bound, so more resident warps pay for a few spilled
+// registers (which stay in L1); the defaults are the fastest caps of a sweep on
+// B200: hexa FP32 7 CTAs (72 registers; C4 hexa pass 200.6 us against 210.8 at 6
+// and 219.5 at 5), shell FP32 3 (168), hexa FP64 4 (128), shell FP64 3 (168).
 #ifndef ORB_HEX_CTAS_F32
-#define ORB_HEX_CTAS_F32 6
+#define ORB_HEX_CTAS_F32 7
 #endif
 #ifndef ORB_SHELL_CTAS_F32
 #define ORB_SHELL_CTAS_F32 3
@@ -384,8 +384,73 @@ __host__ __device__ constexpr int min_blocks(int ctas128, int tile) {
 }
 
 // ===========================================================================
+// asynchronous copies into shared memory
+// ===========================================================================
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+// one-arrival mbarrier of a CTA, made visible to the async proxy
+__device__ __forceinline__ void mbar_init(unsigned long long* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// the arrival, announcing the bytes the bulk copies below will deliver
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// bulk copy (TMA, untiled) of bytes from global to shared memory, completing on bar;
+// both addresses 16-byte aligned, bytes a multiple of 16
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+// waits for phase 0 of bar to complete, at most `tries` polls; false if it did not
+__device__ __forceinline__ bool mbar_wait0(unsigned long long* bar, int tries) {
+  unsigned done = 0;
+  for (int i = 0; i < tries && !done; ++i)
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\tselp.u32 %0, 1, 0, p;\n}"
+                 : "=r"(done) : "r"(smem_u32(bar)) : "memory");
+  return done != 0;
+}
+// element-wise asynchronous copies (no register staging), completed by cp_async_wait_all
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// polls of a CTA's staging mbarrier before it reports OR_E_TIMEOUT; its bulk copies
+// read this GPU's own memory and complete in microseconds
+constexpr int STAGE_WAIT_TRIES = 1 << 22;
+
+// minimum of a 64-bit unsigned value over the warp, from two 32-bit hardware
+// reductions (high words, then the low words of the lanes holding the high minimum)
+__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v) {
+  const unsigned hi = __reduce_min_sync(0xffffffffu, (unsigned)(v >> 32));
+  const unsigned lo = __reduce_min_sync(0xffffffffu, (unsigned)(v >> 32) == hi ? (unsigned)v : 0xffffffffu);
+  return ((unsigned long long)hi << 32) | lo;
+}
+
+// ===========================================================================
 // hexa patch kernel
 // ===========================================================================
+// Shared memory of a hexa patch (R = element precision, NLM = nlmax, TILE elements),
+// in this order, every block 16-byte aligned:
+//   24 corner-force planes of TILE R; planes 0..10 first receive the patch's element
+//      state (sig 1..6, eint, rho, qvis, vol0, pla), each thread reading only its own
+//      entries before it writes its own corners there
+//   conn (uint4) | elem_id (int) | vol0dp (double, split form only)   TILE each
+//   node x, y (double2) | node velocity (R4)                           NLM each
+//   incidence lists (uint16, inc_stride, a multiple of 8)
+//   node z (double)                                                    NLM
+template <class R>
+__host__ __device__ inline size_t hex_smem_bytes(int nl, int tile, int inc_stride) {
+  const bool split = sizeof(R) == 4;
+  return 24 * (size_t)tile * sizeof(R) + (size_t)tile * (16 + 4 + (split ? 8 : 0)) +
+         (size_t)nl * (16 + 4 * sizeof(R) + 8) + 2 * (size_t)inc_stride;
+}
+
 // Per element (thread): SCOOR3, SDERI3, SDLEN3, SDEFO3, SRHO3, SROTA3, MMAIN ->
 // M1LAW / M2LAW -> MQVISCB, SHVIS3, SFINT3; corner forces into shared memory.
 // CORO = 1: groups may use the convected frame (JCVT /= 0, decided per group at
@@ -394,97 +459,110 @@ template <class R, int TILE, int CORO>
 __global__ void __launch_bounds__(TILE, min_blocks(Occupancy<R>::hex, TILE))
 hex_patch_kernel(HexArgs<R> a, int parity) {
   typedef typename Vec4<R>::T R4;
+  constexpr bool split = sizeof(R) == 4;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ unsigned long long s_key[TILE / 32], s_bits[TILE / 32];
   __shared__ double s_s0[TILE / 32], s_s1[TILE / 32];
+  __shared__ __align__(8) unsigned long long s_bar;
   const int p = blockIdx.x;
   const int tid = threadIdx.x;
-  // Patches are padded to TILE elements and their node lists to nlmax entries,
-  // so every address below follows from (p, tid) alone: the per-element loads
-  // and the node gathers are issued without waiting for the patch descriptor.
+  // Patches are padded to TILE elements (element p*TILE + t is thread t's) and their
+  // node lists to nlmax entries, so every address below follows from (p, tid) alone.
   const int NLM = a.nlmax;
+  const int nelpad = a.nelpad;
+  const size_t e0 = (size_t)p * TILE;
   const int e = p * TILE + tid;
-  const PatchInfo pi = a.patch[p];
+  R* sc = reinterpret_cast<R*>(smem_raw);
+  uint4* sconn = reinterpret_cast<uint4*>(sc + 24 * TILE);
+  int* seid = reinterpret_cast<int*>(sconn + TILE);
+  double* svol0dp = reinterpret_cast<double*>(seid + TILE);
+  double2* sxy = reinterpret_cast<double2*>(svol0dp + (split ? TILE : 0));
+  R4* sv = reinterpret_cast<R4*>(sxy + NLM);
+  unsigned short* sinc = reinterpret_cast<unsigned short*>(sv + NLM);
+  double* sz = reinterpret_cast<double*>(sinc + a.inc_stride);
+  // One thread stages the patch's element state, connectivity and incidence lists by
+  // bulk copies.  They were written two launches back or are static, so they are
+  // issued before the wait on the previous kernel (the node pass).
+  if (tid == 0) {
+    mbar_init(&s_bar);
+    const unsigned pl = TILE * sizeof(R);
+    mbar_expect_tx(&s_bar, 11 * pl + TILE * (16 + 4 + (split ? 8 : 0)) + 2 * a.inc_stride);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) bulk_g2s(sc + c * TILE, a.sig + (size_t)c * nelpad + e0, pl, &s_bar);
+    bulk_g2s(sc + 6 * TILE, a.eint + e0, pl, &s_bar);
+    bulk_g2s(sc + 7 * TILE, a.rho + e0, pl, &s_bar);
+    bulk_g2s(sc + 8 * TILE, a.qvis + e0, pl, &s_bar);
+    bulk_g2s(sc + 9 * TILE, a.vol0 + e0, pl, &s_bar);
+    bulk_g2s(sc + 10 * TILE, a.pla + e0, pl, &s_bar);
+    bulk_g2s(sconn, a.conn + e0, TILE * 16, &s_bar);
+    bulk_g2s(seid, a.elem_id + e0, TILE * 4, &s_bar);
+    if (split) bulk_g2s(svol0dp, a.vol0dp + e0, TILE * 8, &s_bar);
+    bulk_g2s(sinc, a.inc + (size_t)p * a.inc_stride, 2 * a.inc_stride, &s_bar);
+  }
   // issued now, used at the end: the patch's slot numbers (up to two per thread)
   // and its cumulative energy partials
+  const PatchInfo pi = a.patch[p];
   const int slot0 = tid < NLM ? a.patch_slots[p * NLM + tid] : -1;
   const int slot1 = tid + TILE < NLM ? a.patch_slots[p * NLM + tid + TILE] : -1;
   double pre_ehour = 0.0, pre_wpla = 0.0;
   if (tid == 0) { pre_ehour = a.blk_ehour[p]; pre_wpla = a.blk_wpla[p]; }
-  // shared layout: planes of NLM x, y, z (double) | vx, vy, vz (R); 24 planes of
-  // TILE corner forces (R), plane (c*8+k) holding component c of corner k; the
-  // patch's incidence lists (uint16)
-  double* sx = reinterpret_cast<double*>(smem_raw);
-  double* sy = sx + NLM;
-  double* sz = sy + NLM;
-  R* svx = reinterpret_cast<R*>(sz + NLM);
-  R* svy = svx + NLM;
-  R* svz = svy + NLM;
-  R* sc = svz + NLM;
-  unsigned short* sinc = reinterpret_cast<unsigned short*>(sc + 24 * TILE);
-  const int nelpad = a.nelpad;
-  // issue every per-element load before the staging barrier so that they are in
-  // flight together with the node gathers
-  uint4 cw = make_uint4(0, 0, 0, 0);
-  R st_sig[6], st_eint = R(0), st_rho = R(1), st_qvis = R(0), st_vol0 = R(1), st_pla = R(0);
-  double st_vol0dp = 1.0;
-  int st_eid = 0;
-  {   // padding elements (tid >= nel) hold valid zero state: load unconditionally
-    cw = a.conn[e];
-#pragma unroll
-    for (int c = 0; c < 6; ++c) st_sig[c] = a.sig[c * nelpad + e];
-    st_eint = a.eint[e];
-    st_rho = a.rho[e];
-    st_qvis = a.qvis[e];
-    st_vol0 = a.vol0[e];
-    if (sizeof(R) == 4) st_vol0dp = a.vol0dp[e];
-    st_pla = a.pla[e];
-    st_eid = a.elem_id[e];
-  }
-  {
-    const unsigned* src = reinterpret_cast<const unsigned*>(a.inc + (size_t)p * a.inc_stride);
-    unsigned* dst = reinterpret_cast<unsigned*>(sinc);
-    for (int i = tid; i < a.inc_stride / 2; i += TILE) dst[i] = src[i];
-  }
-  // X, V and the cycle's time come from the previous node pass (the node numbers
-  // are loaded after the wait: the 80-register budget of the split form has no
-  // room to hold them across it)
+  // X, V and the cycle's time come from the previous node pass: gathered after the
+  // wait, straight into shared memory
   pdl_wait();
   pdl_trigger();
   for (int j = tid; j < NLM; j += TILE) {
     const int g = a.patch_nodes[p * NLM + j];
-    const double4 xx = a.X[g];
-    const R4 vv = a.V[g];
-    sx[j] = xx.x; sy[j] = xx.y; sz[j] = xx.z;
-    svx[j] = vv.x; svy[j] = vv.y; svz[j] = vv.z;
+    const double* xg = reinterpret_cast<const double*>(a.X + g);
+    cp_async16(sxy + j, xg);
+    cp_async8(sz + j, xg + 2);
+    if (split) {
+      cp_async16(sv + j, a.V + g);
+    } else {
+      cp_async16(sv + j, a.V + g);
+      cp_async16(reinterpret_cast<unsigned char*>(sv + j) + 16, reinterpret_cast<const unsigned char*>(a.V + g) + 16);
+    }
   }
-  const HexGroupDesc gd = a.groups[pi.group];
+  // the group constants, read where used (read-only, held in L1) rather than held
+  const HexGroupDesc* __restrict__ gdp = a.groups + pi.group;
   const bool active = tid < pi.nel;
   const int nl = pi.nloc;
   const PartTime& tm = a.time[parity * a.nparts + pi.part];
   const R DT1 = R(tm.dt2);
-  const bool split = sizeof(R) == 4;
-  __syncthreads();
+  cp_async_wait_all();
+  __syncthreads();   // node gathers of every thread landed; the mbarrier is initialised
+  if (!mbar_wait0(&s_bar, STAGE_WAIT_TRIES)) raise_error(a.err, 7, p);
 
-  int lc[8];
-  int color = -1;
   unsigned long long mykey = ~0ull, mybits = ~0ull;
   double my_ehou = 0.0, my_wpla = 0.0;
   if (active) {
-    lc[0] = cw.x & 0xffffu; lc[1] = cw.x >> 16; lc[2] = cw.y & 0xffffu; lc[3] = cw.y >> 16;
-    lc[4] = cw.z & 0xffffu; lc[5] = cw.z >> 16; lc[6] = cw.w & 0xffffu; lc[7] = cw.w >> 16;
-    color = lc[0] >> COLOR_SHIFT;
-    lc[0] &= LOCAL_MASK;
-    // ---- SDERI3 in FP64 (sderi3.F:103-149, 264-298) ----
-    double XD[8], YD[8], ZD[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) { XD[k] = sx[lc[k]]; YD[k] = sy[lc[k]]; ZD[k] = sz[lc[k]]; }
-    // ---- SRCOOR3 (srcoor3.F, JCVT /= 0, ISORTH = 0): convected frame R = [e1 e2 e3] of
-    // SREPISO3 (FP64 differences, r, s, t in R) and SORTHO3 (three symmetric
-    // corrections, then Gram-Schmidt); coordinates (FP64) and velocities in it ----
+    const uint4 cw = sconn[tid];
+    // local node of corner k (the colour bits of corner 0 masked off)
+    auto corner = [&](int k) -> int {
+      const unsigned w = k < 2 ? cw.x : k < 4 ? cw.y : k < 6 ? cw.z : cw.w;
+      const int l = (k & 1) ? (int)(w >> 16) : (int)(w & 0xffffu);
+      return k == 0 ? (l & (int)LOCAL_MASK) : l;
+    };
+    const int st_eid = seid[tid];
+    // ---- SDERI3 in FP64 (sderi3.F:103-149, 264-298): the corner differences of the
+    // pairs 1-7, 2-8, 3-5, 4-6, and the coordinates relative to corner 1 (differences
+    // taken in FP64, then rounded to R: beyond the determinant nothing needs FP64, as in
+    // the reference's -prec=sp build, which forms the inverse Jacobian, the hourglass
+    // vectors and SDLEN3 in my_real) ----
+    double X17, X28, X35, X46, Y17, Y28, Y35, Y46, Z17, Z28, Z35, Z46;
+    R xr[8], yr[8], zr[8];
     R R11 = R(1), R12 = R(0), R13 = R(0), R21 = R(0), R22 = R(1), R23 = R(0), R31 = R(0), R32 = R(0), R33 = R(1);
-    const bool corot = CORO && gd.jcvt;
+    const bool corot = CORO && __ldg(&gdp->jcvt);
     if (corot) {
+      double XD[8], YD[8], ZD[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const int l = corner(k);
+        const double2 xy = sxy[l];
+        XD[k] = xy.x; YD[k] = xy.y; ZD[k] = sz[l];
+      }
+      // SRCOOR3 (srcoor3.F, JCVT /= 0, ISORTH = 0): convected frame R = [e1 e2 e3] of
+      // SREPISO3 (FP64 differences, r, s, t in R) and SORTHO3 (three symmetric
+      // corrections, then Gram-Schmidt); coordinates (FP64) and velocities in it
       const R x17 = R(XD[6] - XD[0]), x28 = R(XD[7] - XD[1]), x35 = R(XD[4] - XD[2]), x46 = R(XD[5] - XD[3]);
       const R y17 = R(YD[6] - YD[0]), y28 = R(YD[7] - YD[1]), y35 = R(YD[4] - YD[2]), y46 = R(YD[5] - YD[3]);
       const R z17 = R(ZD[6] - ZD[0]), z28 = R(ZD[7] - ZD[1]), z35 = R(ZD[4] - ZD[2]), z46 = R(ZD[5] - ZD[3]);
@@ -518,10 +596,33 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
         const double zl = (double)R13 * XD[k] + (double)R23 * YD[k] + (double)R33 * ZD[k];
         XD[k] = xl; YD[k] = yl; ZD[k] = zl;
       }
+      X17 = XD[6] - XD[0]; X28 = XD[7] - XD[1]; X35 = XD[4] - XD[2]; X46 = XD[5] - XD[3];
+      Y17 = YD[6] - YD[0]; Y28 = YD[7] - YD[1]; Y35 = YD[4] - YD[2]; Y46 = YD[5] - YD[3];
+      Z17 = ZD[6] - ZD[0]; Z28 = ZD[7] - ZD[1]; Z35 = ZD[4] - ZD[2]; Z46 = ZD[5] - ZD[3];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) { xr[k] = R(XD[k] - XD[0]); yr[k] = R(YD[k] - YD[0]); zr[k] = R(ZD[k] - ZD[0]); }
+    } else {
+      // corner 1 first, then the pairs, so that at most two corners are held in FP64
+      const int l0 = corner(0);
+      const double2 q0 = sxy[l0];
+      const double x0 = q0.x, y0 = q0.y, z0 = sz[l0];
+      xr[0] = R(0); yr[0] = R(0); zr[0] = R(0);
+      auto ld = [&](int k, double& x, double& y, double& z) {
+        const int l = corner(k);
+        const double2 q = sxy[l];
+        x = q.x; y = q.y; z = sz[l];
+        xr[k] = R(x - x0); yr[k] = R(y - y0); zr[k] = R(z - z0);
+      };
+      double xk, yk, zk, xm, ym, zm;
+      ld(6, xk, yk, zk);
+      X17 = xk - x0; Y17 = yk - y0; Z17 = zk - z0;
+      ld(1, xm, ym, zm); ld(7, xk, yk, zk);
+      X28 = xk - xm; Y28 = yk - ym; Z28 = zk - zm;
+      ld(2, xm, ym, zm); ld(4, xk, yk, zk);
+      X35 = xk - xm; Y35 = yk - ym; Z35 = zk - zm;
+      ld(3, xm, ym, zm); ld(5, xk, yk, zk);
+      X46 = xk - xm; Y46 = yk - ym; Z46 = zk - zm;
     }
-    const double X17 = XD[6] - XD[0], X28 = XD[7] - XD[1], X35 = XD[4] - XD[2], X46 = XD[5] - XD[3];
-    const double Y17 = YD[6] - YD[0], Y28 = YD[7] - YD[1], Y35 = YD[4] - YD[2], Y46 = YD[5] - YD[3];
-    const double Z17 = ZD[6] - ZD[0], Z28 = ZD[7] - ZD[1], Z35 = ZD[4] - ZD[2], Z46 = ZD[5] - ZD[3];
     const double J1 = X17 + X28 - X35 - X46, J2 = Y17 + Y28 - Y35 - Y46, J3 = Z17 + Z28 - Z35 - Z46;
     const double xa = X17 + X46, xb = X28 + X35, ya = Y17 + Y46, yb = Y28 + Y35, za = Z17 + Z46, zb = Z28 + Z35;
     const double J4 = xa + xb, J5 = ya + yb, J6 = za + zb, J7 = xa - xb, J8 = ya - yb, J9 = za - zb;
@@ -531,13 +632,6 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
       raise_error(a.err, 4, st_eid);
       det = 1.0;
     }
-    // Beyond the determinant nothing here needs FP64 (the reference's -prec=sp
-    // build forms the inverse Jacobian, the hourglass vectors and SDLEN3 in
-    // my_real): they use R, with coordinates relative to corner 1 (differences
-    // taken in FP64, then rounded), so the 24 FP64 coordinates die here.
-    R xr[8], yr[8], zr[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) { xr[k] = R(XD[k] - XD[0]); yr[k] = R(YD[k] - YD[0]); zr[k] = R(ZD[k] - ZD[0]); }
     const R j1 = R(J1), j2 = R(J2), j3 = R(J3), j4 = R(J4), j5 = R(J5), j6 = R(J6), j7 = R(J7), j8 = R(J8), j9 = R(J9);
     const R dett = R(1.0 / 64.0) / R(det);
     const R I1 = dett * R(C1), I4 = dett * R(C4), I7 = dett * R(C7);
@@ -590,41 +684,59 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
       }
     }
     const R DELTAX = R(4) * VOLN / ssqrt(AREAM);
-    // ---- SDEFO3 (sdefo3.F:114-170, JHBE=1) ----
-    R VX[8], VY[8], VZ[8];
+    // ---- SDEFO3 (sdefo3.F:114-170, JHBE=1) and the hourglass velocity modes of
+    // SHVIS3, from the velocities taken in the corner pairs (1,7) (2,8) (3,5) (4,6)
+    // that share a row of PX: the mode-j sum  sum_k g_jk v_k  with g_jk = s_jk -+ PXH
+    // splits into the sign sum  sum_k s_jk v_k  and  -sum_q PXH[q][j] (v_k1 - v_k2) ----
+    constexpr int sgn[3][8] = {{1, -1, 1, -1, 1, -1, 1, -1}, {1, 1, -1, -1, -1, -1, 1, 1}, {1, -1, -1, 1, -1, 1, 1, -1}};
+    constexpr int h4[8] = {1, -1, 1, -1, -1, 1, -1, 1};
+    constexpr int pk1[4] = {0, 1, 2, 3}, pk2[4] = {6, 7, 4, 5};
+    R DXX = R(0), DYY = R(0), DZZ = R(0), DXY = R(0), DXZ = R(0), DYX = R(0), DYZ = R(0), DZX = R(0), DZY = R(0);
+    R HGX[4] = {R(0), R(0), R(0), R(0)}, HGY[4] = {R(0), R(0), R(0), R(0)}, HGZ[4] = {R(0), R(0), R(0), R(0)};
 #pragma unroll
-    for (int k = 0; k < 8; ++k) { VX[k] = svx[lc[k]]; VY[k] = svy[lc[k]]; VZ[k] = svz[lc[k]]; }
-    if (corot) {
-#pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        const R vx = R11 * VX[k] + R21 * VY[k] + R31 * VZ[k];
-        const R vy = R12 * VX[k] + R22 * VY[k] + R32 * VZ[k];
-        const R vz = R13 * VX[k] + R23 * VY[k] + R33 * VZ[k];
-        VX[k] = vx; VY[k] = vy; VZ[k] = vz;
+    for (int q = 0; q < 4; ++q) {
+      const int k1 = pk1[q], k2 = pk2[q];
+      const R4 v1 = sv[corner(k1)], v2 = sv[corner(k2)];
+      R u1 = v1.x, w1 = v1.y, t1 = v1.z, u2 = v2.x, w2 = v2.y, t2 = v2.z;
+      if (corot) {
+        const R a1 = R11 * u1 + R21 * w1 + R31 * t1, b1 = R12 * u1 + R22 * w1 + R32 * t1, c1 = R13 * u1 + R23 * w1 + R33 * t1;
+        const R a2 = R11 * u2 + R21 * w2 + R31 * t2, b2 = R12 * u2 + R22 * w2 + R32 * t2, c2 = R13 * u2 + R23 * w2 + R33 * t2;
+        u1 = a1; w1 = b1; t1 = c1; u2 = a2; w2 = b2; t2 = c2;
       }
+      const R dvx = u1 - u2, dvy = w1 - w2, dvz = t1 - t2;
+      DXX += PX[q] * dvx; DYY += PY[q] * dvy; DZZ += PZ[q] * dvz;
+      DXY += PY[q] * dvx; DXZ += PZ[q] * dvx; DYX += PX[q] * dvy;
+      DYZ += PZ[q] * dvy; DZX += PX[q] * dvz; DZY += PY[q] * dvz;
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const R s1 = R(sgn[j][k1]), s2 = R(sgn[j][k2]);
+        HGX[j] += s1 * u1 + s2 * u2 - PXH[q][j] * dvx;
+        HGY[j] += s1 * w1 + s2 * w2 - PXH[q][j] * dvy;
+        HGZ[j] += s1 * t1 + s2 * t2 - PXH[q][j] * dvz;
+      }
+      // the 4th mode (+-+--+-+) (shvis3.F:230-232)
+      HGX[3] += R(h4[k1]) * u1 + R(h4[k2]) * u2;
+      HGY[3] += R(h4[k1]) * w1 + R(h4[k2]) * w2;
+      HGZ[3] += R(h4[k1]) * t1 + R(h4[k2]) * t2;
     }
-    const R vx17 = VX[0] - VX[6], vx28 = VX[1] - VX[7], vx35 = VX[2] - VX[4], vx46 = VX[3] - VX[5];
-    const R vy17 = VY[0] - VY[6], vy28 = VY[1] - VY[7], vy35 = VY[2] - VY[4], vy46 = VY[3] - VY[5];
-    const R vz17 = VZ[0] - VZ[6], vz28 = VZ[1] - VZ[7], vz35 = VZ[2] - VZ[4], vz46 = VZ[3] - VZ[5];
-    const R DXX = PX[0] * vx17 + PX[1] * vx28 + PX[2] * vx35 + PX[3] * vx46;
-    const R DYY = PY[0] * vy17 + PY[1] * vy28 + PY[2] * vy35 + PY[3] * vy46;
-    const R DZZ = PZ[0] * vz17 + PZ[1] * vz28 + PZ[2] * vz35 + PZ[3] * vz46;
-    const R DXY = PY[0] * vx17 + PY[1] * vx28 + PY[2] * vx35 + PY[3] * vx46;
-    const R DXZ = PZ[0] * vx17 + PZ[1] * vx28 + PZ[2] * vx35 + PZ[3] * vx46;
-    const R DYX = PX[0] * vy17 + PX[1] * vy28 + PX[2] * vy35 + PX[3] * vy46;
-    const R DYZ = PZ[0] * vy17 + PZ[1] * vy28 + PZ[2] * vy35 + PZ[3] * vy46;
-    const R DZX = PX[0] * vz17 + PX[1] * vz28 + PX[2] * vz35 + PX[3] * vz46;
-    const R DZY = PY[0] * vz17 + PY[1] * vz28 + PY[2] * vz35 + PY[3] * vz46;
+    // PXH is needed again only by SFINT3: parked in this thread's own entries of the
+    // corner planes 11..22 (free until its corners are written; volatile, so that the
+    // compiler reloads them instead of holding 12 registers across the material law)
+    volatile R* park = sc + 11 * TILE + tid;
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) park[(3 * q + j) * TILE] = PXH[q][j];
     const R DT1D2 = R(0.5) * DT1;
     const R D4 = DXY + DYX, D5 = DYZ + DZY, D6 = DXZ + DZX;
     const R WZZ = DT1D2 * (DYX - DXY), WYY = DT1D2 * (DXZ - DZX), WXX = DT1D2 * (DZY - DYZ);
     // ---- SRHO3 (srho3.F:122-156; FP64 volume ratios in the split form, srho3.F:230-245) ----
-    const R RHO0 = R(gd.rho0);
-    const R rho_old = st_rho;
-    const R VOLO = st_vol0;
+    const R RHO0 = R(__ldg(&gdp->rho0));
+    const R rho_old = sc[7 * TILE + tid];
+    const R VOLO = sc[9 * TILE + tid];
     R DVOL, RHON, AMU;
     if (split) {
-      const double v0 = st_vol0dp;
+      const double v0 = svol0dp[tid];
       DVOL = R(VOLN_D - ((double)RHO0 / (double)rho_old) * v0);
       RHON = R((double)RHO0 * (v0 / VOLN_D));
       AMU = R(v0 / VOLN_D - 1.0);
@@ -633,10 +745,10 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
       RHON = RHO0 * (VOLO / VOLN);
       AMU = RHON / RHO0 - R(1);
     }
-    R EINT = st_eint * VOLO;
+    R EINT = sc[6 * TILE + tid] * VOLO;
     // ---- SROTA3 Jaumann rotation (srota3.F:81-91) ----
-    const R S1 = st_sig[0], S2 = st_sig[1], S3 = st_sig[2];
-    const R S4 = st_sig[3], S5 = st_sig[4], S6 = st_sig[5];
+    const R S1 = sc[0 * TILE + tid], S2 = sc[1 * TILE + tid], S3 = sc[2 * TILE + tid];
+    const R S4 = sc[3 * TILE + tid], S5 = sc[4 * TILE + tid], S6 = sc[5 * TILE + tid];
     R SG[6];
     if (corot) {          // SRMALLA3 (srmall3.F): convected-frame stress, not rotated
       SG[0] = S1; SG[1] = S2; SG[2] = S3; SG[3] = S4; SG[4] = S5; SG[5] = S6;
@@ -650,12 +762,23 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
       SG[5] = S6 + WYY * (S3 - S1) + WXX * S4 - WZZ * S5;
     }
     const R VOL_AVG = VOLN - R(0.5) * DVOL;
-    const R QOLD = st_qvis;
+    const R QOLD = sc[8 * TILE + tid];
+    const R EPXE = sc[10 * TILE + tid];
+    // the state planes 0..10 are read: PX, PY, PZ (needed again only by SFINT3) are
+    // parked in this thread's entries of planes 0..10 and 23 likewise
+    volatile R* park2 = sc + tid;
+    constexpr int pplane[12] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 23};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      park2[pplane[q] * TILE] = PX[q];
+      park2[pplane[4 + q] * TILE] = PY[q];
+      park2[pplane[8 + q] * TILE] = PZ[q];
+    }
     // ---- elastic predictor (m1law.F:124-140 / m2law.F:187-200) ----
     const R OFF = R(1);
-    const R Gs = R(gd.shear) * OFF;
+    const R Gs = R(__ldg(&gdp->shear)) * OFF;
     const R G1 = DT1 * Gs, G2 = R(2) * G1;
-    const R SSP = ssqrt((R(1.333) * Gs + R(gd.bulk)) / RHO0);
+    const R SSP = ssqrt((R(1.333) * Gs + R(__ldg(&gdp->bulk))) / RHO0);
     {
       const R P = -R(1.0 / 3.0) * (SG[0] + SG[1] + SG[2]);
       const R DAV = -R(1.0 / 3.0) * (DXX + DYY + DZZ);
@@ -667,7 +790,7 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
       SG[5] = SG[5] + G1 * D6;
     }
     R DPLA = R(0), SIGY = R(0);
-    if (gd.law == 2) {
+    if (__ldg(&gdp->law) == 2) {
       // ---- M2LAW radial return (m2law.F:197-352), CC=0, FISOKIN=0 ----
       R AJ2 = R(0.5) * (SG[0] * SG[0] + SG[1] * SG[1] + SG[2] * SG[2]) + SG[3] * SG[3] + SG[4] * SG[4] + SG[5] * SG[5];
       AJ2 = ssqrt(R(3) * AJ2);
@@ -675,17 +798,16 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
         const R e4 = R(0.5) * D4, e5 = R(0.5) * D5, e6 = R(0.5) * D6;
         a.epsd[e] = ssqrt(DXX * DXX + DYY * DYY + DZZ * DZZ + R(2) * (e4 * e4 + e5 * e5 + e6 * e6));
       }
-      const R CA = R(gd.jc_a), CB = R(gd.jc_b), CN = R(gd.jc_n);
-      R EPXE = st_pla;
+      const R CA = R(__ldg(&gdp->jc_a)), CB = R(__ldg(&gdp->jc_b)), CN = R(__ldg(&gdp->jc_n));
       R AK, QH;
       if (CN == R(1)) { AK = CA + CB * EPXE; QH = CB; }
       else if (EPXE > R(0)) {
         AK = CA + CB * pow_(EPXE, CN);
         QH = (CN > R(1)) ? CB * CN * pow_(EPXE, CN - R(1)) : CB * CN / pow_(EPXE, R(1) - CN);
       } else { AK = CA; QH = R(0); }
-      if (R(gd.sigmax) < AK) { AK = R(gd.sigmax); QH = R(0); }
+      if (R(__ldg(&gdp->sigmax)) < AK) { AK = R(__ldg(&gdp->sigmax)); QH = R(0); }
       SIGY = AK;
-      if (EPXE > R(gd.epsmax)) { AK = R(0); QH = R(0); }
+      if (EPXE > R(__ldg(&gdp->epsmax))) { AK = R(0); QH = R(0); }
       R SCALE = AK / (AJ2 > R(EM15) ? AJ2 : R(EM15));
       SCALE = SCALE < R(1) ? SCALE : R(1);
       const R den = R(3) * Gs + QH;
@@ -704,25 +826,25 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
     {
       const R DD = -DXX - DYY - DZZ;
       const R AD = DD > R(0) ? DD : R(0);
-      const R QA = R(gd.qa), QB = R(gd.qb);
+      const R QA = R(__ldg(&gdp->qa)), QB = R(__ldg(&gdp->qb));
       const R QAA = QA * QA * AD;
       const R QX = QB * SSP + AL * QAA;
       QNEW = RHON * AD * AL * (QAA * AL + QB * SSP);
       R SSP_EQ = QX + ssqrt(QX * QX + SSP * SSP);
       SSP_EQ = SSP_EQ > R(EM20) ? SSP_EQ : R(EM20);
-      const R DTX = R(gd.dtfac) * (DELTAX / SSP_EQ);
-      if ((double)DTX <= gd.dtmin) raise_error(a.err, 5, st_eid);
+      const R DTX = R(__ldg(&gdp->dtfac)) * (DELTAX / SSP_EQ);
+      if ((double)DTX <= __ldg(&gdp->dtmin)) raise_error(a.err, 5, st_eid);
       const double dtd = (double)DTX;
       mykey = dt_key(dtd, 1, st_eid);
       mybits = (unsigned long long)__double_as_longlong(dtd);
     }
     // ---- pressure and internal energy (m1law.F:172-190 / m2law.F:434-461) ----
-    const R PNEW = R(gd.bulk) * AMU;
+    const R PNEW = R(__ldg(&gdp->bulk)) * AMU;
     SG[0] = (SG[0] - PNEW) * OFF; SG[1] = (SG[1] - PNEW) * OFF; SG[2] = (SG[2] - PNEW) * OFF;
     SG[3] = SG[3] * OFF; SG[4] = SG[4] * OFF; SG[5] = SG[5] * OFF;
     const R DTA = R(0.5) * DT1;
     R EINC;
-    if (gd.law == 1) {
+    if (__ldg(&gdp->law) == 1) {
       const R P2 = -(S1 + SG[0] + S2 + SG[1] + S3 + SG[2]) * R(1.0 / 3.0);
       EINC = VOL_AVG * (DXX * (S1 + SG[0] + P2) + DYY * (S2 + SG[1] + P2) + DZZ * (S3 + SG[2] + P2) +
                         D4 * (S4 + SG[3]) + D5 * (S5 + SG[4]) + D6 * (S6 + SG[5])) * DTA -
@@ -741,33 +863,12 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
     a.rho[e] = RHON;
     a.qvis[e] = QNEW;
     // ---- SHVIS3 Flanagan-Belytschko viscous hourglass (shvis3.F:156-424, JHBE>=1) ----
-    // g-vectors of the three non-trivial modes (Gv[j][k] = sign - or + PXH), recomputed
-    // where used instead of held; the 4th mode is the pure (+-+--+-+) vector
-    const R CAQ = R(0.25) * OFF * R(gd.qh);
+    const R CAQ = R(0.25) * OFF * R(__ldg(&gdp->qh));
     R FCL = CAQ * RHON * (AL * AL);   // VOL**TWO_THIRD
     const R FCQ = FCL * CAQ * R(100);
     FCL = FCL * SSP;
-    constexpr int sgn[3][8] = {{1, -1, 1, -1, 1, -1, 1, -1}, {1, 1, -1, -1, -1, -1, 1, 1}, {1, -1, -1, 1, -1, 1, 1, -1}};
-    constexpr int pq[8] = {0, 1, 2, 3, 2, 3, 0, 1};        // PXH row of corner k
-    auto gvec = [&](int j, int k) -> R {
-      return k < 4 ? R(sgn[j][k]) - PXH[pq[k]][j] : R(sgn[j][k]) + PXH[pq[k]][j];
-    };
     R HX[4], HY[4], HZ[4];
     {
-      R HGX[4], HGY[4], HGZ[4];
-#pragma unroll
-      for (int j = 0; j < 3; ++j) {
-        R hx = R(0), hy = R(0), hz = R(0);
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-          const R g = gvec(j, k);
-          hx += g * VX[k]; hy += g * VY[k]; hz += g * VZ[k];
-        }
-        HGX[j] = hx; HGY[j] = hy; HGZ[j] = hz;
-      }
-      HGX[3] = VX[0] - VX[1] + VX[2] - VX[3] - VX[4] + VX[5] - VX[6] + VX[7];
-      HGY[3] = VY[0] - VY[1] + VY[2] - VY[3] - VY[4] + VY[5] - VY[6] + VY[7];
-      HGZ[3] = VZ[0] - VZ[1] + VZ[2] - VZ[3] - VZ[4] + VZ[5] - VZ[6] + VZ[7];
       R ehou = R(0);
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
@@ -779,43 +880,49 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
       my_ehou = (double)(DT1 * ehou);
     }
     // ---- SFINT3 (sfint3.F:256-321), antisymmetric pairs 1-7, 2-8, 3-5, 4-6: corner
-    // n1[q] gets -f_q, corner n2[q] gets +f_q, added to the hourglass force ----
+    // k1 gets -f_q, corner k2 gets +f_q, added to the hourglass force; the hourglass
+    // force  -sum_j g_jk H_j - h4_k H_4  splits like the mode sums above ----
     const R s1 = (SG[0] - QNEW) * VOLN, s2 = (SG[1] - QNEW) * VOLN, s3 = (SG[2] - QNEW) * VOLN;
     const R s4 = SG[3] * VOLN, s5 = SG[4] * VOLN, s6 = SG[5] * VOLN;
-    constexpr int h4[8] = {1, -1, 1, -1, -1, 1, -1, 1};
-    // corners in the pairs of SFINT3 that share a stress term (1-7, 2-8, 3-5, 4-6),
-    // straight to the corner-force planes
-    constexpr int korder[8] = {0, 6, 1, 7, 2, 4, 3, 5};
-    R f0 = R(0), f1 = R(0), f2 = R(0);
+    // PXH, PX, PY, PZ back from their parking planes, before any corner is written
+    R PH[4][3], QX[4], QY[4], QZ[4];
 #pragma unroll
-    for (int kk = 0; kk < 8; ++kk) {
-      const int k = korder[kk];
-      const R g0 = gvec(0, k), g1 = gvec(1, k), g2 = gvec(2, k);
-      R fx = -g0 * HX[0] - g1 * HX[1] - g2 * HX[2] - R(h4[k]) * HX[3];
-      R fy = -g0 * HY[0] - g1 * HY[1] - g2 * HY[2] - R(h4[k]) * HY[3];
-      R fz = -g0 * HZ[0] - g1 * HZ[1] - g2 * HZ[2] - R(h4[k]) * HZ[3];
-      if ((kk & 1) == 0) {                  // the pair's first corner: its stress term
-        const int q = pq[k];
-        f0 = s1 * PX[q] + s4 * PY[q] + s6 * PZ[q];
-        f1 = s2 * PY[q] + s4 * PX[q] + s5 * PZ[q];
-        f2 = s3 * PZ[q] + s6 * PX[q] + s5 * PY[q];
+    for (int q = 0; q < 4; ++q) {
+#pragma unroll
+      for (int j = 0; j < 3; ++j) PH[q][j] = park[(3 * q + j) * TILE];
+      QX[q] = park2[pplane[q] * TILE];
+      QY[q] = park2[pplane[4 + q] * TILE];
+      QZ[q] = park2[pplane[8 + q] * TILE];
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int k1 = pk1[q], k2 = pk2[q];
+      // common part of the pair: sum_j PXH[q][j] H_j minus the stress term
+      const R ux = PH[q][0] * HX[0] + PH[q][1] * HX[1] + PH[q][2] * HX[2] - (s1 * QX[q] + s4 * QY[q] + s6 * QZ[q]);
+      const R uy = PH[q][0] * HY[0] + PH[q][1] * HY[1] + PH[q][2] * HY[2] - (s2 * QY[q] + s4 * QX[q] + s5 * QZ[q]);
+      const R uz = PH[q][0] * HZ[0] + PH[q][1] * HZ[1] + PH[q][2] * HZ[2] - (s3 * QZ[q] + s6 * QX[q] + s5 * QY[q]);
+#pragma unroll
+      for (int side = 0; side < 2; ++side) {
+        const int k = side ? k2 : k1;
+        const R sg = side ? R(-1) : R(1);
+        R fx = -R(sgn[0][k]) * HX[0] - R(sgn[1][k]) * HX[1] - R(sgn[2][k]) * HX[2] - R(h4[k]) * HX[3] + sg * ux;
+        R fy = -R(sgn[0][k]) * HY[0] - R(sgn[1][k]) * HY[1] - R(sgn[2][k]) * HY[2] - R(h4[k]) * HY[3] + sg * uy;
+        R fz = -R(sgn[0][k]) * HZ[0] - R(sgn[1][k]) * HZ[1] - R(sgn[2][k]) * HZ[2] - R(h4[k]) * HZ[3] + sg * uz;
+        if (corot) {        // SRROTA3 with R transposed (sforc3.F:1603-1614): back to global axes
+          const R gx = R11 * fx + R12 * fy + R13 * fz;
+          const R gy = R21 * fx + R22 * fy + R23 * fz;
+          const R gz = R31 * fx + R32 * fy + R33 * fz;
+          fx = gx; fy = gy; fz = gz;
+        }
+        // planes 0..10 held this thread's own state, read above
+        sc[(0 * 8 + k) * TILE + tid] = fx;
+        sc[(1 * 8 + k) * TILE + tid] = fy;
+        sc[(2 * 8 + k) * TILE + tid] = fz;
       }
-      if (k < 4) { fx -= f0; fy -= f1; fz -= f2; }
-      else { fx += f0; fy += f1; fz += f2; }
-      if (corot) {        // SRROTA3 with R transposed (sforc3.F:1603-1614): back to global axes
-        const R gx = R11 * fx + R12 * fy + R13 * fz;
-        const R gy = R21 * fx + R22 * fy + R23 * fz;
-        const R gz = R31 * fx + R32 * fy + R33 * fz;
-        fx = gx; fy = gy; fz = gz;
-      }
-      sc[(0 * 8 + k) * TILE + tid] = fx;
-      sc[(1 * 8 + k) * TILE + tid] = fy;
-      sc[(2 * 8 + k) * TILE + tid] = fz;
     }
   }
   // ---- patch assembly: each patch node sums its incident corners in ascending
   // (element, corner) order ----
-  (void)color;
   __syncthreads();
   for (int j = tid; j < nl; j += TILE) {
     R fx = R(0), fy = R(0), fz = R(0);
@@ -828,14 +935,34 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
     const int s = j == tid ? slot0 : j == tid + TILE ? slot1 : a.patch_slots[p * NLM + j];
     a.fslot[s] = mk4(fx, fy, fz, R(0));
   }
-  // ---- dt min-reduction and energy partials ----
-  block_reduce<TILE>(mykey, mybits, my_ehou, my_wpla, s_key, s_bits, s_s0, s_s1);
-  if (tid == 0) {
-    PartAcc* acc = &a.acc[parity * a.nparts + pi.part];
-    atomicMin(&acc->dtkey, mykey);
-    atomicMin(&acc->dtbits, mybits);
-    a.blk_ehour[p] = pre_ehour + my_ehou;
-    a.blk_wpla[p] = pre_wpla + my_wpla;
+  // ---- dt min-reduction and energy partials (fixed tree order for the sums) ----
+  {
+    const int lane = tid & 31, warp = tid >> 5;
+    mykey = warp_min_u64(mykey);
+    mybits = warp_min_u64(mybits);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      my_ehou += __shfl_xor_sync(0xffffffffu, my_ehou, o);
+      my_wpla += __shfl_xor_sync(0xffffffffu, my_wpla, o);
+    }
+    if (lane == 0) { s_key[warp] = mykey; s_bits[warp] = mybits; s_s0[warp] = my_ehou; s_s1[warp] = my_wpla; }
+    __syncthreads();
+    if (tid == 0) {
+      unsigned long long k = s_key[0], b = s_bits[0];
+      double h = s_s0[0], w = s_s1[0];
+#pragma unroll
+      for (int i = 1; i < TILE / 32; ++i) {
+        k = s_key[i] < k ? s_key[i] : k;
+        b = s_bits[i] < b ? s_bits[i] : b;
+        h += s_s0[i];
+        w += s_s1[i];
+      }
+      PartAcc* acc = &a.acc[parity * a.nparts + pi.part];
+      atomicMin(&acc->dtkey, k);
+      atomicMin(&acc->dtbits, b);
+      a.blk_ehour[p] = pre_ehour + h;
+      a.blk_wpla[p] = pre_wpla + w;
+    }
   }
 }
 

@@ -107,14 +107,6 @@ template <> struct Vec2<double> { typedef double2 T; };
 __device__ __forceinline__ float2 mk2(float a, float b) { return make_float2(a, b); }
 __device__ __forceinline__ double2 mk2(double a, double b) { return make_double2(a, b); }
 
-// minimum of a 64-bit unsigned value over the warp, from two 32-bit hardware
-// reductions (high words, then the low words of the lanes holding the high minimum)
-__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v) {
-  const unsigned hi = __reduce_min_sync(0xffffffffu, (unsigned)(v >> 32));
-  const unsigned lo = __reduce_min_sync(0xffffffffu, (unsigned)(v >> 32) == hi ? (unsigned)v : 0xffffffffu);
-  return ((unsigned long long)hi << 32) | lo;
-}
-
 // the dt-key / dt-bits min and the two energy sums of a group of TILE threads
 // (threads g*TILE .. g*TILE+TILE-1), with the operation order of block_reduce
 template <int TILE>
