@@ -300,8 +300,9 @@ int build_patches(or_ecycle* h, std::vector<GroupT>& groups, int tile, PatchSet&
 }
 
 // Incidence lists of every patch at a fixed stride: nlmax+1 offsets, then for each
-// patch node the corners t*K+k (t: element of the patch, k: corner) that touch it,
-// in ascending order.  The kernels sum a node's corner forces in this order.
+// patch node the corners (t: element of the patch, k: corner) that touch it, in
+// ascending (t, k) order, each stored as its offset k*tile + t in a corner-force
+// plane of the patch kernels.  The kernels sum a node's corner forces in this order.
 int incidence_stride(const PatchSet& ps, int K, int tile) {
   const int s = ps.nlmax + 1 + K * tile;
   return (s + 7) & ~7;   // 16-byte rows: the hexa kernel stages them by bulk copy
@@ -321,7 +322,7 @@ void incidence_lists(const PatchSet& ps, int K, int tile, std::vector<uint16_t>&
     for (int t = 0; t < pi.nel; ++t)
       for (int k = 0; k < K; ++k) {
         const int l = ps.local[(size_t)(pi.elem0 + t) * K + k] & LOCAL_MASK;
-        ent[cnt[l]++] = (uint16_t)(t * K + k);
+        ent[cnt[l]++] = (uint16_t)(k * tile + t);
       }
   }
 }
@@ -396,6 +397,7 @@ struct Impl {
   struct Persist {
     bool on = false;
     int G = 0, P = 0, ncmax = 0;
+    int T = 0;                 // threads per CTA
     int stall_cta = -1;        // test hook, OR_ECYCLE_TEST_STALL_CTA
     size_t smem = 0;
     DBuf<int> node_ofs, node_glob; DBuf<unsigned char> owner; DBuf<uint2> pconn;
@@ -675,10 +677,13 @@ int persist_build(or_ecycle* h, Impl<R>& m) {
   }
   const size_t smem = persist_smem<R>(ncmax, tile, P, m.sinc_stride, ps.nlmax);
   if (smem > 200 * 1024) return OR_OK;
+  // one thread per element, and per held node where the CTA holds more nodes than
+  // elements (a node phase of one node per thread), in whole TILE groups
+  const int T = std::min(PERSIST_THREADS / tile * tile, std::max(P * tile, (ncmax + tile - 1) / tile * tile));
   const PersistFn<R> fn = persist_fn<R>(tile, m.uniform_npt == 5);
   CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int nb = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, P * tile, smem));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, T, smem));
   if (nb < 1 || G > nb * h->nsm) return OR_OK;
   int rc;
   if ((rc = dput(h, q.node_ofs, ofs)) || (rc = dput(h, q.node_glob, glob)) || (rc = dput(h, q.owner, own)) ||
@@ -690,7 +695,7 @@ int persist_build(or_ecycle* h, Impl<R>& m) {
   q.stall_cta = -1;
   if (const char* st = std::getenv("OR_ECYCLE_TEST_STALL_CTA")) q.stall_cta = std::atoi(st);
   q.on = true;
-  q.G = G; q.P = P; q.ncmax = ncmax; q.smem = smem;
+  q.G = G; q.P = P; q.T = T; q.ncmax = ncmax; q.smem = smem;
   return OR_OK;
 }
 
@@ -708,7 +713,7 @@ int launch_persistent(or_ecycle* h, Impl<R>& m, int ncycles, int parity0) {
   const PersistFn<R> fn = persist_fn<R>(h->tile_shell, m.uniform_npt == 5);
   Trace tr("persistent cycles");
   const cudaError_t e =
-      cudaLaunchCooperativeKernel((const void*)fn, dim3(q.G), dim3(q.P * h->tile_shell), args, q.smem, h->stream);
+      cudaLaunchCooperativeKernel((const void*)fn, dim3(q.G), dim3(q.T), args, q.smem, h->stream);
   if (e == cudaErrorCooperativeLaunchTooLarge) {   // the wave no longer fits (another context holds SMs):
     cudaGetLastError();                             // the per-phase kernels take over for good
     q.on = false;
@@ -2510,10 +2515,10 @@ int or_ecycle_persistent_info(or_ecycle* h, int* on, int* ctas, int* threads) {
   int g = 0, t = 0, o = 0;
   if (h->cfg.precision == OR_PREC_SPLIT) {
     const auto& q = ((Impl<float>*)h->impl)->per;
-    o = q.on; g = q.G; t = q.P * h->tile_shell;
+    o = q.on; g = q.G; t = q.T;
   } else {
     const auto& q = ((Impl<double>*)h->impl)->per;
-    o = q.on; g = q.G; t = q.P * h->tile_shell;
+    o = q.on; g = q.G; t = q.T;
   }
   *on = o;
   if (ctas) *ctas = o ? g : 0;

@@ -50,7 +50,9 @@ struct HexGroupDesc {
   int part, law, nel, jcvt;       // jcvt: 1 = convected frame (Iframe 2)
   double rho0, shear, bulk, jc_a, jc_b, jc_n, epsmax, sigmax;
   double qa, qb, qh, dtfac, dtmin;
+  double pad;                     // 128 bytes: the hexa kernel stages it by bulk copy
 };
+static_assert(sizeof(HexGroupDesc) % 16 == 0, "HexGroupDesc is bulk-copied");
 
 struct ShellGroupDesc {
   int part, law, nel, npt;
@@ -113,7 +115,7 @@ struct HexArgs {
   const int* patch_slots;     // nlmax per patch; padding -1
   const uint4* conn;          // 8 x uint16 local corners per element (colour in corner 0)
   const unsigned short* inc;  // per patch (stride inc_stride): nlmax+1 offsets, then the
-                              // patch nodes' incident corners t*8+k in ascending order
+                              // patch nodes' incident corners (t, k) in ascending order, stored as k*TILE+t
   const int* elem_id;         // element number within its part (for NELTS)
   const double4* X;           // x, y, z, nodal mass
   const typename Vec4<R>::T* V;
@@ -139,7 +141,7 @@ struct ShellArgs {
   const int* patch_slots;     // nlmax per patch; padding -1
   const uint2* conn;          // 4 x uint16 local corners per element (colour in corner 0)
   const unsigned short* inc;  // per patch (stride inc_stride): nlmax+1 offsets, then the
-                              // patch nodes' incident corners t*4+k in ascending order
+                              // patch nodes' incident corners (t, k) in ascending order, stored as k*TILE+t
   const int* elem_id;
   const int* degen;           // 1 if IXC(4)==IXC(5) (triangle stored as quad)
   const double4* X;
@@ -464,6 +466,7 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
   __shared__ unsigned long long s_key[TILE / 32], s_bits[TILE / 32];
   __shared__ double s_s0[TILE / 32], s_s1[TILE / 32];
   __shared__ __align__(8) unsigned long long s_bar;
+  __shared__ __align__(16) HexGroupDesc s_gd;
   const int p = blockIdx.x;
   const int tid = threadIdx.x;
   // Patches are padded to TILE elements (element p*TILE + t is thread t's) and their
@@ -486,7 +489,8 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
   if (tid == 0) {
     mbar_init(&s_bar);
     const unsigned pl = TILE * sizeof(R);
-    mbar_expect_tx(&s_bar, 11 * pl + TILE * (16 + 4 + (split ? 8 : 0)) + 2 * a.inc_stride);
+    mbar_expect_tx(&s_bar, 11 * pl + TILE * (16 + 4 + (split ? 8 : 0)) + 2 * a.inc_stride +
+                               (unsigned)sizeof(HexGroupDesc));
 #pragma unroll
     for (int c = 0; c < 6; ++c) bulk_g2s(sc + c * TILE, a.sig + (size_t)c * nelpad + e0, pl, &s_bar);
     bulk_g2s(sc + 6 * TILE, a.eint + e0, pl, &s_bar);
@@ -499,9 +503,11 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
     if (split) bulk_g2s(svol0dp, a.vol0dp + e0, TILE * 8, &s_bar);
     bulk_g2s(sinc, a.inc + (size_t)p * a.inc_stride, 2 * a.inc_stride, &s_bar);
   }
+  const PatchInfo pi = a.patch[p];
+  // the patch's group constants, staged too (the byte count above includes them)
+  if (tid == 0) bulk_g2s(&s_gd, a.groups + pi.group, sizeof(HexGroupDesc), &s_bar);
   // issued now, used at the end: the patch's slot numbers (up to two per thread)
   // and its cumulative energy partials
-  const PatchInfo pi = a.patch[p];
   const int slot0 = tid < NLM ? a.patch_slots[p * NLM + tid] : -1;
   const int slot1 = tid + TILE < NLM ? a.patch_slots[p * NLM + tid + TILE] : -1;
   double pre_ehour = 0.0, pre_wpla = 0.0;
@@ -522,8 +528,6 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
       cp_async16(reinterpret_cast<unsigned char*>(sv + j) + 16, reinterpret_cast<const unsigned char*>(a.V + g) + 16);
     }
   }
-  // the group constants, read where used (read-only, held in L1) rather than held
-  const HexGroupDesc* __restrict__ gdp = a.groups + pi.group;
   const bool active = tid < pi.nel;
   const int nl = pi.nloc;
   const PartTime& tm = a.time[parity * a.nparts + pi.part];
@@ -551,7 +555,7 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
     double X17, X28, X35, X46, Y17, Y28, Y35, Y46, Z17, Z28, Z35, Z46;
     R xr[8], yr[8], zr[8];
     R R11 = R(1), R12 = R(0), R13 = R(0), R21 = R(0), R22 = R(1), R23 = R(0), R31 = R(0), R32 = R(0), R33 = R(1);
-    const bool corot = CORO && __ldg(&gdp->jcvt);
+    const bool corot = CORO && s_gd.jcvt;
     if (corot) {
       double XD[8], YD[8], ZD[8];
 #pragma unroll
@@ -731,7 +735,7 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
     const R D4 = DXY + DYX, D5 = DYZ + DZY, D6 = DXZ + DZX;
     const R WZZ = DT1D2 * (DYX - DXY), WYY = DT1D2 * (DXZ - DZX), WXX = DT1D2 * (DZY - DYZ);
     // ---- SRHO3 (srho3.F:122-156; FP64 volume ratios in the split form, srho3.F:230-245) ----
-    const R RHO0 = R(__ldg(&gdp->rho0));
+    const R RHO0 = R(s_gd.rho0);
     const R rho_old = sc[7 * TILE + tid];
     const R VOLO = sc[9 * TILE + tid];
     R DVOL, RHON, AMU;
@@ -776,9 +780,9 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
     }
     // ---- elastic predictor (m1law.F:124-140 / m2law.F:187-200) ----
     const R OFF = R(1);
-    const R Gs = R(__ldg(&gdp->shear)) * OFF;
+    const R Gs = R(s_gd.shear) * OFF;
     const R G1 = DT1 * Gs, G2 = R(2) * G1;
-    const R SSP = ssqrt((R(1.333) * Gs + R(__ldg(&gdp->bulk))) / RHO0);
+    const R SSP = ssqrt((R(1.333) * Gs + R(s_gd.bulk)) / RHO0);
     {
       const R P = -R(1.0 / 3.0) * (SG[0] + SG[1] + SG[2]);
       const R DAV = -R(1.0 / 3.0) * (DXX + DYY + DZZ);
@@ -790,7 +794,7 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
       SG[5] = SG[5] + G1 * D6;
     }
     R DPLA = R(0), SIGY = R(0);
-    if (__ldg(&gdp->law) == 2) {
+    if (s_gd.law == 2) {
       // ---- M2LAW radial return (m2law.F:197-352), CC=0, FISOKIN=0 ----
       R AJ2 = R(0.5) * (SG[0] * SG[0] + SG[1] * SG[1] + SG[2] * SG[2]) + SG[3] * SG[3] + SG[4] * SG[4] + SG[5] * SG[5];
       AJ2 = ssqrt(R(3) * AJ2);
@@ -798,16 +802,16 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
         const R e4 = R(0.5) * D4, e5 = R(0.5) * D5, e6 = R(0.5) * D6;
         a.epsd[e] = ssqrt(DXX * DXX + DYY * DYY + DZZ * DZZ + R(2) * (e4 * e4 + e5 * e5 + e6 * e6));
       }
-      const R CA = R(__ldg(&gdp->jc_a)), CB = R(__ldg(&gdp->jc_b)), CN = R(__ldg(&gdp->jc_n));
+      const R CA = R(s_gd.jc_a), CB = R(s_gd.jc_b), CN = R(s_gd.jc_n);
       R AK, QH;
       if (CN == R(1)) { AK = CA + CB * EPXE; QH = CB; }
       else if (EPXE > R(0)) {
         AK = CA + CB * pow_(EPXE, CN);
         QH = (CN > R(1)) ? CB * CN * pow_(EPXE, CN - R(1)) : CB * CN / pow_(EPXE, R(1) - CN);
       } else { AK = CA; QH = R(0); }
-      if (R(__ldg(&gdp->sigmax)) < AK) { AK = R(__ldg(&gdp->sigmax)); QH = R(0); }
+      if (R(s_gd.sigmax) < AK) { AK = R(s_gd.sigmax); QH = R(0); }
       SIGY = AK;
-      if (EPXE > R(__ldg(&gdp->epsmax))) { AK = R(0); QH = R(0); }
+      if (EPXE > R(s_gd.epsmax)) { AK = R(0); QH = R(0); }
       R SCALE = AK / (AJ2 > R(EM15) ? AJ2 : R(EM15));
       SCALE = SCALE < R(1) ? SCALE : R(1);
       const R den = R(3) * Gs + QH;
@@ -826,25 +830,25 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
     {
       const R DD = -DXX - DYY - DZZ;
       const R AD = DD > R(0) ? DD : R(0);
-      const R QA = R(__ldg(&gdp->qa)), QB = R(__ldg(&gdp->qb));
+      const R QA = R(s_gd.qa), QB = R(s_gd.qb);
       const R QAA = QA * QA * AD;
       const R QX = QB * SSP + AL * QAA;
       QNEW = RHON * AD * AL * (QAA * AL + QB * SSP);
       R SSP_EQ = QX + ssqrt(QX * QX + SSP * SSP);
       SSP_EQ = SSP_EQ > R(EM20) ? SSP_EQ : R(EM20);
-      const R DTX = R(__ldg(&gdp->dtfac)) * (DELTAX / SSP_EQ);
-      if ((double)DTX <= __ldg(&gdp->dtmin)) raise_error(a.err, 5, st_eid);
+      const R DTX = R(s_gd.dtfac) * (DELTAX / SSP_EQ);
+      if ((double)DTX <= s_gd.dtmin) raise_error(a.err, 5, st_eid);
       const double dtd = (double)DTX;
       mykey = dt_key(dtd, 1, st_eid);
       mybits = (unsigned long long)__double_as_longlong(dtd);
     }
     // ---- pressure and internal energy (m1law.F:172-190 / m2law.F:434-461) ----
-    const R PNEW = R(__ldg(&gdp->bulk)) * AMU;
+    const R PNEW = R(s_gd.bulk) * AMU;
     SG[0] = (SG[0] - PNEW) * OFF; SG[1] = (SG[1] - PNEW) * OFF; SG[2] = (SG[2] - PNEW) * OFF;
     SG[3] = SG[3] * OFF; SG[4] = SG[4] * OFF; SG[5] = SG[5] * OFF;
     const R DTA = R(0.5) * DT1;
     R EINC;
-    if (__ldg(&gdp->law) == 1) {
+    if (s_gd.law == 1) {
       const R P2 = -(S1 + SG[0] + S2 + SG[1] + S3 + SG[2]) * R(1.0 / 3.0);
       EINC = VOL_AVG * (DXX * (S1 + SG[0] + P2) + DYY * (S2 + SG[1] + P2) + DZZ * (S3 + SG[2] + P2) +
                         D4 * (S4 + SG[3]) + D5 * (S5 + SG[4]) + D6 * (S6 + SG[5])) * DTA -
@@ -863,7 +867,7 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
     a.rho[e] = RHON;
     a.qvis[e] = QNEW;
     // ---- SHVIS3 Flanagan-Belytschko viscous hourglass (shvis3.F:156-424, JHBE>=1) ----
-    const R CAQ = R(0.25) * OFF * R(__ldg(&gdp->qh));
+    const R CAQ = R(0.25) * OFF * R(s_gd.qh);
     R FCL = CAQ * RHON * (AL * AL);   // VOL**TWO_THIRD
     const R FCQ = FCL * CAQ * R(100);
     FCL = FCL * SSP;
@@ -927,9 +931,9 @@ hex_patch_kernel(HexArgs<R> a, int parity) {
   for (int j = tid; j < nl; j += TILE) {
     R fx = R(0), fy = R(0), fz = R(0);
     const int i1 = sinc[j + 1];
+#pragma unroll 4
     for (int i = sinc[j]; i < i1; ++i) {
-      const int q = sinc[NLM + 1 + i];
-      const int o = (q & 7) * TILE + (q >> 3);
+      const int o = sinc[NLM + 1 + i];     // corner k of element t: k * TILE + t
       fx += sc[o]; fy += sc[8 * TILE + o]; fz += sc[16 * TILE + o];
     }
     const int s = j == tid ? slot0 : j == tid + TILE ? slot1 : a.patch_slots[p * NLM + j];
@@ -1670,8 +1674,7 @@ shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
     R f0 = R(0), f1 = R(0), f2 = R(0), m0 = R(0), m1 = R(0), m2 = R(0);
     const int i1 = sinc[j + 1];
     for (int i = sinc[j]; i < i1; ++i) {
-      const int q = sinc[NLM + 1 + i];
-      const int o = (q & 3) * TILE + (q >> 2);
+      const int o = sinc[NLM + 1 + i];     // corner k of element t: k * TILE + t
       f0 += sc[o]; f1 += sc[4 * TILE + o]; f2 += sc[8 * TILE + o];
       m0 += sc[12 * TILE + o]; m1 += sc[16 * TILE + o]; m2 += sc[20 * TILE + o];
     }

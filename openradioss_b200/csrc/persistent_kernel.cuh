@@ -143,9 +143,13 @@ __device__ inline void group_reduce(unsigned long long& key, unsigned long long&
   }
 }
 
-// Threads per CTA: P patches x TILE elements, at most PERSIST_THREADS; one CTA per
-// SM (the register budget of the shell element at that many threads).
+// Threads per CTA: at least P patches x TILE elements (one per element), raised to
+// cover the CTA's held nodes (one per node in the node phase) and at most
+// PERSIST_THREADS; one CTA per SM (the register budget of the shell element at that
+// many threads).  Threads beyond the P patches work in the node phase only.
 constexpr int PERSIST_THREADS = 384;
+// reduction scratch is laid out for every TILE group of PERSIST_THREADS threads
+__host__ __device__ constexpr int persist_groups(int tile) { return (PERSIST_THREADS + tile - 1) / tile; }
 
 template <class R>
 __host__ __device__ inline size_t persist_smem(int ncmax, int tile, int P, int inc_stride, int nlmax) {
@@ -157,7 +161,7 @@ __host__ __device__ inline size_t persist_smem(int ncmax, int tile, int P, int i
   const size_t nodes_al = (nodes + 15) / 16 * 16;
   const size_t corners = (size_t)P * 24 * tile * sizeof(R);
   const size_t inc = ((size_t)P * inc_stride * 2 + 15) / 16 * 16;
-  const size_t red = (size_t)P * (tile / 32) * 32;
+  const size_t red = (size_t)persist_groups(tile) * (tile / 32) * 32;
   const size_t slots = ((size_t)P * nlmax * sizeof(int) + 15) / 16 * 16;
   const size_t ranges = (size_t)ncmax * sizeof(int2);
   return nodes_al + corners + inc + red + slots + ranges;
@@ -204,14 +208,14 @@ shell_persistent_kernel(ShellArgs<R> a, NodeArgs<R> na, PersistArgs pa, int ncyc
   unsigned short* sinc = sinc_all + (size_t)sub * a.inc_stride;
   // slot numbers of the patch nodes and slot ranges of the held nodes, read once
   // here instead of from global memory in every cycle
-  int* sslot_all = reinterpret_cast<int*>(red_base + (size_t)P * NW * 32);
+  int* sslot_all = reinterpret_cast<int*>(red_base + (size_t)persist_groups(TILE) * NW * 32);
   int* sslot = sslot_all + (size_t)sub * a.nlmax;
   int2* srange = reinterpret_cast<int2*>(reinterpret_cast<unsigned char*>(sslot_all) +
                                          ((size_t)P * a.nlmax * sizeof(int) + 15) / 16 * 16);
 
   // ---- this CTA's patch and element ----
   const int p = cta * P + sub;
-  const bool has_patch = p < a.npatch;
+  const bool has_patch = sub < P && p < a.npatch;
   const int e = (has_patch ? p : 0) * TILE + lt;
   PatchInfo pi{};
   if (has_patch) pi = a.patch[p];
@@ -301,8 +305,7 @@ shell_persistent_kernel(ShellArgs<R> a, NodeArgs<R> na, PersistArgs pa, int ncyc
       const typename Vec2<R>::T* sc2 = reinterpret_cast<const typename Vec2<R>::T*>(sc);
 #pragma unroll 4
       for (int i = sinc[j]; i < i1; ++i) {
-        const int q = sinc[NLM + 1 + i];
-        const int o = (q & 3) * TILE + (q >> 2);
+        const int o = sinc[NLM + 1 + i];   // corner k of element t: k * TILE + t
         const typename Vec2<R>::T p0 = sc2[o], p1 = sc2[4 * TILE + o], p2 = sc2[8 * TILE + o];
         f0 += p0.x; f1 += p0.y; f2 += p1.x;
         m0 += p1.y; m1 += p2.x; m2 += p2.y;
