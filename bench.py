@@ -527,7 +527,7 @@ def main():
             "tuning": {"cuda_graph_cycles": 32, "tile_hex": bh_s, "tile_shell": bs_s,
                        "persistent_cycle": persistent_on,
                        "autotune_ms_per_cycle": {"split": tune_s, "fp64": tune_d},
-                       "autotune_keys": "tile, p = persistent shell cycle"},
+                       "autotune_keys": "tile (hAsB: hexa tile A, shell tile B), p = persistent shell cycle"},
             "fp64": {"value": value_fp64, "ms_per_step": t_fp64, "dtype": "f64", "tile_hex": bh_d, "tile_shell": bs_d,
                      "persistent_cycle": pe_d == 0},
             "split_over_fp64": value / value_fp64,
