@@ -75,9 +75,13 @@ typedef struct {
   double dt_growth;     /* growth cap factor of resol.F:6080; the reference
                            multiplies by the REAL literal 1.1, i.e. (double)1.1f     */
   int    graph;         /* 1: replay step() through a captured CUDA graph            */
-  int    block_hex;     /* threads per block, hex kernel   (0 = autotuned)           */
-  int    block_shell;   /* threads per block, shell kernel (0 = autotuned)           */
-  int    block_node;    /* threads per block, nodal kernel (0 = autotuned)           */
+  int    block_hex;     /* threads per block, hex kernel: 64, 128 or 256; 0 = chosen
+                           at finalize from the element count (64 while the patches
+                           at 64 fit one wave of resident CTAs, else 128); the Python
+                           autotuner times all three                                 */
+  int    block_shell;   /* threads per block, shell kernel, likewise                 */
+  int    block_node;    /* reserved, 0: the node pass runs tiles of 128 nodes, in the
+                           form (register budget) the wave count selects            */
   int    persistent;    /* 0: the persistent shell cycle where eligible; -1: never
                            (see or_ecycle_persistent_info)                          */
 } or_ecycle_config;

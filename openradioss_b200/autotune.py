@@ -103,7 +103,7 @@ def tune(deck, precision=abi.OR_PREC_SPLIT, ncycles=256, use_cache=True, device=
         json.dump(cache, open(CACHE, "w"), indent=1, sort_keys=True)
     except OSError:
         pass
-    return bh, bs, best[1], cache[key]["ms_per_cycle"]
+    return bh, bs, best[2], cache[key]["ms_per_cycle"]
 
 
 def main():

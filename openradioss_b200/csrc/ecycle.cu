@@ -790,6 +790,19 @@ int finalize_impl(or_ecycle* h) {
   }
   m.nnodpad = nn;
   m.ntiles = nt;
+  // tiles left to the library (cfg.block_hex / block_shell 0): 64 elements per patch
+  // when the patches at 64 fit one wave of the kernel's resident CTAs (a latency-bound
+  // mesh gains from more CTAs), 128 otherwise; the autotuner times all three
+  {
+    auto tile_for = [&](long long nel, int ctas128) {
+      return nel <= (long long)h->nsm * (2 * ctas128) * 64 ? 64 : 128;
+    };
+    long long nh = 0, ns = 0;
+    for (auto& g : h->hex) nh += g.nel;
+    for (auto& g : h->shell) ns += g.nel;
+    if (h->cfg.block_hex == 0) h->tile_hex = tile_for(nh, Occupancy<R>::hex);
+    if (h->cfg.block_shell == 0) h->tile_shell = tile_for(ns, Occupancy<R>::shell);
+  }
   // patches
   std::vector<std::vector<std::pair<int, int>>> node_patch(nn);
   int rc = build_patches<8>(h, h->hex, h->tile_hex, m.hps, node_patch, 0);

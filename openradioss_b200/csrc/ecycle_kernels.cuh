@@ -405,14 +405,16 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
                ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
 }
-// waits for phase 0 of bar to complete, at most `tries` polls; false if it did not
-__device__ __forceinline__ bool mbar_wait0(unsigned long long* bar, int tries) {
+// waits for the phase of bar with the given parity to complete, at most `tries`
+// polls; false if it did not
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, int tries) {
   unsigned done = 0;
   for (int i = 0; i < tries && !done; ++i)
-    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\tselp.u32 %0, 1, 0, p;\n}"
-                 : "=r"(done) : "r"(smem_u32(bar)) : "memory");
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+                 : "=r"(done) : "r"(smem_u32(bar)), "r"(parity) : "memory");
   return done != 0;
 }
+__device__ __forceinline__ bool mbar_wait0(unsigned long long* bar, int tries) { return mbar_wait(bar, 0u, tries); }
 // element-wise asynchronous copies (no register staging), completed by cp_async_wait_all
 __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
