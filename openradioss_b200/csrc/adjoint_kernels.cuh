@@ -167,8 +167,21 @@ struct AdjShellArgs {
   int nelpad;
 };
 
+// Threads per CTA and resident CTAs per SM of the reverse shell kernel (its
+// register budget: 65536 / (threads x CTAs) per thread).  64 x 5 (204 registers)
+// puts a 40,000-shell plate in one wave of 148 SMs, where 128 x 2 at 255
+// registers left a 6 % tail wave: the C5 adjoint 92-93 -> 88.4 ms on B200
+// (96 x 3: 88.6 ms); the gradients are bitwise the same.
+#ifndef ORB_ADJ_SHELL_THREADS
+#define ORB_ADJ_SHELL_THREADS 64
+#endif
+#ifndef ORB_ADJ_SHELL_CTAS
+#define ORB_ADJ_SHELL_CTAS 5
+#endif
+constexpr int ADJ_SHELL_THREADS = ORB_ADJ_SHELL_THREADS;
+
 template <int NP>
-__global__ void __launch_bounds__(128) adj_shell_kernel(AdjShellArgs a) {
+__global__ void __launch_bounds__(ADJ_SHELL_THREADS, ORB_ADJ_SHELL_CTAS) adj_shell_kernel(AdjShellArgs a) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= a.nelpad) return;
   const int gi = a.egroup[e];

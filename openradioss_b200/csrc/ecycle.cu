@@ -1834,7 +1834,8 @@ double adj_plastic_work(or_ecycle* h) {
 
 template <int NP>
 int launch_adj_shell(or_ecycle* h, const AdjShellArgs& a) {
-  adj_shell_kernel<NP><<<(unsigned)((a.nelpad + 127) / 128), 128, 0, h->stream>>>(a);
+  adj_shell_kernel<NP><<<(unsigned)((a.nelpad + ADJ_SHELL_THREADS - 1) / ADJ_SHELL_THREADS), ADJ_SHELL_THREADS, 0,
+                         h->stream>>>(a);
   CK(cudaGetLastError());
   h->launches++;
   return OR_OK;
