@@ -126,6 +126,7 @@ struct or_ecycle {
   int spmd_k = -1;                    // cycle index of a running domain-decomposed step, -1 outside one
   int next_parity = 0;                // time-buffer parity of the state after the last step
   bool pdl = true;                    // programmatic dependent launch of the cycle kernels
+  int shell_staged = -1;              // staged 5-point shell kernel: -1 by wave count, 0 never, 1 always
   int nsm = 148;                      // multiprocessors of the device
   long long graph_launches = 0;       // kernel launches in one replay of graph_exec
 };
@@ -471,15 +472,17 @@ struct Impl {
 };
 
 // dynamic shared memory of a patch kernel.  Hexa: the layout of hex_smem_bytes.
-// Shell: node planes (x, y, z in FP64; velocities and rotational velocities in R),
-// 24 planes of TILE corner forces, the incidence lists.
+// Shell: for the NPT-point kernels the staged integration-point planes (6 NPT of
+// TILE), then node planes (x, y, z in FP64; velocities and rotational velocities in
+// R), 24 planes of TILE corner forces, the incidence lists.
 template <class R>
 size_t hex_smem(int nl, int tile, int inc_stride) {
   return hex_smem_bytes<R>(nl, tile, inc_stride);
 }
 template <class R>
-size_t shell_smem(int nl, int tile, int inc_stride) {
-  return (size_t)nl * (3 * sizeof(double) + 6 * sizeof(R)) + 24 * (size_t)tile * sizeof(R) + 2 * (size_t)inc_stride;
+size_t shell_smem(int nl, int tile, int inc_stride, int npt = 0) {
+  return (size_t)shell_staged_planes(npt) * tile * sizeof(R) + (size_t)nl * (3 * sizeof(double) + 6 * sizeof(R)) +
+         24 * (size_t)tile * sizeof(R) + 2 * (size_t)inc_stride;
 }
 
 // A cycle kernel launch; with pdl, programmatic stream serialization lets its
@@ -513,18 +516,31 @@ int launch_hex(or_ecycle* h, Impl<R>& m, int parity, bool pdl = false) {
   h->launches++;
   return OR_OK;
 }
-template <class R, int T, int NPT>
+template <class R, int T, int NPT, bool STG>
 int launch_shell(or_ecycle* h, Impl<R>& m, int parity, bool pdl) {
   if (m.sps.info.empty()) return OR_OK;
-  size_t sm = shell_smem<R>(m.sps.nlmax, T, m.sinc_stride);
-  CK(launch_k(shell_patch_kernel<R, T, NPT>, (unsigned)m.sps.info.size(), T, sm, h->stream, pdl, m.sargs(), parity,
-              (const float*)m.zw.p));
+  size_t sm = shell_smem<R>(m.sps.nlmax, T, m.sinc_stride, STG ? NPT : 0);
+  CK(launch_k(shell_patch_kernel<R, T, NPT, STG>, (unsigned)m.sps.info.size(), T, sm, h->stream, pdl, m.sargs(),
+              parity, (const float*)m.zw.p));
   h->launches++;
   return OR_OK;
 }
+// The 5-point form with staged integration-point state where the shell patches
+// exceed one wave of the register-held form (split precision)
+// (OR_ECYCLE_SHELL_STAGED=0 never, =1 always, read at create)
+template <class R>
+bool shell_staged(const or_ecycle* h, const Impl<R>& m) {
+  if (sizeof(R) != 4 || m.uniform_npt != 5 || h->shell_staged == 0) return false;
+  return h->shell_staged == 1 ||
+         (long long)m.sps.info.size() > (long long)h->nsm * min_blocks(Occupancy<R>::shell, h->tile_shell);
+}
 template <class R, int T>
 int launch_shell_npt(or_ecycle* h, Impl<R>& m, int parity, bool pdl = false) {
-  return m.uniform_npt == 5 ? launch_shell<R, T, 5>(h, m, parity, pdl) : launch_shell<R, T, 0>(h, m, parity, pdl);
+  if (m.uniform_npt != 5) return launch_shell<R, T, 0, false>(h, m, parity, pdl);
+  if constexpr (sizeof(R) == 4) {
+    if (shell_staged(h, m)) return launch_shell<R, T, 5, true>(h, m, parity, pdl);
+  }
+  return launch_shell<R, T, 5, false>(h, m, parity, pdl);
 }
 template <class R>
 int launch_link(or_ecycle* h, Impl<R>& m) {
@@ -580,7 +596,7 @@ cudaError_t set_smem(F* f, int bytes) {
 template <class R>
 int set_smem_attrs(or_ecycle* h, Impl<R>& m) {
   int hs = (int)hex_smem<R>(m.hps.nlmax, h->tile_hex, m.hinc_stride);
-  int ss = (int)shell_smem<R>(m.sps.nlmax, h->tile_shell, m.sinc_stride);
+  int ss = (int)shell_smem<R>(m.sps.nlmax, h->tile_shell, m.sinc_stride, 5);   // the largest: the 5-point kernels
   if (hs > 200 * 1024 || ss > 200 * 1024) return fail(h, OR_E_UNSUPPORTED, "patch shared memory above 200 KB");
   CK(set_smem(hex_patch_kernel<R, 64, 0>, hs));
   CK(set_smem(hex_patch_kernel<R, 128, 0>, hs));
@@ -588,12 +604,17 @@ int set_smem_attrs(or_ecycle* h, Impl<R>& m) {
   CK(set_smem(hex_patch_kernel<R, 64, 1>, hs));
   CK(set_smem(hex_patch_kernel<R, 128, 1>, hs));
   CK(set_smem(hex_patch_kernel<R, 256, 1>, hs));
-  CK(set_smem(shell_patch_kernel<R, 64, 0>, ss));
-  CK(set_smem(shell_patch_kernel<R, 128, 0>, ss));
-  CK(set_smem(shell_patch_kernel<R, 256, 0>, ss));
-  CK(set_smem(shell_patch_kernel<R, 64, 5>, ss));
-  CK(set_smem(shell_patch_kernel<R, 128, 5>, ss));
-  CK(set_smem(shell_patch_kernel<R, 256, 5>, ss));
+  CK(set_smem(shell_patch_kernel<R, 64, 0, false>, ss));
+  CK(set_smem(shell_patch_kernel<R, 128, 0, false>, ss));
+  CK(set_smem(shell_patch_kernel<R, 256, 0, false>, ss));
+  CK(set_smem(shell_patch_kernel<R, 64, 5, false>, ss));
+  CK(set_smem(shell_patch_kernel<R, 128, 5, false>, ss));
+  CK(set_smem(shell_patch_kernel<R, 256, 5, false>, ss));
+  if constexpr (sizeof(R) == 4) {
+    CK(set_smem(shell_patch_kernel<R, 64, 5, true>, ss));
+    CK(set_smem(shell_patch_kernel<R, 128, 5, true>, ss));
+    CK(set_smem(shell_patch_kernel<R, 256, 5, true>, ss));
+  }
   return OR_OK;
 }
 
@@ -2023,6 +2044,7 @@ int or_ecycle_create(const or_ecycle_config* cfg, or_ecycle** out) {
   if (tile_ok(h->cfg.block_hex)) h->tile_hex = h->cfg.block_hex;
   if (tile_ok(h->cfg.block_shell)) h->tile_shell = h->cfg.block_shell;
   if (const char* s = std::getenv("OR_ECYCLE_PDL")) h->pdl = std::atoi(s) != 0;
+  if (const char* s = std::getenv("OR_ECYCLE_SHELL_STAGED")) h->shell_staged = std::atoi(s) != 0 ? 1 : 0;
   if (cudaSetDevice(cfg->device) != cudaSuccess || cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
     delete h;
     return OR_E_CUDA;

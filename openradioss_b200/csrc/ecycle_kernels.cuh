@@ -365,6 +365,15 @@ __device__ inline void block_reduce(unsigned long long& key, unsigned long long&
 #ifndef ORB_SHELL_CTAS_F64
 #define ORB_SHELL_CTAS_F64 3
 #endif
+// The 5-point shell kernel with its integration-point state staged in shared memory
+// holds 30 fewer registers per thread: 5 CTAs (102 registers, 152 B spilled) ran
+// C3's shell pass in 221.2 us against 233.5 at 4 CTAs and 256.3 at 3, and 259.3 for
+// the register-held form at 3.  It is the form for meshes of more than one wave of
+// the register-held kernel; a single wave (the C2 plate at tile 64: 8.0 against
+// 8.9 us) keeps the register-held form, whose chain is shorter.
+#ifndef ORB_SHELL_STAGED_CTAS_F32
+#define ORB_SHELL_STAGED_CTAS_F32 5
+#endif
 // The 5-point rule of COQINI (coqini.F:45-130) as compile-time constants for the
 // NPT = 5 shell kernels (row 0: Z0, 1: WF, 2: WM); the host build checks them
 // against the shared table of coqini_table.h.
@@ -376,10 +385,10 @@ __host__ __device__ constexpr float coq5(int row, int ip) {
 
 template <class R> struct Occupancy;
 template <> struct Occupancy<float> {
-  static constexpr int hex = ORB_HEX_CTAS_F32, shell = ORB_SHELL_CTAS_F32;
+  static constexpr int hex = ORB_HEX_CTAS_F32, shell = ORB_SHELL_CTAS_F32, shell_staged = ORB_SHELL_STAGED_CTAS_F32;
 };
 template <> struct Occupancy<double> {
-  static constexpr int hex = ORB_HEX_CTAS_F64, shell = ORB_SHELL_CTAS_F64;
+  static constexpr int hex = ORB_HEX_CTAS_F64, shell = ORB_SHELL_CTAS_F64, shell_staged = ORB_SHELL_CTAS_F64;
 };
 __host__ __device__ constexpr int min_blocks(int ctas128, int tile) {
   return ctas128 * 128 / tile > 0 ? ctas128 * 128 / tile : 1;
@@ -1054,7 +1063,9 @@ struct ShellState {
   int degen, eid;
 };
 
-template <class R, int NPT>
+// IP = false leaves the integration-point stresses and plastic strains out (a caller
+// that stages them in shared memory).
+template <class R, int NPT, bool IP = true>
 __device__ __forceinline__ void shell_load_state(const ShellArgs<R>& a, int e, ShellState<R, NPT>& st) {
   const int nelpad = a.nelpad;
   st.thk = a.thk[e];
@@ -1064,7 +1075,7 @@ __device__ __forceinline__ void shell_load_state(const ShellArgs<R>& a, int e, S
   st.jca = a.jca ? a.jca[e] : R(0);
   st.degen = a.degen[e];
   st.eid = a.elem_id[e];
-  if (NPT > 0) {
+  if (NPT > 0 && IP) {
 #pragma unroll
     for (int ip = 0; ip < ShellState<R, NPT>::NP; ++ip) {
 #pragma unroll
@@ -1096,14 +1107,19 @@ __device__ __forceinline__ void shell_store_state(const ShellArgs<R>& a, int e, 
 // integration point), CHVIS3, CDT3, CFINT3, the group pressure; corner forces and
 // moments out in global axes with CUPDT3P signs.  KEEP = false writes the new
 // state to memory at index e, as each quantity is formed; KEEP = true leaves it
-// in st (for a caller that keeps the state in registers across cycles).
-template <class R, int NPT, bool KEEP>
+// in st (for a caller that keeps the state in registers across cycles).  STAGED
+// (with NPT > 0, KEEP false): the old integration-point state is read from shared
+// planes, stress component c of point ip at sip[(ip * 5 + c) * sstride] and the
+// plastic strain of point ip at sip[(NPT * 5 + ip) * sstride], instead of from st.
+template <class R, int NPT, bool KEEP, bool STAGED = false>
 __device__ __forceinline__ void shell_element(const ShellArgs<R>& a, const int e, const ShellGroupDesc& gd,
                                               const R DT1, const float* __restrict__ zw, const double* sx,
                                               const double* sy, const double* sz, const R* sv, const int NLM,
                                               const int (&lc)[4], ShellState<R, NPT>& st, R (&Fg)[3][4],
                                               R (&Mg)[3][4], unsigned long long& mykey, unsigned long long& mybits,
-                                              double& my_ehou, double& my_wpla) {
+                                              double& my_ehou, double& my_wpla, const R* sip = nullptr,
+                                              const int sstride = 0) {
+  static_assert(!STAGED || (NPT > 0 && !KEEP), "staged state: fixed points, written to memory");
   static_assert(!KEEP || NPT > 0, "kept state needs a fixed number of integration points");
   const int nelpad = a.nelpad;
   const R OFF = R(1);
@@ -1298,7 +1314,10 @@ __device__ __forceinline__ void shell_element(const ShellArgs<R>& a, const int e
     if (NPT == 0 && ip >= npt) break;
     const R wf = R(NPT == 5 ? coq5(1, ip) : WF[ip]), wm = R(NPT == 5 ? coq5(2, ip) : WM[ip]);
     R SO[5], SN[5];
-    if (NPT > 0) {
+    if (STAGED) {
+#pragma unroll
+      for (int c = 0; c < 5; ++c) SO[c] = sip[(ip * 5 + c) * sstride];
+    } else if (NPT > 0) {
 #pragma unroll
       for (int c = 0; c < 5; ++c) SO[c] = st.sig[NPT > 0 ? ip : 0][c];
     } else {
@@ -1329,7 +1348,8 @@ __device__ __forceinline__ void shell_element(const ShellArgs<R>& a, const int e
       SN[2] = SO[2] + GG * DXY;
       SN[3] = SO[3] + GS * EYZ;
       SN[4] = SO[4] + GS * EXZ;
-      R PLA = NPT > 0 ? st.pla[NPT > 0 ? ip : 0] : a.pla[ip * nelpad + e];
+      R PLA = STAGED ? sip[((NPT > 0 ? NPT : 1) * 5 + ip) * sstride]
+              : NPT > 0 ? st.pla[NPT > 0 ? ip : 0] : a.pla[ip * nelpad + e];
       R YLD = PLA == R(0) ? CA : CA + CB * exp_(CN * log_(PLA));
       YLD = fmin(YLD, YMAX);
       R DPLA = R(0);
@@ -1578,21 +1598,31 @@ __device__ __forceinline__ void shell_element(const ShellArgs<R>& a, const int e
   }
 }
 
+// Shared planes of staged integration-point state of the NPT-point shell patch
+// kernel: 5 stresses and the plastic strain per point (none for the generic kernel).
+__host__ __device__ constexpr int shell_staged_planes(int npt) { return npt > 0 ? 6 * npt : 0; }
+
 // ===========================================================================
 // shell patch kernel
 // ===========================================================================
 // Per element (thread): CCOOR3, CNVEC3, CDERI3, CCOEF3, CDLEN3, CDEFO3, CCURV3,
 // CSTRA3, MULAWC (SIGEPS01C / SIGEPS02C -> M2CPLR per integration point),
 // CHVIS3, CDT3, CFINT3; forces and moments into shared memory (CUPDT3P signs).
-// NPT > 0: every group of the launch has NPT integration points and the
-// integration-point state is loaded up front; NPT = 0: generic 1..10 points.
-template <class R, int TILE, int NPT>
-__global__ void __launch_bounds__(TILE, min_blocks(Occupancy<R>::shell, TILE))
+// NPT > 0: every group of the launch has NPT integration points; their state is
+// loaded up front into registers, or with STG staged in shared memory by bulk
+// copies and read point by point; NPT = 0: generic 1..10 points, read from global
+// memory in the layer loop.
+template <class R, int TILE, int NPT, bool STG>
+__global__ void __launch_bounds__(TILE, min_blocks(STG ? Occupancy<R>::shell_staged : Occupancy<R>::shell, TILE))
 shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
   typedef typename Vec4<R>::T R4;
+  // NPT > 0: the patch's integration-point stresses and plastic strains are staged in
+  // NSP shared planes of TILE by bulk copies, read point by point in the layer loop
+  constexpr int NSP = STG ? shell_staged_planes(NPT) : 0;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ unsigned long long s_key[TILE / 32], s_bits[TILE / 32];
   __shared__ double s_s0[TILE / 32], s_s1[TILE / 32];
+  __shared__ __align__(8) unsigned long long s_bar;
   const int p = blockIdx.x;
   const int tid = threadIdx.x;
   // element index and node-list slots follow from (p, tid) alone (patches padded
@@ -1606,7 +1636,8 @@ shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
   const int slot1 = tid + TILE < NLM ? a.patch_slots[p * NLM + tid + TILE] : -1;
   double pre_ehour = 0.0, pre_wpla = 0.0;
   if (tid == 0) { pre_ehour = a.blk_ehour[p]; pre_wpla = a.blk_wpla[p]; }
-  double* sx = reinterpret_cast<double*>(smem_raw);
+  R* sip = reinterpret_cast<R*>(smem_raw);
+  double* sx = reinterpret_cast<double*>(sip + NSP * TILE);
   double* sy = sx + NLM;
   double* sz = sy + NLM;
   R* sv = reinterpret_cast<R*>(sz + NLM);   // vx vy vz rx ry rz: 6 planes of NLM
@@ -1615,9 +1646,20 @@ shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
   const int nelpad = a.nelpad;
   // per-element loads issued before the staging barrier (overlap with the gathers)
   // padding elements (tid >= nel) hold valid state: load unconditionally
+  if (NSP > 0 && tid == 0) {   // written two launches back: issued before the wait
+    mbar_init(&s_bar);
+    const unsigned pl = TILE * sizeof(R);
+    const size_t e0 = (size_t)p * TILE;
+    mbar_expect_tx(&s_bar, NSP * pl);
+#pragma unroll 1
+    for (int q = 0; q < 5 * NPT; ++q) bulk_g2s(sip + q * TILE, a.sig + (size_t)q * nelpad + e0, pl, &s_bar);
+#pragma unroll 1
+    for (int ip = 0; ip < NPT; ++ip)
+      bulk_g2s(sip + (5 * NPT + ip) * TILE, a.pla + (size_t)ip * nelpad + e0, pl, &s_bar);
+  }
   const uint2 cw = a.conn[e];
   ShellState<R, NPT> st;
-  shell_load_state<R, NPT>(a, e, st);
+  shell_load_state<R, NPT, NSP == 0>(a, e, st);
   {
     const unsigned* src = reinterpret_cast<const unsigned*>(a.inc + (size_t)p * a.inc_stride);
     unsigned* dst = reinterpret_cast<unsigned*>(sinc);
@@ -1645,6 +1687,7 @@ shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
   const PartTime& tm = a.time[parity * a.nparts + pi.part];
   const R DT1 = R(tm.dt2);
   __syncthreads();
+  if (NSP > 0 && !mbar_wait0(&s_bar, STAGE_WAIT_TRIES)) raise_error(a.err, 7, p);
 
   int lc[4];
   int color = -1;
@@ -1655,8 +1698,8 @@ shell_patch_kernel(ShellArgs<R> a, int parity, const float* __restrict__ zw) {
     lc[0] = cw.x & 0xffffu; lc[1] = cw.x >> 16; lc[2] = cw.y & 0xffffu; lc[3] = cw.y >> 16;
     color = lc[0] >> COLOR_SHIFT;
     lc[0] &= LOCAL_MASK;
-    shell_element<R, NPT, false>(a, e, gd, DT1, zw, sx, sy, sz, sv, NLM, lc, st, Fg, Mg, mykey, mybits, my_ehou,
-                                 my_wpla);
+    shell_element<R, NPT, false, (NSP > 0)>(a, e, gd, DT1, zw, sx, sy, sz, sv, NLM, lc, st, Fg, Mg, mykey, mybits,
+                                            my_ehou, my_wpla, sip + tid, TILE);
   }
   // ---- patch assembly: corner forces and moments to shared memory, then each patch
   // node sums its incident corners in ascending (element, corner) order ----

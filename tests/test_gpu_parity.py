@@ -354,3 +354,34 @@ def test_shell_iterative_returns_fp64_and_split(lib, ipla):
     check_energies(g, o, FP64_TOL)
     s, _ = run_pair(d, 400, precision=abi.OR_PREC_SPLIT)
     assert rel(s.get_nodes()["d"], o.get_nodes()["d"]) < SPLIT_TOL
+
+
+def test_staged_shell_form(lib, monkeypatch):
+    """The 5-point shell kernel with its integration-point state staged in shared
+    memory (OR_ECYCLE_SHELL_STAGED=1; by default chosen beyond one wave of patches)
+    against the register-held form (=0): bit for bit on the parity build without
+    FMA contraction, where both perform the oracle's operations in the same order,
+    and each within the split bar of the FP64 oracle on the product build."""
+    from openradioss_b200 import build
+    from openradioss_b200.ecycle import ECycle, load_library
+    from oracle.oracle import Oracle
+    d = decks.c2_shell_plate(n=24, size=0.024, pressure=5e6)
+    build.build(variant="nofma")
+    nofma = load_library(build.OUT_NOFMA)
+    o = Oracle(d, nthreads=8)
+    o.step(150)
+    ref = o.get_nodes()["d"]
+    for glib, bitwise in ((nofma, True), (lib, False)):
+        r = []
+        for flag in ("1", "0"):
+            monkeypatch.setenv("OR_ECYCLE_SHELL_STAGED", flag)
+            h = ECycle(d, precision=abi.OR_PREC_SPLIT, lib=glib, persistent=-1)
+            h.step(150)
+            r.append((h.get_nodes(), h.shell_state(0)))
+            h.close()
+        (na, sa), (nb, sb) = r
+        if bitwise:
+            assert all(np.array_equal(na[k], nb[k]) for k in ("d", "v", "vr"))
+            assert all(np.array_equal(sa[k], sb[k]) for k in ("sig", "pla", "thk"))
+        for nodes in (na, nb):
+            assert rel(nodes["d"], ref) < SPLIT_TOL
