@@ -1983,8 +1983,15 @@ template <class R, int TILE>
 __global__ void __launch_bounds__(TILE) node_kernel(NodeArgs<R> a, int parity) {
   node_pass<R, TILE>(a, parity);
 }
+// Resident threads per SM the wide form is compiled for (its register budget).  On
+// the C4 mixed mesh (2.05 M nodes, split) 1024 (64 registers, 20 B spilled) ran
+// the pass in 78.7 us per cycle, 1280 (48 registers, 96 B spilled) in 86.3 and 1536
+// (40 registers, 128 B spilled) in 84.8 (eager cycles timed with events, B200).
+#ifndef ORB_NODE_WIDE_THREADS
+#define ORB_NODE_WIDE_THREADS 1024
+#endif
 template <class R, int TILE>
-__global__ void __launch_bounds__(TILE, 1024 / TILE) node_kernel_wide(NodeArgs<R> a, int parity) {
+__global__ void __launch_bounds__(TILE, ORB_NODE_WIDE_THREADS / TILE) node_kernel_wide(NodeArgs<R> a, int parity) {
   node_pass<R, TILE>(a, parity);
 }
 
