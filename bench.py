@@ -203,11 +203,19 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except OSError:
             self.proc = None
+            return
+        # nvidia-smi takes a few hundred ms to start: wait for its first row, so that
+        # a timed region of a few hundred ms is sampled from its start, then drop the
+        # rows taken before it
+        t0 = time.time()
+        while not self.rows and self.proc.poll() is None and time.time() - t0 < 10.0:
+            time.sleep(0.01)
+        self.rows.clear()
 
     def _read(self):
         for line in self.proc.stdout:
